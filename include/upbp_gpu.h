@@ -1,0 +1,294 @@
+/*
+ * upbp_gpu.h -- C ABI of the B200 volumetric estimator stage (PP3D, PB2D, BB1D).
+ *
+ * This is the drop-in boundary for SmallUPBP's estimator interface.  The
+ * reference renderer calls, per iteration,
+ *
+ *   HashGrid::Reserve/Build            (Misc/HashGrid.hxx:41-126)      PP3D build
+ *   EmbreeBre::build                   (Bre/Bre.hxx:93-99, Bre.cxx:649-755)  PB2D build
+ *   PhotonBeamsEvaluator::build        (Beams/PhBeams.hxx:71-76, PhBeams.cxx:66-148) BB1D build
+ *   EmbreeBre::evalBre                 (Bre/Bre.hxx:125-131, Bre.cxx:812-964) per camera segment
+ *   PhotonBeamsEvaluator::evalBeamBeamEstimate (PhBeams.hxx:96-113, PhBeams.cxx:177-324) per camera segment
+ *   HashGrid::Process + UPBP::RangeQuery (HashGrid.hxx:129-188, Renderers/UPBP.hxx:86-133) per camera medium vertex
+ *   EmbreeBre::destroy / PhotonBeamsEvaluator::destroy (UPBP.hxx:1172-1181)
+ *
+ * one query at a time and adds each returned Rgb into the pixel colour
+ * (UPBP.hxx:782-783, 795-796, 890-891, 908-909, 1120; Framebuffer::AddColor
+ * at UPBP.hxx:1162).  No control flow depends on the returned value, so the
+ * calls can be RECORDED during the camera pass and evaluated in one batch at
+ * the end of the iteration: that batch is what this library evaluates.
+ *
+ * Data crosses the boundary as plain arrays (host or device pointers; the
+ * library copies them).  The light-vertex, beam and MIS records carry exactly
+ * the fields the reference estimators read from UPBPLightVertex
+ * (Path/UPBPLightVertex.hxx:32-78), PhotonBeam (Beams/PhotonBeam.hxx:40-64),
+ * VolumeSegment (Path/Ray.hxx:131-227) and AdditionalRayDataForMis
+ * (embree-2.0/embree/common/ray.h:31-99).
+ *
+ * Every entry point returns an int status: UPBP_OK (0) or a negative
+ * UPBP_ERR_* code; upbp_last_error() gives the message.  The reference has no
+ * error returns (it calls exit(2) on failed asserts, Misc/Defs.hxx:96-97).
+ * One context per host thread, as the reference keeps one renderer (and so
+ * one set of estimator structures) per OpenMP thread (SmallUPBP.cxx:66-79).
+ */
+#ifndef UPBP_GPU_H
+#define UPBP_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define UPBP_OK 0
+#define UPBP_ERR_INVALID_ARG (-1)
+#define UPBP_ERR_OUT_OF_MEMORY (-2)
+#define UPBP_ERR_CUDA (-3)
+#define UPBP_ERR_NOT_BUILT (-4)
+#define UPBP_ERR_WATCHDOG (-5)
+#define UPBP_ERR_CAPACITY (-6)
+
+/* ---- flags: values identical to the reference enums (Misc/Defs.hxx:140-194,
+ *      Scene/Media.hxx:44-48) ------------------------------------------- */
+#define UPBP_SHORT_BEAM 1u
+#define UPBP_LONG_BEAM 2u
+#define UPBP_BPT 4u
+#define UPBP_SURF 8u
+#define UPBP_PP3D 16u
+#define UPBP_PB2D 32u
+#define UPBP_BB1D 64u
+#define UPBP_NO_SINE_IN_WEIGHTS 128u
+#define UPBP_PREVIOUS 256u
+#define UPBP_COMPATIBLE 512u
+#define UPBP_BB1D_PREVIOUS 1024u
+#define UPBP_ORIGIN_IN_MEDIUM 1u /* AbstractMedium::kOriginInMedium */
+#define UPBP_END_IN_MEDIUM 2u    /* AbstractMedium::kEndInMedium */
+
+/* upbp_mis.flags bits (the four bools of MisData) */
+#define UPBP_MIS_IS_DELTA 1u
+#define UPBP_MIS_ON_LIGHT_SOURCE 2u
+#define UPBP_MIS_IS_SPECULAR 4u
+#define UPBP_MIS_IN_MEDIUM_WITH_BEAMS 8u
+
+/* light-vertex flags */
+#define UPBP_LV_IN_MEDIUM 1u
+#define UPBP_LV_CONNECTABLE 2u
+#define UPBP_LV_IS_FINITE 4u
+
+/* segment-query flags */
+#define UPBP_Q_ORIGIN_IN_MEDIUM 1u /* raySamplingFlags of the call */
+#define UPBP_Q_LITE 2u             /* segments are LiteVolumeSegments: pdfs and attenuation come from the medium */
+#define UPBP_Q_PB2D 4u             /* evaluate evalBre for this segment */
+#define UPBP_Q_BB1D 8u             /* evaluate evalBeamBeamEstimate for this segment */
+
+/* evaluation modes */
+#define UPBP_MODE_PLAIN 0 /* all-FP32, MIS walks the stored subpaths per candidate (reference order) */
+#define UPBP_MODE_MIXED 1 /* FP32 bulk, FP64 near-parallel BB1D solve and FP64 MIS suffix sums */
+
+/* ---- records ------------------------------------------------------------ */
+
+/* Homogeneous medium (Scene/Media.hxx:129-159).  Derived quantities
+ * (sigma_t, min positive sigma_t component, MFP) are computed by the library
+ * exactly as the reference constructor does. */
+typedef struct upbp_medium {
+    float absorption[3];     /* sigma_a */
+    float scattering[3];     /* sigma_s */
+    float mean_cosine;       /* HG g */
+    float continuation_prob; /* MEDIUM_SURVIVAL_PROB 0.8 for scene media, 1.0 for the clear medium */
+} upbp_medium;
+
+/* MisData (Path/UPBPLightVertex.hxx:32-52): 14 floats + 4 bools as flags. 60 bytes. */
+typedef struct upbp_mis {
+    float pdf_a_inv;
+    float rev_pdf_a;
+    float rev_pdf_a_without_bsdf;
+    float ray_sample_pdf_inv;
+    float ray_sample_rev_pdf_inv;
+    float ray_sample_pdfs_ratio;
+    float ray_sample_rev_pdfs_ratio;
+    float sin_theta;
+    float cos_theta_out;
+    float surf_factor;
+    float pp3d_factor;
+    float pb2d_factor;
+    float bb1d_factor;
+    float bb1d_beam_selection_pdf;
+    uint32_t flags; /* UPBP_MIS_* */
+} upbp_mis;
+
+/* Per-iteration constants (Renderers/UPBP.hxx:415-460) and options. */
+typedef struct upbp_params {
+    uint32_t techniques;        /* mEstimatorTechniques: UPBP_BPT|SURF|PP3D|PB2D|BB1D|NO_SINE|PREVIOUS|BB1D_PREVIOUS */
+    uint32_t query_beam_type;   /* mQueryBeamType  */
+    uint32_t photon_beam_type;  /* mPhotonBeamType */
+    uint32_t min_path_length;
+    uint32_t max_path_length;
+    float radius_pp3d;
+    float radius_pb2d;
+    float radius_bb1d;
+    float mis_factor_surf;      /* etaSurf */
+    float mis_factor_pp3d;      /* etaPP3D */
+    float mis_factor_pb2d;      /* etaPB2D */
+    float mis_factor_bb1d;      /* etaBB1D */
+    float norm_pp3d;            /* mPP3DNormalization */
+    float norm_pb2d;            /* mPB2DNormalization */
+    float norm_bb1d;            /* mBB1DNormalization */
+    float bb1d_min_mfp;         /* mBB1DMinMFP */
+    float min_dist_to_med;      /* mMinDistToMed */
+    int32_t hash_cells;         /* PP3D HashGrid::Reserve(pathCountL) */
+    int32_t image_width;
+    int32_t image_height;
+} upbp_params;
+
+/* Light vertices (mLightVertices): n entries, stored per light path in
+ * increasing path length, path p occupying [path_ends[p-1], path_ends[p]). */
+typedef struct upbp_light_vertices {
+    int64_t n;
+    const float* position;   /* [n][3] mHitpoint */
+    const float* throughput; /* [n][3] mThroughput */
+    const float* dir_fix;    /* [n][3] mBSDF.WorldDirFix() */
+    const float* cont_prob;  /* [n]    mBSDF.ContinuationProb() */
+    const int32_t* path_idx;    /* [n] mPathIdx */
+    const int32_t* path_length; /* [n] mPathLength */
+    const int32_t* medium_id;   /* [n] medium of mBSDF (-1 on surface) */
+    const uint32_t* flags;      /* [n] UPBP_LV_* */
+    const upbp_mis* mis;        /* [n] mMisData */
+    int32_t n_paths;
+    const int32_t* path_ends;   /* [n_paths] mPathEnds */
+} upbp_light_vertices;
+
+/* Photon beams (mPhotonBeamsArray, filled by UPBP::AddBeams, UPBP.hxx:1783-1870). */
+typedef struct upbp_beams {
+    int64_t n;
+    const float* origin;          /* [n][3] mRay.origin */
+    const float* direction;       /* [n][3] mRay.direction */
+    const float* length;          /* [n] mLength */
+    const float* throughput;      /* [n][3] mThroughputAtOrigin */
+    const uint32_t* flags;        /* [n] mFlags (SHORT/LONG) */
+    const float* ray_sample_pdf;  /* [n] mRaySamplePdf */
+    const float* ray_sample_rev_pdf; /* [n] mRaySampleRevPdf */
+    const uint32_t* ray_sampling_flags; /* [n] mRaySamplingFlags */
+    const float* last_pdf_w_inv;  /* [n] mLastPdfWInv */
+    const int32_t* medium_id;     /* [n] mMedium */
+    const int32_t* light_vertex;  /* [n] mLightVertex as an index into the light vertices */
+} upbp_beams;
+
+/* Camera segment queries: one entry per evalBre/evalBeamBeamEstimate call
+ * pair at a camera path length L.  cam_mis[cam_mis_begin .. +L) is the
+ * snapshot of mCameraVerticesMisData[0..L-1] taken at the call. */
+typedef struct upbp_segment_queries {
+    int64_t n;
+    const float* origin;        /* [n][3] ray.origin */
+    const float* direction;     /* [n][3] ray.direction */
+    const int32_t* seg_begin;   /* [n] first segment in the segment arrays */
+    const int32_t* seg_count;   /* [n] number of segments */
+    const uint32_t* flags;      /* [n] UPBP_Q_* */
+    const int32_t* path_length; /* [n] cameraState.mPathLength */
+    const float* last_pdf_w_inv;/* [n] cameraState.mLastPdfWInv */
+    const float* throughput;    /* [n][3] cameraState.mThroughput */
+    const int32_t* pixel;       /* [n] framebuffer index (y*W+x) or -1 */
+    const int64_t* cam_mis_begin; /* [n] */
+    int64_t n_segments;
+    const float* seg_dist_min;  /* [s] mDistMin */
+    const float* seg_dist_max;  /* [s] mDistMax */
+    const float* seg_pdf;       /* [s] mRaySamplePdf */
+    const float* seg_rev_pdf;   /* [s] mRaySampleRevPdf */
+    const float* seg_attenuation; /* [s][3] mAttenuation */
+    const int32_t* seg_medium;  /* [s] mMediumID */
+} upbp_segment_queries;
+
+/* Camera point queries (PP3D RangeQuery at a camera medium vertex).
+ * cam_mis[cam_mis_begin .. +L+1) is mCameraVerticesMisData[0..L]. */
+typedef struct upbp_point_queries {
+    int64_t n;
+    const float* position;      /* [n][3] hitPoint */
+    const float* dir_fix;       /* [n][3] camera bsdf WorldDirFix */
+    const int32_t* medium_id;   /* [n] camera bsdf medium */
+    const int32_t* path_length; /* [n] cameraState.mPathLength */
+    const float* throughput;    /* [n][3] cameraState.mThroughput */
+    const int32_t* pixel;       /* [n] */
+    const int64_t* cam_mis_begin; /* [n] */
+} upbp_point_queries;
+
+/* Per-query candidate statistics for candidate-set parity.  A candidate is a
+ * (query, photon|beam) pair that passes the reference's geometric test:
+ * testIntersectionBre (Bre.cxx:199-223) for PB2D, testIntersectionBeamBeam
+ * plus same medium and radius >= distance (PhotonBeam.hxx:238-296, 390-413)
+ * for BB1D, and distSqr <= r^2 over the 8 hashed cells (HashGrid.hxx:177-185,
+ * counted with multiplicity) for PP3D.  hash = sum over candidates of
+ * mix64(id) (wrapping), which is order independent. */
+typedef struct upbp_query_stats {
+    uint32_t* count_pb2d; uint64_t* hash_pb2d; /* [n_segment_queries] or NULL */
+    uint32_t* count_bb1d; uint64_t* hash_bb1d; /* [n_segment_queries] or NULL */
+    uint32_t* count_pp3d; uint64_t* hash_pp3d; /* [n_point_queries]  or NULL */
+} upbp_query_stats;
+
+typedef struct upbp_ctx upbp_ctx;
+
+/* ---- entry points ------------------------------------------------------- */
+
+/* Create a context on CUDA device `device`.  Replaces the construction of
+ * EmbreeBre(scene) / PhotonBeamsEvaluator(scene) / HashGrid in the UPBP ctor
+ * (Renderers/UPBP.hxx:160-216). */
+int upbp_ctx_create(upbp_ctx** out, int device);
+/* Replaces EmbreeBre::~EmbreeBre / PhotonBeamsEvaluator destructor. */
+int upbp_ctx_destroy(upbp_ctx* ctx);
+const char* upbp_last_error(const upbp_ctx* ctx);
+
+/* Evaluation mode (UPBP_MODE_*). */
+int upbp_set_mode(upbp_ctx* ctx, int mode);
+/* Tunables picked by the autotuner: leaf size of the LBVHs and the gather block size. */
+int upbp_set_tuning(upbp_ctx* ctx, int pb2d_leaf, int bb1d_leaf, int block_threads);
+/* CUDA stream (cudaStream_t as void*) used by all later calls; NULL = the context's own stream. */
+int upbp_set_stream(upbp_ctx* ctx, void* stream);
+
+/* Scene media table: scene.mMedia (Scene/Scene.hxx).  Replaces the
+ * `scene` member read by EmbreeBre / PhotonBeamsEvaluator. */
+int upbp_set_media(upbp_ctx* ctx, const upbp_medium* media, int32_t n_media);
+/* Per-iteration constants (Renderers/UPBP.hxx:415-460). */
+int upbp_set_params(upbp_ctx* ctx, const upbp_params* params);
+
+/* Upload mLightVertices + mPathEnds.  Together with upbp_build this replaces
+ * HashGrid::Reserve/Build (UPBP.hxx:699-704) and EmbreeBre::build
+ * (Bre.cxx:649-755). */
+int upbp_set_light_vertices(upbp_ctx* ctx, const upbp_light_vertices* lv);
+/* Upload mPhotonBeamsArray.  With upbp_build replaces
+ * PhotonBeamsEvaluator::build (PhBeams.cxx:66-148). */
+int upbp_set_beams(upbp_ctx* ctx, const upbp_beams* beams);
+/* Build every acceleration structure for the uploaded photons and beams:
+ * PP3D hash grid, PB2D photon LBVH, BB1D beam LBVH, MIS suffix sums. */
+int upbp_build(upbp_ctx* ctx);
+
+/* Upload the recorded camera MIS snapshots and queries of this iteration. */
+int upbp_set_camera_mis(upbp_ctx* ctx, const upbp_mis* records, int64_t n_records);
+int upbp_set_segment_queries(upbp_ctx* ctx, const upbp_segment_queries* q);
+int upbp_set_point_queries(upbp_ctx* ctx, const upbp_point_queries* q);
+
+/* Evaluate all recorded queries: the batched equivalent of every
+ * evalBre / evalBeamBeamEstimate / HashGrid::Process call of the iteration,
+ * with the contributions splatted into the device framebuffer
+ * (color += throughput * normalisation * contrib, UPBP.hxx:782-796, 890-909, 1120). */
+int upbp_evaluate(upbp_ctx* ctx);
+
+/* Results. */
+int upbp_read_segment_results(upbp_ctx* ctx, float* pb2d_rgb, float* bb1d_rgb); /* [n][3] each, may be NULL */
+int upbp_read_point_results(upbp_ctx* ctx, float* pp3d_rgb);                    /* [n][3] */
+int upbp_read_query_stats(upbp_ctx* ctx, const upbp_query_stats* stats);
+int upbp_clear_image(upbp_ctx* ctx);
+int upbp_read_image(upbp_ctx* ctx, float* rgb); /* [H*W][3] accumulated */
+/* Device-side counters: number of kernels launched by the last upbp_build and upbp_evaluate. */
+int upbp_last_launch_count(const upbp_ctx* ctx, int* build_launches, int* evaluate_launches);
+/* Average duration (ms) of the last evaluate's dominant gather kernel, measured with CUDA events. */
+int upbp_last_timings(const upbp_ctx* ctx, float* build_ms, float* pp3d_ms, float* pb2d_ms, float* bb1d_ms);
+
+/* Releases the per-iteration structures; replaces EmbreeBre::destroy and
+ * PhotonBeamsEvaluator::destroy (UPBP.hxx:1172-1181).  Device buffers are
+ * kept for reuse by the next iteration. */
+int upbp_destroy_structures(upbp_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UPBP_GPU_H */

@@ -1,0 +1,49 @@
+/*
+ * Reference harness TU for BB1D (test infrastructure): compiles the
+ * reference's Beams/PhBeams.cxx unchanged.  Built twice by
+ * oracle/build_ref.py: once as is (USE_GRID, the reference default,
+ * PhBeams.hxx:30-34) and once with UPBP_REF_USE_BRUTE (the reference's
+ * brute-force AccelStruct, PhBrute.hxx:36-104) under the class names
+ * PhotonBeamsEvaluatorBrute / AccelStructBrute.
+ */
+#include <vector>
+#include <list>
+#include <forward_list>
+#include <string>
+#include <sstream>
+#include <iostream>
+#include <iomanip>
+#include <algorithm>
+#include <cmath>
+#if defined(UPBP_REF_USE_BRUTE)
+#define PhotonBeamsEvaluator PhotonBeamsEvaluatorBrute
+#define AccelStruct AccelStructBrute
+#endif
+#include "Beams/PhBeams.cxx"
+
+#if defined(UPBP_REF_USE_BRUTE)
+/* Opaque entry points so the main harness TU (which sees the grid class
+ * under the reference name) can drive the brute-force evaluator. */
+void* ref_brute_create(const Scene& scene, PhotonBeamsArray& beams, float radius)
+{
+    PhotonBeamsEvaluatorBrute* e = new PhotonBeamsEvaluatorBrute(scene);
+    e->build(beams, CONSTANT_RADIUS, radius, 0, false);
+    return e;
+}
+Rgb ref_brute_eval(void* h, BeamType bt, const Ray& ray, const VolumeSegments& segs, uint tech, uint rsf,
+                   embree::AdditionalRayDataForMis* data)
+{
+    return static_cast<PhotonBeamsEvaluatorBrute*>(h)->evalBeamBeamEstimate(bt, ray, segs, tech, rsf, data, NULL);
+}
+Rgb ref_brute_eval_lite(void* h, BeamType bt, const Ray& ray, const LiteVolumeSegments& segs, uint tech, uint rsf,
+                        embree::AdditionalRayDataForMis* data)
+{
+    return static_cast<PhotonBeamsEvaluatorBrute*>(h)->evalBeamBeamEstimate(bt, ray, segs, tech, rsf, data, NULL);
+}
+void ref_brute_destroy(void* h)
+{
+    PhotonBeamsEvaluatorBrute* e = static_cast<PhotonBeamsEvaluatorBrute*>(h);
+    e->destroy();
+    delete e;
+}
+#endif

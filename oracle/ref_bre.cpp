@@ -1,0 +1,36 @@
+/*
+ * Reference harness TU for PB2D (test infrastructure): compiles the
+ * reference's Bre/Bre.cxx unchanged (EmbreeBre::build / evalBre / destroy and
+ * the BRE callbacks) and adds the candidate enumerator used for
+ * candidate-set parity.
+ */
+#include <vector>
+#include <list>
+#include <forward_list>
+#include <string>
+#include <sstream>
+#include <iostream>
+#include <iomanip>
+#include <algorithm>
+#include <cmath>
+#define private public
+#define protected public
+#include "Bre/Bre.cxx"
+#undef private
+#undef protected
+
+#include "ref_internal.h"
+
+void ref_bre_candidates(const EmbreeBre& bre, const float* origin, const float* dir, float tnear, float tfar,
+                        const UPBPLightVertex* lv_base, uint32_t& count, uint64_t& hash)
+{
+    Ray ray(Pos(origin[0], origin[1], origin[2]), Dir(dir[0], dir[1], dir[2]));
+    for (int i = 0; i < bre.numEmbreePhotons; ++i) {
+        const EmbreePhoton& ph = bre.embreePhotons[i];
+        float t, d2;
+        if (EmbreePhoton::testIntersectionBre(t, d2, ray, tnear, tfar, ph.lightVertex->mHitpoint, ph.radiusSqr)) {
+            ++count;
+            hash += ref_mix64((uint64_t)(ph.lightVertex - lv_base));
+        }
+    }
+}

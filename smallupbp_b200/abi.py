@@ -1,0 +1,124 @@
+"""ctypes mirror of ``include/upbp_gpu.h`` and helpers that point its structs at numpy arrays.
+
+A workload is a dict of numpy arrays (see :mod:`smallupbp_b200.workload`).  :func:`make_structs`
+returns the C structs for it together with the list of arrays they reference (keep it alive while
+the structs are in use).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+from .workload import MEDIUM_DTYPE, MIS_DTYPE, PARAMS_DTYPE
+
+f32p = C.POINTER(C.c_float)
+i32p = C.POINTER(C.c_int32)
+u32p = C.POINTER(C.c_uint32)
+i64p = C.POINTER(C.c_int64)
+u64p = C.POINTER(C.c_uint64)
+
+
+class Medium(C.Structure):
+    _fields_ = [("absorption", C.c_float * 3), ("scattering", C.c_float * 3), ("mean_cosine", C.c_float),
+                ("continuation_prob", C.c_float)]
+
+
+class Mis(C.Structure):
+    _fields_ = [(n, C.c_float) for n in MIS_DTYPE.names[:-1]] + [("flags", C.c_uint32)]
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_uint32 if PARAMS_DTYPE[n].kind == "u" else (C.c_int32 if PARAMS_DTYPE[n].kind == "i" else C.c_float))
+                for n in PARAMS_DTYPE.names]
+
+
+class LightVertices(C.Structure):
+    _fields_ = [("n", C.c_int64), ("position", f32p), ("throughput", f32p), ("dir_fix", f32p), ("cont_prob", f32p),
+                ("path_idx", i32p), ("path_length", i32p), ("medium_id", i32p), ("flags", u32p),
+                ("mis", C.POINTER(Mis)), ("n_paths", C.c_int32), ("path_ends", i32p)]
+
+
+class Beams(C.Structure):
+    _fields_ = [("n", C.c_int64), ("origin", f32p), ("direction", f32p), ("length", f32p), ("throughput", f32p),
+                ("flags", u32p), ("ray_sample_pdf", f32p), ("ray_sample_rev_pdf", f32p),
+                ("ray_sampling_flags", u32p), ("last_pdf_w_inv", f32p), ("medium_id", i32p), ("light_vertex", i32p)]
+
+
+class SegmentQueries(C.Structure):
+    _fields_ = [("n", C.c_int64), ("origin", f32p), ("direction", f32p), ("seg_begin", i32p), ("seg_count", i32p),
+                ("flags", u32p), ("path_length", i32p), ("last_pdf_w_inv", f32p), ("throughput", f32p),
+                ("pixel", i32p), ("cam_mis_begin", i64p), ("n_segments", C.c_int64), ("seg_dist_min", f32p),
+                ("seg_dist_max", f32p), ("seg_pdf", f32p), ("seg_rev_pdf", f32p), ("seg_attenuation", f32p),
+                ("seg_medium", i32p)]
+
+
+class PointQueries(C.Structure):
+    _fields_ = [("n", C.c_int64), ("position", f32p), ("dir_fix", f32p), ("medium_id", i32p),
+                ("path_length", i32p), ("throughput", f32p), ("pixel", i32p), ("cam_mis_begin", i64p)]
+
+
+class QueryStats(C.Structure):
+    _fields_ = [("count_pb2d", u32p), ("hash_pb2d", u64p), ("count_bb1d", u32p), ("hash_bb1d", u64p),
+                ("count_pp3d", u32p), ("hash_pp3d", u64p)]
+
+
+assert C.sizeof(Mis) == 60
+assert C.sizeof(Medium) == MEDIUM_DTYPE.itemsize
+assert C.sizeof(Params) == PARAMS_DTYPE.itemsize
+
+_PTR = {np.float32: f32p, np.int32: i32p, np.uint32: u32p, np.int64: i64p, np.uint64: u64p}
+
+
+def ptr(a: np.ndarray, ctype=None):
+    """Pointer to a C-contiguous numpy array (NULL for None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    if ctype is None:
+        ctype = _PTR[a.dtype.type]
+    return a.ctypes.data_as(ctype)
+
+
+def make_structs(w: Dict[str, np.ndarray]) -> Tuple[dict, List[np.ndarray]]:
+    """Build the upbp_gpu.h structs for workload ``w``; returns (structs, keepalive)."""
+    keep: List[np.ndarray] = []
+
+    def a(name, dtype=None):
+        x = np.ascontiguousarray(w[name]) if dtype is None else np.ascontiguousarray(w[name], dtype=dtype)
+        keep.append(x)
+        return x
+
+    params = Params.from_buffer_copy(a("params").tobytes())
+    media_arr = a("media")
+    media = (Medium * len(media_arr)).from_buffer_copy(media_arr.tobytes())
+    lvm = a("lv_mis")
+    lv = LightVertices(
+        n=len(w["lv_path_idx"]), position=ptr(a("lv_position")), throughput=ptr(a("lv_throughput")),
+        dir_fix=ptr(a("lv_dir_fix")), cont_prob=ptr(a("lv_cont_prob")), path_idx=ptr(a("lv_path_idx")),
+        path_length=ptr(a("lv_path_length")), medium_id=ptr(a("lv_medium_id")), flags=ptr(a("lv_flags")),
+        mis=lvm.ctypes.data_as(C.POINTER(Mis)), n_paths=len(w["lv_path_ends"]), path_ends=ptr(a("lv_path_ends")))
+    beams = Beams(
+        n=len(w["beam_length"]), origin=ptr(a("beam_origin")), direction=ptr(a("beam_direction")),
+        length=ptr(a("beam_length")), throughput=ptr(a("beam_throughput")), flags=ptr(a("beam_flags")),
+        ray_sample_pdf=ptr(a("beam_ray_sample_pdf")), ray_sample_rev_pdf=ptr(a("beam_ray_sample_rev_pdf")),
+        ray_sampling_flags=ptr(a("beam_ray_sampling_flags")), last_pdf_w_inv=ptr(a("beam_last_pdf_w_inv")),
+        medium_id=ptr(a("beam_medium_id")), light_vertex=ptr(a("beam_light_vertex")))
+    sq = SegmentQueries(
+        n=len(w["sq_path_length"]), origin=ptr(a("sq_origin")), direction=ptr(a("sq_direction")),
+        seg_begin=ptr(a("sq_seg_begin")), seg_count=ptr(a("sq_seg_count")), flags=ptr(a("sq_flags")),
+        path_length=ptr(a("sq_path_length")), last_pdf_w_inv=ptr(a("sq_last_pdf_w_inv")),
+        throughput=ptr(a("sq_throughput")), pixel=ptr(a("sq_pixel")), cam_mis_begin=ptr(a("sq_cam_mis_begin")),
+        n_segments=len(w["seg_dist_min"]), seg_dist_min=ptr(a("seg_dist_min")), seg_dist_max=ptr(a("seg_dist_max")),
+        seg_pdf=ptr(a("seg_pdf")), seg_rev_pdf=ptr(a("seg_rev_pdf")), seg_attenuation=ptr(a("seg_attenuation")),
+        seg_medium=ptr(a("seg_medium")))
+    pq = PointQueries(
+        n=len(w["pq_path_length"]), position=ptr(a("pq_position")), dir_fix=ptr(a("pq_dir_fix")),
+        medium_id=ptr(a("pq_medium_id")), path_length=ptr(a("pq_path_length")), throughput=ptr(a("pq_throughput")),
+        pixel=ptr(a("pq_pixel")), cam_mis_begin=ptr(a("pq_cam_mis_begin")))
+    cm = a("cam_mis")
+    cam = cm.ctypes.data_as(C.POINTER(Mis))
+    structs = dict(params=params, media=media, n_media=len(media_arr), lv=lv, beams=beams, sq=sq, pq=pq,
+                   cam_mis=cam, n_cam_mis=len(cm))
+    return structs, keep
