@@ -1,0 +1,19 @@
+"""Compile the oracle's C restatement (oracle/upbp_oracle.c) into oracle/liboracle.so (test infrastructure)."""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+def build() -> str:
+    cmd = ["gcc", "-std=c99", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-Wall",
+           "-Wno-unused-function", os.path.join(HERE, "upbp_oracle.c"), "-o", LIB, "-lm"]
+    subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build())
+    sys.exit(0)

@@ -1,0 +1,55 @@
+"""Python driver of the oracle's C restatement ``oracle/liboracle.so`` (test infrastructure only).
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict
+
+import numpy as np
+
+from smallupbp_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build_oracle  # noqa: F401  (python oracle/build_oracle.py builds it)
+            raise FileNotFoundError(LIB_PATH + " is not built (python oracle/build_oracle.py)")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.upbp_oracle_run.restype = C.c_int
+        _lib.upbp_oracle_run.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Medium), C.c_int32,
+                                         C.POINTER(abi.LightVertices), C.POINTER(abi.Beams), C.POINTER(abi.Mis),
+                                         C.POINTER(abi.SegmentQueries), C.POINTER(abi.PointQueries), C.c_int64,
+                                         abi.f32p, abi.f32p, abi.f32p, abi.u32p, abi.u64p, abi.u32p, abi.u64p,
+                                         abi.u32p, abi.u64p, abi.f32p]
+    return _lib
+
+
+def run(w: Dict[str, np.ndarray], stride: int = 1) -> Dict[str, np.ndarray]:
+    s, keep = abi.make_structs(w)
+    nq, npq = s["sq"].n, s["pq"].n
+    p = s["params"]
+    out = {"pb2d": np.zeros((nq, 3), np.float32), "bb1d": np.zeros((nq, 3), np.float32),
+           "pp3d": np.zeros((npq, 3), np.float32), "count_pb2d": np.zeros(nq, np.uint32),
+           "hash_pb2d": np.zeros(nq, np.uint64), "count_bb1d": np.zeros(nq, np.uint32),
+           "hash_bb1d": np.zeros(nq, np.uint64), "count_pp3d": np.zeros(npq, np.uint32),
+           "hash_pp3d": np.zeros(npq, np.uint64),
+           "image": np.zeros((p.image_width * p.image_height, 3), np.float32)}
+    P = abi.ptr
+    rc = lib().upbp_oracle_run(C.byref(p), s["media"], s["n_media"], C.byref(s["lv"]), C.byref(s["beams"]),
+                               s["cam_mis"], C.byref(s["sq"]), C.byref(s["pq"]), stride, P(out["pb2d"]),
+                               P(out["bb1d"]), P(out["pp3d"]), P(out["count_pb2d"]), P(out["hash_pb2d"]),
+                               P(out["count_bb1d"]), P(out["hash_bb1d"]), P(out["count_pp3d"]), P(out["hash_pp3d"]),
+                               P(out["image"]))
+    if rc != 0:
+        raise RuntimeError("upbp_oracle_run failed (%d)" % rc)
+    del keep
+    return out

@@ -391,7 +391,10 @@ extern "C" int ref_run(const upbp_params* params, const upbp_medium* media, int3
                     float* dst = variant == 0 ? out->bb1d_rgb : out->bb1d_brute_rgb;
                     if (dst) for (int k = 0; k < 3; ++k) dst[3 * q + k] = c[k];
                     const int px = sq->pixel[q];
-                    const bool splat = variant == 0 || !(what & REF_BB1D_GRID);
+                    // The image follows the brute-force estimate when it is computed: it
+                    // defines the candidate set (the grid can differ where t1 falls on a
+                    // DDA cell boundary, Grid.hxx:359-364).
+                    const bool splat = variant == 1 || !(what & REF_BB1D_BRUTE);
                     if (img && px >= 0 && splat) {
                         const Rgb add = thr * U.mBB1DNormalization * c;
                         for (int k = 0; k < 3; ++k) img[3 * px + k] += add[k];

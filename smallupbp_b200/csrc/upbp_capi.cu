@@ -1,0 +1,844 @@
+// C ABI of the B200 estimator stage (include/upbp_gpu.h): context, uploads, builds, evaluation.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "upbp_kernels.cuh"
+
+using namespace upbp;
+
+namespace {
+
+// Grow-only device buffer.
+struct DBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct Error {
+    int code;
+};
+
+}  // namespace
+
+struct upbp_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int mode = UPBP_MODE_PLAIN;
+    int pb2d_leaf = 4;
+    int bb1d_leaf = 4;
+    int block = 128;
+    float piece_len_r = 8.f;  // beam piece length in units of the beam radius
+    std::string err;
+    upbp_params P{};
+    bool have_params = false;
+    std::vector<DMedium> media;
+    size_t bytes = 0;
+
+    // inputs
+    int64_t n_lv = 0;
+    int32_t n_paths = 0;
+    DBuf lv_pos_in, lv_thr_in, lv_dir_in, lv_cont_in, lv_pidx_in, lv_plen_in, lv_med_in, lv_flags_in, lv_mis,
+        path_ends;
+    int64_t n_beams = 0;
+    DBuf b_origin, b_dir, b_len, b_thr_in, b_flags_in, b_rsp_in, b_rsr_in, b_rsf_in, b_lpw_in, b_med_in, b_lv_in;
+    int64_t n_cam = 0;
+    DBuf cam_mis;
+    int64_t n_sq = 0, n_seg = 0;
+    DBuf sq_origin, sq_dir, sq_seg_begin, sq_seg_count, sq_flags, sq_plen, sq_lpw, sq_thr, sq_pixel, sq_cam_begin,
+        seg_dmin, seg_dmax, seg_pdf, seg_rev, seg_att, seg_med;
+    int64_t n_pq = 0;
+    DBuf pq_pos, pq_dir, pq_med, pq_plen, pq_thr, pq_pixel, pq_cam_begin;
+
+    // packed light vertices
+    DBuf lv_pos4, lv_dir4, lv_thr4, lv_info4, lv_inmed;
+    // photons
+    int n_ph = 0;
+    DBuf ph_lv, ph_lv_sorted, ph_keys, ph_keys_sorted, bbox_partial, bbox_ph;
+    // hash grid
+    DBuf hg_start, hg_end, hg_pos;
+    float hg_bbox[6] = {0, 0, 0, 0, 0, 0};
+    float hg_inv_cell = 0.f;
+    // photon LBVH
+    DBuf pb_pos, pb_leaf_codes, pb_nodes, pb_parent_int, pb_parent_leaf, pb_leaf_boxes, pb_node_boxes, pb_flags;
+    int pb_n_leaves = 0;
+    // beams
+    DBuf bm_thr4, bm_pdf4, bm_link, bm_radius, bm_counts, bm_offsets, pc_a, pc_b, pc_c, pc_boxes, pc_a2, pc_b2, pc_c2,
+        pc_boxes2, pc_codes, pc_codes_sorted, pc_perm, pc_perm_sorted, bbox_pc;
+    int n_pieces = 0;
+    DBuf bm_leaf_codes, bm_nodes, bm_parent_int, bm_parent_leaf, bm_leaf_boxes, bm_node_boxes, bm_flagsbuf;
+    int bm_n_leaves = 0;
+    // temp storage for CUB
+    DBuf cub_tmp;
+    // outputs
+    DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
+    bool built = false;
+    int build_launches = 0, eval_launches = 0;
+    float t_build = 0.f, t_pp3d = 0.f, t_pb2d = 0.f, t_bb1d = 0.f;
+    cudaEvent_t ev[8] = {};
+};
+
+namespace {
+
+void fail(upbp_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    throw Error{code};
+}
+
+void ck(upbp_ctx* c, cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) {
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            fail(c, UPBP_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+        }
+        fail(c, UPBP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    }
+}
+
+void ensure(upbp_ctx* c, DBuf& b, size_t bytes)
+{
+    if (bytes <= b.cap) return;
+    if (b.p) {
+        ck(c, cudaFreeAsync(b.p, c->stream), "cudaFreeAsync");
+        c->bytes -= b.cap;
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    const size_t want = std::max<size_t>(bytes + bytes / 4, 256);
+    ck(c, cudaMallocAsync(&b.p, want, c->stream), "cudaMallocAsync");
+    b.cap = want;
+    c->bytes += want;
+}
+
+template <class T>
+void upload(upbp_ctx* c, DBuf& b, const T* src, int64_t count, const char* name)
+{
+    if (count <= 0) return;
+    if (!src) fail(c, UPBP_ERR_INVALID_ARG, "%s is NULL", name);
+    ensure(c, b, sizeof(T) * (size_t)count);
+    ck(c, cudaMemcpyAsync(b.p, src, sizeof(T) * (size_t)count, cudaMemcpyDefault, c->stream), name);
+}
+
+void free_buf(DBuf& b)
+{
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+DMedium derive_medium(const upbp_medium& m)
+{
+    // HomogeneousMedium ctor (Scene/Media.hxx:129-159), same float operations.
+    DMedium d{};
+    for (int c = 0; c < 3; ++c) {
+        const float a = std::fabs(m.absorption[c]);
+        const float s = std::fabs(m.scattering[c]);
+        d.ss[c] = s;
+        d.st[c] = a + s;
+    }
+    float mn = d.st[0];
+    int idx = 0;
+    if (d.st[1] > 0 && (mn == 0 || d.st[1] < mn)) mn = d.st[1], idx = 1;
+    if (d.st[2] > 0 && (mn == 0 || d.st[2] < mn)) mn = d.st[2], idx = 2;
+    d.min_st = mn;
+    d.min_idx = idx;
+    d.has_scat = (d.ss[0] > 0 || d.ss[1] > 0 || d.ss[2] > 0) ? 1 : 0;
+    const bool has_att = d.st[0] > 0 || d.st[1] > 0 || d.st[2] > 0;
+    const float mx = std::max(d.st[0], std::max(d.st[1], d.st[2]));
+    d.mfp = has_att ? 1.0f / mx : INFINITY;
+    d.g = m.mean_cosine;
+    d.cont = m.continuation_prob;
+    return d;
+}
+
+void sort_pairs(upbp_ctx* c, const uint32_t* kin, uint32_t* kout, const int32_t* vin, int32_t* vout, int n,
+                int end_bit)
+{
+    size_t b = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b, kin, kout, vin, vout, n, 0, end_bit, c->stream);
+    ensure(c, c->cub_tmp, b);
+    ck(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, b, kin, kout, vin, vout, n, 0, end_bit, c->stream),
+       "SortPairs");
+    c->build_launches += 4;
+}
+
+int bits_for(uint32_t maxv)
+{
+    int b = 1;
+    while (b < 32 && (maxv >> b)) ++b;
+    return b;
+}
+
+__global__ void k_iota(int32_t* v, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+void build_lbvh(upbp_ctx* c, const uint32_t* codes_sorted, int n, int leaf, DBuf& leaf_codes, DBuf& nodes,
+                DBuf& parent_int, DBuf& parent_leaf, DBuf& leaf_boxes, DBuf& node_boxes, DBuf& flags, int& n_leaves)
+{
+    n_leaves = (n + leaf - 1) / leaf;
+    const int ni = std::max(1, n_leaves - 1);
+    ensure(c, leaf_codes, sizeof(uint32_t) * n_leaves);
+    ensure(c, nodes, sizeof(BNode) * ni);
+    ensure(c, parent_int, sizeof(int32_t) * ni);
+    ensure(c, parent_leaf, sizeof(int32_t) * n_leaves);
+    ensure(c, node_boxes, sizeof(Box) * ni);
+    ensure(c, flags, sizeof(int32_t) * ni);
+    launch_leaf_codes(codes_sorted, n, leaf, leaf_codes.as<uint32_t>(), c->stream);
+    launch_karras(leaf_codes.as<uint32_t>(), n_leaves, nodes.as<BNode>(), parent_int.as<int32_t>(),
+                  parent_leaf.as<int32_t>(), c->stream);
+    ck(c, cudaMemsetAsync(flags.p, 0, sizeof(int32_t) * ni, c->stream), "memset");
+    launch_bottom_up(leaf_boxes.as<Box>(), n_leaves, nodes.as<BNode>(), parent_int.as<int32_t>(),
+                     parent_leaf.as<int32_t>(), node_boxes.as<Box>(), flags.as<int32_t>(), c->stream);
+    c->build_launches += 3;
+}
+
+void do_build(upbp_ctx* c)
+{
+    if (!c->have_params) fail(c, UPBP_ERR_INVALID_ARG, "upbp_set_params was not called");
+    if (c->media.empty()) fail(c, UPBP_ERR_INVALID_ARG, "upbp_set_media was not called");
+    cudaStream_t s = c->stream;
+    c->build_launches = 0;
+    ck(c, cudaEventRecord(c->ev[0], s), "event");
+    const upbp_params& P = c->P;
+    const int64_t n = c->n_lv;
+    // ---- light vertices
+    ensure(c, c->lv_pos4, sizeof(float4) * std::max<int64_t>(n, 1));
+    ensure(c, c->lv_dir4, sizeof(float4) * std::max<int64_t>(n, 1));
+    ensure(c, c->lv_thr4, sizeof(float4) * std::max<int64_t>(n, 1));
+    ensure(c, c->lv_info4, sizeof(int4) * std::max<int64_t>(n, 1));
+    ensure(c, c->lv_inmed, sizeof(uint32_t) * std::max<int64_t>(n, 1));
+    ensure(c, c->ph_lv, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    launch_pack_lights(c->lv_pos_in.as<float>(), c->lv_thr_in.as<float>(), c->lv_dir_in.as<float>(),
+                       c->lv_cont_in.as<float>(), c->lv_pidx_in.as<int32_t>(), c->lv_plen_in.as<int32_t>(),
+                       c->lv_med_in.as<int32_t>(), c->lv_flags_in.as<uint32_t>(), n, c->lv_pos4.as<float4>(),
+                       c->lv_dir4.as<float4>(), c->lv_thr4.as<float4>(), c->lv_info4.as<int4>(),
+                       c->lv_inmed.as<uint32_t>(), s);
+    c->build_launches += 1;
+    // ---- photons = light vertices in media (stable compaction keeps light-vertex order)
+    c->n_ph = 0;
+    if (n > 0) {
+        ensure(c, c->bbox_partial, sizeof(int32_t) * 8 + sizeof(float) * 6 * 1024);
+        int32_t* d_nsel = c->bbox_partial.as<int32_t>();
+        ensure(c, c->ph_lv_sorted, sizeof(int32_t) * n);
+        {
+            ensure(c, c->ph_keys, sizeof(int32_t) * n);
+            k_iota<<<(int)((n + 255) / 256), 256, 0, s>>>(c->ph_keys.as<int32_t>(), (int)n);
+            size_t b = 0;
+            cub::DeviceSelect::Flagged(nullptr, b, c->ph_keys.as<int32_t>(), c->lv_inmed.as<uint32_t>(),
+                                       c->ph_lv.as<int32_t>(), d_nsel, (int)n, s);
+            ensure(c, c->cub_tmp, b);
+            ck(c, cub::DeviceSelect::Flagged(c->cub_tmp.p, b, c->ph_keys.as<int32_t>(), c->lv_inmed.as<uint32_t>(),
+                                             c->ph_lv.as<int32_t>(), d_nsel, (int)n, s),
+               "DeviceSelect");
+            c->build_launches += 2;
+        }
+        int32_t h_nsel = 0;
+        ck(c, cudaMemcpyAsync(&h_nsel, d_nsel, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "copy n_sel");
+        ck(c, cudaStreamSynchronize(s), "sync");
+        c->n_ph = h_nsel;
+    }
+    const int nph = c->n_ph;
+    const int blocks = std::max(1, std::min(1024, (nph + 255) / 256));
+    if (nph > 0) {
+        ensure(c, c->bbox_ph, sizeof(float) * 6);
+        float* partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
+        launch_bbox_partial(c->lv_pos4.as<float4>(), c->ph_lv.as<int32_t>(), nph, partial, blocks, s);
+        launch_bbox_final(partial, blocks, c->bbox_ph.as<float>(), s);
+        ck(c, cudaMemcpyAsync(c->hg_bbox, c->bbox_ph.p, sizeof(float) * 6, cudaMemcpyDeviceToHost, s), "bbox");
+        c->build_launches += 2;
+    }
+    // ---- PP3D hash grid (HashGrid::Build, Misc/HashGrid.hxx:47-126)
+    if (nph > 0 && (P.techniques & UPBP_PP3D)) {
+        const int cells = std::max(1, P.hash_cells);
+        const float cell_size = P.radius_pp3d * 2.f;
+        c->hg_inv_cell = 1.f / cell_size;
+        ensure(c, c->ph_keys, sizeof(uint32_t) * nph);
+        ensure(c, c->ph_keys_sorted, sizeof(uint32_t) * nph);
+        ensure(c, c->hg_start, sizeof(int32_t) * cells);
+        ensure(c, c->hg_end, sizeof(int32_t) * cells);
+        ensure(c, c->hg_pos, sizeof(float4) * nph);
+        launch_hash_keys(c->lv_pos4.as<float4>(), c->ph_lv.as<int32_t>(), nph, c->bbox_ph.as<float>(),
+                         c->hg_inv_cell, cells, c->ph_keys.as<uint32_t>(), s);
+        sort_pairs(c, c->ph_keys.as<uint32_t>(), c->ph_keys_sorted.as<uint32_t>(), c->ph_lv.as<int32_t>(),
+                   c->ph_lv_sorted.as<int32_t>(), nph, bits_for((uint32_t)cells - 1));
+        ck(c, cudaMemsetAsync(c->hg_start.p, 0, sizeof(int32_t) * cells, s), "memset");
+        ck(c, cudaMemsetAsync(c->hg_end.p, 0, sizeof(int32_t) * cells, s), "memset");
+        launch_hash_ranges(c->ph_keys_sorted.as<uint32_t>(), c->ph_lv_sorted.as<int32_t>(), c->lv_pos4.as<float4>(),
+                           nph, c->hg_start.as<int32_t>(), c->hg_end.as<int32_t>(), c->hg_pos.as<float4>(), s);
+        c->build_launches += 2;
+    }
+    // ---- PB2D photon LBVH
+    c->pb_n_leaves = 0;
+    if (nph > 0 && (P.techniques & UPBP_PB2D)) {
+        ensure(c, c->ph_keys, sizeof(uint32_t) * nph);
+        ensure(c, c->ph_keys_sorted, sizeof(uint32_t) * nph);
+        ensure(c, c->pb_pos, sizeof(float4) * nph);
+        launch_morton_points(c->lv_pos4.as<float4>(), c->ph_lv.as<int32_t>(), nph, c->bbox_ph.as<float>(),
+                             c->ph_keys.as<uint32_t>(), s);
+        sort_pairs(c, c->ph_keys.as<uint32_t>(), c->ph_keys_sorted.as<uint32_t>(), c->ph_lv.as<int32_t>(),
+                   c->ph_lv_sorted.as<int32_t>(), nph, 30);
+        launch_gather_photons(c->ph_lv_sorted.as<int32_t>(), c->lv_pos4.as<float4>(), nph, c->pb_pos.as<float4>(), s);
+        const int leaf = std::max(1, c->pb2d_leaf);
+        const int nl = (nph + leaf - 1) / leaf;
+        ensure(c, c->pb_leaf_boxes, sizeof(Box) * nl);
+        const float eps = 1e-5f + 1e-3f * P.radius_pb2d;
+        launch_photon_leaf_boxes(c->pb_pos.as<float4>(), nph, leaf, P.radius_pb2d, eps, c->pb_leaf_boxes.as<Box>(), s);
+        build_lbvh(c, c->ph_keys_sorted.as<uint32_t>(), nph, leaf, c->pb_leaf_codes, c->pb_nodes, c->pb_parent_int,
+                   c->pb_parent_leaf, c->pb_leaf_boxes, c->pb_node_boxes, c->pb_flags, c->pb_n_leaves);
+        c->build_launches += 3;
+    }
+    // ---- BB1D beams: pieces + LBVH
+    c->n_pieces = 0;
+    c->bm_n_leaves = 0;
+    const int64_t nb = c->n_beams;
+    if (nb > 0 && (P.techniques & UPBP_BB1D)) {
+        const float r = P.radius_bb1d;
+        ensure(c, c->bm_thr4, sizeof(float4) * nb);
+        ensure(c, c->bm_pdf4, sizeof(float4) * nb);
+        ensure(c, c->bm_link, sizeof(int2) * nb);
+        ensure(c, c->bm_radius, sizeof(float) * nb);
+        launch_pack_beams(c->b_thr_in.as<float>(), c->b_flags_in.as<uint32_t>(), c->b_rsp_in.as<float>(),
+                          c->b_rsr_in.as<float>(), c->b_lpw_in.as<float>(), c->b_rsf_in.as<uint32_t>(),
+                          c->b_lv_in.as<int32_t>(), c->b_med_in.as<int32_t>(), nb, r, c->bm_thr4.as<float4>(),
+                          c->bm_pdf4.as<float4>(), c->bm_link.as<int2>(), c->bm_radius.as<float>(), s);
+        const float piece_len = std::max(1e-6f, c->piece_len_r * r);
+        ensure(c, c->bm_counts, sizeof(int32_t) * (nb + 1));
+        ensure(c, c->bm_offsets, sizeof(int32_t) * (nb + 1));
+        launch_piece_counts(c->b_len.as<float>(), nb, piece_len, c->bm_counts.as<int32_t>(), s);
+        ck(c, cudaMemsetAsync(c->bm_counts.as<int32_t>() + nb, 0, sizeof(int32_t), s), "memset");
+        size_t b = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, b, c->bm_counts.as<int32_t>(), c->bm_offsets.as<int32_t>(),
+                                      (int)(nb + 1), s);
+        ensure(c, c->cub_tmp, b);
+        ck(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, b, c->bm_counts.as<int32_t>(), c->bm_offsets.as<int32_t>(),
+                                            (int)(nb + 1), s),
+           "ExclusiveSum");
+        int32_t total = 0;
+        ck(c, cudaMemcpyAsync(&total, c->bm_offsets.as<int32_t>() + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+           "copy pieces");
+        ck(c, cudaStreamSynchronize(s), "sync");
+        const int np = total;
+        c->n_pieces = np;
+        ensure(c, c->pc_a, sizeof(float4) * np);
+        ensure(c, c->pc_b, sizeof(float4) * np);
+        ensure(c, c->pc_c, sizeof(float4) * np);
+        ensure(c, c->pc_boxes, sizeof(Box) * np);
+        ensure(c, c->pc_a2, sizeof(float4) * np);
+        ensure(c, c->pc_b2, sizeof(float4) * np);
+        ensure(c, c->pc_c2, sizeof(float4) * np);
+        ensure(c, c->pc_boxes2, sizeof(Box) * np);
+        ensure(c, c->pc_codes, sizeof(uint32_t) * np);
+        ensure(c, c->pc_codes_sorted, sizeof(uint32_t) * np);
+        ensure(c, c->pc_perm, sizeof(int32_t) * np);
+        ensure(c, c->pc_perm_sorted, sizeof(int32_t) * np);
+        ensure(c, c->bbox_pc, sizeof(float) * 6);
+        const float eps = 1e-5f + 1e-3f * r;
+        launch_emit_pieces(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(),
+                           c->b_med_in.as<int32_t>(), nb, c->bm_offsets.as<int32_t>(), piece_len, r, eps,
+                           c->pc_a.as<float4>(), c->pc_b.as<float4>(), c->pc_c.as<float4>(), c->pc_boxes.as<Box>(), s);
+        const int pblocks = std::max(1, std::min(1024, (np + 255) / 256));
+        float* partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
+        ensure(c, c->bbox_partial, sizeof(int32_t) * 8 + sizeof(float) * 6 * 1024);
+        partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
+        launch_bbox_boxes_partial(c->pc_boxes.as<Box>(), np, partial, pblocks, s);
+        launch_bbox_final(partial, pblocks, c->bbox_pc.as<float>(), s);
+        launch_morton_boxes(c->pc_boxes.as<Box>(), np, c->bbox_pc.as<float>(), c->pc_codes.as<uint32_t>(), s);
+        k_iota<<<(np + 255) / 256, 256, 0, s>>>(c->pc_perm.as<int32_t>(), np);
+        sort_pairs(c, c->pc_codes.as<uint32_t>(), c->pc_codes_sorted.as<uint32_t>(), c->pc_perm.as<int32_t>(),
+                   c->pc_perm_sorted.as<int32_t>(), np, 30);
+        launch_permute_pieces(c->pc_perm_sorted.as<int32_t>(), np, c->pc_a.as<float4>(), c->pc_b.as<float4>(),
+                              c->pc_c.as<float4>(), c->pc_boxes.as<Box>(), c->pc_a2.as<float4>(),
+                              c->pc_b2.as<float4>(), c->pc_c2.as<float4>(), c->pc_boxes2.as<Box>(), s);
+        const int leaf = std::max(1, c->bb1d_leaf);
+        const int nl = (np + leaf - 1) / leaf;
+        ensure(c, c->bm_leaf_boxes, sizeof(Box) * nl);
+        launch_box_leaf_boxes(c->pc_boxes2.as<Box>(), np, leaf, c->bm_leaf_boxes.as<Box>(), s);
+        build_lbvh(c, c->pc_codes_sorted.as<uint32_t>(), np, leaf, c->bm_leaf_codes, c->bm_nodes, c->bm_parent_int,
+                   c->bm_parent_leaf, c->bm_leaf_boxes, c->bm_node_boxes, c->bm_flagsbuf, c->bm_n_leaves);
+        c->build_launches += 10;
+    }
+    ck(c, cudaEventRecord(c->ev[1], s), "event");
+    ck(c, cudaGetLastError(), "build launch");
+    c->built = true;
+}
+
+GatherConsts make_consts(upbp_ctx* c)
+{
+    GatherConsts K{};
+    K.P = c->P;
+    K.n_media = (int)c->media.size();
+    for (int i = 0; i < K.n_media; ++i) K.media[i] = c->media[i];
+    K.has_bb1d_beams = (c->P.techniques & UPBP_BB1D) && c->n_beams > 0;
+    K.eps = 1e-4f;
+    return K;
+}
+
+LightSoA light_soa(upbp_ctx* c)
+{
+    LightSoA L{};
+    L.pos = c->lv_pos4.as<float4>();
+    L.dir = c->lv_dir4.as<float4>();
+    L.thr = c->lv_thr4.as<float4>();
+    L.info = c->lv_info4.as<int4>();
+    L.mis = c->lv_mis.as<upbp_mis>();
+    L.path_ends = c->path_ends.as<int32_t>();
+    L.n = c->n_lv;
+    return L;
+}
+
+SegQueriesDev seg_dev(upbp_ctx* c)
+{
+    SegQueriesDev Q{};
+    Q.origin = c->sq_origin.as<float>();
+    Q.direction = c->sq_dir.as<float>();
+    Q.seg_begin = c->sq_seg_begin.as<int32_t>();
+    Q.seg_count = c->sq_seg_count.as<int32_t>();
+    Q.flags = c->sq_flags.as<uint32_t>();
+    Q.path_length = c->sq_plen.as<int32_t>();
+    Q.last_pdf_w_inv = c->sq_lpw.as<float>();
+    Q.throughput = c->sq_thr.as<float>();
+    Q.pixel = c->sq_pixel.as<int32_t>();
+    Q.cam_mis_begin = c->sq_cam_begin.as<int64_t>();
+    Q.seg_dist_min = c->seg_dmin.as<float>();
+    Q.seg_dist_max = c->seg_dmax.as<float>();
+    Q.seg_pdf = c->seg_pdf.as<float>();
+    Q.seg_rev_pdf = c->seg_rev.as<float>();
+    Q.seg_attenuation = c->seg_att.as<float>();
+    Q.seg_medium = c->seg_med.as<int32_t>();
+    Q.n = c->n_sq;
+    return Q;
+}
+
+void do_evaluate(upbp_ctx* c)
+{
+    if (!c->built) fail(c, UPBP_ERR_NOT_BUILT, "upbp_build was not called");
+    cudaStream_t s = c->stream;
+    c->eval_launches = 0;
+    const GatherConsts K = make_consts(c);
+    const LightSoA L = light_soa(c);
+    const int64_t nq = c->n_sq, np = c->n_pq;
+    const size_t npix = (size_t)std::max(0, c->P.image_width) * (size_t)std::max(0, c->P.image_height);
+    ensure(c, c->image, sizeof(float) * 3 * std::max<size_t>(npix, 1));
+    ensure(c, c->out_pb2d, sizeof(float) * 3 * std::max<int64_t>(nq, 1));
+    ensure(c, c->out_bb1d, sizeof(float) * 3 * std::max<int64_t>(nq, 1));
+    ensure(c, c->out_pp3d, sizeof(float) * 3 * std::max<int64_t>(np, 1));
+    ensure(c, c->cnt_pb2d, sizeof(uint32_t) * std::max<int64_t>(nq, 1));
+    ensure(c, c->cnt_bb1d, sizeof(uint32_t) * std::max<int64_t>(nq, 1));
+    ensure(c, c->cnt_pp3d, sizeof(uint32_t) * std::max<int64_t>(np, 1));
+    ensure(c, c->hash_pb2d, sizeof(uint64_t) * std::max<int64_t>(nq, 1));
+    ensure(c, c->hash_bb1d, sizeof(uint64_t) * std::max<int64_t>(nq, 1));
+    ensure(c, c->hash_pp3d, sizeof(uint64_t) * std::max<int64_t>(np, 1));
+    ensure(c, c->tested, sizeof(unsigned long long) * 4);
+    ck(c, cudaMemsetAsync(c->tested.p, 0, sizeof(unsigned long long) * 4, s), "memset");
+    const upbp_mis* cam = c->cam_mis.as<upbp_mis>();
+    float* img = npix ? c->image.as<float>() : nullptr;
+    unsigned long long* tested = c->tested.as<unsigned long long>();
+
+    ck(c, cudaEventRecord(c->ev[2], s), "event");
+    if (np > 0) {
+        HashGridDev G{};
+        G.pos = c->hg_pos.as<float4>();
+        G.start = c->hg_start.as<int32_t>();
+        G.end = c->hg_end.as<int32_t>();
+        for (int k = 0; k < 3; ++k) {
+            G.bbox_min[k] = c->hg_bbox[k];
+            G.bbox_max[k] = c->hg_bbox[3 + k];
+        }
+        G.inv_cell = c->hg_inv_cell;
+        G.r2 = c->P.radius_pp3d * c->P.radius_pp3d;
+        G.cells = std::max(1, c->P.hash_cells);
+        G.n = (c->P.techniques & UPBP_PP3D) ? c->n_ph : 0;
+        PointQueriesDev Q{};
+        Q.position = c->pq_pos.as<float>();
+        Q.dir_fix = c->pq_dir.as<float>();
+        Q.medium_id = c->pq_med.as<int32_t>();
+        Q.path_length = c->pq_plen.as<int32_t>();
+        Q.throughput = c->pq_thr.as<float>();
+        Q.pixel = c->pq_pixel.as<int32_t>();
+        Q.cam_mis_begin = c->pq_cam_begin.as<int64_t>();
+        Q.n = np;
+        Outputs O{c->out_pp3d.as<float>(), img, c->cnt_pp3d.as<uint32_t>(),
+                  c->hash_pp3d.as<unsigned long long>(), tested + 2};
+        launch_gather_pp3d(K, L, G, Q, cam, O, c->block, s);
+        c->eval_launches += 1;
+    }
+    ck(c, cudaEventRecord(c->ev[3], s), "event");
+    const SegQueriesDev Q = seg_dev(c);
+    if (nq > 0) {
+        PhotonBVH B{};
+        B.pos = c->pb_pos.as<float4>();
+        B.nodes = c->pb_nodes.as<BNode>();
+        B.n = (c->P.techniques & UPBP_PB2D) ? c->n_ph : 0;
+        B.leaf = std::max(1, c->pb2d_leaf);
+        B.n_leaves = c->pb_n_leaves;
+        Outputs O{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
+                  c->hash_pb2d.as<unsigned long long>(), tested + 0};
+        launch_gather_pb2d(K, L, B, Q, cam, O, c->block, s);
+        c->eval_launches += 1;
+    }
+    ck(c, cudaEventRecord(c->ev[4], s), "event");
+    if (nq > 0) {
+        BeamBVH B{};
+        B.pa = c->pc_a2.as<float4>();
+        B.pb = c->pc_b2.as<float4>();
+        B.pc = c->pc_c2.as<float4>();
+        B.nodes = c->bm_nodes.as<BNode>();
+        B.n = c->n_pieces;
+        B.leaf = std::max(1, c->bb1d_leaf);
+        B.n_leaves = c->bm_n_leaves;
+        BeamSoA S{};
+        S.thr = c->bm_thr4.as<float4>();
+        S.pdf = c->bm_pdf4.as<float4>();
+        S.link = c->bm_link.as<int2>();
+        S.radius = c->bm_radius.as<float>();
+        S.n = c->n_beams;
+        Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
+                  c->hash_bb1d.as<unsigned long long>(), tested + 1};
+        launch_gather_bb1d(K, L, B, S, Q, cam, O, c->block, s);
+        c->eval_launches += 1;
+    }
+    ck(c, cudaEventRecord(c->ev[5], s), "event");
+    ck(c, cudaGetLastError(), "gather launch");
+}
+
+template <class F>
+int guarded(upbp_ctx* c, F&& f)
+{
+    if (!c) return UPBP_ERR_INVALID_ARG;
+    try {
+        ck(c, cudaSetDevice(c->device), "cudaSetDevice");
+        f();
+        return UPBP_OK;
+    } catch (const Error& e) {
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        c->err = "host allocation failed";
+        return UPBP_ERR_OUT_OF_MEMORY;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int upbp_ctx_create(upbp_ctx** out, int device)
+{
+    if (!out) return UPBP_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return UPBP_ERR_CUDA;
+    }
+    upbp_ctx* c = new (std::nothrow) upbp_ctx();
+    if (!c) return UPBP_ERR_OUT_OF_MEMORY;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return UPBP_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    for (auto& e : c->ev) cudaEventCreate(&e);
+    *out = c;
+    return UPBP_OK;
+}
+
+int upbp_ctx_destroy(upbp_ctx* c)
+{
+    if (!c) return UPBP_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DBuf* all[] = {&c->lv_pos_in, &c->lv_thr_in, &c->lv_dir_in, &c->lv_cont_in, &c->lv_pidx_in, &c->lv_plen_in,
+                   &c->lv_med_in, &c->lv_flags_in, &c->lv_mis, &c->path_ends, &c->b_origin, &c->b_dir, &c->b_len,
+                   &c->b_thr_in, &c->b_flags_in, &c->b_rsp_in, &c->b_rsr_in, &c->b_rsf_in, &c->b_lpw_in,
+                   &c->b_med_in, &c->b_lv_in, &c->cam_mis, &c->sq_origin, &c->sq_dir, &c->sq_seg_begin,
+                   &c->sq_seg_count, &c->sq_flags, &c->sq_plen, &c->sq_lpw, &c->sq_thr, &c->sq_pixel,
+                   &c->sq_cam_begin, &c->seg_dmin, &c->seg_dmax, &c->seg_pdf, &c->seg_rev, &c->seg_att, &c->seg_med,
+                   &c->pq_pos, &c->pq_dir, &c->pq_med, &c->pq_plen, &c->pq_thr, &c->pq_pixel, &c->pq_cam_begin,
+                   &c->lv_pos4, &c->lv_dir4, &c->lv_thr4, &c->lv_info4, &c->lv_inmed, &c->ph_lv, &c->ph_lv_sorted,
+                   &c->ph_keys, &c->ph_keys_sorted, &c->bbox_partial, &c->bbox_ph, &c->hg_start, &c->hg_end,
+                   &c->hg_pos, &c->pb_pos, &c->pb_leaf_codes, &c->pb_nodes, &c->pb_parent_int, &c->pb_parent_leaf,
+                   &c->pb_leaf_boxes, &c->pb_node_boxes, &c->pb_flags, &c->bm_thr4, &c->bm_pdf4, &c->bm_link,
+                   &c->bm_radius, &c->bm_counts, &c->bm_offsets, &c->pc_a, &c->pc_b, &c->pc_c, &c->pc_boxes,
+                   &c->pc_a2, &c->pc_b2, &c->pc_c2, &c->pc_boxes2, &c->pc_codes, &c->pc_codes_sorted, &c->pc_perm,
+                   &c->pc_perm_sorted, &c->bbox_pc, &c->bm_leaf_codes, &c->bm_nodes, &c->bm_parent_int,
+                   &c->bm_parent_leaf, &c->bm_leaf_boxes, &c->bm_node_boxes, &c->bm_flagsbuf, &c->cub_tmp,
+                   &c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->image, &c->cnt_pb2d, &c->cnt_bb1d, &c->cnt_pp3d,
+                   &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested};
+    for (DBuf* b : all) free_buf(*b);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return UPBP_OK;
+}
+
+const char* upbp_last_error(const upbp_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int upbp_set_mode(upbp_ctx* c, int mode)
+{
+    return guarded(c, [&] {
+        if (mode != UPBP_MODE_PLAIN && mode != UPBP_MODE_MIXED) fail(c, UPBP_ERR_INVALID_ARG, "unknown mode %d", mode);
+        c->mode = mode;
+    });
+}
+
+int upbp_set_tuning(upbp_ctx* c, int pb2d_leaf, int bb1d_leaf, int block_threads)
+{
+    return guarded(c, [&] {
+        if (pb2d_leaf < 1 || pb2d_leaf > 64 || bb1d_leaf < 1 || bb1d_leaf > 64)
+            fail(c, UPBP_ERR_INVALID_ARG, "leaf sizes must be in [1, 64]");
+        if (block_threads < 32 || block_threads > 256 || (block_threads % 32))
+            fail(c, UPBP_ERR_INVALID_ARG, "block_threads must be a multiple of 32 in [32, 256]");
+        c->pb2d_leaf = pb2d_leaf;
+        c->bb1d_leaf = bb1d_leaf;
+        c->block = block_threads;
+        c->built = false;
+    });
+}
+
+int upbp_set_stream(upbp_ctx* c, void* stream)
+{
+    return guarded(c, [&] { c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream; });
+}
+
+int upbp_set_media(upbp_ctx* c, const upbp_medium* media, int32_t n)
+{
+    return guarded(c, [&] {
+        if (!media || n <= 0 || n > UPBP_MAX_MEDIA) fail(c, UPBP_ERR_INVALID_ARG, "n_media must be in [1, %d]", UPBP_MAX_MEDIA);
+        c->media.clear();
+        for (int i = 0; i < n; ++i) c->media.push_back(derive_medium(media[i]));
+    });
+}
+
+int upbp_set_params(upbp_ctx* c, const upbp_params* p)
+{
+    return guarded(c, [&] {
+        if (!p) fail(c, UPBP_ERR_INVALID_ARG, "params is NULL");
+        if (p->max_path_length + 1 > UPBP_MAX_CAM) fail(c, UPBP_ERR_INVALID_ARG, "max_path_length too large");
+        if (!(p->radius_pp3d > 0) || !(p->radius_pb2d > 0) || !(p->radius_bb1d > 0))
+            fail(c, UPBP_ERR_INVALID_ARG, "radii must be positive");
+        if ((p->query_beam_type != UPBP_SHORT_BEAM && p->query_beam_type != UPBP_LONG_BEAM) ||
+            (p->photon_beam_type != UPBP_SHORT_BEAM && p->photon_beam_type != UPBP_LONG_BEAM))
+            fail(c, UPBP_ERR_INVALID_ARG, "beam types must be SHORT_BEAM or LONG_BEAM");
+        if (p->image_width < 0 || p->image_height < 0) fail(c, UPBP_ERR_INVALID_ARG, "negative image size");
+        c->P = *p;
+        c->have_params = true;
+        c->built = false;
+    });
+}
+
+int upbp_set_light_vertices(upbp_ctx* c, const upbp_light_vertices* lv)
+{
+    return guarded(c, [&] {
+        if (!lv || lv->n < 0 || lv->n > (int64_t)INT32_MAX || lv->n_paths < 0)
+            fail(c, UPBP_ERR_INVALID_ARG, "bad light vertex count");
+        const int64_t n = lv->n;
+        upload(c, c->lv_pos_in, lv->position, 3 * n, "position");
+        upload(c, c->lv_thr_in, lv->throughput, 3 * n, "throughput");
+        upload(c, c->lv_dir_in, lv->dir_fix, 3 * n, "dir_fix");
+        upload(c, c->lv_cont_in, lv->cont_prob, n, "cont_prob");
+        upload(c, c->lv_pidx_in, lv->path_idx, n, "path_idx");
+        upload(c, c->lv_plen_in, lv->path_length, n, "path_length");
+        upload(c, c->lv_med_in, lv->medium_id, n, "medium_id");
+        upload(c, c->lv_flags_in, lv->flags, n, "flags");
+        upload(c, c->lv_mis, lv->mis, n, "mis");
+        upload(c, c->path_ends, lv->path_ends, lv->n_paths, "path_ends");
+        c->n_lv = n;
+        c->n_paths = lv->n_paths;
+        c->built = false;
+    });
+}
+
+int upbp_set_beams(upbp_ctx* c, const upbp_beams* b)
+{
+    return guarded(c, [&] {
+        if (!b || b->n < 0 || b->n > (int64_t)(1 << 28)) fail(c, UPBP_ERR_INVALID_ARG, "bad beam count");
+        const int64_t n = b->n;
+        upload(c, c->b_origin, b->origin, 3 * n, "beam origin");
+        upload(c, c->b_dir, b->direction, 3 * n, "beam direction");
+        upload(c, c->b_len, b->length, n, "beam length");
+        upload(c, c->b_thr_in, b->throughput, 3 * n, "beam throughput");
+        upload(c, c->b_flags_in, b->flags, n, "beam flags");
+        upload(c, c->b_rsp_in, b->ray_sample_pdf, n, "beam ray_sample_pdf");
+        upload(c, c->b_rsr_in, b->ray_sample_rev_pdf, n, "beam ray_sample_rev_pdf");
+        upload(c, c->b_rsf_in, b->ray_sampling_flags, n, "beam ray_sampling_flags");
+        upload(c, c->b_lpw_in, b->last_pdf_w_inv, n, "beam last_pdf_w_inv");
+        upload(c, c->b_med_in, b->medium_id, n, "beam medium_id");
+        upload(c, c->b_lv_in, b->light_vertex, n, "beam light_vertex");
+        c->n_beams = n;
+        c->built = false;
+    });
+}
+
+int upbp_build(upbp_ctx* c)
+{
+    return guarded(c, [&] { do_build(c); });
+}
+
+int upbp_set_camera_mis(upbp_ctx* c, const upbp_mis* rec, int64_t n)
+{
+    return guarded(c, [&] {
+        if (n < 0) fail(c, UPBP_ERR_INVALID_ARG, "negative camera record count");
+        upload(c, c->cam_mis, rec, n, "camera mis");
+        c->n_cam = n;
+    });
+}
+
+int upbp_set_segment_queries(upbp_ctx* c, const upbp_segment_queries* q)
+{
+    return guarded(c, [&] {
+        if (!q || q->n < 0 || q->n_segments < 0) fail(c, UPBP_ERR_INVALID_ARG, "bad segment query counts");
+        const int64_t n = q->n, s = q->n_segments;
+        upload(c, c->sq_origin, q->origin, 3 * n, "origin");
+        upload(c, c->sq_dir, q->direction, 3 * n, "direction");
+        upload(c, c->sq_seg_begin, q->seg_begin, n, "seg_begin");
+        upload(c, c->sq_seg_count, q->seg_count, n, "seg_count");
+        upload(c, c->sq_flags, q->flags, n, "flags");
+        upload(c, c->sq_plen, q->path_length, n, "path_length");
+        upload(c, c->sq_lpw, q->last_pdf_w_inv, n, "last_pdf_w_inv");
+        upload(c, c->sq_thr, q->throughput, 3 * n, "throughput");
+        upload(c, c->sq_pixel, q->pixel, n, "pixel");
+        upload(c, c->sq_cam_begin, q->cam_mis_begin, n, "cam_mis_begin");
+        upload(c, c->seg_dmin, q->seg_dist_min, s, "seg_dist_min");
+        upload(c, c->seg_dmax, q->seg_dist_max, s, "seg_dist_max");
+        upload(c, c->seg_pdf, q->seg_pdf, s, "seg_pdf");
+        upload(c, c->seg_rev, q->seg_rev_pdf, s, "seg_rev_pdf");
+        upload(c, c->seg_att, q->seg_attenuation, 3 * s, "seg_attenuation");
+        upload(c, c->seg_med, q->seg_medium, s, "seg_medium");
+        c->n_sq = n;
+        c->n_seg = s;
+    });
+}
+
+int upbp_set_point_queries(upbp_ctx* c, const upbp_point_queries* q)
+{
+    return guarded(c, [&] {
+        if (!q || q->n < 0) fail(c, UPBP_ERR_INVALID_ARG, "bad point query count");
+        const int64_t n = q->n;
+        upload(c, c->pq_pos, q->position, 3 * n, "position");
+        upload(c, c->pq_dir, q->dir_fix, 3 * n, "dir_fix");
+        upload(c, c->pq_med, q->medium_id, n, "medium_id");
+        upload(c, c->pq_plen, q->path_length, n, "path_length");
+        upload(c, c->pq_thr, q->throughput, 3 * n, "throughput");
+        upload(c, c->pq_pixel, q->pixel, n, "pixel");
+        upload(c, c->pq_cam_begin, q->cam_mis_begin, n, "cam_mis_begin");
+        c->n_pq = n;
+    });
+}
+
+int upbp_evaluate(upbp_ctx* c)
+{
+    return guarded(c, [&] { do_evaluate(c); });
+}
+
+int upbp_read_segment_results(upbp_ctx* c, float* pb2d, float* bb1d)
+{
+    return guarded(c, [&] {
+        const size_t bytes = sizeof(float) * 3 * (size_t)c->n_sq;
+        if (pb2d && bytes) ck(c, cudaMemcpyAsync(pb2d, c->out_pb2d.p, bytes, cudaMemcpyDefault, c->stream), "read");
+        if (bb1d && bytes) ck(c, cudaMemcpyAsync(bb1d, c->out_bb1d.p, bytes, cudaMemcpyDefault, c->stream), "read");
+        ck(c, cudaStreamSynchronize(c->stream), "sync");
+    });
+}
+
+int upbp_read_point_results(upbp_ctx* c, float* pp3d)
+{
+    return guarded(c, [&] {
+        const size_t bytes = sizeof(float) * 3 * (size_t)c->n_pq;
+        if (pp3d && bytes) ck(c, cudaMemcpyAsync(pp3d, c->out_pp3d.p, bytes, cudaMemcpyDefault, c->stream), "read");
+        ck(c, cudaStreamSynchronize(c->stream), "sync");
+    });
+}
+
+int upbp_read_query_stats(upbp_ctx* c, const upbp_query_stats* st)
+{
+    return guarded(c, [&] {
+        if (!st) fail(c, UPBP_ERR_INVALID_ARG, "stats is NULL");
+        const size_t nq = (size_t)c->n_sq, np = (size_t)c->n_pq;
+        auto rd = [&](void* dst, const DBuf& src, size_t bytes) {
+            if (dst && bytes) ck(c, cudaMemcpyAsync(dst, src.p, bytes, cudaMemcpyDefault, c->stream), "read stats");
+        };
+        rd(st->count_pb2d, c->cnt_pb2d, 4 * nq);
+        rd(st->hash_pb2d, c->hash_pb2d, 8 * nq);
+        rd(st->count_bb1d, c->cnt_bb1d, 4 * nq);
+        rd(st->hash_bb1d, c->hash_bb1d, 8 * nq);
+        rd(st->count_pp3d, c->cnt_pp3d, 4 * np);
+        rd(st->hash_pp3d, c->hash_pp3d, 8 * np);
+        ck(c, cudaStreamSynchronize(c->stream), "sync");
+    });
+}
+
+int upbp_clear_image(upbp_ctx* c)
+{
+    return guarded(c, [&] {
+        const size_t npix = (size_t)std::max(0, c->P.image_width) * (size_t)std::max(0, c->P.image_height);
+        ensure(c, c->image, sizeof(float) * 3 * std::max<size_t>(npix, 1));
+        ck(c, cudaMemsetAsync(c->image.p, 0, sizeof(float) * 3 * npix, c->stream), "memset image");
+    });
+}
+
+int upbp_read_image(upbp_ctx* c, float* rgb)
+{
+    return guarded(c, [&] {
+        if (!rgb) fail(c, UPBP_ERR_INVALID_ARG, "rgb is NULL");
+        const size_t npix = (size_t)std::max(0, c->P.image_width) * (size_t)std::max(0, c->P.image_height);
+        if (npix) ck(c, cudaMemcpyAsync(rgb, c->image.p, sizeof(float) * 3 * npix, cudaMemcpyDefault, c->stream), "read image");
+        ck(c, cudaStreamSynchronize(c->stream), "sync");
+    });
+}
+
+int upbp_last_launch_count(const upbp_ctx* c, int* b, int* e)
+{
+    if (!c) return UPBP_ERR_INVALID_ARG;
+    if (b) *b = c->build_launches;
+    if (e) *e = c->eval_launches;
+    return UPBP_OK;
+}
+
+int upbp_last_timings(const upbp_ctx* cc, float* build_ms, float* pp3d_ms, float* pb2d_ms, float* bb1d_ms)
+{
+    upbp_ctx* c = const_cast<upbp_ctx*>(cc);
+    return guarded(c, [&] {
+        ck(c, cudaStreamSynchronize(c->stream), "sync");
+        float v = 0.f;
+        if (build_ms) { cudaEventElapsedTime(&v, c->ev[0], c->ev[1]); *build_ms = v; }
+        if (pp3d_ms) { cudaEventElapsedTime(&v, c->ev[2], c->ev[3]); *pp3d_ms = v; }
+        if (pb2d_ms) { cudaEventElapsedTime(&v, c->ev[3], c->ev[4]); *pb2d_ms = v; }
+        if (bb1d_ms) { cudaEventElapsedTime(&v, c->ev[4], c->ev[5]); *bb1d_ms = v; }
+        cudaGetLastError();
+    });
+}
+
+int upbp_destroy_structures(upbp_ctx* c)
+{
+    return guarded(c, [&] {
+        c->built = false;
+        c->n_ph = 0;
+        c->pb_n_leaves = 0;
+        c->n_pieces = 0;
+        c->bm_n_leaves = 0;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,549 @@
+// Gather kernels of the B200 estimator stage: one thread per recorded query.
+//
+//  * PB2D  : EmbreeBre::evalBre + breIntersectFuncHomogeneous2 (Bre/Bre.cxx:293-464, 812-964)
+//  * BB1D  : PhotonBeamsEvaluator::evalBeamBeamEstimate + PhotonBeam::accumulate2
+//            (Beams/PhBeams.cxx:177-324, Beams/PhotonBeam.hxx:386-607)
+//  * PP3D  : HashGrid::Process + UPBP::RangeQuery::Process (Misc/HashGrid.hxx:129-188,
+//            Renderers/UPBP.hxx:86-133)
+// Candidate predicates use the reference operation order (upbp_device.cuh); the MIS weights
+// walk the stored camera snapshot and light subpath exactly as Path/PathWeight.hxx does.
+#include <cfloat>
+#include <cstdint>
+
+#include "upbp_kernels.cuh"
+
+namespace upbp {
+
+namespace {
+
+__device__ __forceinline__ void stage_media(const GatherConsts& K, DMedium* s)
+{
+    for (int i = threadIdx.x; i < K.n_media; i += blockDim.x) s[i] = K.media[i];
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool slab(float lx, float ly, float lz, float hx, float hy, float hz, V3 o, V3 inv,
+                                     float tmin, float tmax)
+{
+    const float tx0 = (lx - o.x) * inv.x, tx1 = (hx - o.x) * inv.x;
+    const float ty0 = (ly - o.y) * inv.y, ty1 = (hy - o.y) * inv.y;
+    const float tz0 = (lz - o.z) * inv.z, tz1 = (hz - o.z) * inv.z;
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    return tn <= tf;
+}
+
+__device__ __forceinline__ float safe_inv(float d) { return 1.f / (d == 0.f ? copysignf(1e-30f, d) : d); }
+
+// Stack traversal of a BVH2 with child boxes; calls leaf(k) for every leaf whose box the
+// segment [tmin, tmax] overlaps.  Returns false on stack overflow (reported through the
+// status word; the 30-bit Morton build never gets that deep).
+template <class LeafFn>
+__device__ __forceinline__ bool traverse(const BNode* __restrict__ nodes, int n_leaves, V3 o, V3 inv, float tmin,
+                                         float tmax, LeafFn&& leaf)
+{
+    if (n_leaves <= 0) return true;
+    if (n_leaves == 1) {
+        leaf(0);
+        return true;
+    }
+    constexpr int kStack = 96;
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int node = stack[--sp];
+        const float4 a = __ldg(&nodes[node].a);
+        const float4 b = __ldg(&nodes[node].b);
+        const float4 c = __ldg(&nodes[node].c);
+        const int4 d = __ldg(&nodes[node].d);
+        const bool hl = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, tmin, tmax);
+        const bool hr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv, tmin, tmax);
+        if (hl) {
+            if (d.x < 0) leaf(~d.x);
+            else if (sp < kStack) stack[sp++] = d.x;
+            else return false;
+        }
+        if (hr) {
+            if (d.y < 0) leaf(~d.y);
+            else if (sp < kStack) stack[sp++] = d.y;
+            else return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void splat(float* image, int px, Rgb v)
+{
+    if (!image || px < 0) return;
+    atomicAdd(&image[3 * px + 0], v.r);
+    atomicAdd(&image[3 * px + 1], v.g);
+    atomicAdd(&image[3 * px + 2], v.b);
+}
+
+// Camera MisData as the reference array holds it during an estimator call at path length L:
+// entries < L-1 from the snapshot, entry L-1 from the snapshot with mRaySampleRevPdfInv set by
+// the estimator, entry L written by the estimator for the candidate.
+struct CamView {
+    const upbp_mis* snap;
+    int L;
+    const upbp_mis* cand;
+    float prev_ray_rev_inv;
+    __device__ upbp_mis operator()(int k) const
+    {
+        if (k == L) return *cand;
+        upbp_mis m = load_mis(snap + k);
+        if (k == L - 1) m.ray_sample_rev_pdf_inv = prev_ray_rev_inv;
+        return m;
+    }
+};
+
+struct CamSnap {
+    const upbp_mis* snap;
+    __device__ upbp_mis operator()(int k) const { return load_mis(snap + k); }
+};
+
+struct LightView {
+    const upbp_mis* mis;
+    int override_idx;
+    float override_ray_rev_inv;
+    __device__ upbp_mis operator()(int k) const
+    {
+        upbp_mis m = load_mis(mis + k);
+        if (k == override_idx) m.ray_sample_rev_pdf_inv = override_ray_rev_inv;
+        return m;
+    }
+};
+
+// Per-segment state that evalBre / evalBeamBeamEstimate hand to the callbacks through
+// AdditionalRayDataForMis (Bre.cxx:839-850, PhBeams.cxx:198-210).
+struct SegCtx {
+    V3 o, d;
+    float dmin, dmax;
+    float rs_pdf, rs_rev_pdf;  // mRaySamplePdf / mRaySampleRevPdf accumulated over earlier segments
+    uint32_t rsf;              // mRaySamplingFlags
+    int L;
+    float last_pdf_w_inv;
+    uint32_t ray_flags;        // beamType | estimatorTechniques
+    const upbp_mis* cam;
+};
+
+__device__ __forceinline__ void fill_cand(upbp_mis& c, const upbp_params& P, float pdf_a_inv, float rsp_inv,
+                                          float ratio, float sel_pdf, uint32_t flags)
+{
+    c.pdf_a_inv = pdf_a_inv;
+    c.rev_pdf_a = 1.f;
+    c.rev_pdf_a_without_bsdf = 1.f;
+    c.ray_sample_pdf_inv = rsp_inv;
+    c.ray_sample_rev_pdf_inv = 1.f;
+    c.ray_sample_pdfs_ratio = ratio;
+    c.ray_sample_rev_pdfs_ratio = 0.f;
+    c.sin_theta = 0.f;
+    c.cos_theta_out = 0.f;
+    c.surf_factor = 0.f;
+    c.pp3d_factor = P.mis_factor_pp3d;
+    c.pb2d_factor = P.mis_factor_pb2d;
+    c.bb1d_factor = P.mis_factor_bb1d;
+    c.bb1d_beam_selection_pdf = sel_pdf;
+    c.flags = flags;
+}
+
+// ----------------------------------------------------------------- PB2D contribution
+// breIntersectFuncHomogeneous2 after testIntersectionBre accepted photon `lv` at (t, d2).
+__device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const LightSoA& Lv, const SegCtx& s, int lv,
+                            float t, float d2)
+{
+    const upbp_params& P = K.P;
+    const int4 info = __ldg(&Lv.info[lv]);
+    const int pl = info.y;
+    if ((uint32_t)(pl + s.L) > P.max_path_length || (uint32_t)(pl + s.L) < P.min_path_length) return rgb(0.f);
+    if (s.L == 1 && t < P.min_dist_to_med) return rgb(0.f);
+    Rgb att = eval_att(m, t - s.dmin);
+    const float pdf = comp(att, m.min_idx);
+    if (s.ray_flags & UPBP_SHORT_BEAM) att = att / pdf;
+    float rsp = m.min_st * pdf;
+    float rsr = (s.rsf & UPBP_ORIGIN_IN_MEDIUM) ? rsp : pdf;
+    const float ratio = 1.0f / m.min_st;
+    if (!rgb_positive(att)) return rgb(0.f);
+    rsp *= s.rs_pdf;
+    rsr *= s.rs_rev_pdf;
+    const float4 ld = __ldg(&Lv.dir[lv]);
+    float sinT;
+    const float phase = hg_pdf(neg3(s.d), v3(ld.x, ld.y, ld.z), m.g, &sinT);
+    if (phase <= 0.f) return rgb(0.f);
+    const float camDirPdfW = phase * m.cont;
+    const float camRevPdfW = phase * __ldg(&Lv.pos[lv]).w;
+    const float r2 = P.radius_pb2d * P.radius_pb2d;
+    const float kernel = (1.f - d2 / r2) / (r2 * UPBP_PI_F * 0.5f);
+    if (!is_pos(kernel)) return rgb(0.f);
+    const float4 th = __ldg(&Lv.thr[lv]);
+    const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
+    const Rgb unweighted = Rgb{th.x, th.y, th.z} * att * ss * phase * kernel;
+    if (rgb_black_or_neg(unweighted)) return rgb(0.f);
+    const float distSq = t * t;
+    const float rspInv = 1.0f / rsp;
+    upbp_mis cand;
+    fill_cand(cand, P, s.last_pdf_w_inv * distSq * rspInv, rspInv, ratio, K.has_bb1d_beams ? 1.f : 0.f,
+              (m.mfp > P.bb1d_min_mfp) ? UPBP_MIS_IN_MEDIUM_WITH_BEAMS : 0u);
+    const float last = (s.ray_flags & UPBP_SHORT_BEAM) ? (float)(1.0 / (double)(ratio * cand.pb2d_factor))
+                                                       : rsp / cand.pb2d_factor;
+    const upbp_mis lvm = load_mis(Lv.mis + lv);
+    const CamView cam{s.cam, s.L, &cand, 1.0f / rsr};
+    const float wCamera = camera_path_weight(s.L, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
+                                             camRevPdfW * rsr / distSq, P.query_beam_type, P.photon_beam_type,
+                                             s.ray_flags, cam);
+    const LightView lview{Lv.mis, -1, 0.f};
+    const float wLight = light_path_weight(info.x, pl, last, 0.f, 0.f, 0.f, camDirPdfW, UPBP_PB2D, P.query_beam_type,
+                                           P.photon_beam_type, s.ray_flags, Lv.path_ends, lview, nullptr);
+    const float w = 1.f / (wLight + wCamera);
+    return w * unweighted;
+}
+
+// ----------------------------------------------------------------- BB1D contribution
+// PhotonBeam::accumulate2 after testIntersectionBeamBeam and the radius test accepted `beam`.
+__device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const LightSoA& Lv, const BeamSoA& Bs,
+                            const SegCtx& s, int beam, V3 bdir, float radius, float dist, float sinTheta, float t1,
+                            float t2)
+{
+    const upbp_params& P = K.P;
+    const int2 link = __ldg(&Bs.link[beam]);
+    const int lvi = link.x;
+    const int4 info = __ldg(&Lv.info[lvi]);
+    const int pl = info.y;
+    if ((uint32_t)(pl + 1 + s.L) > P.max_path_length || (uint32_t)(pl + 1 + s.L) < P.min_path_length) return rgb(0.f);
+    if (s.L == 1 && t1 < P.min_dist_to_med) return rgb(0.f);
+    const float4 bthr = __ldg(&Bs.thr[beam]);
+    const float4 bpdf = __ldg(&Bs.pdf[beam]);
+    const uint32_t bflags = (uint32_t)__float_as_int(bthr.w);
+    const uint32_t brsf = (uint32_t)__float_as_int(bpdf.w);
+    // query side
+    Rgb att = eval_att(m, t1 - s.dmin);
+    const float pfdQ = comp(att, m.min_idx);
+    if (s.ray_flags & UPBP_SHORT_BEAM) att = att / pfdQ;
+    float rspQ = m.min_st * pfdQ;
+    float rsrQ = (s.rsf & UPBP_ORIGIN_IN_MEDIUM) ? rspQ : pfdQ;
+    const float ratioQ = 1.0f / m.min_st;
+    // beam side
+    const Rgb batt = eval_att(m, t2);
+    att = att * batt;
+    const float pfdB = comp(batt, m.min_idx);
+    if (bflags & UPBP_SHORT_BEAM) att = att / pfdB;
+    float rspB = m.min_st * pfdB;
+    float rsrB = (brsf & UPBP_ORIGIN_IN_MEDIUM) ? rspB : pfdB;
+    const float ratioB = 1.0f / m.min_st;
+    if (!rgb_positive(att)) return rgb(0.f);
+    rspQ *= s.rs_pdf;
+    rsrQ *= s.rs_rev_pdf;
+    rspB *= bpdf.x;
+    rsrB *= bpdf.y;
+    float sinDummy;
+    const float phase = hg_pdf(neg3(s.d), neg3(bdir), m.g, &sinDummy);
+    if (phase <= 0.f) return rgb(0.f);
+    const float bsdfDirPdfW = phase * m.cont;
+    const float bsdfRevPdfW = phase * m.cont;
+    const float sel = 1.0f;  // no beam reduction (sMaxBeamsInCell == 0)
+    const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
+    const Rgb unweighted = ((1.0f / sel) * Rgb{bthr.x, bthr.y, bthr.z} * ss * att * phase *
+                            (1.f - dist * dist / (radius * radius))) * 3.f / (4.f * radius * sinTheta);
+    if (rgb_black_or_neg(unweighted)) return rgb(0.f);
+    const float distSqQ = t1 * t1;
+    const float rspInvQ = 1.0f / rspQ;
+    upbp_mis cand;
+    fill_cand(cand, P, s.last_pdf_w_inv * distSqQ * rspInvQ, rspInvQ, ratioQ, sel, UPBP_MIS_IN_MEDIUM_WITH_BEAMS);
+    const bool finite = (info.z & UPBP_LV_IS_FINITE) != 0;
+    const float distSqB = finite ? t2 * t2 : 1.0f;
+    const float rspInvB = 1.0f / rspB;
+    upbp_mis brec;
+    fill_cand(brec, P, bpdf.z * distSqB * rspInvB, rspInvB, ratioB, sel, UPBP_MIS_IN_MEDIUM_WITH_BEAMS);
+    float sinT = sinTheta;
+    if (s.ray_flags & UPBP_NO_SINE_IN_WEIGHTS) sinT = 1.0f;
+    const float f = cand.bb1d_factor;
+    float last;
+    if (s.ray_flags & UPBP_SHORT_BEAM)
+        last = (bflags & UPBP_SHORT_BEAM) ? (float)(1.0 / (double)(ratioQ * ratioB * f * sel * sinT))
+                                          : rspB / (ratioQ * f * sel * sinT);
+    else
+        last = (bflags & UPBP_SHORT_BEAM) ? rspQ / (ratioB * f * sel * sinT) : rspQ * rspB / (f * sel * sinT);
+    const CamView cam{s.cam, s.L, &cand, 1.0f / rsrQ};
+    const float wCamera = camera_path_weight(s.L, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ,
+                                             P.query_beam_type, P.photon_beam_type, s.ray_flags, cam);
+    const upbp_mis lvm = load_mis(Lv.mis + lvi);
+    const bool onDeltaLight = (lvm.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (lvm.flags & UPBP_MIS_IS_DELTA);
+    const float ntl = onDeltaLight ? 0.f : bsdfDirPdfW * rsrB * fabsf(lvm.cos_theta_out) / distSqB;
+    const LightView lview{Lv.mis, lvi, 1.0f / rsrB};
+    const float wLight = light_path_weight(info.x, pl + 1, last, 0.f, 0.f, 0.f, ntl, UPBP_BB1D, P.query_beam_type,
+                                           P.photon_beam_type, s.ray_flags, Lv.path_ends, lview, &brec);
+    const float w = 1.f / (wLight + wCamera);
+    return w * unweighted;
+}
+
+// ----------------------------------------------------------------- segment loop
+// The per-segment driver of evalBre / evalBeamBeamEstimate (full and lite segments).
+template <class PerSegment>
+__device__ __forceinline__ Rgb segment_loop(const GatherConsts& K, const DMedium* media, const SegQueriesDev& Q,
+                                            int64_t q, SegCtx& s, PerSegment&& per_segment)
+{
+    const uint32_t qf = Q.flags[q];
+    const bool lite = (qf & UPBP_Q_LITE) != 0;
+    const uint32_t qrsf = (qf & UPBP_Q_ORIGIN_IN_MEDIUM) ? UPBP_ORIGIN_IN_MEDIUM : 0u;
+    const uint32_t bt = K.P.query_beam_type;
+    Rgb result = rgb(0.f), attn = rgb(1.f);
+    float rsp = 1.f, rsr = 1.f;
+    const int sb = Q.seg_begin[q], sc = Q.seg_count[q];
+    for (int i = 0; i < sc; ++i) {
+        const int sg = sb + i;
+        const DMedium& m = media[Q.seg_medium[sg]];
+        const float dmin = Q.seg_dist_min[sg], dmax = Q.seg_dist_max[sg];
+        Rgb seg = rgb(0.f);
+        if (m.has_scat) {
+            s.dmin = dmin;
+            s.dmax = dmax;
+            s.rs_pdf = rsp;
+            s.rs_rev_pdf = rsr;
+            s.rsf = UPBP_END_IN_MEDIUM | (i == 0 ? qrsf : 0u);
+            seg = per_segment(m);
+        }
+        result = result + attn * seg;
+        if (lite) {
+            attn = attn * eval_att(m, dmax - dmin);
+            float srev;
+            const float spdf = ray_sample_pdf(m, dmin, dmax, i == 0 ? qrsf : 0u, &srev);
+            if (!rgb_positive(attn)) break;
+            rsp *= spdf;
+            rsr *= srev;
+        } else {
+            const Rgb sa{Q.seg_attenuation[3 * sg], Q.seg_attenuation[3 * sg + 1], Q.seg_attenuation[3 * sg + 2]};
+            attn = attn * (bt == UPBP_SHORT_BEAM ? sa / Q.seg_pdf[sg] : sa);
+            if (!rgb_positive(attn)) break;
+            rsp *= Q.seg_pdf[sg];
+            rsr *= Q.seg_rev_pdf[sg];
+        }
+    }
+    return result;
+}
+
+__device__ __forceinline__ void init_seg_ctx(SegCtx& s, const GatherConsts& K, const SegQueriesDev& Q,
+                                             const upbp_mis* cam, int64_t q)
+{
+    s.o = v3(Q.origin[3 * q], Q.origin[3 * q + 1], Q.origin[3 * q + 2]);
+    s.d = v3(Q.direction[3 * q], Q.direction[3 * q + 1], Q.direction[3 * q + 2]);
+    s.L = Q.path_length[q];
+    s.last_pdf_w_inv = Q.last_pdf_w_inv[q];
+    s.ray_flags = K.P.query_beam_type | K.P.techniques;
+    s.cam = cam + Q.cam_mis_begin[q];
+}
+
+__device__ __forceinline__ void write_out(const Outputs& O, int64_t q, Rgb v, uint32_t cnt, unsigned long long h,
+                                          const SegQueriesDev& Q, float norm)
+{
+    O.rgb[3 * q + 0] = v.r;
+    O.rgb[3 * q + 1] = v.g;
+    O.rgb[3 * q + 2] = v.b;
+    if (O.count) O.count[q] = cnt;
+    if (O.hash) O.hash[q] = h;
+    const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+    splat(O.image, Q.pixel[q], thr * norm * v);
+}
+
+// ----------------------------------------------------------------- kernels
+__global__ void __launch_bounds__(256) k_gather_pb2d(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+                                                     const PhotonBVH B, const SegQueriesDev Q,
+                                                     const upbp_mis* __restrict__ cam, const Outputs O)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    stage_media(K, media);
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= Q.n) return;
+    uint32_t cnt = 0;
+    unsigned long long h = 0, tested = 0;
+    Rgb res = rgb(0.f);
+    if ((Q.flags[q] & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && B.n > 0) {
+        SegCtx s;
+        init_seg_ctx(s, K, Q, cam, q);
+        const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
+        const float r2 = K.P.radius_pb2d * K.P.radius_pb2d;
+        res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
+            Rgb acc = rgb(0.f);
+            traverse(B.nodes, B.n_leaves, s.o, inv, s.dmin - K.eps, s.dmax + K.eps, [&](int leaf) {
+                const int e = min(B.n, (leaf + 1) * B.leaf);
+                for (int i = leaf * B.leaf; i < e; ++i) {
+                    const float4 p = __ldg(&B.pos[i]);
+                    ++tested;
+                    float t, d2;
+                    if (test_bre(s.o, s.d, s.dmin, s.dmax, v3(p.x, p.y, p.z), r2, &t, &d2)) {
+                        const int lv = __float_as_int(p.w);
+                        ++cnt;
+                        h += mix64((unsigned long long)lv);
+                        acc = acc + pb2d_contrib(K, m, Lv, s, lv, t, d2);
+                    }
+                }
+            });
+            return acc;
+        });
+    }
+    write_out(O, q, res, cnt, h, Q, K.P.norm_pb2d);
+    if (O.tested) atomicAdd(O.tested, tested);
+}
+
+__global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+                                                     const BeamBVH B, const BeamSoA Bs, const SegQueriesDev Q,
+                                                     const upbp_mis* __restrict__ cam, const Outputs O)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    stage_media(K, media);
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= Q.n) return;
+    uint32_t cnt = 0;
+    unsigned long long h = 0, tested = 0;
+    Rgb res = rgb(0.f);
+    if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D) && B.n > 0) {
+        SegCtx s;
+        init_seg_ctx(s, K, Q, cam, q);
+        const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
+        res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
+            Rgb acc = rgb(0.f);
+            const int mid = (int)(&m - media);
+            traverse(B.nodes, B.n_leaves, s.o, inv, s.dmin - K.eps, s.dmax + K.eps, [&](int leaf) {
+                const int e = min(B.n, (leaf + 1) * B.leaf);
+                for (int i = leaf * B.leaf; i < e; ++i) {
+                    const float4 pc = __ldg(&B.pc[i]);
+                    if (__float_as_int(pc.w) != mid) continue;  // mMedium == medium (PhotonBeam.hxx:390)
+                    const float4 pa = __ldg(&B.pa[i]);
+                    const float4 pb = __ldg(&B.pb[i]);
+                    ++tested;
+                    float dist, sinT, t1, t2;
+                    if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
+                                        pc.y, &dist, &sinT, &t1, &t2))
+                        continue;
+                    if (!(t2 >= pb.w && t2 < pc.x)) continue;  // this piece owns t2
+                    const int beam = __float_as_int(pc.z);
+                    const float radius = __ldg(&Bs.radius[beam]);
+                    if (radius < dist) continue;  // PhotonBeam.hxx:411-413
+                    ++cnt;
+                    h += mix64((unsigned long long)beam);
+                    acc = acc + bb1d_contrib(K, m, Lv, Bs, s, beam, v3(pb.x, pb.y, pb.z), radius, dist, sinT, t1, t2);
+                }
+            });
+            return acc;
+        });
+    }
+    write_out(O, q, res, cnt, h, Q, K.P.norm_bb1d);
+    if (O.tested) atomicAdd(O.tested, tested);
+}
+
+// HashGrid::GetCellIndex (Misc/HashGrid.hxx:198-206)
+__device__ __forceinline__ uint32_t hash_cell(int x, int y, int z, int cells)
+{
+    const uint32_t ux = (uint32_t)x, uy = (uint32_t)y, uz = (uint32_t)z;
+    return ((ux * 73856093u) ^ (uy * 19349663u) ^ (uz * 83492791u)) % (uint32_t)cells;
+}
+
+__global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+                                                     const HashGridDev G, const PointQueriesDev Q,
+                                                     const upbp_mis* __restrict__ cam, const Outputs O)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    stage_media(K, media);
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= Q.n) return;
+    const upbp_params& P = K.P;
+    uint32_t cnt = 0;
+    unsigned long long h = 0, tested = 0;
+    Rgb res = rgb(0.f);
+    const V3 qp = v3(Q.position[3 * q], Q.position[3 * q + 1], Q.position[3 * q + 2]);
+    bool inside = (P.techniques & UPBP_PP3D) && G.n > 0;
+    V3 dmin{0.f, 0.f, 0.f};
+    if (inside) {
+        dmin = xsub3(qp, v3(G.bbox_min[0], G.bbox_min[1], G.bbox_min[2]));
+        const V3 dmax = xsub3(v3(G.bbox_max[0], G.bbox_max[1], G.bbox_max[2]), qp);
+        inside = !(dmin.x < 0.f || dmin.y < 0.f || dmin.z < 0.f || dmax.x < 0.f || dmax.y < 0.f || dmax.z < 0.f);
+    }
+    if (inside) {
+        const DMedium& m = media[Q.medium_id[q]];
+        const V3 cfix = v3(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
+        const int L = Q.path_length[q];
+        const CamSnap camv{cam + Q.cam_mis_begin[q]};
+        const bool scat_pos = !(m.ss[0] <= 0.f && m.ss[1] <= 0.f && m.ss[2] <= 0.f);
+        const V3 cell = v3(xmul(G.inv_cell, dmin.x), xmul(G.inv_cell, dmin.y), xmul(G.inv_cell, dmin.z));
+        const V3 cf = v3(floorf(cell.x), floorf(cell.y), floorf(cell.z));
+        const int px = (int)cf.x, py = (int)cf.y, pz = (int)cf.z;
+        const int pxo = px + (xsub(cell.x, cf.x) < 0.5f ? -1 : 1);
+        const int pyo = py + (xsub(cell.y, cf.y) < 0.5f ? -1 : 1);
+        const int pzo = pz + (xsub(cell.z, cf.z) < 0.5f ? -1 : 1);
+        for (int j = 0; j < 8; ++j) {
+            const int cx = (j & 4) ? pxo : px, cy = (j & 2) ? pyo : py, cz = (j & 1) ? pzo : pz;
+            const uint32_t c = hash_cell(cx, cy, cz, G.cells);
+            const int e = __ldg(&G.end[c]);
+            for (int i = __ldg(&G.start[c]); i < e; ++i) {
+                const float4 p = __ldg(&G.pos[i]);
+                ++tested;
+                const V3 dd = xsub3(qp, v3(p.x, p.y, p.z));
+                if (!(xdot3(dd, dd) <= G.r2)) continue;
+                const int lv = __float_as_int(p.w);
+                ++cnt;
+                h += mix64((unsigned long long)lv);
+                // UPBP::RangeQuery::Process (UPBP.hxx:86-133)
+                const int4 info = __ldg(&Lv.info[lv]);
+                if (!(info.z & UPBP_LV_CONNECTABLE)) continue;
+                const int pl = info.y;
+                if ((uint32_t)(pl + L) > P.max_path_length || (uint32_t)(pl + L) < P.min_path_length) continue;
+                if (!scat_pos) continue;
+                const float4 ld = __ldg(&Lv.dir[lv]);
+                float sinT;
+                const float phase = hg_pdf(cfix, v3(ld.x, ld.y, ld.z), m.g, &sinT);
+                const Rgb factor = Rgb{m.ss[0], m.ss[1], m.ss[2]} * phase;
+                if (rgb_black_or_neg(factor)) continue;
+                const float dirPdf = phase * m.cont;
+                const float revPdf = phase * __ldg(&Lv.pos[lv]).w;
+                const upbp_mis lvm = load_mis(Lv.mis + lv);
+                const float mwfInv = 1.0f / lvm.pp3d_factor;
+                const float wCamera = camera_path_weight(L, mwfInv, sinT, lvm.ray_sample_pdf_inv,
+                                                         lvm.ray_sample_pdfs_ratio, revPdf, P.query_beam_type,
+                                                         P.photon_beam_type, P.techniques, camv);
+                const LightView lview{Lv.mis, -1, 0.f};
+                const float wLight = light_path_weight(info.x, pl, mwfInv, 0.f, 0.f, 0.f, dirPdf, UPBP_PP3D,
+                                                       P.query_beam_type, P.photon_beam_type, P.techniques,
+                                                       Lv.path_ends, lview, nullptr);
+                const float w = 1.f / (wLight + wCamera);
+                const float4 th = __ldg(&Lv.thr[lv]);
+                res = res + w * (factor * Rgb{th.x, th.y, th.z});
+            }
+        }
+    }
+    O.rgb[3 * q + 0] = res.r;
+    O.rgb[3 * q + 1] = res.g;
+    O.rgb[3 * q + 2] = res.b;
+    if (O.count) O.count[q] = cnt;
+    if (O.hash) O.hash[q] = h;
+    const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+    splat(O.image, Q.pixel[q], thr * P.norm_pp3d * res);
+    if (O.tested) atomicAdd(O.tested, tested);
+}
+
+}  // namespace
+
+void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,
+                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream)
+{
+    if (Q.n <= 0) return;
+    const int grid = (int)((Q.n + block - 1) / block);
+    k_gather_pb2d<<<grid, block, 0, stream>>>(K, L, B, Q, cam, O);
+}
+
+void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
+                        const SegQueriesDev& Q, const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream)
+{
+    if (Q.n <= 0) return;
+    const int grid = (int)((Q.n + block - 1) / block);
+    k_gather_bb1d<<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, O);
+}
+
+void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,
+                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream)
+{
+    if (Q.n <= 0) return;
+    const int grid = (int)((Q.n + block - 1) / block);
+    k_gather_pp3d<<<grid, block, 0, stream>>>(K, L, G, Q, cam, O);
+}
+
+}  // namespace upbp

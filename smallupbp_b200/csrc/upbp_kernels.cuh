@@ -1,0 +1,171 @@
+// Kernel interfaces of the B200 estimator stage (device data layout in HBM).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "upbp_device.cuh"
+
+namespace upbp {
+
+// BVH2 node with both child boxes (64 B, one 4x16-byte load per visit).
+// Children: >= 0 internal node index, < 0 leaf ~index.
+struct __align__(16) BNode {
+    float4 a;  // left.lo.xyz, left.hi.x
+    float4 b;  // left.hi.yz, right.lo.xy
+    float4 c;  // right.lo.z, right.hi.xyz
+    int4 d;    // left, right, -, -
+};
+
+struct Box {
+    float lo[3], hi[3];
+};
+
+// Light vertices, packed for the gathers (index = light vertex index).
+struct LightSoA {
+    const float4* pos;      // xyz, continuation prob of its BSDF
+    const float4* dir;      // dir_fix xyz, -
+    const float4* thr;      // throughput rgb, -
+    const int4* info;       // path_idx, path_length, flags, medium_id
+    const upbp_mis* mis;    // MisData
+    const int32_t* path_ends;
+    int64_t n;
+};
+
+// Photon LBVH (PB2D): photons in leaf order, leaf k = photons [k*leaf, min((k+1)*leaf, n)).
+struct PhotonBVH {
+    const float4* pos;   // xyz, light-vertex index (int bits)
+    const BNode* nodes;  // n_leaves - 1 internal nodes, root 0
+    int n;
+    int leaf;
+    int n_leaves;
+};
+
+// Beam pieces (BB1D) in leaf order.  Piece = beam sub-interval [t_lo, t_hi).
+struct BeamBVH {
+    const float4* pa;    // beam origin xyz, beam length
+    const float4* pb;    // beam direction xyz, t_lo
+    const float4* pc;    // t_hi, max radius^2, beam id (int bits), medium (int bits)
+    const BNode* nodes;
+    int n;
+    int leaf;
+    int n_leaves;
+};
+
+// Beam payload (index = beam id).
+struct BeamSoA {
+    const float4* thr;   // throughput at origin rgb, flags (int bits)
+    const float4* pdf;   // ray_sample_pdf, ray_sample_rev_pdf, last_pdf_w_inv, ray_sampling_flags (int bits)
+    const int2* link;    // light vertex, medium
+    const float* radius; // start radius (constant-radius build)
+    int64_t n;
+};
+
+// PP3D hash grid (Misc/HashGrid.hxx), photons sorted by bucket, stable in light-vertex order.
+struct HashGridDev {
+    const float4* pos;      // xyz, light-vertex index (int bits)
+    const int32_t* start;   // [cells]
+    const int32_t* end;     // [cells]
+    float bbox_min[3], bbox_max[3];
+    float inv_cell;
+    float r2;
+    int cells;
+    int n;
+};
+
+struct SegQueriesDev {
+    const float* origin;
+    const float* direction;
+    const int32_t* seg_begin;
+    const int32_t* seg_count;
+    const uint32_t* flags;
+    const int32_t* path_length;
+    const float* last_pdf_w_inv;
+    const float* throughput;
+    const int32_t* pixel;
+    const int64_t* cam_mis_begin;
+    const float* seg_dist_min;
+    const float* seg_dist_max;
+    const float* seg_pdf;
+    const float* seg_rev_pdf;
+    const float* seg_attenuation;
+    const int32_t* seg_medium;
+    int64_t n;
+};
+
+struct PointQueriesDev {
+    const float* position;
+    const float* dir_fix;
+    const int32_t* medium_id;
+    const int32_t* path_length;
+    const float* throughput;
+    const int32_t* pixel;
+    const int64_t* cam_mis_begin;
+    int64_t n;
+};
+
+struct Outputs {
+    float* rgb;                 // [n][3]
+    float* image;               // [H*W][3] or null
+    uint32_t* count;            // [n] or null
+    unsigned long long* hash;   // [n] or null
+    unsigned long long* tested; // total candidates tested (diagnostic), or null
+};
+
+struct GatherConsts {
+    upbp_params P;
+    DMedium media[UPBP_MAX_MEDIA];
+    int n_media;
+    int has_bb1d_beams;  // PB2D: mBB1DPhotonBeams != NULL
+    float eps;           // conservative box slack for traversal
+};
+
+// ---- launches (all asynchronous on `stream`) ----------------------------------------
+void launch_pack_lights(const float* pos, const float* thr, const float* dir, const float* cont,
+                        const int32_t* path_idx, const int32_t* path_length, const int32_t* medium,
+                        const uint32_t* flags, int64_t n, float4* o_pos, float4* o_dir, float4* o_thr, int4* o_info,
+                        uint32_t* o_in_medium, cudaStream_t stream);
+
+void launch_bbox_partial(const float4* pts, const int32_t* idx, int n, float* partial, int blocks,
+                         cudaStream_t stream);
+void launch_bbox_final(const float* partial, int blocks, float* out, cudaStream_t stream);
+
+void launch_hash_keys(const float4* lv_pos, const int32_t* ph_lv, int n, const float* bbox, float inv_cell, int cells,
+                      uint32_t* keys, cudaStream_t stream);
+void launch_hash_ranges(const uint32_t* keys_sorted, const int32_t* lv_sorted, const float4* lv_pos, int n,
+                        int32_t* start, int32_t* end, float4* out_pos, cudaStream_t stream);
+
+void launch_morton_points(const float4* lv_pos, const int32_t* ph_lv, int n, const float* bbox, uint32_t* codes,
+                          cudaStream_t stream);
+void launch_gather_photons(const int32_t* lv_sorted, const float4* lv_pos, int n, float4* out_pos,
+                           cudaStream_t stream);
+void launch_leaf_codes(const uint32_t* codes_sorted, int n, int leaf, uint32_t* leaf_codes, cudaStream_t stream);
+void launch_karras(const uint32_t* leaf_codes, int n_leaves, BNode* nodes, int32_t* parent_int,
+                   int32_t* parent_leaf, cudaStream_t stream);
+void launch_photon_leaf_boxes(const float4* pos, int n, int leaf, float r, float eps, Box* leaf_boxes,
+                              cudaStream_t stream);
+void launch_bottom_up(const Box* leaf_boxes, int n_leaves, BNode* nodes, const int32_t* parent_int,
+                      const int32_t* parent_leaf, Box* node_boxes, int32_t* flags, cudaStream_t stream);
+
+void launch_pack_beams(const float* thr, const uint32_t* flags, const float* rsp, const float* rsr, const float* lpw,
+                       const uint32_t* rsf, const int32_t* lv, const int32_t* medium, int64_t n, float radius,
+                       float4* o_thr, float4* o_pdf, int2* o_link, float* o_radius, cudaStream_t stream);
+void launch_piece_counts(const float* length, int64_t n, float piece_len, int32_t* counts, cudaStream_t stream);
+void launch_emit_pieces(const float* origin, const float* dir, const float* length, const int32_t* medium,
+                        int64_t n, const int32_t* offsets, float piece_len, float radius, float eps,
+                        float4* pa, float4* pb, float4* pc, Box* boxes, cudaStream_t stream);
+void launch_bbox_boxes_partial(const Box* boxes, int n, float* partial, int blocks, cudaStream_t stream);
+void launch_morton_boxes(const Box* boxes, int n, const float* bbox, uint32_t* codes, cudaStream_t stream);
+void launch_permute_pieces(const int32_t* perm, int n, const float4* pa, const float4* pb, const float4* pc,
+                           const Box* boxes, float4* opa, float4* opb, float4* opc, Box* oboxes, cudaStream_t stream);
+void launch_box_leaf_boxes(const Box* boxes, int n, int leaf, Box* leaf_boxes, cudaStream_t stream);
+
+void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,
+                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream);
+void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
+                        const SegQueriesDev& Q, const upbp_mis* cam, const Outputs& O, int block,
+                        cudaStream_t stream);
+void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,
+                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream);
+
+}  // namespace upbp

@@ -1,0 +1,207 @@
+"""Python binding of the C ABI (``include/upbp_gpu.h``) implemented by ``libupbp_b200.so``.
+
+:class:`EstimatorStage` owns one device context and mirrors the reference's per-iteration estimator
+calls in batched form::
+
+    stage = EstimatorStage(device=0)
+    stage.load(workload)          # media, params, light vertices, beams  (HashGrid/EmbreeBre/PhotonBeamsEvaluator build inputs)
+    stage.build()                 # HashGrid::Build + EmbreeBre::build + PhotonBeamsEvaluator::build
+    stage.set_queries(workload)   # the recorded evalBre / evalBeamBeamEstimate / HashGrid::Process calls
+    stage.evaluate()              # all of them in one batch
+    stage.segment_results()       # per-call Rgb returned by evalBre / evalBeamBeamEstimate
+    stage.point_results()         # per-call RangeQuery contribution
+    stage.image()                 # framebuffer with the normalised contributions splatted
+
+There is no CPU fallback: a missing or unloadable library, or a machine without a CUDA device,
+raises :class:`UpbpError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import abi
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libupbp_b200.so")
+
+MODE_PLAIN, MODE_MIXED = 0, 1
+
+EXPORTS = (
+    "upbp_ctx_create", "upbp_ctx_destroy", "upbp_last_error", "upbp_set_mode", "upbp_set_tuning",
+    "upbp_set_stream", "upbp_set_media", "upbp_set_params", "upbp_set_light_vertices", "upbp_set_beams",
+    "upbp_build", "upbp_set_camera_mis", "upbp_set_segment_queries", "upbp_set_point_queries", "upbp_evaluate",
+    "upbp_read_segment_results", "upbp_read_point_results", "upbp_read_query_stats", "upbp_clear_image",
+    "upbp_read_image", "upbp_last_launch_count", "upbp_last_timings", "upbp_destroy_structures",
+)
+
+
+class UpbpError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("upbp error %d: %s" % (code, msg))
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libupbp_b200.so (raises if it is missing: the CUDA path is the only path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise UpbpError(-4, "%s not built (python -m smallupbp_b200.build)" % LIB_PATH)
+        l = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        l.upbp_ctx_create.argtypes = [C.POINTER(vp), C.c_int]
+        l.upbp_ctx_destroy.argtypes = [vp]
+        l.upbp_last_error.argtypes = [vp]
+        l.upbp_last_error.restype = C.c_char_p
+        l.upbp_set_mode.argtypes = [vp, C.c_int]
+        l.upbp_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        l.upbp_set_stream.argtypes = [vp, vp]
+        l.upbp_set_media.argtypes = [vp, C.POINTER(abi.Medium), C.c_int32]
+        l.upbp_set_params.argtypes = [vp, C.POINTER(abi.Params)]
+        l.upbp_set_light_vertices.argtypes = [vp, C.POINTER(abi.LightVertices)]
+        l.upbp_set_beams.argtypes = [vp, C.POINTER(abi.Beams)]
+        l.upbp_build.argtypes = [vp]
+        l.upbp_set_camera_mis.argtypes = [vp, C.POINTER(abi.Mis), C.c_int64]
+        l.upbp_set_segment_queries.argtypes = [vp, C.POINTER(abi.SegmentQueries)]
+        l.upbp_set_point_queries.argtypes = [vp, C.POINTER(abi.PointQueries)]
+        l.upbp_evaluate.argtypes = [vp]
+        l.upbp_read_segment_results.argtypes = [vp, abi.f32p, abi.f32p]
+        l.upbp_read_point_results.argtypes = [vp, abi.f32p]
+        l.upbp_read_query_stats.argtypes = [vp, C.POINTER(abi.QueryStats)]
+        l.upbp_clear_image.argtypes = [vp]
+        l.upbp_read_image.argtypes = [vp, abi.f32p]
+        l.upbp_last_launch_count.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        l.upbp_last_timings.argtypes = [vp] + [C.POINTER(C.c_float)] * 4
+        l.upbp_destroy_structures.argtypes = [vp]
+        for name in EXPORTS:
+            if name != "upbp_last_error":
+                getattr(l, name).restype = C.c_int
+        _lib = l
+    return _lib
+
+
+class EstimatorStage:
+    """One device context of the batched estimator stage."""
+
+    def __init__(self, device: int = 0, mode: int = MODE_PLAIN):
+        self._l = lib()
+        self._ctx = C.c_void_p()
+        rc = self._l.upbp_ctx_create(C.byref(self._ctx), device)
+        if rc != 0:
+            raise UpbpError(rc, "upbp_ctx_create(device=%d) failed (no usable CUDA device?)" % device)
+        self._keep = []
+        self._nq = 0
+        self._np = 0
+        self._npix = 0
+        self.set_mode(mode)
+
+    # -------------------------------------------------------------- plumbing
+    def _ck(self, rc: int):
+        if rc != 0:
+            raise UpbpError(rc, self._l.upbp_last_error(self._ctx).decode())
+
+    def close(self):
+        if self._ctx:
+            self._l.upbp_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_mode(self, mode: int):
+        self._ck(self._l.upbp_set_mode(self._ctx, mode))
+
+    def set_tuning(self, pb2d_leaf: int, bb1d_leaf: int, block_threads: int):
+        self._ck(self._l.upbp_set_tuning(self._ctx, pb2d_leaf, bb1d_leaf, block_threads))
+
+    def set_stream(self, stream_ptr: int):
+        self._ck(self._l.upbp_set_stream(self._ctx, C.c_void_p(stream_ptr)))
+
+    # -------------------------------------------------------------- inputs
+    def load(self, w: Dict[str, np.ndarray], structs=None):
+        """Upload media, params, light vertices and beams of workload ``w``."""
+        s, keep = structs if structs is not None else abi.make_structs(w)
+        self._keep = [keep, s]
+        self._ck(self._l.upbp_set_media(self._ctx, s["media"], s["n_media"]))
+        self._ck(self._l.upbp_set_params(self._ctx, C.byref(s["params"])))
+        self._ck(self._l.upbp_set_light_vertices(self._ctx, C.byref(s["lv"])))
+        self._ck(self._l.upbp_set_beams(self._ctx, C.byref(s["beams"])))
+        self._npix = s["params"].image_width * s["params"].image_height
+        return s
+
+    def build(self):
+        self._ck(self._l.upbp_build(self._ctx))
+
+    def set_queries(self, w: Dict[str, np.ndarray], structs=None):
+        s, keep = structs if structs is not None else abi.make_structs(w)
+        self._keep.append((keep, s))
+        self._ck(self._l.upbp_set_camera_mis(self._ctx, s["cam_mis"], s["n_cam_mis"]))
+        self._ck(self._l.upbp_set_segment_queries(self._ctx, C.byref(s["sq"])))
+        self._ck(self._l.upbp_set_point_queries(self._ctx, C.byref(s["pq"])))
+        self._nq = s["sq"].n
+        self._np = s["pq"].n
+
+    def clear_image(self):
+        self._ck(self._l.upbp_clear_image(self._ctx))
+
+    def evaluate(self):
+        self._ck(self._l.upbp_evaluate(self._ctx))
+
+    # -------------------------------------------------------------- outputs
+    def segment_results(self):
+        pb2d = np.zeros((self._nq, 3), np.float32)
+        bb1d = np.zeros((self._nq, 3), np.float32)
+        self._ck(self._l.upbp_read_segment_results(self._ctx, abi.ptr(pb2d), abi.ptr(bb1d)))
+        return pb2d, bb1d
+
+    def point_results(self):
+        pp3d = np.zeros((self._np, 3), np.float32)
+        self._ck(self._l.upbp_read_point_results(self._ctx, abi.ptr(pp3d)))
+        return pp3d
+
+    def query_stats(self):
+        out = {k: np.zeros(self._nq if "pp3d" not in k else self._np, np.uint32 if k.startswith("count") else np.uint64)
+               for k in ("count_pb2d", "hash_pb2d", "count_bb1d", "hash_bb1d", "count_pp3d", "hash_pp3d")}
+        st = abi.QueryStats(**{k: abi.ptr(v) for k, v in out.items()})
+        self._ck(self._l.upbp_read_query_stats(self._ctx, C.byref(st)))
+        return out
+
+    def image(self):
+        img = np.zeros((self._npix, 3), np.float32)
+        self._ck(self._l.upbp_read_image(self._ctx, abi.ptr(img)))
+        return img
+
+    def launch_counts(self):
+        b, e = C.c_int(), C.c_int()
+        self._ck(self._l.upbp_last_launch_count(self._ctx, C.byref(b), C.byref(e)))
+        return b.value, e.value
+
+    def timings(self):
+        v = [C.c_float() for _ in range(4)]
+        self._ck(self._l.upbp_last_timings(self._ctx, *[C.byref(x) for x in v]))
+        return dict(build_ms=v[0].value, pp3d_ms=v[1].value, pb2d_ms=v[2].value, bb1d_ms=v[3].value)
+
+    def run(self, w: Dict[str, np.ndarray]):
+        """Convenience: load, build, set queries, clear the image and evaluate."""
+        s = abi.make_structs(w)
+        self.load(w, s)
+        self.build()
+        self.set_queries(w, s)
+        self.clear_image()
+        self.evaluate()
+        return self

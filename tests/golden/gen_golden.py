@@ -1,0 +1,65 @@
+"""Generate the golden fixtures of the estimator stage from the reference itself.
+
+Each fixture holds one seeded workload (the arrays of include/upbp_gpu.h, produced by
+smallupbp_b200.workload) and the outputs of the reference SmallUPBP estimator code run on it by
+the reference harness (oracle/_ref/libupbp_ref.so, built from the reference sources by
+oracle/build_ref.py):  per-query PB2D / BB1D (grid and brute force) / PP3D contributions,
+per-query candidate counts and hashes, and the splatted image.
+
+Run from the repository root:  python tests/golden/gen_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from smallupbp_b200 import workload as W  # noqa: E402
+from oracle import ref  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# (fixture name, scene config name, overrides)
+CASES = [
+    ("cube_long_short", "cube32x2048", dict()),
+    ("cube_short_long", "cube32x2048", dict(query_beam_type=W.SHORT_BEAM, photon_beam_type=W.LONG_BEAM, seed=77)),
+    ("cube_nosine_mindist", "cube24x1536", dict(techniques=W.BPT | W.SURF | W.PP3D | W.PB2D | W.BB1D | W.NO_SINE_IN_WEIGHTS,
+                                                min_dist_to_med=0.3, min_path_length=2, max_path_length=5, seed=5)),
+    ("cube_previous", "cube24x1536", dict(techniques=W.PP3D | W.PB2D | W.BB1D | W.PREVIOUS | W.BB1D_PREVIOUS, seed=9)),
+    ("boxes_all", "boxes", dict()),
+    ("cube_wide_radius", "cube24x1536", dict(radius=0.08, seed=21)),
+]
+
+
+def scene(name: str, overrides: dict) -> W.SceneConfig:
+    if name == "boxes":
+        cfg = W.nested_boxes_scene("boxes_small", 24, 24, 2048, 6, 0.02)
+    else:
+        cfg = W.config(name)
+    for k, v in overrides.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def main():
+    for fname, cname, over in CASES:
+        cfg = scene(cname, over)
+        w = W.generate(cfg)
+        o = ref.run(w, threads=8)
+        out = {"in_" + k: v for k, v in w.items()}
+        for k in ("pb2d", "bb1d", "bb1d_brute", "pp3d", "count_pb2d", "hash_pb2d", "count_bb1d", "hash_bb1d",
+                  "count_pp3d", "hash_pp3d", "image"):
+            out["ref_" + k] = o[k]
+        path = os.path.join(HERE, fname + ".npz")
+        np.savez_compressed(path, **out)
+        print("%-22s lv=%d beams=%d sq=%d pq=%d  cand pb2d=%d bb1d=%d pp3d=%d  %.0f KB" % (
+            fname, len(w["lv_path_idx"]), len(w["beam_length"]), len(w["sq_path_length"]), len(w["pq_path_length"]),
+            o["count_pb2d"].sum(), o["count_bb1d"].sum(), o["count_pp3d"].sum(), os.path.getsize(path) / 1024))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,45 @@
+"""Loading of the golden fixtures (tests/golden/*.npz) and the parity comparison helpers."""
+from __future__ import annotations
+
+import glob
+import os
+from typing import Dict, Tuple
+
+import numpy as np
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+# Per-query contribution tolerance of the FP32 path against the reference (relative), with an
+# absolute floor of ATOL_FRAC times the largest contribution of that estimator in the fixture.
+RTOL = 1e-4
+ATOL_FRAC = 1e-6
+
+
+def load(path: str) -> Tuple[Dict[str, np.ndarray], Dict[str, np.ndarray]]:
+    z = np.load(path)
+    w = {k[3:]: z[k] for k in z.files if k.startswith("in_")}
+    r = {k[4:]: z[k] for k in z.files if k.startswith("ref_")}
+    return w, r
+
+
+def name(path: str) -> str:
+    return os.path.basename(path)[:-4]
+
+
+def rel_errors(got: np.ndarray, want: np.ndarray) -> np.ndarray:
+    """Per-query max-channel relative error with the absolute floor."""
+    floor = ATOL_FRAC * max(float(np.abs(want).max()), 1e-30)
+    return (np.abs(got - want) / (np.abs(want) + floor)).max(axis=1)
+
+
+def assert_close(got: np.ndarray, want: np.ndarray, what: str):
+    assert got.shape == want.shape, what
+    err = rel_errors(got.astype(np.float64), want.astype(np.float64))
+    worst = int(np.argmax(err)) if len(err) else -1
+    assert (err <= RTOL).all(), "%s: %d/%d queries above %.0e, worst %.3e at %d (got %s want %s)" % (
+        what, int((err > RTOL).sum()), len(err), RTOL, err[worst], worst, got[worst], want[worst])
+
+
+def image_rel_l2(got: np.ndarray, want: np.ndarray) -> float:
+    return float(np.linalg.norm((got - want).ravel()) / max(np.linalg.norm(want.ravel()), 1e-30))
