@@ -44,7 +44,14 @@ def lib():
                                  C.POINTER(abi.LightVertices), C.POINTER(abi.Beams), C.POINTER(abi.Mis), C.c_int64,
                                  C.POINTER(abi.SegmentQueries), C.POINTER(abi.PointQueries), C.c_int32, C.c_int64,
                                  C.c_int32, C.POINTER(RefOutputs)]
+        _lib.ref_set_grid_options.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
+        _lib.ref_set_grid_options.restype = None
     return _lib
+
+
+def set_grid_options(grid_size: int = 256, max_beams_in_cell: int = 0, reduction_type: int = 0) -> None:
+    """The reference's -gridres / -gridmax / -gridred options (defaults 256, 0, 0)."""
+    lib().ref_set_grid_options(grid_size, max_beams_in_cell, reduction_type)
 
 
 def run(w: Dict[str, np.ndarray], what: int = PB2D | BB1D_GRID | BB1D_BRUTE | PP3D | CANDIDATES,
@@ -75,3 +82,49 @@ def run(w: Dict[str, np.ndarray], what: int = PB2D | BB1D_GRID | BB1D_BRUTE | PP
     out["gather_ms"] = o.gather_ms
     del keep
     return out
+
+
+class Session:
+    """Reference structures built once (one world per thread, as the reference keeps one renderer
+    per OpenMP thread); ``eval(offset, stride)`` runs the reference estimators on a query subset."""
+
+    def __init__(self, w: Dict[str, np.ndarray], what: int = PB2D | BB1D_GRID | PP3D, threads: int = 0):
+        l = lib()
+        l.ref_prepare.restype = C.c_void_p
+        l.ref_prepare.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Medium), C.c_int32,
+                                  C.POINTER(abi.LightVertices), C.POINTER(abi.Beams), C.POINTER(abi.Mis),
+                                  C.POINTER(abi.SegmentQueries), C.POINTER(abi.PointQueries), C.c_int32, C.c_int32]
+        l.ref_eval.restype = C.c_int
+        l.ref_eval.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.POINTER(RefOutputs)]
+        l.ref_release.argtypes = [C.c_void_p]
+        self._l = l
+        self._s, self._keep = abi.make_structs(w)
+        s = self._s
+        self.n_segment = s["sq"].n
+        self.n_point = s["pq"].n
+        self._h = l.ref_prepare(C.byref(s["params"]), s["media"], s["n_media"], C.byref(s["lv"]),
+                                C.byref(s["beams"]), s["cam_mis"], C.byref(s["sq"]), C.byref(s["pq"]), what, threads)
+        if not self._h:
+            raise RuntimeError("ref_prepare failed")
+        o = RefOutputs()
+        self._l.ref_eval(self._h, max(self.n_segment, self.n_point), 1, C.byref(o))  # no queries: reads the build time
+        self.build_ms = o.build_ms
+
+    def eval(self, offset: int, stride: int) -> float:
+        """Evaluate queries offset, offset+stride, ...; returns the wall time in ms."""
+        o = RefOutputs()
+        rc = self._l.ref_eval(self._h, offset, stride, C.byref(o))
+        if rc != 0:
+            raise RuntimeError("ref_eval failed")
+        return o.gather_ms
+
+    def close(self):
+        if self._h:
+            self._l.ref_release(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -258,13 +258,34 @@ template struct PP3DExposer<UPBP::RangeQuery, UPBP::SubPathState>;
 
 }  // namespace
 
-extern "C" int ref_run(const upbp_params* params, const upbp_medium* media, int32_t n_media,
-                       const upbp_light_vertices* lv, const upbp_beams* beams, const upbp_mis* cam_mis,
-                       int64_t n_cam_mis, const upbp_segment_queries* sq, const upbp_point_queries* pq, int32_t what,
-                       int64_t stride, int32_t threads, ref_outputs* out)
+extern "C" void ref_set_grid_options(uint32_t grid_size, uint32_t max_beams_in_cell, uint32_t reduction_type)
 {
-    (void)n_cam_mis;
-    if (!params || !media || !lv || !out || stride < 1) return -1;
+    PhotonBeamsEvaluator::sGridSize = grid_size;
+    PhotonBeamsEvaluator::sMaxBeamsInCell = max_beams_in_cell;
+    PhotonBeamsEvaluator::sReductionType = reduction_type;
+}
+
+struct RefSession {
+    upbp_params P;
+    const upbp_medium* media;
+    int32_t n_media;
+    const upbp_light_vertices* lv;
+    const upbp_beams* beams;
+    const upbp_mis* cam_mis;
+    const upbp_segment_queries* sq;
+    const upbp_point_queries* pq;
+    int32_t what;
+    int nthreads;
+    std::vector<std::unique_ptr<World>> worlds;
+    double build_ms;
+};
+
+extern "C" void* ref_prepare(const upbp_params* params, const upbp_medium* media, int32_t n_media,
+                             const upbp_light_vertices* lv, const upbp_beams* beams, const upbp_mis* cam_mis,
+                             const upbp_segment_queries* sq, const upbp_point_queries* pq, int32_t what,
+                             int32_t threads)
+{
+    if (!params || !media || !lv) return nullptr;
     // Embree library init, as EmbreeAcc::initLib (Bre/EmbreeAcc.hxx:42-49).
     static std::once_flag embree_once;
     std::call_once(embree_once, [] {
@@ -272,25 +293,46 @@ extern "C" int ref_run(const upbp_params* params, const upbp_medium* media, int3
         embree::rtcSetVerbose(0);
         embree::rtcStartThreads(0);
     });
-    const upbp_params P = *params;
-    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
-    const int64_t npix = (int64_t)P.image_width * P.image_height;
-    std::vector<std::vector<float>> images(out->image ? nthreads : 0, std::vector<float>(out->image ? 3 * npix : 0, 0.f));
-    std::vector<std::unique_ptr<World>> worlds(nthreads);
-    int status = 0;
-
-    // The brute-force BB1D evaluator needs the radii the grid build writes; when only
-    // the brute force is requested it computes them itself (PhBeams.cxx:66-122).
+    RefSession* S = new RefSession();
+    S->P = *params;
+    S->media = media;
+    S->n_media = n_media;
+    S->lv = lv;
+    S->beams = beams;
+    S->cam_mis = cam_mis;
+    S->sq = sq;
+    S->pq = pq;
+    S->what = what;
+    S->nthreads = threads > 0 ? threads : omp_get_max_threads();
+    S->worlds.resize(S->nthreads);
     auto t0 = std::chrono::steady_clock::now();
-#pragma omp parallel num_threads(nthreads)
+#pragma omp parallel num_threads(S->nthreads)
     {
         const int tid = omp_get_thread_num();
-        worlds[tid].reset(new World());
-        setup_world(*worlds[tid], P, media, n_media, lv, beams, what);
+        S->worlds[tid].reset(new World());
+        setup_world(*S->worlds[tid], S->P, media, n_media, lv, beams, what);
     }
-    auto t1 = std::chrono::steady_clock::now();
-    out->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    S->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return S;
+}
 
+extern "C" void ref_release(void* h) { delete static_cast<RefSession*>(h); }
+
+/* Evaluate queries q = offset + k*stride; returns the wall time in ms through out->gather_ms. */
+extern "C" int ref_eval(void* h, int64_t offset, int64_t stride, ref_outputs* out)
+{
+    RefSession* S = static_cast<RefSession*>(h);
+    if (!S || !out || stride < 1 || offset < 0) return -1;
+    const upbp_params& P = S->P;
+    const int nthreads = S->nthreads;
+    const int32_t what = S->what;
+    const upbp_segment_queries* sq = S->sq;
+    const upbp_point_queries* pq = S->pq;
+    const upbp_mis* cam_mis = S->cam_mis;
+    const int64_t npix = (int64_t)P.image_width * P.image_height;
+    std::vector<std::vector<float>> images(out->image ? nthreads : 0, std::vector<float>(out->image ? 3 * npix : 0, 0.f));
+    std::vector<std::unique_ptr<World>>& worlds = S->worlds;
+    auto t1 = std::chrono::steady_clock::now();
     const int64_t nq = sq ? sq->n : 0;
     const int64_t np = pq ? pq->n : 0;
 #pragma omp parallel num_threads(nthreads)
@@ -302,7 +344,7 @@ extern "C" int ref_run(const upbp_params* params, const upbp_medium* media, int3
         const uint tech = P.techniques;
         const uint rsf_in = AbstractMedium::kOriginInMedium;
 #pragma omp for schedule(dynamic, 16)
-        for (int64_t q = 0; q < nq; q += stride) {
+        for (int64_t q = offset; q < nq; q += stride) {
             const int L = sq->path_length[q];
             const uint qf = sq->flags[q];
             const bool lite = (qf & UPBP_Q_LITE) != 0;
@@ -420,7 +462,7 @@ extern "C" int ref_run(const upbp_params* params, const upbp_medium* media, int3
         }
         // PP3D, UPBP.hxx:1114-1122
 #pragma omp for schedule(dynamic, 16)
-        for (int64_t q = 0; q < np; q += stride) {
+        for (int64_t q = offset; q < np; q += stride) {
             if (!U.mMergeWithLightVerticesPP3D || U.mLightVerticesInMediumCount == 0) continue;
             const int L = pq->path_length[q];
             const Pos hit = P3(pq->position + 3 * q);
@@ -447,10 +489,24 @@ extern "C" int ref_run(const upbp_params* params, const upbp_medium* media, int3
     }
     auto t2 = std::chrono::steady_clock::now();
     out->gather_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    out->build_ms = S->build_ms;
     if (out->image) {
         for (int t = 0; t < nthreads; ++t)
             for (int64_t i = 0; i < 3 * npix; ++i) out->image[i] += images[t][i];
     }
-    worlds.clear();
-    return status;
+    return 0;
+}
+
+extern "C" int ref_run(const upbp_params* params, const upbp_medium* media, int32_t n_media,
+                       const upbp_light_vertices* lv, const upbp_beams* beams, const upbp_mis* cam_mis,
+                       int64_t n_cam_mis, const upbp_segment_queries* sq, const upbp_point_queries* pq, int32_t what,
+                       int64_t stride, int32_t threads, ref_outputs* out)
+{
+    (void)n_cam_mis;
+    if (!out || stride < 1) return -1;
+    void* h = ref_prepare(params, media, n_media, lv, beams, cam_mis, sq, pq, what, threads);
+    if (!h) return -1;
+    const int rc = ref_eval(h, 0, stride, out);
+    ref_release(h);
+    return rc;
 }

@@ -47,6 +47,19 @@ int ref_run(const upbp_params* params, const upbp_medium* media, int32_t n_media
             const upbp_segment_queries* sq, const upbp_point_queries* pq,
             int32_t what, int64_t stride, int32_t threads, ref_outputs* out);
 
+/* The same in three steps, so that a caller can time the per-thread builds once and then
+ * evaluate several query subsets (q = offset + k*stride) on the built structures. */
+void* ref_prepare(const upbp_params* params, const upbp_medium* media, int32_t n_media,
+                  const upbp_light_vertices* lv, const upbp_beams* beams, const upbp_mis* cam_mis,
+                  const upbp_segment_queries* sq, const upbp_point_queries* pq, int32_t what, int32_t threads);
+int ref_eval(void* session, int64_t offset, int64_t stride, ref_outputs* out);
+void ref_release(void* session);
+
+/* The reference's BB1D grid options, set from the command line in the renderer
+ * (-gridres / -gridmax / -gridred, Misc/Config.hxx:1964-1966): statics of
+ * PhotonBeamsEvaluator (Beams/PhBeams.cxx:44-46). */
+void ref_set_grid_options(uint32_t grid_size, uint32_t max_beams_in_cell, uint32_t reduction_type);
+
 #ifdef __cplusplus
 }
 #endif

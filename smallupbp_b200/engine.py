@@ -186,6 +186,10 @@ class EstimatorStage:
         self._ck(self._l.upbp_read_image(self._ctx, abi.ptr(img)))
         return img
 
+    def read_image_into(self, ptr: int):
+        """Copy the framebuffer (H*W*3 float32) to ``ptr`` (host or device address)."""
+        self._ck(self._l.upbp_read_image(self._ctx, C.cast(C.c_void_p(ptr), abi.f32p)))
+
     def launch_counts(self):
         b, e = C.c_int(), C.c_int()
         self._ck(self._l.upbp_last_launch_count(self._ctx, C.byref(b), C.byref(e)))

@@ -143,6 +143,8 @@ def config(name: str) -> SceneConfig:
     if name == "cube1024":     # 1024^2, 1,048,576 light paths, r=0.005, LONG photon beams capped at 2.0
         return cube_scene("cube1024", 1024, 1024, 1_048_576, 6, 0.005, photon_beam_type=LONG_BEAM,
                           beam_length_cap=2.0)
+    if name == "cube512":      # quarter-size cube1024 (profiling case): 512^2, 262,144 light paths
+        return cube_scene("cube512", 512, 512, 262_144, 6, 0.005, photon_beam_type=LONG_BEAM, beam_length_cap=2.0)
     if name == "boxes3":       # heavy-tailed: nested sigma_t 0.05 / 1 / 10
         return nested_boxes_scene()
     if name == "diff512":      # differentiable-estimator scene: 512^2, 262,144 light paths
@@ -188,65 +190,62 @@ def _medium_at(cfg: SceneConfig, p: np.ndarray) -> np.ndarray:
 
 
 def _trace(cfg: SceneConfig, rng: np.random.Generator, o: np.ndarray, d: np.ndarray, origin_in_medium: np.ndarray):
-    """Scene::Intersect for imaginary-boundary media: split the ray into medium segments and sample a
-    free-flight distance in each scattering medium in order (HomogeneousMedium::SampleRay,
-    Scene/Media.hxx:240-290).  Returns per-ray lists of full segments (up to the scattering point)
-    and lite segments (the whole traversal), plus the scattering distance (inf when the ray leaves).
+    """Scene::Intersect for imaginary-boundary media, vectorised over rays.
+
+    The ray is split at every box face into medium segments; a free-flight distance is sampled in
+    each scattering medium in order (HomogeneousMedium::SampleRay, Scene/Media.hxx:240-290) until
+    one scatters.  Returns a dict of (n, K) arrays: ``full`` marks the VolumeSegments (up to the
+    scattering point, clear-medium segments included), ``lite`` the LiteVolumeSegments (every
+    scattering medium on the ray), with distances, pdfs, attenuation and medium ids, plus the
+    scattering distance per ray (inf when the ray leaves the scene).
     """
     n = o.shape[0]
     breaks = _box_breaks(cfg, o, d)
     K = breaks.shape[1]
-    starts = np.concatenate([np.zeros((n, 1)), breaks[:, :-1]], axis=1) if K else np.zeros((n, 0))
-    ends = breaks
-    full: List[list] = [[] for _ in range(n)]
-    lite: List[list] = [[] for _ in range(n)]
-    scatter_t = np.full(n, np.inf)
-    alive = np.ones(n, bool)
-    first = np.ones(n, bool)
+    starts = np.concatenate([np.zeros((n, 1)), breaks[:, :-1]], axis=1)
+    ends = breaks.copy()
+    valid = np.isfinite(ends) & (ends > starts)
+    mids = np.where(valid, 0.5 * (starts + np.where(np.isfinite(ends), ends, starts)), 0.0)
+    med = np.zeros((n, K), np.int32)
     for k in range(K):
-        s0 = starts[:, k]
-        s1 = ends[:, k]
-        valid = np.isfinite(s1) & (s1 > s0)
-        mid = o + d * ((s0 + np.where(np.isfinite(s1), s1, s0 + 1.0)) * 0.5)[:, None]
-        med = _medium_at(cfg, mid)
-        u = rng.random(n)
-        for i in np.nonzero(valid)[0]:
-            m = cfg.media[med[i]]
-            seglen = s1[i] - s0[i]
-            if med[i] == 0 and not m.has_scattering:
-                flags_first = first[i]
-                if alive[i]:
-                    full[i].append((s0[i], s1[i], 1.0, 1.0, (1.0, 1.0, 1.0), int(med[i])))
-                first[i] = False
-                continue
-            lite[i].append((s0[i], s1[i], int(med[i])))
-            if not alive[i]:
-                first[i] = False
-                continue
-            st = m.sigma_t
-            smin = m.min_pos_sigma_t
-            rflags = ORIGIN_IN_MEDIUM if (first[i] and origin_in_medium[i]) else 0
-            if smin > 0 and m.has_scattering:
-                s = -math.log(max(u[i], 1e-300)) / smin
-                if s < seglen:
-                    att1 = math.exp(-smin * s)
-                    pdf = smin * att1
-                    rev = pdf if rflags & ORIGIN_IN_MEDIUM else att1
-                    a = tuple(np.exp(-st * s))
-                    full[i].append((s0[i], s0[i] + s, pdf, rev, a, int(med[i])))
-                    scatter_t[i] = s0[i] + s
-                    alive[i] = False
-                else:
-                    att1 = math.exp(-smin * seglen)
-                    pdf = att1
-                    rev = smin * att1 if rflags & ORIGIN_IN_MEDIUM else att1
-                    a = tuple(np.exp(-st * seglen))
-                    full[i].append((s0[i], s1[i], pdf, rev, a, int(med[i])))
-            else:
-                a = tuple(np.exp(-st * seglen))
-                full[i].append((s0[i], s1[i], 1.0, 1.0, a, int(med[i])))
-            first[i] = False
-    return full, lite, scatter_t
+        med[:, k] = _medium_at(cfg, o + d * mids[:, k:k + 1])
+    st_tab = np.array([m.sigma_t for m in cfg.media])                 # (M, 3)
+    smin_tab = np.array([m.min_pos_sigma_t for m in cfg.media])
+    scat_tab = np.array([m.has_scattering for m in cfg.media])
+    u = rng.random((n, K))
+    np.seterr(invalid="ignore")
+    alive = np.ones(n, bool)
+    full = np.zeros((n, K), bool)
+    dmax = ends.copy()
+    pdf = np.ones((n, K))
+    rev = np.ones((n, K))
+    att = np.ones((n, K, 3))
+    scatter_t = np.full(n, np.inf)
+    for k in range(K):
+        v = valid[:, k]
+        m = med[:, k]
+        seglen = np.where(v, ends[:, k] - starts[:, k], 0.0)
+        smin = smin_tab[m]
+        sampled = v & alive & scat_tab[m] & (smin > 0)
+        full[:, k] = v & alive
+        first = np.full(n, k == 0) & origin_in_medium
+        with np.errstate(divide="ignore", invalid="ignore"):
+            s = -np.log(np.maximum(u[:, k], 1e-300)) / np.where(smin > 0, smin, 1.0)
+        hit = sampled & (s < seglen)
+        through = sampled & ~hit
+        a_hit = np.exp(-smin * s)
+        a_thr = np.exp(-smin * seglen)
+        pdf[:, k] = np.where(hit, smin * a_hit, np.where(through, a_thr, 1.0))
+        rev[:, k] = np.where(hit, np.where(first, smin * a_hit, a_hit),
+                             np.where(through, np.where(first, smin * a_thr, a_thr), 1.0))
+        ln = np.where(hit, s, seglen)
+        att[:, k, :] = np.exp(-st_tab[m] * ln[:, None])
+        dmax[:, k] = np.where(hit, starts[:, k] + s, ends[:, k])
+        scatter_t = np.where(hit, starts[:, k] + s, scatter_t)
+        alive &= ~hit
+    lite = valid & scat_tab[med]
+    return dict(K=K, dmin=starts, dmax_full=dmax, dmax_lite=ends, pdf=pdf, rev=rev, att=att, med=med, full=full,
+                lite=lite, scatter_t=scatter_t)
 
 
 def _hg_sample(rng: np.random.Generator, wfix: np.ndarray, g: np.ndarray):
@@ -294,13 +293,45 @@ def _mis_record(**kw) -> tuple:
     return tuple(vals) + (int(kw.get("flags", 0)),)
 
 
+def _media_tables(cfg: SceneConfig):
+    M = cfg.media
+    return dict(st=np.array([m.sigma_t for m in M]), ss=np.array([np.asarray(m.scattering, float) for m in M]),
+                smin=np.array([m.min_pos_sigma_t for m in M]), scat=np.array([m.has_scattering for m in M]),
+                mfp=np.array([m.mfp for m in M]), g=np.array([m.mean_cosine for m in M]),
+                cont=np.array([m.continuation_prob for m in M]),
+                maxlen=np.array([(-math.log(1e-9) / m.sigma_t.max()) if m.sigma_t.max() > 0 else math.inf for m in M]))
+
+
+def _new_mis(n: int) -> np.ndarray:
+    return np.zeros(n, MIS_DTYPE)
+
+
+def _full_products(tr, sel: np.ndarray):
+    """Products over the VolumeSegments of rays `sel`: pdf, rev pdf and attenuation."""
+    f = tr["full"][sel]
+    rsp = np.prod(np.where(f, tr["pdf"][sel], 1.0), axis=1)
+    rsr = np.prod(np.where(f, tr["rev"][sel], 1.0), axis=1)
+    att = np.prod(np.where(f[:, :, None], tr["att"][sel], 1.0), axis=1)
+    return rsp, rsr, att
+
+
+def _last_full_medium(tr, sel: np.ndarray) -> np.ndarray:
+    f = tr["full"][sel]
+    last = f.shape[1] - 1 - np.argmax(f[:, ::-1], axis=1)
+    return tr["med"][sel][np.arange(len(last)), last]
+
+
 def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     """Run the light and camera passes of one iteration and return the estimator-stage inputs."""
     rng = np.random.Generator(np.random.Philox(key=cfg.seed + iteration))
     k = iteration_constants(cfg, iteration)
     tech = cfg.techniques
     merge_pb2d = bool(tech & PB2D)
-    media = cfg.media
+    T = _media_tables(cfg)
+    maxL = cfg.max_path_length
+    min_mfp = k["bb1d_min_mfp"]
+    beam_ok_med = T["scat"] & (~np.bool_(merge_pb2d) | (T["mfp"] > min_mfp))
+    in_beams_med = (~np.bool_(merge_pb2d)) | (T["mfp"] > min_mfp)
 
     # ------------------------------------------------------------------ light pass
     NL = cfg.light_paths
@@ -308,218 +339,195 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     area = cfg.light_size * cfg.light_size
     lo_box, hi_box = np.asarray(cfg.boxes[0][0], float), np.asarray(cfg.boxes[0][1], float)
     cx, cz = 0.5 * (lo_box[0] + hi_box[0]), 0.5 * (lo_box[2] + hi_box[2])
-    pos = np.stack([cx - half + cfg.light_size * rng.random(NL), np.full(NL, hi_box[1]),
-                    cz - half + cfg.light_size * rng.random(NL)], axis=1)
+    pos0 = np.stack([cx - half + cfg.light_size * rng.random(NL), np.full(NL, hi_box[1]),
+                     cz - half + cfg.light_size * rng.random(NL)], axis=1)
     u1, u2 = rng.random(NL), rng.random(NL)
-    # SampleCosHemisphereW around the light normal (-y)
     r_ = np.sqrt(u1)
     phi = 2 * math.pi * u2
-    cos_l = np.maximum(np.sqrt(np.maximum(0.0, 1 - u1)), EPS_COSINE)
+    cos_l = np.maximum(np.sqrt(np.maximum(0.0, 1 - u1)), EPS_COSINE)   # SampleCosHemisphereW around -y
     dirs = np.stack([r_ * np.cos(phi), -cos_l, r_ * np.sin(phi)], axis=1)
     dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
     emission_pdf_w = cos_l * INV_PI / area
     direct_pdf_a = np.full(NL, 1.0 / area)
 
-    lv: Dict[str, list] = {k_: [] for k_ in ("position", "throughput", "dir_fix", "cont_prob", "path_idx",
-                                              "path_length", "medium_id", "flags", "mis")}
-    beams: Dict[str, list] = {k_: [] for k_ in ("origin", "direction", "length", "throughput", "flags",
-                                                 "ray_sample_pdf", "ray_sample_rev_pdf", "ray_sampling_flags",
-                                                 "last_pdf_w_inv", "medium_id", "light_vertex")}
-    path_ends = np.zeros(NL, np.int32)
-
-    # per-path state arrays
-    thr = np.tile(np.full(3, cfg.light_intensity), (NL, 1)) * cos_l[:, None] / emission_pdf_w[:, None]
-    last_pdf_w_inv = direct_pdf_a / emission_pdf_w
-    origin = pos.copy()
+    # vertex records per bounce; bounce b holds the vertices of path length b
+    V: List[Dict[str, np.ndarray]] = []
+    m0 = _new_mis(NL)
+    m0["pdf_a_inv"] = 1.0 / direct_pdf_a
+    m0["rev_pdf_a"] = cos_l
+    m0["rev_pdf_a_without_bsdf"] = cos_l
+    m0["ray_sample_rev_pdf_inv"] = 1.0
+    m0["cos_theta_out"] = cos_l
+    m0["flags"] = MIS_ON_LIGHT_SOURCE
+    V.append(dict(path=np.arange(NL), pos=pos0, thr=np.ones((NL, 3)), dir_fix=np.zeros((NL, 3)), cont=np.ones(NL),
+                  med=np.full(NL, -1, np.int32), flags=np.full(NL, LV_IS_FINITE, np.uint32), mis=m0))
+    B: List[Dict[str, np.ndarray]] = []   # beams per bounce
+    act = np.arange(NL)
+    origin = pos0.copy()
     direction = dirs.copy()
-    origin_in_med = np.zeros(NL, bool)
-    # records are appended path by path; to keep paths contiguous we build per-path lists first
-    per_path_lv: List[list] = [[] for _ in range(NL)]
-    per_path_beams: List[list] = [[] for _ in range(NL)]
-    for p in range(NL):
-        per_path_lv[p].append(dict(
-            position=pos[p], throughput=(1.0, 1.0, 1.0), dir_fix=(0.0, 0.0, 0.0), cont_prob=1.0, path_idx=p,
-            path_length=0, medium_id=-1, flags=LV_IS_FINITE,
-            mis=dict(pdf_a_inv=1.0 / direct_pdf_a[p], rev_pdf_a=cos_l[p], rev_pdf_a_without_bsdf=cos_l[p],
-                     ray_sample_pdf_inv=0.0, ray_sample_rev_pdf_inv=1.0, cos_theta_out=cos_l[p],
-                     flags=MIS_ON_LIGHT_SOURCE)))
-    active = np.arange(NL)
-    path_len = 1
-    while active.size and cfg.max_path_length > 1:
-        o = origin[active]
-        d = direction[active]
-        full, lite, st = _trace(cfg, rng, o, d, origin_in_med[active])
-        # AddBeams (UPBP.hxx:532-535 -> 1783-1870) from the ray of this segment
-        for j, p in enumerate(active):
-            prev_idx = len(per_path_lv[p]) - 1
-            oflag = ORIGIN_IN_MEDIUM if origin_in_med[p] else 0
-            t3 = np.array(thr[p], np.float64)
-            rsp, rsr = 1.0, 1.0
-            if cfg.photon_beam_type == SHORT_BEAM:
-                for si, (d0, d1, pdf, rev, att, mid) in enumerate(full[j]):
-                    m = media[mid]
-                    if m.has_scattering and (not merge_pb2d or m.mfp > k["bb1d_min_mfp"]):
-                        per_path_beams[p].append(dict(
-                            origin=o[j] + d[j] * d0, direction=d[j], length=d1 - d0, throughput=t3.copy(),
-                            flags=SHORT_BEAM, ray_sample_pdf=rsp, ray_sample_rev_pdf=rsr,
-                            ray_sampling_flags=END_IN_MEDIUM | (oflag if si == 0 else 0),
-                            last_pdf_w_inv=last_pdf_w_inv[p], medium_id=mid, light_vertex=prev_idx))
-                    t3 = t3 * np.asarray(att) / pdf
-                    rsp *= pdf
-                    rsr *= rev
-            else:
-                lite_all = [(s0, s1, mid) for (s0, s1, mid) in lite[j]]
-                for si, (d0, d1, mid) in enumerate(lite_all):
-                    m = media[mid]
-                    added = False
-                    if m.has_scattering and (not merge_pb2d or m.mfp > k["bb1d_min_mfp"]):
-                        per_path_beams[p].append(dict(
-                            origin=o[j] + d[j] * d0, direction=d[j], length=d1 - d0, throughput=t3.copy(),
-                            flags=LONG_BEAM, ray_sample_pdf=rsp, ray_sample_rev_pdf=rsr,
-                            ray_sampling_flags=END_IN_MEDIUM | (oflag if si == 0 else 0),
-                            last_pdf_w_inv=last_pdf_w_inv[p], medium_id=mid, light_vertex=prev_idx))
-                        added = True
-                    seglen = d1 - d0
-                    t3 = t3 * np.exp(-m.sigma_t * seglen)
-                    smin = m.min_pos_sigma_t
-                    if smin > 0 and m.has_scattering:
-                        att1 = max(math.exp(-smin * seglen), 1e-35)
-                        spdf = att1
-                        srev = smin * att1 if (si == 0 and oflag) else att1
-                    else:
-                        spdf = srev = 1.0
-                    rsp *= spdf
-                    rsr *= srev
-                # cap the last beam of this ray (UPBP.hxx:1867-1868; config cap on top)
-                if per_path_beams[p] and per_path_beams[p][-1]["light_vertex"] == prev_idx:
-                    b = per_path_beams[p][-1]
-                    cap = min(media[b["medium_id"]].sigma_t.max() and (-math.log(1e-9) / media[b["medium_id"]].sigma_t.max()) or math.inf,
-                              cfg.beam_length_cap)
-                    if b["length"] > cap:
-                        b["length"] = cap
-        # intersect: scattering vertices
-        nxt = []
-        scattered = np.isfinite(st)
-        for j, p in enumerate(active):
-            if not scattered[j]:
+    thr = np.tile(np.full(3, cfg.light_intensity), (NL, 1)) * cos_l[:, None] / emission_pdf_w[:, None]
+    lpw = direct_pdf_a / emission_pdf_w
+    oim = np.zeros(NL, bool)
+    prev_row = np.arange(NL)          # row of each active path's last vertex in V[L-1]
+    L = 1
+    while act.size and maxL > 1:
+        o, d = origin[act], direction[act]
+        tr = _trace(cfg, rng, o, d, oim[act])
+        K = tr["K"]
+        # ---- UPBP::AddBeams (UPBP.hxx:1783-1870) for the ray of this segment
+        bl = []
+        t3 = thr[act].copy()
+        rsp = np.ones(len(act))
+        rsr = np.ones(len(act))
+        if cfg.photon_beam_type == SHORT_BEAM:
+            for kk in range(K):
+                f = tr["full"][:, kk]
+                mk = tr["med"][:, kk]
+                ok = f & beam_ok_med[mk]
+                bl.append(dict(sel=np.nonzero(ok)[0], kk=kk, origin=o + d * tr["dmin"][:, kk:kk + 1],
+                               length=tr["dmax_full"][:, kk] - tr["dmin"][:, kk], thr=t3.copy(), rsp=rsp.copy(),
+                               rsr=rsr.copy(), flags=SHORT_BEAM,
+                               rsf=END_IN_MEDIUM | np.where((kk == 0) & oim[act], ORIGIN_IN_MEDIUM, 0), med=mk))
+                t3 = np.where(f[:, None], t3 * tr["att"][:, kk] / tr["pdf"][:, kk:kk + 1], t3)
+                rsp = np.where(f, rsp * tr["pdf"][:, kk], rsp)
+                rsr = np.where(f, rsr * tr["rev"][:, kk], rsr)
+        else:
+            first_lite = np.argmax(tr["lite"], axis=1)
+            for kk in range(K):
+                f = tr["lite"][:, kk]
+                mk = tr["med"][:, kk]
+                ok = f & beam_ok_med[mk]
+                seglen = tr["dmax_lite"][:, kk] - tr["dmin"][:, kk]
+                isfirst = (first_lite == kk) & oim[act]
+                bl.append(dict(sel=np.nonzero(ok)[0], kk=kk, origin=o + d * tr["dmin"][:, kk:kk + 1],
+                               length=seglen.copy(), thr=t3.copy(), rsp=rsp.copy(), rsr=rsr.copy(), flags=LONG_BEAM,
+                               rsf=END_IN_MEDIUM | np.where(isfirst, ORIGIN_IN_MEDIUM, 0), med=mk))
+                with np.errstate(invalid="ignore"):
+                    t3 = np.where(f[:, None], t3 * np.exp(-T["st"][mk] * np.where(f, seglen, 0.0)[:, None]), t3)
+                smin = T["smin"][mk]
+                a1 = np.maximum(np.exp(-smin * np.where(f, seglen, 0.0)), 1e-35)
+                samp = f & (smin > 0) & T["scat"][mk]
+                rsp = np.where(samp, rsp * a1, rsp)
+                rsr = np.where(samp, rsr * np.where(isfirst, smin * a1, a1), rsr)
+            # cap the last beam of the ray (UPBP.hxx:1867-1868) and the configured cap
+            last_k = np.full(len(act), -1)
+            for e in bl:
+                last_k[e["sel"]] = e["kk"]
+            for e in bl:
+                s = e["sel"][last_k[e["sel"]] == e["kk"]]
+                cap = np.minimum(T["maxlen"][e["med"][s]], cfg.beam_length_cap)
+                e["length"][s] = np.minimum(e["length"][s], cap)
+        for e in bl:
+            s = e["sel"]
+            if s.size == 0:
                 continue
-            segs = full[j]
-            rsp = float(np.prod([s[2] for s in segs])) if segs else 1.0
-            rsr = float(np.prod([s[3] for s in segs])) if segs else 1.0
-            att = np.prod(np.asarray([s[4] for s in segs]), axis=0) if segs else np.ones(3)
-            thr[p] = thr[p] * att / rsp
-            if not np.any(thr[p] > 0):
-                continue
-            mid = segs[-1][5]
-            m = media[mid]
-            hit = o[j] + d[j] * st[j]
-            dist2 = st[j] * st[j]
-            rsp_inv = 1.0 / rsp
-            flags = 0
-            if (not merge_pb2d) or m.mfp > k["bb1d_min_mfp"]:
-                flags |= MIS_IN_MEDIUM_WITH_BEAMS
-            ratio = 1.0 / m.min_pos_sigma_t
-            rec = dict(pdf_a_inv=last_pdf_w_inv[p] * dist2 * rsp_inv, rev_pdf_a=1.0, rev_pdf_a_without_bsdf=1.0,
-                       ray_sample_pdf_inv=rsp_inv, ray_sample_rev_pdf_inv=1.0, sin_theta=0.0, cos_theta_out=0.0,
-                       surf_factor=0.0, pp3d_factor=k["eta_pp3d"], pb2d_factor=k["eta_pb2d"],
-                       bb1d_factor=k["eta_bb1d"], bb1d_beam_selection_pdf=1.0,
-                       ray_sample_pdfs_ratio=ratio, ray_sample_rev_pdfs_ratio=ratio, flags=flags)
-            prev = per_path_lv[p][-1]["mis"]
-            prev["rev_pdf_a"] = prev.get("rev_pdf_a", 0.0) * rsr / dist2
-            prev["rev_pdf_a_without_bsdf"] = prev["rev_pdf_a"]
-            prev["ray_sample_rev_pdf_inv"] = 1.0 / rsr
-            per_path_lv[p].append(dict(position=hit, throughput=thr[p].copy(), dir_fix=-d[j],
-                                       cont_prob=m.continuation_prob, path_idx=p, path_length=path_len,
-                                       medium_id=mid, flags=LV_IN_MEDIUM | LV_CONNECTABLE | LV_IS_FINITE, mis=rec))
-            origin[p] = hit
-            origin_in_med[p] = True
-            if path_len + 2 > cfg.max_path_length:
-                continue
-            nxt.append((j, p))
-        if not nxt:
+            B.append(dict(path=act[s], lvlen=np.full(s.size, L - 1), kk=np.full(s.size, e["kk"]),
+                          origin=e["origin"][s], direction=d[s], length=e["length"][s], thr=e["thr"][s],
+                          flags=np.full(s.size, e["flags"], np.uint32), rsp=e["rsp"][s], rsr=e["rsr"][s],
+                          rsf=np.asarray(e["rsf"])[s].astype(np.uint32) if np.ndim(e["rsf"]) else np.full(s.size, e["rsf"], np.uint32),
+                          lpw=lpw[act[s]], med=e["med"][s]))
+        # ---- scattering vertices (UPBP.hxx:560-655)
+        sc = np.nonzero(np.isfinite(tr["scatter_t"]))[0]
+        rsp_s, rsr_s, att_s = _full_products(tr, sc)
+        pth = act[sc]
+        new_thr = thr[pth] * att_s / rsp_s[:, None]
+        ok = np.any(new_thr > 0, axis=1)
+        sc, pth, rsp_s, rsr_s, new_thr = sc[ok], pth[ok], rsp_s[ok], rsr_s[ok], new_thr[ok]
+        thr[pth] = new_thr
+        st = tr["scatter_t"][sc]
+        hit = o[sc] + d[sc] * st[:, None]
+        mid = _last_full_medium(tr, sc)
+        dist2 = st * st
+        mis = _new_mis(len(sc))
+        mis["pdf_a_inv"] = lpw[pth] * dist2 / rsp_s
+        mis["rev_pdf_a"] = 1.0
+        mis["rev_pdf_a_without_bsdf"] = 1.0
+        mis["ray_sample_pdf_inv"] = 1.0 / rsp_s
+        mis["ray_sample_rev_pdf_inv"] = 1.0
+        mis["pp3d_factor"] = k["eta_pp3d"]
+        mis["pb2d_factor"] = k["eta_pb2d"]
+        mis["bb1d_factor"] = k["eta_bb1d"]
+        mis["bb1d_beam_selection_pdf"] = 1.0
+        mis["ray_sample_pdfs_ratio"] = 1.0 / T["smin"][mid]
+        mis["ray_sample_rev_pdfs_ratio"] = 1.0 / T["smin"][mid]
+        mis["flags"] = np.where(in_beams_med[mid], MIS_IN_MEDIUM_WITH_BEAMS, 0)
+        pm = V[L - 1]["mis"]
+        pr = prev_row[sc]
+        pm["rev_pdf_a"][pr] = pm["rev_pdf_a"][pr] * rsr_s / dist2
+        pm["rev_pdf_a_without_bsdf"][pr] = pm["rev_pdf_a"][pr]
+        pm["ray_sample_rev_pdf_inv"][pr] = 1.0 / rsr_s
+        V.append(dict(path=pth, pos=hit, thr=new_thr.copy(), dir_fix=-d[sc], cont=T["cont"][mid], med=mid.astype(np.int32),
+                      flags=np.full(len(sc), LV_IN_MEDIUM | LV_CONNECTABLE | LV_IS_FINITE, np.uint32), mis=mis))
+        origin[pth] = hit
+        oim[pth] = True
+        cont_ok = np.full(len(sc), L + 2 <= maxL)
+        rows = np.nonzero(cont_ok)[0]
+        if rows.size == 0:
             break
-        js = np.array([j for j, _ in nxt])
-        ps = np.array([p for _, p in nxt])
-        gs = np.array([media[per_path_lv[p][-1]["medium_id"]].mean_cosine for p in ps])
-        wfix = -d[js]
-        wnew, pdfw, sin_t = _hg_sample(rng, wfix, gs)
-        rr = rng.random(len(ps))
-        cont = np.array([media[per_path_lv[p][-1]["medium_id"]].continuation_prob for p in ps])
+        # ---- SampleScattering (UPBP.hxx:1908-1969): HG direction, Russian roulette
+        gvals = T["g"][mid[rows]]
+        wnew, pdfw, sin_t = _hg_sample(rng, -d[sc[rows]], gvals)
+        rr = rng.random(rows.size)
+        cont = T["cont"][mid[rows]]
         keep = ~((cont == 0) | ((cont < 1) & (rr > cont)))
-        survivors = []
-        for t_, p in enumerate(ps):
-            if not keep[t_]:
-                continue
-            m = media[per_path_lv[p][-1]["medium_id"]]
-            dir_pdf = pdfw[t_] * cont[t_]
-            rev_pdf = pdfw[t_] * cont[t_]  # HG is symmetric: reverse pdf equals forward pdf
-            thr[p] = thr[p] * np.asarray(m.scattering) * pdfw[t_] / dir_pdf
-            last_pdf_w_inv[p] = 1.0 / dir_pdf
-            cur = per_path_lv[p][-1]["mis"]
-            cur["rev_pdf_a_without_bsdf"] = cur["rev_pdf_a"]
-            cur["sin_theta"] = sin_t[t_]
-            cur["cos_theta_out"] = 1.0
-            per_path_lv[p][-2]["mis"]["rev_pdf_a"] *= rev_pdf
-            direction[p] = wnew[t_]
-            survivors.append(p)
-        active = np.array(survivors, dtype=np.int64)
-        path_len += 1
+        rows, wnew, pdfw, sin_t, cont = rows[keep], wnew[keep], pdfw[keep], sin_t[keep], cont[keep]
+        p2 = pth[rows]
+        dir_pdf = pdfw * cont
+        thr[p2] = thr[p2] * T["ss"][mid[rows]] * (pdfw / dir_pdf)[:, None]
+        lpw[p2] = 1.0 / dir_pdf
+        cm = V[L]["mis"]
+        cm["rev_pdf_a_without_bsdf"][rows] = cm["rev_pdf_a"][rows]
+        cm["sin_theta"][rows] = sin_t
+        cm["cos_theta_out"][rows] = 1.0
+        pm["rev_pdf_a"][prev_row[sc[rows]]] *= dir_pdf   # reverse pdf of the previous vertex (HG is symmetric)
+        direction[p2] = wnew
+        act = p2
+        prev_row = rows  # row of each surviving path's vertex in V[L], by position in act
+        L += 1
 
-    # flatten light vertices and beams
-    lv_base = np.zeros(NL + 1, np.int64)
-    for p in range(NL):
-        lv_base[p + 1] = lv_base[p] + len(per_path_lv[p])
-    n_lv = int(lv_base[-1])
+    # ---- flatten light vertices in path order (path p, increasing path length)
+    keys = np.concatenate([v["path"].astype(np.int64) * maxL + b for b, v in enumerate(V)])
+    order = np.argsort(keys, kind="stable")
+    cat = lambda f: np.concatenate([v[f] for v in V])[order]
     out: Dict[str, np.ndarray] = {}
-    out["lv_position"] = np.zeros((n_lv, 3), np.float32)
-    out["lv_throughput"] = np.zeros((n_lv, 3), np.float32)
-    out["lv_dir_fix"] = np.zeros((n_lv, 3), np.float32)
-    out["lv_cont_prob"] = np.zeros(n_lv, np.float32)
-    out["lv_path_idx"] = np.zeros(n_lv, np.int32)
-    out["lv_path_length"] = np.zeros(n_lv, np.int32)
-    out["lv_medium_id"] = np.zeros(n_lv, np.int32)
-    out["lv_flags"] = np.zeros(n_lv, np.uint32)
-    mis = np.zeros(n_lv, MIS_DTYPE)
-    bl = []
-    i = 0
-    for p in range(NL):
-        for v in per_path_lv[p]:
-            out["lv_position"][i] = v["position"]
-            out["lv_throughput"][i] = v["throughput"]
-            out["lv_dir_fix"][i] = v["dir_fix"]
-            out["lv_cont_prob"][i] = v["cont_prob"]
-            out["lv_path_idx"][i] = v["path_idx"]
-            out["lv_path_length"][i] = v["path_length"]
-            out["lv_medium_id"][i] = v["medium_id"]
-            out["lv_flags"][i] = v["flags"]
-            mis[i] = _mis_record(**v["mis"])
-            i += 1
-        path_ends[p] = i
-        for b in per_path_beams[p]:
-            b = dict(b)
-            b["light_vertex"] = int(lv_base[p] + b["light_vertex"])
-            bl.append(b)
-    out["lv_mis"] = mis
-    out["lv_path_ends"] = path_ends
-    nb = len(bl)
-    out["beam_origin"] = np.array([b["origin"] for b in bl], np.float32).reshape(nb, 3)
-    out["beam_direction"] = np.array([b["direction"] for b in bl], np.float32).reshape(nb, 3)
-    out["beam_length"] = np.array([b["length"] for b in bl], np.float32)
-    out["beam_throughput"] = np.array([b["throughput"] for b in bl], np.float32).reshape(nb, 3)
-    out["beam_flags"] = np.array([b["flags"] for b in bl], np.uint32)
-    out["beam_ray_sample_pdf"] = np.array([b["ray_sample_pdf"] for b in bl], np.float32)
-    out["beam_ray_sample_rev_pdf"] = np.array([b["ray_sample_rev_pdf"] for b in bl], np.float32)
-    out["beam_ray_sampling_flags"] = np.array([b["ray_sampling_flags"] for b in bl], np.uint32)
-    out["beam_last_pdf_w_inv"] = np.array([b["last_pdf_w_inv"] for b in bl], np.float32)
-    out["beam_medium_id"] = np.array([b["medium_id"] for b in bl], np.int32)
-    out["beam_light_vertex"] = np.array([b["light_vertex"] for b in bl], np.int32)
+    out["lv_position"] = cat("pos").astype(np.float32)
+    out["lv_throughput"] = cat("thr").astype(np.float32)
+    out["lv_dir_fix"] = cat("dir_fix").astype(np.float32)
+    out["lv_cont_prob"] = cat("cont").astype(np.float32)
+    out["lv_path_idx"] = cat("path").astype(np.int32)
+    out["lv_path_length"] = np.concatenate([np.full(len(v["path"]), b) for b, v in enumerate(V)])[order].astype(np.int32)
+    out["lv_medium_id"] = cat("med").astype(np.int32)
+    out["lv_flags"] = cat("flags").astype(np.uint32)
+    out["lv_mis"] = np.concatenate([v["mis"] for v in V])[order]
+    out["lv_path_ends"] = np.cumsum(np.bincount(out["lv_path_idx"], minlength=NL)).astype(np.int32)
+    skeys = keys[order]
+    if B:
+        bk = np.concatenate([b["path"].astype(np.int64) * maxL + b["lvlen"] for b in B])
+        bkk = np.concatenate([b["kk"] for b in B])
+        border = np.lexsort((bkk, bk))
+        bcat = lambda f: np.concatenate([b[f] for b in B])[border]
+        out["beam_origin"] = bcat("origin").astype(np.float32)
+        out["beam_direction"] = bcat("direction").astype(np.float32)
+        out["beam_length"] = bcat("length").astype(np.float32)
+        out["beam_throughput"] = bcat("thr").astype(np.float32)
+        out["beam_flags"] = bcat("flags").astype(np.uint32)
+        out["beam_ray_sample_pdf"] = bcat("rsp").astype(np.float32)
+        out["beam_ray_sample_rev_pdf"] = bcat("rsr").astype(np.float32)
+        out["beam_ray_sampling_flags"] = bcat("rsf").astype(np.uint32)
+        out["beam_last_pdf_w_inv"] = bcat("lpw").astype(np.float32)
+        out["beam_medium_id"] = bcat("med").astype(np.int32)
+        out["beam_light_vertex"] = np.searchsorted(skeys, bk[border]).astype(np.int32)
+    else:
+        for f, dt, sh in (("origin", np.float32, 3), ("direction", np.float32, 3), ("length", np.float32, 0),
+                          ("throughput", np.float32, 3), ("flags", np.uint32, 0), ("ray_sample_pdf", np.float32, 0),
+                          ("ray_sample_rev_pdf", np.float32, 0), ("ray_sampling_flags", np.uint32, 0),
+                          ("last_pdf_w_inv", np.float32, 0), ("medium_id", np.int32, 0), ("light_vertex", np.int32, 0)):
+            out["beam_" + f] = np.zeros((0, 3) if sh else 0, dt)
 
-    # ------------------------------------------------------------------ camera pass
-    _camera_pass(cfg, rng, k, out)
+    _camera_pass(cfg, rng, k, T, out)
 
-    # ------------------------------------------------------------------ media / params
-    med = np.zeros(len(media), MEDIUM_DTYPE)
-    for mi, m in enumerate(media):
+    med = np.zeros(len(cfg.media), MEDIUM_DTYPE)
+    for mi, m in enumerate(cfg.media):
         med[mi] = (m.absorption, m.scattering, m.mean_cosine, m.continuation_prob)
     out["media"] = med
     prm = np.zeros(1, PARAMS_DTYPE)
@@ -545,183 +553,163 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     return out
 
 
-def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float], out: Dict[str, np.ndarray]):
-    """Camera sub-paths (UPBP.hxx:742-1160): record one segment query per traced ray and one PP3D point
-    query per medium vertex, each with the snapshot of the camera MIS records at the call."""
-    W, H = cfg.width, cfg.height
-    npix = W * H
-    media = cfg.media
+def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float], T, out: Dict[str, np.ndarray]):
+    """Camera sub-paths (UPBP.hxx:742-1160): one segment query per traced ray that crosses a scattering
+    medium and one PP3D point query per camera medium vertex, each with the snapshot of
+    mCameraVerticesMisData at the call."""
+    W_, H_ = cfg.width, cfg.height
+    npix = W_ * H_
     tech = cfg.techniques
     merge_pb2d = bool(tech & PB2D)
+    maxL = cfg.max_path_length
+    in_beams_med = (~np.bool_(merge_pb2d)) | (T["mfp"] > k["bb1d_min_mfp"])
     cam = np.asarray(cfg.camera_pos, np.float64)
     tan_half = math.tan(math.radians(cfg.fov_deg) * 0.5)
-    image_plane_dist = W / (2.0 * tan_half)
+    ipd = W_ / (2.0 * tan_half)
     pix = np.arange(npix)
-    px, py = pix % W, pix // W
-    jx, jy = rng.random(npix), rng.random(npix)
-    sx = (px + jx) - W * 0.5
-    sy = (py + jy) - H * 0.5
-    d = np.stack([sx, -sy, np.full(npix, image_plane_dist)], axis=1)
-    d /= np.linalg.norm(d, axis=1, keepdims=True)
-    cos_cam = d[:, 2]
-    cam_pdf_w = (image_plane_dist / cos_cam) ** 2 / cos_cam
-    last_pdf_w_inv = float(npix) / cam_pdf_w
-    origin = np.tile(cam, (npix, 1))
+    sx = (pix % W_ + rng.random(npix)) - W_ * 0.5
+    sy = (pix // W_ + rng.random(npix)) - H_ * 0.5
+    d_all = np.stack([sx, -sy, np.full(npix, ipd)], axis=1)
+    d_all /= np.linalg.norm(d_all, axis=1, keepdims=True)
+    cos_cam = d_all[:, 2]
+    cam_pdf_w = (ipd / cos_cam) ** 2 / cos_cam
+    # active state
+    act = pix.copy()
+    d = d_all
+    o = np.tile(cam, (npix, 1))
     thr = np.ones((npix, 3))
-    origin_in_med = np.zeros(npix, bool)
+    lpw = float(npix) / cam_pdf_w
+    oim = np.zeros(npix, bool)
     stop_bb1d = np.zeros(npix, bool)
-    # per-path camera MIS arrays (list of dict records, index = path length)
-    cmis: List[list] = [[dict(pdf_a_inv=0.0, rev_pdf_a=1.0, flags=0)] for _ in range(npix)]
-
-    sq: Dict[str, list] = {k_: [] for k_ in ("origin", "direction", "seg_begin", "seg_count", "flags", "path_length",
-                                             "last_pdf_w_inv", "throughput", "pixel", "cam_mis_begin")}
-    seg: Dict[str, list] = {k_: [] for k_ in ("dist_min", "dist_max", "pdf", "rev_pdf", "attenuation", "medium")}
-    pq: Dict[str, list] = {k_: [] for k_ in ("position", "dir_fix", "medium_id", "path_length", "throughput",
-                                             "pixel", "cam_mis_begin")}
-    cam_records: List[tuple] = []
-
-    def snapshot(p, count):
-        b = len(cam_records)
-        for rec in cmis[p][:count]:
-            cam_records.append(_mis_record(**rec))
-        return b
-
-    active = np.arange(npix)
+    table = np.zeros((npix, maxL + 1), MIS_DTYPE)
+    table["rev_pdf_a"][:, 0] = 1.0
+    Q: List[dict] = []
+    S: List[dict] = []
+    PQ: List[dict] = []
+    CR: List[np.ndarray] = []
+    n_cam = 0
+    n_seg = 0
     L = 1
-    while active.size:
-        o = origin[active]
-        dd = d[active]
-        full, lite, st = _trace(cfg, rng, o, dd, origin_in_med[active])
-        for j, p in enumerate(active):
-            scattered = np.isfinite(st[j])
-            use_lite = scattered and cfg.query_beam_type == LONG_BEAM
-            if use_lite:
-                segs = [(s0, s1, 1.0, 1.0, (1.0, 1.0, 1.0), mid) for (s0, s1, mid) in lite[j]]
-            else:
-                segs = full[j]
-            has_medium = any(media[s[5]].has_scattering for s in segs)
-            if has_medium:
-                qf = (Q_ORIGIN_IN_MEDIUM if origin_in_med[p] else 0) | (Q_LITE if use_lite else 0)
-                if tech & PB2D:
-                    qf |= Q_PB2D
-                if (tech & BB1D) and not stop_bb1d[p]:
-                    qf |= Q_BB1D
-                sq["origin"].append(o[j])
-                sq["direction"].append(dd[j])
-                sq["seg_begin"].append(len(seg["dist_min"]))
-                sq["seg_count"].append(len(segs))
-                for (s0, s1, pdf, rev, att, mid) in segs:
-                    seg["dist_min"].append(s0)
-                    seg["dist_max"].append(s1)
-                    seg["pdf"].append(pdf)
-                    seg["rev_pdf"].append(rev)
-                    seg["attenuation"].append(att)
-                    seg["medium"].append(mid)
-                sq["flags"].append(qf)
-                sq["path_length"].append(L)
-                sq["last_pdf_w_inv"].append(last_pdf_w_inv[p])
-                sq["throughput"].append(thr[p].copy())
-                sq["pixel"].append(p)
-                sq["cam_mis_begin"].append(snapshot(p, L))
-        nxt = []
-        for j, p in enumerate(active):
-            if not np.isfinite(st[j]):
-                continue
-            segs = full[j]
-            rsp = float(np.prod([s[2] for s in segs]))
-            rsr = float(np.prod([s[3] for s in segs]))
-            att = np.prod(np.asarray([s[4] for s in segs]), axis=0)
-            thr[p] = thr[p] * att / rsp
-            if not np.any(thr[p] > 0):
-                continue
-            mid = segs[-1][5]
-            m = media[mid]
-            hit = o[j] + dd[j] * st[j]
-            dist2 = st[j] * st[j]
-            ratio = 1.0 / m.min_pos_sigma_t
-            flags = 0
-            if (not merge_pb2d) or m.mfp > k["bb1d_min_mfp"]:
-                flags |= MIS_IN_MEDIUM_WITH_BEAMS
-            rec = dict(pdf_a_inv=last_pdf_w_inv[p] * dist2 / rsp, rev_pdf_a=1.0, ray_sample_pdf_inv=1.0 / rsp,
-                       ray_sample_rev_pdf_inv=1.0, ray_sample_pdfs_ratio=ratio, ray_sample_rev_pdfs_ratio=ratio,
-                       pp3d_factor=k["eta_pp3d"], pb2d_factor=k["eta_pb2d"], bb1d_factor=k["eta_bb1d"],
-                       bb1d_beam_selection_pdf=1.0, flags=flags)
-            prev = cmis[p][L - 1]
-            prev["rev_pdf_a"] = prev.get("rev_pdf_a", 0.0) * rsr / dist2
-            prev["ray_sample_rev_pdf_inv"] = 1.0 / rsr
-            cmis[p].append(rec)
-            if L >= cfg.max_path_length:
-                continue
-            if L > 1 or st[j] >= cfg.min_dist_to_med:
-                if tech & PP3D:
-                    pq["position"].append(hit)
-                    pq["dir_fix"].append(-dd[j])
-                    pq["medium_id"].append(mid)
-                    pq["path_length"].append(L)
-                    pq["throughput"].append(thr[p].copy())
-                    pq["pixel"].append(p)
-                    pq["cam_mis_begin"].append(snapshot(p, L + 1))
-            origin[p] = hit
-            origin_in_med[p] = True
-            nxt.append((j, p))
-        if not nxt:
+    while act.size:
+        tr = _trace(cfg, rng, o, d, oim)
+        sc_mask = np.isfinite(tr["scatter_t"])
+        use_lite = sc_mask & (cfg.query_beam_type == LONG_BEAM)
+        seg_mask = np.where(use_lite[:, None], tr["lite"], tr["full"])
+        dmax = np.where(use_lite[:, None], tr["dmax_lite"], tr["dmax_full"])
+        has_med = np.any(seg_mask & T["scat"][tr["med"]], axis=1)
+        qr = np.nonzero(has_med)[0]
+        if qr.size:
+            qf = (np.where(oim[qr], Q_ORIGIN_IN_MEDIUM, 0) | np.where(use_lite[qr], Q_LITE, 0)).astype(np.uint32)
+            if tech & PB2D:
+                qf |= Q_PB2D
+            if tech & BB1D:
+                qf |= np.where(stop_bb1d[qr], 0, Q_BB1D).astype(np.uint32)
+            cnt = seg_mask[qr].sum(axis=1)
+            sm = seg_mask[qr]
+            ii, kk = np.nonzero(sm)
+            rows = qr[ii]
+            lite_rows = use_lite[rows]
+            S.append(dict(dmin=tr["dmin"][rows, kk], dmax=dmax[rows, kk],
+                          pdf=np.where(lite_rows, 1.0, tr["pdf"][rows, kk]),
+                          rev=np.where(lite_rows, 1.0, tr["rev"][rows, kk]),
+                          att=np.where(lite_rows[:, None], 1.0, tr["att"][rows, kk]), med=tr["med"][rows, kk]))
+            begin = n_seg + np.concatenate([[0], np.cumsum(cnt)[:-1]])
+            n_seg += int(cnt.sum())
+            snap = table[qr, :L].reshape(-1)
+            CR.append(snap)
+            Q.append(dict(origin=o[qr], direction=d[qr], seg_begin=begin, seg_count=cnt, flags=qf,
+                          path_length=np.full(qr.size, L), lpw=lpw[qr], thr=thr[qr], pixel=act[qr],
+                          cam_begin=n_cam + np.arange(qr.size) * L))
+            n_cam += snap.size
+        # scattering events: camera vertex in a medium
+        sc = np.nonzero(sc_mask)[0]
+        if sc.size == 0:
             break
-        js = np.array([j for j, _ in nxt])
-        ps = np.array([p for _, p in nxt])
-        gvals = np.array([cfg.media[_medium_of(cfg, origin[p])].mean_cosine for p in ps])
-        wnew, pdfw, sin_t = _hg_sample(rng, -dd[js], gvals)
-        rr = rng.random(len(ps))
-        survivors = []
-        for t_, p in enumerate(ps):
-            m = cfg.media[_medium_of(cfg, origin[p])]
-            cont = m.continuation_prob
-            if cont == 0 or (cont < 1 and rr[t_] > cont):
-                continue
-            dir_pdf = pdfw[t_] * cont
-            thr[p] = thr[p] * np.asarray(m.scattering) * pdfw[t_] / dir_pdf
-            last_pdf_w_inv[p] = 1.0 / dir_pdf
-            cur = cmis[p][L]
-            cur["sin_theta"] = sin_t[t_]
-            cur["cos_theta_out"] = 1.0
-            cmis[p][L - 1]["rev_pdf_a"] = cmis[p][L - 1].get("rev_pdf_a", 0.0) * dir_pdf
-            d[p] = wnew[t_]
-            if tech & BB1D_PREVIOUS:
-                stop_bb1d[p] = True
-            survivors.append(p)
-        active = np.array(survivors, dtype=np.int64)
+        rsp, rsr, att = _full_products(tr, sc)
+        nthr = thr[sc] * att / rsp[:, None]
+        ok = np.any(nthr > 0, axis=1)
+        sc, rsp, rsr, nthr = sc[ok], rsp[ok], rsr[ok], nthr[ok]
+        thr[sc] = nthr
+        st = tr["scatter_t"][sc]
+        hit = o[sc] + d[sc] * st[:, None]
+        mid = _last_full_medium(tr, sc)
+        dist2 = st * st
+        rec = table[sc, L]
+        rec["pdf_a_inv"] = lpw[sc] * dist2 / rsp
+        rec["rev_pdf_a"] = 1.0
+        rec["ray_sample_pdf_inv"] = 1.0 / rsp
+        rec["ray_sample_rev_pdf_inv"] = 1.0
+        rec["ray_sample_pdfs_ratio"] = 1.0 / T["smin"][mid]
+        rec["ray_sample_rev_pdfs_ratio"] = 1.0 / T["smin"][mid]
+        rec["pp3d_factor"] = k["eta_pp3d"]
+        rec["pb2d_factor"] = k["eta_pb2d"]
+        rec["bb1d_factor"] = k["eta_bb1d"]
+        rec["bb1d_beam_selection_pdf"] = 1.0
+        rec["flags"] = np.where(in_beams_med[mid], MIS_IN_MEDIUM_WITH_BEAMS, 0)
+        table[sc, L] = rec
+        prev = table[sc, L - 1]
+        prev["rev_pdf_a"] = prev["rev_pdf_a"] * rsr / dist2
+        prev["ray_sample_rev_pdf_inv"] = 1.0 / rsr
+        table[sc, L - 1] = prev
+        if L >= maxL:
+            break
+        pq_ok = (L > 1) | (st >= cfg.min_dist_to_med)
+        if tech & PP3D:
+            r = np.nonzero(pq_ok)[0]
+            if r.size:
+                snap = table[sc[r], :L + 1].reshape(-1)
+                CR.append(snap)
+                PQ.append(dict(position=hit[r], dir_fix=-d[sc[r]], medium=mid[r], path_length=np.full(r.size, L),
+                               thr=nthr[r], pixel=act[sc[r]], cam_begin=n_cam + np.arange(r.size) * (L + 1)))
+                n_cam += snap.size
+        # SampleScattering at the camera vertex
+        wnew, pdfw, sin_t = _hg_sample(rng, -d[sc], T["g"][mid])
+        rr = rng.random(sc.size)
+        cont = T["cont"][mid]
+        keep = ~((cont == 0) | ((cont < 1) & (rr > cont)))
+        sc, mid, wnew, pdfw, sin_t, cont, hit = sc[keep], mid[keep], wnew[keep], pdfw[keep], sin_t[keep], cont[keep], hit[keep]
+        dir_pdf = pdfw * cont
+        thr[sc] = thr[sc] * T["ss"][mid] * (pdfw / dir_pdf)[:, None]
+        cur = table[sc, L]
+        cur["sin_theta"] = sin_t
+        cur["cos_theta_out"] = 1.0
+        table[sc, L] = cur
+        prev = table[sc, L - 1]
+        prev["rev_pdf_a"] = prev["rev_pdf_a"] * dir_pdf
+        table[sc, L - 1] = prev
+        if tech & BB1D_PREVIOUS:
+            stop_bb1d[sc] = True
+        # compact the active set
+        act, table, thr, stop_bb1d = act[sc], table[sc], thr[sc], stop_bb1d[sc]
+        lpw = 1.0 / dir_pdf
+        o, d, oim = hit, wnew, np.ones(sc.size, bool)
         L += 1
 
-    nq = len(sq["origin"])
-    out["sq_origin"] = np.asarray(sq["origin"], np.float32).reshape(nq, 3)
-    out["sq_direction"] = np.asarray(sq["direction"], np.float32).reshape(nq, 3)
-    out["sq_seg_begin"] = np.asarray(sq["seg_begin"], np.int32)
-    out["sq_seg_count"] = np.asarray(sq["seg_count"], np.int32)
-    out["sq_flags"] = np.asarray(sq["flags"], np.uint32)
-    out["sq_path_length"] = np.asarray(sq["path_length"], np.int32)
-    out["sq_last_pdf_w_inv"] = np.asarray(sq["last_pdf_w_inv"], np.float32)
-    out["sq_throughput"] = np.asarray(sq["throughput"], np.float32).reshape(nq, 3)
-    out["sq_pixel"] = np.asarray(sq["pixel"], np.int32)
-    out["sq_cam_mis_begin"] = np.asarray(sq["cam_mis_begin"], np.int64)
-    ns = len(seg["dist_min"])
-    out["seg_dist_min"] = np.asarray(seg["dist_min"], np.float32)
-    out["seg_dist_max"] = np.asarray(seg["dist_max"], np.float32)
-    out["seg_pdf"] = np.asarray(seg["pdf"], np.float32)
-    out["seg_rev_pdf"] = np.asarray(seg["rev_pdf"], np.float32)
-    out["seg_attenuation"] = np.asarray(seg["attenuation"], np.float32).reshape(ns, 3)
-    out["seg_medium"] = np.asarray(seg["medium"], np.int32)
-    npq = len(pq["position"])
-    out["pq_position"] = np.asarray(pq["position"], np.float32).reshape(npq, 3)
-    out["pq_dir_fix"] = np.asarray(pq["dir_fix"], np.float32).reshape(npq, 3)
-    out["pq_medium_id"] = np.asarray(pq["medium_id"], np.int32)
-    out["pq_path_length"] = np.asarray(pq["path_length"], np.int32)
-    out["pq_throughput"] = np.asarray(pq["throughput"], np.float32).reshape(npq, 3)
-    out["pq_pixel"] = np.asarray(pq["pixel"], np.int32)
-    out["pq_cam_mis_begin"] = np.asarray(pq["cam_mis_begin"], np.int64)
-    cm = np.zeros(len(cam_records), MIS_DTYPE)
-    if cam_records:
-        cm[:] = cam_records
-    out["cam_mis"] = cm
-
-
-def _medium_of(cfg: SceneConfig, p: np.ndarray) -> int:
-    return int(_medium_at(cfg, p[None, :])[0])
+    cat = lambda lst, f, dt: (np.concatenate([x[f] for x in lst]) if lst else np.zeros(0)).astype(dt)
+    nq = sum(len(x["flags"]) for x in Q)
+    out["sq_origin"] = cat(Q, "origin", np.float32).reshape(nq, 3)
+    out["sq_direction"] = cat(Q, "direction", np.float32).reshape(nq, 3)
+    out["sq_seg_begin"] = cat(Q, "seg_begin", np.int32)
+    out["sq_seg_count"] = cat(Q, "seg_count", np.int32)
+    out["sq_flags"] = cat(Q, "flags", np.uint32)
+    out["sq_path_length"] = cat(Q, "path_length", np.int32)
+    out["sq_last_pdf_w_inv"] = cat(Q, "lpw", np.float32)
+    out["sq_throughput"] = cat(Q, "thr", np.float32).reshape(nq, 3)
+    out["sq_pixel"] = cat(Q, "pixel", np.int32)
+    out["sq_cam_mis_begin"] = cat(Q, "cam_begin", np.int64)
+    ns = sum(len(x["dmin"]) for x in S)
+    out["seg_dist_min"] = cat(S, "dmin", np.float32)
+    out["seg_dist_max"] = cat(S, "dmax", np.float32)
+    out["seg_pdf"] = cat(S, "pdf", np.float32)
+    out["seg_rev_pdf"] = cat(S, "rev", np.float32)
+    out["seg_attenuation"] = cat(S, "att", np.float32).reshape(ns, 3)
+    out["seg_medium"] = cat(S, "med", np.int32)
+    npq = sum(len(x["pixel"]) for x in PQ)
+    out["pq_position"] = cat(PQ, "position", np.float32).reshape(npq, 3)
+    out["pq_dir_fix"] = cat(PQ, "dir_fix", np.float32).reshape(npq, 3)
+    out["pq_medium_id"] = cat(PQ, "medium", np.int32)
+    out["pq_path_length"] = cat(PQ, "path_length", np.int32)
+    out["pq_throughput"] = cat(PQ, "thr", np.float32).reshape(npq, 3)
+    out["pq_pixel"] = cat(PQ, "pixel", np.int32)
+    out["pq_cam_mis_begin"] = cat(PQ, "cam_begin", np.int64)
+    out["cam_mis"] = np.concatenate(CR) if CR else np.zeros(0, MIS_DTYPE)
