@@ -13,27 +13,29 @@ import numpy as np
 from smallupbp_b200 import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liboracle.so")
-_lib = None
+LIB_PATH = os.path.join(HERE, "liboracle.so")      # FP32 restatement
+LIB64_PATH = os.path.join(HERE, "liboracle64.so")  # FP64 oracle
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            from . import build_oracle  # noqa: F401  (python oracle/build_oracle.py builds it)
-            raise FileNotFoundError(LIB_PATH + " is not built (python oracle/build_oracle.py)")
-        _lib = C.CDLL(LIB_PATH)
-        _lib.upbp_oracle_run.restype = C.c_int
-        _lib.upbp_oracle_run.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Medium), C.c_int32,
+def lib(fp64: bool = False):
+    path = LIB64_PATH if fp64 else LIB_PATH
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " is not built (python oracle/build_oracle.py)")
+        l = C.CDLL(path)
+        l.upbp_oracle_run.restype = C.c_int
+        l.upbp_oracle_run.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Medium), C.c_int32,
                                          C.POINTER(abi.LightVertices), C.POINTER(abi.Beams), C.POINTER(abi.Mis),
                                          C.POINTER(abi.SegmentQueries), C.POINTER(abi.PointQueries), C.c_int64,
                                          abi.f32p, abi.f32p, abi.f32p, abi.u32p, abi.u64p, abi.u32p, abi.u64p,
                                          abi.u32p, abi.u64p, abi.f32p]
-    return _lib
+        _libs[path] = l
+    return _libs[path]
 
 
-def run(w: Dict[str, np.ndarray], stride: int = 1) -> Dict[str, np.ndarray]:
+def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False) -> Dict[str, np.ndarray]:
+    """Evaluate workload ``w`` with the C restatement (``fp64``: the FP64 oracle build)."""
     s, keep = abi.make_structs(w)
     nq, npq = s["sq"].n, s["pq"].n
     p = s["params"]
@@ -44,7 +46,7 @@ def run(w: Dict[str, np.ndarray], stride: int = 1) -> Dict[str, np.ndarray]:
            "hash_pp3d": np.zeros(npq, np.uint64),
            "image": np.zeros((p.image_width * p.image_height, 3), np.float32)}
     P = abi.ptr
-    rc = lib().upbp_oracle_run(C.byref(p), s["media"], s["n_media"], C.byref(s["lv"]), C.byref(s["beams"]),
+    rc = lib(fp64).upbp_oracle_run(C.byref(p), s["media"], s["n_media"], C.byref(s["lv"]), C.byref(s["beams"]),
                                s["cam_mis"], C.byref(s["sq"]), C.byref(s["pq"]), stride, P(out["pb2d"]),
                                P(out["bb1d"]), P(out["pp3d"]), P(out["count_pb2d"]), P(out["hash_pb2d"]),
                                P(out["count_bb1d"]), P(out["hash_bb1d"]), P(out["count_pp3d"]), P(out["hash_pp3d"]),

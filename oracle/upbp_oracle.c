@@ -26,6 +26,13 @@
  *
  * Compiled with -O2 -ffp-contract=off so that float operations round like the
  * reference's SSE build (no FMA).  Candidates are enumerated by brute force.
+ *
+ * Two builds: ORACLE_REAL=float (liboracle.so, the FP32 restatement) and
+ * ORACLE_REAL=double (liboracle64.so, the FP64 oracle).  Candidate predicates
+ * are always evaluated in the reference's exact FP32 order, so both builds
+ * accept the same candidates; in the FP64 build the candidate geometry
+ * (distances along the rays, closest approach, sin theta) is re-solved in FP64
+ * and all contribution and MIS arithmetic is FP64.
  */
 #include <math.h>
 #include <stdint.h>
@@ -37,35 +44,76 @@
 #define PI_F 3.141592653589793238462643383279f
 #define ORACLE_MAX_MEDIA 64
 
-typedef struct { float x, y, z; } v3;
-typedef struct { float r, g, b; } rgb;
+#ifndef ORACLE_REAL
+#define ORACLE_REAL float
+#endif
+typedef ORACLE_REAL real;
+#define IS_F64 (sizeof(real) == sizeof(double))
 
-typedef struct {
-    float st[3], ss[3], g, cont, min_st, mfp;
-    int min_idx, has_scat;
-} medium;
+static real rexp(real x) { return IS_F64 ? (real)exp((double)x) : (real)expf((float)x); }
+static real rsqrt(real x) { return IS_F64 ? (real)sqrt((double)x) : (real)sqrtf((float)x); }
+static real rabs(real x) { return x < 0 ? -x : x; }
 
-/* ---------------------------------------------------------------- vectors */
+/* float vectors: the candidate predicates, in the reference's exact operation order */
+typedef struct { float x, y, z; } v3f;
+static v3f Vf(const float* p) { v3f v = {p[0], p[1], p[2]}; return v; }
+static v3f subf(v3f a, v3f b) { v3f v = {a.x - b.x, a.y - b.y, a.z - b.z}; return v; }
+static v3f addf(v3f a, v3f b) { v3f v = {a.x + b.x, a.y + b.y, a.z + b.z}; return v; }
+static v3f scalef(v3f a, float s) { v3f v = {a.x * s, a.y * s, a.z * s}; return v; }
+/* _mm_dp_ps(a, b, 0x71): (x*x' + y*y') + (z*z' + 0) */
+static float dotf(v3f a, v3f b) { float xy = a.x * b.x + a.y * b.y; float z = a.z * b.z; return xy + z; }
+static v3f crossf(v3f a, v3f b)
+{
+    v3f v = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return v;
+}
+
+/* real vectors / colours: contribution arithmetic */
+typedef struct { real x, y, z; } v3;
+typedef struct { real r, g, b; } rgb;
 static v3 V(const float* p) { v3 v = {p[0], p[1], p[2]}; return v; }
 static v3 sub(v3 a, v3 b) { v3 v = {a.x - b.x, a.y - b.y, a.z - b.z}; return v; }
-static v3 add(v3 a, v3 b) { v3 v = {a.x + b.x, a.y + b.y, a.z + b.z}; return v; }
-static v3 scale(v3 a, float s) { v3 v = {a.x * s, a.y * s, a.z * s}; return v; }
 static v3 neg(v3 a) { v3 v = {-a.x, -a.y, -a.z}; return v; }
-/* _mm_dp_ps(a, b, 0x71): (x*x' + y*y') + (z*z' + 0) */
-static float dot(v3 a, v3 b) { float xy = a.x * b.x + a.y * b.y; float z = a.z * b.z; return xy + z; }
+static real dot(v3 a, v3 b) { real xy = a.x * b.x + a.y * b.y; real z = a.z * b.z; return xy + z; }
 static v3 cross(v3 a, v3 b)
 {
     v3 v = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
     return v;
 }
 static rgb C3(const float* p) { rgb c = {p[0], p[1], p[2]}; return c; }
-static rgb cs(float v) { rgb c = {v, v, v}; return c; }
+static rgb Cr(const real* p) { rgb c = {p[0], p[1], p[2]}; return c; }
+static rgb cs(real v) { rgb c = {v, v, v}; return c; }
 static rgb cmul(rgb a, rgb b) { rgb c = {a.r * b.r, a.g * b.g, a.b * b.b}; return c; }
-static rgb cscale(rgb a, float s) { rgb c = {a.r * s, a.g * s, a.b * s}; return c; }
-static rgb cdiv(rgb a, float s) { rgb c = {a.r / s, a.g / s, a.b / s}; return c; }
+static rgb cscale(rgb a, real s) { rgb c = {a.r * s, a.g * s, a.b * s}; return c; }
+static rgb cdiv(rgb a, real s) { rgb c = {a.r / s, a.g / s, a.b / s}; return c; }
 static rgb cadd(rgb a, rgb b) { rgb c = {a.r + b.r, a.g + b.g, a.b + b.b}; return c; }
-static float comp(rgb a, int i) { return i == 0 ? a.r : (i == 1 ? a.g : a.b); }
-static int is_pos(float x) { return x > 1e-20f; }                       /* Utils.hxx:109 */
+static real comp(rgb a, int i) { return i == 0 ? a.r : (i == 1 ? a.g : a.b); }
+static int is_pos(real x) { return x > 1e-20f; }                        /* Utils.hxx:109 */
+
+typedef struct {
+    real st[3], ss[3], g, cont, min_st, mfp;
+    int min_idx, has_scat;
+} medium;
+
+/* MisData with real fields (the candidate records are computed in `real`) */
+typedef struct {
+    real pdf_a_inv, rev_pdf_a, rev_pdf_a_without_bsdf, ray_sample_pdf_inv, ray_sample_rev_pdf_inv,
+        ray_sample_pdfs_ratio, ray_sample_rev_pdfs_ratio, sin_theta, cos_theta_out, surf_factor, pp3d_factor,
+        pb2d_factor, bb1d_factor, bb1d_beam_selection_pdf;
+    uint32_t flags;
+} rmis;
+
+static rmis R(const upbp_mis* m)
+{
+    rmis r;
+    r.pdf_a_inv = m->pdf_a_inv; r.rev_pdf_a = m->rev_pdf_a; r.rev_pdf_a_without_bsdf = m->rev_pdf_a_without_bsdf;
+    r.ray_sample_pdf_inv = m->ray_sample_pdf_inv; r.ray_sample_rev_pdf_inv = m->ray_sample_rev_pdf_inv;
+    r.ray_sample_pdfs_ratio = m->ray_sample_pdfs_ratio; r.ray_sample_rev_pdfs_ratio = m->ray_sample_rev_pdfs_ratio;
+    r.sin_theta = m->sin_theta; r.cos_theta_out = m->cos_theta_out; r.surf_factor = m->surf_factor;
+    r.pp3d_factor = m->pp3d_factor; r.pb2d_factor = m->pb2d_factor; r.bb1d_factor = m->bb1d_factor;
+    r.bb1d_beam_selection_pdf = m->bb1d_beam_selection_pdf; r.flags = m->flags;
+    return r;
+}
 static int c_positive(rgb a) { return is_pos(a.r) && is_pos(a.g) && is_pos(a.b); }
 static int c_black_neg(rgb a) { return a.r <= 0.f && a.g <= 0.f && a.b <= 0.f; }
 
@@ -73,12 +121,12 @@ static int c_black_neg(rgb a) { return a.r <= 0.f && a.g <= 0.f && a.b <= 0.f; }
 static medium make_medium(const upbp_medium* m)
 {
     medium d;
-    float mn;
+    real mn;
     int c, idx = 0;
     memset(&d, 0, sizeof d);
     for (c = 0; c < 3; ++c) {
         d.ss[c] = fabsf(m->scattering[c]);
-        d.st[c] = fabsf(m->absorption[c]) + d.ss[c];
+        d.st[c] = (real)fabsf(m->absorption[c]) + d.ss[c];
     }
     mn = d.st[0];
     if (d.st[1] > 0 && (mn == 0 || d.st[1] < mn)) { mn = d.st[1]; idx = 1; }
@@ -87,28 +135,28 @@ static medium make_medium(const upbp_medium* m)
     d.min_idx = idx;
     d.has_scat = d.ss[0] > 0 || d.ss[1] > 0 || d.ss[2] > 0;
     {
-        float mx = d.st[0] > d.st[1] ? d.st[0] : d.st[1];
+        real mx = d.st[0] > d.st[1] ? d.st[0] : d.st[1];
         mx = mx > d.st[2] ? mx : d.st[2];
-        d.mfp = (d.st[0] > 0 || d.st[1] > 0 || d.st[2] > 0) ? 1.0f / mx : INFINITY;
+        d.mfp = (d.st[0] > 0 || d.st[1] > 0 || d.st[2] > 0) ? (real)1 / mx : (real)INFINITY;
     }
     d.g = m->mean_cosine;
     d.cont = m->continuation_prob;
     return d;
 }
 
-static rgb eval_att(const medium* m, float dist)
+static rgb eval_att(const medium* m, real dist)
 {
-    rgb c = {expf(-m->st[0] * dist), expf(-m->st[1] * dist), expf(-m->st[2] * dist)};
+    rgb c = {rexp(-m->st[0] * dist), rexp(-m->st[1] * dist), rexp(-m->st[2] * dist)};
     return c;
 }
 
-static float ray_sample_pdf(const medium* m, float dmin, float dmax, uint32_t flags, float* rev)
+static real ray_sample_pdf(const medium* m, real dmin, real dmax, uint32_t flags, real* rev)
 {
-    float pdf = 1.f;
+    real pdf = 1.f;
     *rev = 1.f;
     if (m->min_st != 0.f && m->has_scat) {
-        float att = expf(-m->min_st * (dmax - dmin));
-        float minatt;
+        real att = rexp(-m->min_st * (dmax - dmin));
+        real minatt;
         if (att < 1e-35f) att = 1e-35f;
         minatt = m->min_st * att;
         pdf = (flags & UPBP_END_IN_MEDIUM) ? minatt : att;
@@ -117,47 +165,47 @@ static float ray_sample_pdf(const medium* m, float dmin, float dmax, uint32_t fl
     return pdf;
 }
 
-static float hg_pdf(v3 fix, v3 gen, float g, float* sin_theta)
+static real hg_pdf(v3 fix, v3 gen, real g, real* sin_theta)
 {
-    const float inv4pi = (1.f / PI_F) * 0.25f;
-    const float cos_t = -dot(gen, fix);
-    float s = 1.f - cos_t * cos_t;
-    *sin_theta = sqrtf(s > 0.f ? s : 0.f);
-    if (fabsf(g) < 1e-3f) return inv4pi;
+    const real inv4pi = IS_F64 ? (real)(0.25 / 3.14159265358979323846) : (real)((1.f / PI_F) * 0.25f);
+    const real cos_t = -dot(gen, fix);
+    real s = 1 - cos_t * cos_t;
+    *sin_theta = rsqrt(s > 0 ? s : 0);
+    if (rabs(g) < 1e-3f) return inv4pi;
     {
-        const float g2 = g * g;
-        const float d = 1.f + g2 - (g + g) * cos_t;
-        return d > 0.f ? (inv4pi * (1.f - g2) / (d * sqrtf(d))) : 0.f;
+        const real g2 = g * g;
+        const real d = 1 + g2 - (g + g) * cos_t;
+        return d > 0 ? (inv4pi * (1 - g2) / (d * rsqrt(d))) : 0;
     }
 }
 
 /* ---------------------------------------------------------------- predicates */
-static int test_bre(v3 o, v3 d, float tmin, float tmax, v3 p, float r2, float* t_out, float* d2_out)
+static int test_bre(v3f o, v3f d, float tmin, float tmax, v3f p, float r2, float* t_out, float* d2_out)
 {
-    const v3 op = sub(p, o);
-    const float t = dot(op, d);
+    const v3f op = subf(p, o);
+    const float t = dotf(op, d);
     if (t > tmin && t < tmax) {
-        const v3 q = sub(add(o, scale(d, t)), p);
-        const float d2 = dot(q, q);
+        const v3f q = subf(addf(o, scalef(d, t)), p);
+        const float d2 = dotf(q, q);
         if (d2 <= r2) { *t_out = t; *d2_out = d2; return 1; }
     }
     return 0;
 }
 
-static int test_beam_beam(v3 O1, v3 d1, float minT1, float maxT1, v3 O2, v3 d2, float minT2, float maxT2,
+static int test_beam_beam(v3f O1, v3f d1, float minT1, float maxT1, v3f O2, v3f d2, float minT2, float maxT2,
                           float maxDistSqr, float* oDist, float* oSin, float* oT1, float* oT2)
 {
-    const v3 c = cross(d1, d2);
-    const float sinThetaSqr = dot(c, c);
-    const float ad = dot(sub(O2, O1), c);
+    const v3f c = crossf(d1, d2);
+    const float sinThetaSqr = dotf(c, c);
+    const float ad = dotf(subf(O2, O1), c);
     float d1d2, d1d2SqrMinus1, d1O1, d1O2, t1, t2, s;
     if (ad * ad >= maxDistSqr * sinThetaSqr) return 0;
-    d1d2 = dot(d1, d2);
+    d1d2 = dotf(d1, d2);
     d1d2SqrMinus1 = d1d2 * d1d2 - 1.0f;
     if (d1d2SqrMinus1 < 1e-5f && d1d2SqrMinus1 > -1e-5f) return 0;
-    d1O1 = dot(d1, O1);
-    d1O2 = dot(d1, O2);
-    t1 = (d1O1 - d1O2 - d1d2 * (dot(d2, O1) - dot(d2, O2))) / d1d2SqrMinus1;
+    d1O1 = dotf(d1, O1);
+    d1O2 = dotf(d1, O2);
+    t1 = (d1O1 - d1O2 - d1d2 * (dotf(d2, O1) - dotf(d2, O2))) / d1d2SqrMinus1;
     if (t1 <= minT1 || t1 >= maxT1) return 0;
     t2 = (t1 + d1O1 - d1O2) / d1d2;
     if (t2 <= minT2 || t2 >= maxT2 || isnan(t2)) return 0;
@@ -173,31 +221,31 @@ static int test_beam_beam(v3 O1, v3 d1, float minT1, float maxT1, v3 O2, v3 d2, 
 typedef struct {
     const upbp_mis* snap; /* camera snapshot (entries 0..) */
     int L;
-    const upbp_mis* cand; /* entry L during an estimator call, or NULL (read from snapshot) */
+    const rmis* cand;      /* entry L during an estimator call, or NULL (read from snapshot) */
     int prev_override;
-    float prev_ray_rev_inv;
+    real prev_ray_rev_inv;
 } cam_view;
 
-static upbp_mis cam_at(const cam_view* c, int k)
+static rmis cam_at(const cam_view* c, int k)
 {
-    upbp_mis m;
+    rmis m;
     if (c->cand && k == c->L) return *c->cand;
-    m = c->snap[k];
+    m = R(&c->snap[k]);
     if (c->prev_override && k == c->L - 1) m.ray_sample_rev_pdf_inv = c->prev_ray_rev_inv;
     return m;
 }
 
-static int spec(const upbp_mis* m) { return (m->flags & UPBP_MIS_IS_SPECULAR) != 0; }
+static int spec(const rmis* m) { return (m->flags & UPBP_MIS_IS_SPECULAR) != 0; }
 
-static float camera_path_weight(int L, float lastRev, float lastSin, float lastRayRev, float lastRayRevRatio,
-                                float ntl, uint32_t qbt, uint32_t pbt, uint32_t tech, const cam_view* cam)
+static real camera_path_weight(int L, real lastRev, real lastSin, real lastRayRev, real lastRayRevRatio,
+                               real ntl, uint32_t qbt, uint32_t pbt, uint32_t tech, const cam_view* cam)
 {
-    float weight = 0.f, product = 1.f, weightBB1D = 0.f;
+    real weight = 0, product = 1, weightBB1D = 0;
     int index;
     for (index = 0; index < L; ++index) {
-        const upbp_mis cur = cam_at(cam, L - index);
-        upbp_mis nx = index < L - 1 ? cam_at(cam, L - index - 1) : cur;
-        float rev = cur.rev_pdf_a, sinT = cur.sin_theta, rayRev = cur.ray_sample_rev_pdf_inv,
+        const rmis cur = cam_at(cam, L - index);
+        rmis nx = index < L - 1 ? cam_at(cam, L - index - 1) : cur;
+        real rev = cur.rev_pdf_a, sinT = cur.sin_theta, rayRev = cur.ray_sample_rev_pdf_inv,
               rayRevRatio = cur.ray_sample_rev_pdfs_ratio;
         int usable;
         if ((tech & UPBP_BB1D_PREVIOUS) && !spec(&cur)) weightBB1D = 0.f;
@@ -212,7 +260,7 @@ static float camera_path_weight(int L, float lastRev, float lastSin, float lastR
             else weight += product * cur.pb2d_factor * cur.ray_sample_pdfs_ratio;
         }
         if ((tech & UPBP_BB1D) && (cur.flags & UPBP_MIS_IN_MEDIUM_WITH_BEAMS)) {
-            float a, b;
+            real a, b;
             if (tech & UPBP_NO_SINE_IN_WEIGHTS) sinT = 1.f;
             a = (qbt & UPBP_LONG_BEAM) ? cur.ray_sample_pdf_inv : cur.ray_sample_pdfs_ratio;
             b = (pbt & UPBP_LONG_BEAM) ? rayRev : rayRevRatio;
@@ -227,27 +275,27 @@ static float camera_path_weight(int L, float lastRev, float lastSin, float lastR
 typedef struct {
     const upbp_mis* mis;
     int override_idx;
-    float override_ray_rev_inv;
+    real override_ray_rev_inv;
 } light_view;
 
-static upbp_mis lv_at(const light_view* l, int k)
+static rmis lv_at(const light_view* l, int k)
 {
-    upbp_mis m = l->mis[k];
+    rmis m = R(&l->mis[k]);
     if (k == l->override_idx) m.ray_sample_rev_pdf_inv = l->override_ray_rev_inv;
     return m;
 }
 
-static float light_path_weight(int pathIdx, int pathLength, float lastRev, float lastSin, float lastRayRev,
-                               float lastRayRevRatio, float ntl, uint32_t technique, uint32_t qbt, uint32_t pbt,
-                               uint32_t tech, const int32_t* pathEnds, const light_view* lv, const upbp_mis* beam_rec)
+static real light_path_weight(int pathIdx, int pathLength, real lastRev, real lastSin, real lastRayRev,
+                              real lastRayRevRatio, real ntl, uint32_t technique, uint32_t qbt, uint32_t pbt,
+                              uint32_t tech, const int32_t* pathEnds, const light_view* lv, const rmis* beam_rec)
 {
-    float weight = 0.f, product = 1.f;
+    real weight = 0, product = 1;
     const int lastIndex = (pathIdx == 0) ? pathLength : pathEnds[pathIdx - 1] + pathLength;
     int index;
     for (index = 0; index <= pathLength; ++index) {
-        const upbp_mis cur = (technique == UPBP_BB1D && index == 0) ? *beam_rec : lv_at(lv, lastIndex - index);
-        upbp_mis nx = index < pathLength ? lv_at(lv, lastIndex - index - 1) : cur;
-        float rev = cur.rev_pdf_a, sinT = cur.sin_theta, rayRev = cur.ray_sample_rev_pdf_inv,
+        const rmis cur = (technique == UPBP_BB1D && index == 0) ? *beam_rec : lv_at(lv, lastIndex - index);
+        rmis nx = index < pathLength ? lv_at(lv, lastIndex - index - 1) : cur;
+        real rev = cur.rev_pdf_a, sinT = cur.sin_theta, rayRev = cur.ray_sample_rev_pdf_inv,
               rayRevRatio = cur.ray_sample_rev_pdfs_ratio;
         int usable;
         if (index == 0) { rev = lastRev; sinT = lastSin; rayRev = lastRayRev; rayRevRatio = lastRayRevRatio; }
@@ -263,7 +311,7 @@ static float light_path_weight(int pathIdx, int pathLength, float lastRev, float
                 else weight += product * cur.pb2d_factor * rayRevRatio;
             }
             if ((tech & UPBP_BB1D) && !(tech & UPBP_BB1D_PREVIOUS) && (cur.flags & UPBP_MIS_IN_MEDIUM_WITH_BEAMS)) {
-                float a, b;
+                real a, b;
                 if (tech & UPBP_NO_SINE_IN_WEIGHTS) sinT = 1.f;
                 a = (qbt & UPBP_LONG_BEAM) ? rayRev : rayRevRatio;
                 b = (pbt & UPBP_LONG_BEAM) ? cur.ray_sample_pdf_inv : cur.ray_sample_pdfs_ratio;
@@ -285,7 +333,7 @@ static uint64_t mix64(uint64_t id)
     return z ^ (z >> 31);
 }
 
-static void fill_cand(upbp_mis* c, const upbp_params* P, float pdf_a_inv, float rsp_inv, float ratio, float sel,
+static void fill_cand(rmis* c, const upbp_params* P, real pdf_a_inv, real rsp_inv, real ratio, real sel,
                       uint32_t flags)
 {
     memset(c, 0, sizeof *c);
@@ -314,62 +362,93 @@ typedef struct {
 } oracle;
 
 typedef struct {
-    v3 o, d;
-    float dmin, dmax, rs_pdf, rs_rev;
+    v3f of, df;   /* query ray, float (predicates) */
+    v3 o, d;      /* the same in `real` (contributions) */
+    real dmin, dmax, rs_pdf, rs_rev;
     uint32_t rsf, ray_flags;
     int L;
-    float lpw;
+    real lpw;
     const upbp_mis* snap;
 } seg_ctx;
 
-/* breIntersectFuncHomogeneous2 after testIntersectionBre accepted light vertex j. */
-static rgb pb2d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int64_t j, float t, float d2)
+/* breIntersectFuncHomogeneous2 after testIntersectionBre accepted light vertex j (the FP64
+ * build re-solves t and d2 from the inputs). */
+static rgb pb2d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int64_t j, real t, real d2)
 {
     const upbp_params* P = O->P;
     const upbp_light_vertices* lv = O->lv;
     const int pl = lv->path_length[j];
     rgb att, un;
-    float pdf, rsp, rsr, ratio, sinT, phase, dirPdf, revPdf, r2, kernel, distSq, rspInv, last, wc, wl;
-    upbp_mis cand;
+    real pdf, rsp, rsr, ratio, sinT, phase, dirPdf, revPdf, r2, kernel, distSq, rspInv, last, wc, wl;
+    rmis cand, lvm;
     cam_view cv;
     light_view lview;
-    if ((uint32_t)(pl + s->L) > P->max_path_length || (uint32_t)(pl + s->L) < P->min_path_length) return cs(0.f);
-    if (s->L == 1 && t < P->min_dist_to_med) return cs(0.f);
+    if (IS_F64) {
+        const v3 p = V(lv->position + 3 * j);
+        const v3 op = sub(p, s->o);
+        v3 q;
+        t = dot(op, s->d);
+        q.x = s->o.x + s->d.x * t - p.x; q.y = s->o.y + s->d.y * t - p.y; q.z = s->o.z + s->d.z * t - p.z;
+        d2 = dot(q, q);
+    }
+    if ((uint32_t)(pl + s->L) > P->max_path_length || (uint32_t)(pl + s->L) < P->min_path_length) return cs(0);
+    if (s->L == 1 && t < P->min_dist_to_med) return cs(0);
     att = eval_att(m, t - s->dmin);
     pdf = comp(att, m->min_idx);
     if (s->ray_flags & UPBP_SHORT_BEAM) att = cdiv(att, pdf);
     rsp = m->min_st * pdf;
     rsr = (s->rsf & UPBP_ORIGIN_IN_MEDIUM) ? rsp : pdf;
-    ratio = 1.0f / m->min_st;
-    if (!c_positive(att)) return cs(0.f);
+    ratio = (real)1 / m->min_st;
+    if (!c_positive(att)) return cs(0);
     rsp *= s->rs_pdf;
     rsr *= s->rs_rev;
     phase = hg_pdf(neg(s->d), V(lv->dir_fix + 3 * j), m->g, &sinT);
-    if (phase <= 0.f) return cs(0.f);
+    if (phase <= 0) return cs(0);
     dirPdf = phase * m->cont;
     revPdf = phase * lv->cont_prob[j];
-    r2 = P->radius_pb2d * P->radius_pb2d;
-    kernel = (1.f - d2 / r2) / (r2 * PI_F * 0.5f);
-    if (!is_pos(kernel)) return cs(0.f);
-    un = cscale(cscale(cmul(cmul(C3(lv->throughput + 3 * j), att), C3(m->ss)), phase), kernel);
-    if (c_black_neg(un)) return cs(0.f);
+    r2 = (real)P->radius_pb2d * P->radius_pb2d;
+    kernel = (1 - d2 / r2) / (r2 * (IS_F64 ? (real)3.14159265358979323846 : (real)PI_F) * (real)0.5);
+    if (!is_pos(kernel)) return cs(0);
+    un = cscale(cscale(cmul(cmul(C3(lv->throughput + 3 * j), att), Cr(m->ss)), phase), kernel);
+    if (c_black_neg(un)) return cs(0);
     distSq = t * t;
-    rspInv = 1.0f / rsp;
-    fill_cand(&cand, P, s->lpw * distSq * rspInv, rspInv, ratio, O->has_beams ? 1.f : 0.f,
+    rspInv = (real)1 / rsp;
+    fill_cand(&cand, P, s->lpw * distSq * rspInv, rspInv, ratio, O->has_beams ? 1 : 0,
               m->mfp > P->bb1d_min_mfp ? UPBP_MIS_IN_MEDIUM_WITH_BEAMS : 0u);
-    last = (s->ray_flags & UPBP_SHORT_BEAM) ? (float)(1.0 / (double)(ratio * cand.pb2d_factor)) : rsp / cand.pb2d_factor;
-    cv.snap = s->snap; cv.L = s->L; cv.cand = &cand; cv.prev_override = 1; cv.prev_ray_rev_inv = 1.0f / rsr;
-    wc = camera_path_weight(s->L, last, sinT, lv->mis[j].ray_sample_pdf_inv, lv->mis[j].ray_sample_pdfs_ratio,
+    last = (s->ray_flags & UPBP_SHORT_BEAM) ? (real)(1.0 / (double)(ratio * cand.pb2d_factor)) : rsp / cand.pb2d_factor;
+    cv.snap = s->snap; cv.L = s->L; cv.cand = &cand; cv.prev_override = 1; cv.prev_ray_rev_inv = (real)1 / rsr;
+    lvm = R(&lv->mis[j]);
+    wc = camera_path_weight(s->L, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
                             revPdf * rsr / distSq, P->query_beam_type, P->photon_beam_type, s->ray_flags, &cv);
-    lview.mis = lv->mis; lview.override_idx = -1; lview.override_ray_rev_inv = 0.f;
-    wl = light_path_weight(lv->path_idx[j], pl, last, 0.f, 0.f, 0.f, dirPdf, UPBP_PB2D, P->query_beam_type,
+    lview.mis = lv->mis; lview.override_idx = -1; lview.override_ray_rev_inv = 0;
+    wl = light_path_weight(lv->path_idx[j], pl, last, 0, 0, 0, dirPdf, UPBP_PB2D, P->query_beam_type,
                            P->photon_beam_type, s->ray_flags, lv->path_ends, &lview, NULL);
-    return cscale(un, 1.f / (wl + wc));
+    return cscale(un, (real)1 / (wl + wc));
+}
+
+/* FP64 closest approach of two lines with unit directions (the FP64 build re-solves the
+ * candidate geometry that PhotonBeam::testIntersectionBeamBeam computed in FP32). */
+static void closest_f64(v3 O1, v3 d1, v3 O2, v3 d2, real* dist, real* sinT, real* t1, real* t2)
+{
+    const double wx = (double)O1.x - O2.x, wy = (double)O1.y - O2.y, wz = (double)O1.z - O2.z;
+    const double cx = (double)d1.y * d2.z - (double)d1.z * d2.y, cy = (double)d1.z * d2.x - (double)d1.x * d2.z,
+                 cz = (double)d1.x * d2.y - (double)d1.y * d2.x;
+    const double aa = (double)d1.x * d1.x + (double)d1.y * d1.y + (double)d1.z * d1.z;
+    const double cc = (double)d2.x * d2.x + (double)d2.y * d2.y + (double)d2.z * d2.z;
+    const double b = (double)d1.x * d2.x + (double)d1.y * d2.y + (double)d1.z * d2.z;
+    const double dd = (double)d1.x * wx + (double)d1.y * wy + (double)d1.z * wz;
+    const double ee = (double)d2.x * wx + (double)d2.y * wy + (double)d2.z * wz;
+    const double den = aa * cc - b * b;
+    const double s = sqrt(cx * cx + cy * cy + cz * cz);
+    *t1 = (real)((b * ee - cc * dd) / den);
+    *t2 = (real)((aa * ee - b * dd) / den);
+    *dist = (real)(fabs(wx * cx + wy * cy + wz * cz) / s);
+    *sinT = (real)s;
 }
 
 /* PhotonBeam::accumulate2 after the test and the radius check accepted beam b. */
-static rgb bb1d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int64_t b, float dist, float sinTheta,
-                        float t1, float t2, float radius)
+static rgb bb1d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int64_t b, real dist, real sinTheta,
+                        real t1, real t2, real radius)
 {
     const upbp_params* P = O->P;
     const upbp_beams* B = O->bm;
@@ -378,63 +457,64 @@ static rgb bb1d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int6
     const int pl = lv->path_length[lvi];
     const uint32_t bflags = B->flags[b], brsf = B->ray_sampling_flags[b];
     rgb att, batt, un;
-    float pfdQ, rspQ, rsrQ, ratioQ, pfdB, rspB, rsrB, ratioB, phase, sinDummy, dirPdf, revPdf, sel = 1.0f;
-    float distSqQ, rspInvQ, distSqB, rspInvB, sinT, f, last, wc, wl, ntl;
-    upbp_mis cand, brec;
+    real pfdQ, rspQ, rsrQ, ratioQ, pfdB, rspB, rsrB, ratioB, phase, sinDummy, dirPdf, revPdf, sel = 1;
+    real distSqQ, rspInvQ, distSqB, rspInvB, sinT, f, last, wc, wl, ntl;
+    rmis cand, brec, lvm;
     cam_view cv;
     light_view lview;
-    const upbp_mis* lvm;
-    if ((uint32_t)(pl + 1 + s->L) > P->max_path_length || (uint32_t)(pl + 1 + s->L) < P->min_path_length) return cs(0.f);
-    if (s->L == 1 && t1 < P->min_dist_to_med) return cs(0.f);
+    if (IS_F64) closest_f64(s->o, s->d, V(B->origin + 3 * b), V(B->direction + 3 * b), &dist, &sinTheta, &t1, &t2);
+    if ((uint32_t)(pl + 1 + s->L) > P->max_path_length || (uint32_t)(pl + 1 + s->L) < P->min_path_length) return cs(0);
+    if (s->L == 1 && t1 < P->min_dist_to_med) return cs(0);
     att = eval_att(m, t1 - s->dmin);
     pfdQ = comp(att, m->min_idx);
     if (s->ray_flags & UPBP_SHORT_BEAM) att = cdiv(att, pfdQ);
     rspQ = m->min_st * pfdQ;
     rsrQ = (s->rsf & UPBP_ORIGIN_IN_MEDIUM) ? rspQ : pfdQ;
-    ratioQ = 1.0f / m->min_st;
+    ratioQ = (real)1 / m->min_st;
     batt = eval_att(m, t2);
     att = cmul(att, batt);
     pfdB = comp(batt, m->min_idx);
     if (bflags & UPBP_SHORT_BEAM) att = cdiv(att, pfdB);
     rspB = m->min_st * pfdB;
     rsrB = (brsf & UPBP_ORIGIN_IN_MEDIUM) ? rspB : pfdB;
-    ratioB = 1.0f / m->min_st;
-    if (!c_positive(att)) return cs(0.f);
+    ratioB = (real)1 / m->min_st;
+    if (!c_positive(att)) return cs(0);
     rspQ *= s->rs_pdf;
     rsrQ *= s->rs_rev;
     rspB *= B->ray_sample_pdf[b];
     rsrB *= B->ray_sample_rev_pdf[b];
     phase = hg_pdf(neg(s->d), neg(V(B->direction + 3 * b)), m->g, &sinDummy);
-    if (phase <= 0.f) return cs(0.f);
+    if (phase <= 0) return cs(0);
     dirPdf = phase * m->cont;
     revPdf = phase * m->cont;
-    un = cdiv(cscale(cscale(cscale(cmul(cmul(cscale(C3(B->throughput + 3 * b), 1.0f / sel), C3(m->ss)), att), phase),
-                            1.f - dist * dist / (radius * radius)), 3.f),
-              4.f * radius * sinTheta);
-    if (c_black_neg(un)) return cs(0.f);
+    un = cdiv(cscale(cscale(cscale(cmul(cmul(cscale(C3(B->throughput + 3 * b), (real)1 / sel), Cr(m->ss)), att), phase),
+                            1 - dist * dist / (radius * radius)), 3),
+              4 * radius * sinTheta);
+    if (c_black_neg(un)) return cs(0);
     distSqQ = t1 * t1;
-    rspInvQ = 1.0f / rspQ;
+    rspInvQ = (real)1 / rspQ;
     fill_cand(&cand, P, s->lpw * distSqQ * rspInvQ, rspInvQ, ratioQ, sel, UPBP_MIS_IN_MEDIUM_WITH_BEAMS);
-    distSqB = (lv->flags[lvi] & UPBP_LV_IS_FINITE) ? t2 * t2 : 1.0f;
-    rspInvB = 1.0f / rspB;
-    fill_cand(&brec, P, B->last_pdf_w_inv[b] * distSqB * rspInvB, rspInvB, ratioB, sel, UPBP_MIS_IN_MEDIUM_WITH_BEAMS);
-    sinT = (s->ray_flags & UPBP_NO_SINE_IN_WEIGHTS) ? 1.0f : sinTheta;
+    distSqB = (lv->flags[lvi] & UPBP_LV_IS_FINITE) ? t2 * t2 : 1;
+    rspInvB = (real)1 / rspB;
+    fill_cand(&brec, P, (real)B->last_pdf_w_inv[b] * distSqB * rspInvB, rspInvB, ratioB, sel,
+              UPBP_MIS_IN_MEDIUM_WITH_BEAMS);
+    sinT = (s->ray_flags & UPBP_NO_SINE_IN_WEIGHTS) ? 1 : sinTheta;
     f = cand.bb1d_factor;
     if (s->ray_flags & UPBP_SHORT_BEAM)
-        last = (bflags & UPBP_SHORT_BEAM) ? (float)(1.0 / (double)(ratioQ * ratioB * f * sel * sinT))
+        last = (bflags & UPBP_SHORT_BEAM) ? (real)(1.0 / (double)(ratioQ * ratioB * f * sel * sinT))
                                           : rspB / (ratioQ * f * sel * sinT);
     else
         last = (bflags & UPBP_SHORT_BEAM) ? rspQ / (ratioB * f * sel * sinT) : rspQ * rspB / (f * sel * sinT);
-    cv.snap = s->snap; cv.L = s->L; cv.cand = &cand; cv.prev_override = 1; cv.prev_ray_rev_inv = 1.0f / rsrQ;
+    cv.snap = s->snap; cv.L = s->L; cv.cand = &cand; cv.prev_override = 1; cv.prev_ray_rev_inv = (real)1 / rsrQ;
     wc = camera_path_weight(s->L, last, sinT, rspInvB, ratioB, revPdf * rsrQ / distSqQ, P->query_beam_type,
                             P->photon_beam_type, s->ray_flags, &cv);
-    lvm = &lv->mis[lvi];
-    ntl = ((lvm->flags & UPBP_MIS_ON_LIGHT_SOURCE) && (lvm->flags & UPBP_MIS_IS_DELTA))
-              ? 0.f : dirPdf * rsrB * fabsf(lvm->cos_theta_out) / distSqB;
-    lview.mis = lv->mis; lview.override_idx = lvi; lview.override_ray_rev_inv = 1.0f / rsrB;
-    wl = light_path_weight(lv->path_idx[lvi], pl + 1, last, 0.f, 0.f, 0.f, ntl, UPBP_BB1D, P->query_beam_type,
+    lvm = R(&lv->mis[lvi]);
+    ntl = ((lvm.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (lvm.flags & UPBP_MIS_IS_DELTA))
+              ? 0 : dirPdf * rsrB * rabs(lvm.cos_theta_out) / distSqB;
+    lview.mis = lv->mis; lview.override_idx = lvi; lview.override_ray_rev_inv = (real)1 / rsrB;
+    wl = light_path_weight(lv->path_idx[lvi], pl + 1, last, 0, 0, 0, ntl, UPBP_BB1D, P->query_beam_type,
                            P->photon_beam_type, s->ray_flags, lv->path_ends, &lview, &brec);
-    return cscale(un, 1.f / (wl + wc));
+    return cscale(un, (real)1 / (wl + wc));
 }
 
 /* evalBre / evalBeamBeamEstimate segment loop for one query; est = UPBP_PB2D or UPBP_BB1D. */
@@ -446,10 +526,12 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
     const int lite = (qf & UPBP_Q_LITE) != 0;
     const uint32_t qrsf = (qf & UPBP_Q_ORIGIN_IN_MEDIUM) ? UPBP_ORIGIN_IN_MEDIUM : 0u;
     const uint32_t bt = P->query_beam_type;
-    rgb result = cs(0.f), attn = cs(1.f);
-    float rsp = 1.f, rsr = 1.f;
+    rgb result = cs(0), attn = cs(1);
+    real rsp = 1, rsr = 1;
     seg_ctx s;
     int i;
+    s.of = Vf(Q->origin + 3 * q);
+    s.df = Vf(Q->direction + 3 * q);
     s.o = V(Q->origin + 3 * q);
     s.d = V(Q->direction + 3 * q);
     s.L = Q->path_length[q];
@@ -459,8 +541,9 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
     for (i = 0; i < Q->seg_count[q]; ++i) {
         const int sg = Q->seg_begin[q] + i;
         const medium* m = &O->media[Q->seg_medium[sg]];
-        const float dmin = Q->seg_dist_min[sg], dmax = Q->seg_dist_max[sg];
-        rgb seg = cs(0.f);
+        const float dminf = Q->seg_dist_min[sg], dmaxf = Q->seg_dist_max[sg];
+        const real dmin = dminf, dmax = dmaxf;
+        rgb seg = cs(0);
         if (m->has_scat) {
             s.dmin = dmin;
             s.dmax = dmax;
@@ -474,7 +557,7 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
                 for (j = 0; j < lv->n; ++j) {
                     float t, d2;
                     if (!(lv->flags[j] & UPBP_LV_IN_MEDIUM)) continue;
-                    if (!test_bre(s.o, s.d, dmin, dmax, V(lv->position + 3 * j), r2, &t, &d2)) continue;
+                    if (!test_bre(s.of, s.df, dminf, dmaxf, Vf(lv->position + 3 * j), r2, &t, &d2)) continue;
                     ++*cnt;
                     *hash += mix64((uint64_t)j);
                     seg = cadd(seg, pb2d_contrib(O, m, &s, j, t, d2));
@@ -486,7 +569,7 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
                 for (b = 0; b < B->n; ++b) {
                     float dist, sinT, t1, t2;
                     if (&O->media[B->medium_id[b]] != m) continue;
-                    if (!test_beam_beam(s.o, s.d, dmin, dmax, V(B->origin + 3 * b), V(B->direction + 3 * b), 0.f,
+                    if (!test_beam_beam(s.of, s.df, dminf, dmaxf, Vf(B->origin + 3 * b), Vf(B->direction + 3 * b), 0.f,
                                         B->length[b], r2, &dist, &sinT, &t1, &t2))
                         continue;
                     if (radius < dist) continue;
@@ -498,7 +581,7 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
         }
         result = cadd(result, cmul(attn, seg));
         if (lite) {
-            float srev, spdf;
+            real srev, spdf;
             attn = cmul(attn, eval_att(m, dmax - dmin));
             spdf = ray_sample_pdf(m, dmin, dmax, i == 0 ? qrsf : 0u, &srev);
             if (!c_positive(attn)) break;
@@ -579,7 +662,7 @@ static rgb pp3d_query(const oracle* O, const hashgrid* g, const upbp_point_queri
     const upbp_params* P = O->P;
     const upbp_light_vertices* lv = O->lv;
     rgb res = cs(0.f);
-    const v3 qp = V(Q->position + 3 * q);
+    const v3f qp = Vf(Q->position + 3 * q);
     const float qa[3] = {qp.x, qp.y, qp.z};
     const medium* m = &O->media[Q->medium_id[q]];
     const v3 cfix = V(Q->dir_fix + 3 * q);
@@ -598,18 +681,19 @@ static rgb pp3d_query(const oracle* O, const hashgrid* g, const upbp_point_queri
         p[c] = (int)cf[c];
         po[c] = p[c] + (cell[c] - cf[c] < 0.5f ? -1 : 1);
     }
-    cv.snap = O->cam + Q->cam_mis_begin[q]; cv.L = L; cv.cand = NULL; cv.prev_override = 0; cv.prev_ray_rev_inv = 0.f;
-    lview.mis = lv->mis; lview.override_idx = -1; lview.override_ray_rev_inv = 0.f;
+    cv.snap = O->cam + Q->cam_mis_begin[q]; cv.L = L; cv.cand = NULL; cv.prev_override = 0; cv.prev_ray_rev_inv = 0;
+    lview.mis = lv->mis; lview.override_idx = -1; lview.override_ray_rev_inv = 0;
     for (j = 0; j < 8; ++j) {
         const uint32_t b = hash_cell((j & 4) ? po[0] : p[0], (j & 2) ? po[1] : p[1], (j & 1) ? po[2] : p[2], g->cells);
         int k;
         for (k = g->start[b]; k < g->end[b]; ++k) {
             const int32_t i = g->idx[k];
-            const v3 dd = sub(qp, V(lv->position + 3 * i));
-            float sinT, phase, dirPdf, revPdf, mwfInv, wc, wl;
+            const v3f dd = subf(qp, Vf(lv->position + 3 * i));
+            real sinT, phase, dirPdf, revPdf, mwfInv, wc, wl;
+            rmis lvm;
             rgb factor;
             int pl;
-            if (!(dot(dd, dd) <= g->r2)) continue;
+            if (!(dotf(dd, dd) <= g->r2)) continue;
             ++*cnt;
             *hash += mix64((uint64_t)i);
             if (!(lv->flags[i] & UPBP_LV_CONNECTABLE)) continue;
@@ -617,16 +701,17 @@ static rgb pp3d_query(const oracle* O, const hashgrid* g, const upbp_point_queri
             if ((uint32_t)(pl + L) > P->max_path_length || (uint32_t)(pl + L) < P->min_path_length) continue;
             if (m->ss[0] <= 0.f && m->ss[1] <= 0.f && m->ss[2] <= 0.f) continue;
             phase = hg_pdf(cfix, V(lv->dir_fix + 3 * i), m->g, &sinT);
-            factor = cscale(C3(m->ss), phase);
+            factor = cscale(Cr(m->ss), phase);
             if (c_black_neg(factor)) continue;
             dirPdf = phase * m->cont;
             revPdf = phase * lv->cont_prob[i];
-            mwfInv = 1.0f / lv->mis[i].pp3d_factor;
-            wc = camera_path_weight(L, mwfInv, sinT, lv->mis[i].ray_sample_pdf_inv, lv->mis[i].ray_sample_pdfs_ratio,
+            lvm = R(&lv->mis[i]);
+            mwfInv = (real)1 / lvm.pp3d_factor;
+            wc = camera_path_weight(L, mwfInv, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
                                     revPdf, P->query_beam_type, P->photon_beam_type, P->techniques, &cv);
-            wl = light_path_weight(lv->path_idx[i], pl, mwfInv, 0.f, 0.f, 0.f, dirPdf, UPBP_PP3D, P->query_beam_type,
+            wl = light_path_weight(lv->path_idx[i], pl, mwfInv, 0, 0, 0, dirPdf, UPBP_PP3D, P->query_beam_type,
                                    P->photon_beam_type, P->techniques, lv->path_ends, &lview, NULL);
-            res = cadd(res, cscale(cmul(factor, C3(lv->throughput + 3 * i)), 1.f / (wl + wc)));
+            res = cadd(res, cscale(cmul(factor, C3(lv->throughput + 3 * i)), (real)1 / (wl + wc)));
         }
     }
     return res;

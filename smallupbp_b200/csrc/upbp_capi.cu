@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "upbp_kernels.cuh"
+#include "upbp_mis_prep.cuh"
 
 using namespace upbp;
 
@@ -78,6 +79,8 @@ struct upbp_ctx {
     int n_pieces = 0;
     DBuf bm_leaf_codes, bm_nodes, bm_parent_int, bm_parent_leaf, bm_leaf_boxes, bm_node_boxes, bm_flagsbuf;
     int bm_n_leaves = 0;
+    // mixed mode: FP64 partial sums of the MIS walks
+    DBuf light_sums, cam_sums_seg, cam_sums_pt;
     // temp storage for CUB
     DBuf cub_tmp;
     // outputs
@@ -234,6 +237,13 @@ void do_build(upbp_ctx* c)
                        c->lv_dir4.as<float4>(), c->lv_thr4.as<float4>(), c->lv_info4.as<int4>(),
                        c->lv_inmed.as<uint32_t>(), s);
     c->build_launches += 1;
+    if (c->mode == UPBP_MODE_MIXED && n > 0) {
+        ensure(c, c->light_sums, sizeof(LightSum) * n);
+        // the PB2D / BB1D walks see beamType | techniques, PP3D the techniques: same terms
+        launch_light_sums(c->lv_mis.as<upbp_mis>(), c->path_ends.as<int32_t>(), c->n_paths, P.techniques,
+                          P.query_beam_type, P.photon_beam_type, c->light_sums.as<LightSum>(), s);
+        c->build_launches += 1;
+    }
     // ---- photons = light vertices in media (stable compaction keeps light-vertex order)
     c->n_ph = 0;
     if (n > 0) {
@@ -402,6 +412,7 @@ LightSoA light_soa(upbp_ctx* c)
     L.info = c->lv_info4.as<int4>();
     L.mis = c->lv_mis.as<upbp_mis>();
     L.path_ends = c->path_ends.as<int32_t>();
+    L.sums = c->mode == UPBP_MODE_MIXED ? c->light_sums.as<LightSum>() : nullptr;
     L.n = c->n_lv;
     return L;
 }
@@ -454,6 +465,21 @@ void do_evaluate(upbp_ctx* c)
     float* img = npix ? c->image.as<float>() : nullptr;
     unsigned long long* tested = c->tested.as<unsigned long long>();
 
+    const bool mixed = c->mode == UPBP_MODE_MIXED;
+    const CamSum* cs_seg = nullptr;
+    const CamSum* cs_pt = nullptr;
+    if (mixed) {
+        ensure(c, c->cam_sums_seg, sizeof(CamSum) * std::max<int64_t>(nq, 1));
+        ensure(c, c->cam_sums_pt, sizeof(CamSum) * std::max<int64_t>(np, 1));
+        const uint32_t tq = c->P.query_beam_type | c->P.techniques;
+        launch_cam_sums(cam, c->sq_cam_begin.as<int64_t>(), c->sq_plen.as<int32_t>(), nq, tq, c->P.query_beam_type,
+                        c->P.photon_beam_type, c->cam_sums_seg.as<CamSum>(), s);
+        launch_cam_sums(cam, c->pq_cam_begin.as<int64_t>(), c->pq_plen.as<int32_t>(), np, c->P.techniques,
+                        c->P.query_beam_type, c->P.photon_beam_type, c->cam_sums_pt.as<CamSum>(), s);
+        cs_seg = c->cam_sums_seg.as<CamSum>();
+        cs_pt = c->cam_sums_pt.as<CamSum>();
+        c->eval_launches += 2;
+    }
     ck(c, cudaEventRecord(c->ev[2], s), "event");
     if (np > 0) {
         HashGridDev G{};
@@ -479,7 +505,7 @@ void do_evaluate(upbp_ctx* c)
         Q.n = np;
         Outputs O{c->out_pp3d.as<float>(), img, c->cnt_pp3d.as<uint32_t>(),
                   c->hash_pp3d.as<unsigned long long>(), tested + 2};
-        launch_gather_pp3d(K, L, G, Q, cam, O, c->block, s);
+        launch_gather_pp3d(K, L, G, Q, cam, cs_pt, O, c->block, mixed, s);
         c->eval_launches += 1;
     }
     ck(c, cudaEventRecord(c->ev[3], s), "event");
@@ -493,7 +519,7 @@ void do_evaluate(upbp_ctx* c)
         B.n_leaves = c->pb_n_leaves;
         Outputs O{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
                   c->hash_pb2d.as<unsigned long long>(), tested + 0};
-        launch_gather_pb2d(K, L, B, Q, cam, O, c->block, s);
+        launch_gather_pb2d(K, L, B, Q, cam, cs_seg, O, c->block, mixed, s);
         c->eval_launches += 1;
     }
     ck(c, cudaEventRecord(c->ev[4], s), "event");
@@ -514,7 +540,7 @@ void do_evaluate(upbp_ctx* c)
         S.n = c->n_beams;
         Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                   c->hash_bb1d.as<unsigned long long>(), tested + 1};
-        launch_gather_bb1d(K, L, B, S, Q, cam, O, c->block, s);
+        launch_gather_bb1d(K, L, B, S, Q, cam, cs_seg, O, c->block, mixed, s);
         c->eval_launches += 1;
     }
     ck(c, cudaEventRecord(c->ev[5], s), "event");
@@ -584,7 +610,8 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->pc_perm_sorted, &c->bbox_pc, &c->bm_leaf_codes, &c->bm_nodes, &c->bm_parent_int,
                    &c->bm_parent_leaf, &c->bm_leaf_boxes, &c->bm_node_boxes, &c->bm_flagsbuf, &c->cub_tmp,
                    &c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->image, &c->cnt_pb2d, &c->cnt_bb1d, &c->cnt_pp3d,
-                   &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested};
+                   &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested, &c->light_sums, &c->cam_sums_seg,
+                   &c->cam_sums_pt};
     for (DBuf* b : all) free_buf(*b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
@@ -599,6 +626,7 @@ int upbp_set_mode(upbp_ctx* c, int mode)
 {
     return guarded(c, [&] {
         if (mode != UPBP_MODE_PLAIN && mode != UPBP_MODE_MIXED) fail(c, UPBP_ERR_INVALID_ARG, "unknown mode %d", mode);
+        if (mode != c->mode) c->built = false;
         c->mode = mode;
     });
 }

@@ -11,6 +11,7 @@
 #include <cstdint>
 
 #include "upbp_kernels.cuh"
+#include "upbp_mis_prep.cuh"
 
 namespace upbp {
 
@@ -126,6 +127,9 @@ struct SegCtx {
     float last_pdf_w_inv;
     uint32_t ray_flags;        // beamType | estimatorTechniques
     const upbp_mis* cam;
+    // mixed mode: camera entry L-1 and the FP64 suffix of the camera walk
+    upbp_mis e;
+    CamSum cs;
 };
 
 __device__ __forceinline__ void fill_cand(upbp_mis& c, const upbp_params& P, float pdf_a_inv, float rsp_inv,
@@ -150,6 +154,7 @@ __device__ __forceinline__ void fill_cand(upbp_mis& c, const upbp_params& P, flo
 
 // ----------------------------------------------------------------- PB2D contribution
 // breIntersectFuncHomogeneous2 after testIntersectionBre accepted photon `lv` at (t, d2).
+template <bool kMixed>
 __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const LightSoA& Lv, const SegCtx& s, int lv,
                             float t, float d2)
 {
@@ -188,6 +193,14 @@ __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const Light
     const float last = (s.ray_flags & UPBP_SHORT_BEAM) ? (float)(1.0 / (double)(ratio * cand.pb2d_factor))
                                                        : rsp / cand.pb2d_factor;
     const upbp_mis lvm = load_mis(Lv.mis + lv);
+    if (kMixed) {
+        const double wc = camera_weight_fast(s.L, cand, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
+                                             camRevPdfW * rsr / distSq, s.e, 1.0f / rsr, s.cs, s.ray_flags,
+                                             P.query_beam_type, P.photon_beam_type);
+        const LightSum ls = Lv.sums[lv];
+        const double wl = (double)last * (ls.a + (double)camDirPdfW * ls.c);
+        return (float)(1.0 / (wl + wc)) * unweighted;
+    }
     const CamView cam{s.cam, s.L, &cand, 1.0f / rsr};
     const float wCamera = camera_path_weight(s.L, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
                                              camRevPdfW * rsr / distSq, P.query_beam_type, P.photon_beam_type,
@@ -201,10 +214,37 @@ __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const Light
 
 // ----------------------------------------------------------------- BB1D contribution
 // PhotonBeam::accumulate2 after testIntersectionBeamBeam and the radius test accepted `beam`.
-__device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const LightSoA& Lv, const BeamSoA& Bs,
-                            const SegCtx& s, int beam, V3 bdir, float radius, float dist, float sinTheta, float t1,
-                            float t2)
+// FP64 closest approach of the query line and the beam line (unit directions), used in mixed
+// mode for near-parallel pairs where the FP32 solve of PhotonBeam.hxx:253-293 cancels.
+__device__ __forceinline__ void closest_approach_f64(V3 O1, V3 d1, V3 O2, V3 d2, float& dist, float& sinT, float& t1,
+                                                     float& t2)
 {
+    const double ax = d1.x, ay = d1.y, az = d1.z, bx = d2.x, by = d2.y, bz = d2.z;
+    const double wx = (double)O1.x - O2.x, wy = (double)O1.y - O2.y, wz = (double)O1.z - O2.z;
+    const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+    const double s2 = cx * cx + cy * cy + cz * cz;
+    const double b = ax * bx + ay * by + az * bz;
+    const double dd = ax * wx + ay * wy + az * wz;
+    const double ee = bx * wx + by * wy + bz * wz;
+    const double aa = ax * ax + ay * ay + az * az, cc = bx * bx + by * by + bz * bz;
+    const double den = aa * cc - b * b;
+    const double s = sqrt(s2);
+    t1 = (float)((b * ee - cc * dd) / den);
+    t2 = (float)((aa * ee - b * dd) / den);
+    dist = (float)(fabs(-wx * cx - wy * cy - wz * cz) / s);
+    sinT = (float)s;
+}
+
+template <bool kMixed>
+__device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const LightSoA& Lv, const BeamSoA& Bs,
+                            const SegCtx& s, int beam, V3 bo, V3 bdir, float radius, float dist, float sinTheta,
+                            float t1, float t2)
+{
+    if (kMixed) {
+        // near-parallel lines: 1 - (d1.d2)^2 small (PhotonBeam.hxx:267-273 rejects only below 1e-5)
+        const float c = s.d.x * bdir.x + s.d.y * bdir.y + s.d.z * bdir.z;
+        if (1.f - c * c < 1e-2f) closest_approach_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
+    }
     const upbp_params& P = K.P;
     const int2 link = __ldg(&Bs.link[beam]);
     const int lvi = link.x;
@@ -264,12 +304,21 @@ __device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const Light
                                           : rspB / (ratioQ * f * sel * sinT);
     else
         last = (bflags & UPBP_SHORT_BEAM) ? rspQ / (ratioB * f * sel * sinT) : rspQ * rspB / (f * sel * sinT);
-    const CamView cam{s.cam, s.L, &cand, 1.0f / rsrQ};
-    const float wCamera = camera_path_weight(s.L, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ,
-                                             P.query_beam_type, P.photon_beam_type, s.ray_flags, cam);
     const upbp_mis lvm = load_mis(Lv.mis + lvi);
     const bool onDeltaLight = (lvm.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (lvm.flags & UPBP_MIS_IS_DELTA);
     const float ntl = onDeltaLight ? 0.f : bsdfDirPdfW * rsrB * fabsf(lvm.cos_theta_out) / distSqB;
+    if (kMixed) {
+        const double wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ, s.e,
+                                             1.0f / rsrQ, s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
+        const LightSum ls = Lv.sums[lvi];
+        double inner = (double)ls.bptb;
+        if (!(s.ray_flags & UPBP_PREVIOUS)) inner += (double)ntl * (ls.d + ls.e * (double)(1.0f / rsrB));
+        const double wl = (double)last * (double)brec.pdf_a_inv * inner;
+        return (float)(1.0 / (wl + wc)) * unweighted;
+    }
+    const CamView cam{s.cam, s.L, &cand, 1.0f / rsrQ};
+    const float wCamera = camera_path_weight(s.L, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ,
+                                             P.query_beam_type, P.photon_beam_type, s.ray_flags, cam);
     const LightView lview{Lv.mis, lvi, 1.0f / rsrB};
     const float wLight = light_path_weight(info.x, pl + 1, last, 0.f, 0.f, 0.f, ntl, UPBP_BB1D, P.query_beam_type,
                                            P.photon_beam_type, s.ray_flags, Lv.path_ends, lview, &brec);
@@ -322,8 +371,9 @@ __device__ __forceinline__ Rgb segment_loop(const GatherConsts& K, const DMedium
     return result;
 }
 
+template <bool kMixed>
 __device__ __forceinline__ void init_seg_ctx(SegCtx& s, const GatherConsts& K, const SegQueriesDev& Q,
-                                             const upbp_mis* cam, int64_t q)
+                                             const upbp_mis* cam, const CamSum* cs, int64_t q)
 {
     s.o = v3(Q.origin[3 * q], Q.origin[3 * q + 1], Q.origin[3 * q + 2]);
     s.d = v3(Q.direction[3 * q], Q.direction[3 * q + 1], Q.direction[3 * q + 2]);
@@ -331,6 +381,10 @@ __device__ __forceinline__ void init_seg_ctx(SegCtx& s, const GatherConsts& K, c
     s.last_pdf_w_inv = Q.last_pdf_w_inv[q];
     s.ray_flags = K.P.query_beam_type | K.P.techniques;
     s.cam = cam + Q.cam_mis_begin[q];
+    if (kMixed) {
+        if (s.L >= 2) s.e = load_mis(s.cam + s.L - 1);
+        s.cs = cs[q];
+    }
 }
 
 __device__ __forceinline__ void write_out(const Outputs& O, int64_t q, Rgb v, uint32_t cnt, unsigned long long h,
@@ -346,9 +400,11 @@ __device__ __forceinline__ void write_out(const Outputs& O, int64_t q, Rgb v, ui
 }
 
 // ----------------------------------------------------------------- kernels
+template <bool kMixed>
 __global__ void __launch_bounds__(256) k_gather_pb2d(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                      const PhotonBVH B, const SegQueriesDev Q,
-                                                     const upbp_mis* __restrict__ cam, const Outputs O)
+                                                     const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
+                                                     const Outputs O)
 {
     __shared__ DMedium media[UPBP_MAX_MEDIA];
     stage_media(K, media);
@@ -359,7 +415,7 @@ __global__ void __launch_bounds__(256) k_gather_pb2d(const __grid_constant__ Gat
     Rgb res = rgb(0.f);
     if ((Q.flags[q] & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && B.n > 0) {
         SegCtx s;
-        init_seg_ctx(s, K, Q, cam, q);
+        init_seg_ctx<kMixed>(s, K, Q, cam, cs, q);
         const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
         const float r2 = K.P.radius_pb2d * K.P.radius_pb2d;
         res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
@@ -374,7 +430,7 @@ __global__ void __launch_bounds__(256) k_gather_pb2d(const __grid_constant__ Gat
                         const int lv = __float_as_int(p.w);
                         ++cnt;
                         h += mix64((unsigned long long)lv);
-                        acc = acc + pb2d_contrib(K, m, Lv, s, lv, t, d2);
+                        acc = acc + pb2d_contrib<kMixed>(K, m, Lv, s, lv, t, d2);
                     }
                 }
             });
@@ -385,9 +441,11 @@ __global__ void __launch_bounds__(256) k_gather_pb2d(const __grid_constant__ Gat
     if (O.tested) atomicAdd(O.tested, tested);
 }
 
+template <bool kMixed>
 __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                      const BeamBVH B, const BeamSoA Bs, const SegQueriesDev Q,
-                                                     const upbp_mis* __restrict__ cam, const Outputs O)
+                                                     const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
+                                                     const Outputs O)
 {
     __shared__ DMedium media[UPBP_MAX_MEDIA];
     stage_media(K, media);
@@ -398,7 +456,7 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
     Rgb res = rgb(0.f);
     if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D) && B.n > 0) {
         SegCtx s;
-        init_seg_ctx(s, K, Q, cam, q);
+        init_seg_ctx<kMixed>(s, K, Q, cam, cs, q);
         const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
         res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
             Rgb acc = rgb(0.f);
@@ -421,7 +479,8 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                     if (radius < dist) continue;  // PhotonBeam.hxx:411-413
                     ++cnt;
                     h += mix64((unsigned long long)beam);
-                    acc = acc + bb1d_contrib(K, m, Lv, Bs, s, beam, v3(pb.x, pb.y, pb.z), radius, dist, sinT, t1, t2);
+                    acc = acc + bb1d_contrib<kMixed>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), radius,
+                                                          dist, sinT, t1, t2);
                 }
             });
             return acc;
@@ -438,9 +497,11 @@ __device__ __forceinline__ uint32_t hash_cell(int x, int y, int z, int cells)
     return ((ux * 73856093u) ^ (uy * 19349663u) ^ (uz * 83492791u)) % (uint32_t)cells;
 }
 
+template <bool kMixed>
 __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                      const HashGridDev G, const PointQueriesDev Q,
-                                                     const upbp_mis* __restrict__ cam, const Outputs O)
+                                                     const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
+                                                     const Outputs O)
 {
     __shared__ DMedium media[UPBP_MAX_MEDIA];
     stage_media(K, media);
@@ -463,6 +524,13 @@ __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ Gat
         const V3 cfix = v3(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
         const int L = Q.path_length[q];
         const CamSnap camv{cam + Q.cam_mis_begin[q]};
+        upbp_mis eL, eL1;
+        CamSum csq;
+        if (kMixed) {
+            eL = load_mis(camv.snap + L);
+            if (L >= 2) eL1 = load_mis(camv.snap + L - 1);
+            csq = cs[q];
+        }
         const bool scat_pos = !(m.ss[0] <= 0.f && m.ss[1] <= 0.f && m.ss[2] <= 0.f);
         const V3 cell = v3(xmul(G.inv_cell, dmin.x), xmul(G.inv_cell, dmin.y), xmul(G.inv_cell, dmin.z));
         const V3 cf = v3(floorf(cell.x), floorf(cell.y), floorf(cell.z));
@@ -497,13 +565,24 @@ __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ Gat
                 const float revPdf = phase * __ldg(&Lv.pos[lv]).w;
                 const upbp_mis lvm = load_mis(Lv.mis + lv);
                 const float mwfInv = 1.0f / lvm.pp3d_factor;
-                const float wCamera = camera_path_weight(L, mwfInv, sinT, lvm.ray_sample_pdf_inv,
-                                                         lvm.ray_sample_pdfs_ratio, revPdf, P.query_beam_type,
-                                                         P.photon_beam_type, P.techniques, camv);
-                const LightView lview{Lv.mis, -1, 0.f};
-                const float wLight = light_path_weight(info.x, pl, mwfInv, 0.f, 0.f, 0.f, dirPdf, UPBP_PP3D,
-                                                       P.query_beam_type, P.photon_beam_type, P.techniques,
-                                                       Lv.path_ends, lview, nullptr);
+                float wCamera, wLight;
+                if (kMixed) {
+                    const double wc = camera_weight_fast(L, eL, mwfInv, sinT, lvm.ray_sample_pdf_inv,
+                                                         lvm.ray_sample_pdfs_ratio, revPdf, eL1,
+                                                         eL1.ray_sample_rev_pdf_inv, csq, P.techniques,
+                                                         P.query_beam_type, P.photon_beam_type);
+                    const LightSum ls = Lv.sums[lv];
+                    const double wl = (double)mwfInv * (ls.a + (double)dirPdf * ls.c);
+                    wCamera = (float)wc;
+                    wLight = (float)wl;
+                } else {
+                    wCamera = camera_path_weight(L, mwfInv, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
+                                                 revPdf, P.query_beam_type, P.photon_beam_type, P.techniques, camv);
+                    const LightView lview{Lv.mis, -1, 0.f};
+                    wLight = light_path_weight(info.x, pl, mwfInv, 0.f, 0.f, 0.f, dirPdf, UPBP_PP3D,
+                                               P.query_beam_type, P.photon_beam_type, P.techniques, Lv.path_ends,
+                                               lview, nullptr);
+                }
                 const float w = 1.f / (wLight + wCamera);
                 const float4 th = __ldg(&Lv.thr[lv]);
                 res = res + w * (factor * Rgb{th.x, th.y, th.z});
@@ -523,27 +602,33 @@ __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ Gat
 }  // namespace
 
 void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,
-                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream)
+                        const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
+                        cudaStream_t stream)
 {
     if (Q.n <= 0) return;
     const int grid = (int)((Q.n + block - 1) / block);
-    k_gather_pb2d<<<grid, block, 0, stream>>>(K, L, B, Q, cam, O);
+    if (mixed) k_gather_pb2d<true><<<grid, block, 0, stream>>>(K, L, B, Q, cam, cs, O);
+    else k_gather_pb2d<false><<<grid, block, 0, stream>>>(K, L, B, Q, cam, cs, O);
 }
 
 void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
-                        const SegQueriesDev& Q, const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream)
+                        const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block,
+                        bool mixed, cudaStream_t stream)
 {
     if (Q.n <= 0) return;
     const int grid = (int)((Q.n + block - 1) / block);
-    k_gather_bb1d<<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, O);
+    if (mixed) k_gather_bb1d<true><<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, cs, O);
+    else k_gather_bb1d<false><<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, cs, O);
 }
 
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,
-                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream)
+                        const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
+                        cudaStream_t stream)
 {
     if (Q.n <= 0) return;
     const int grid = (int)((Q.n + block - 1) / block);
-    k_gather_pp3d<<<grid, block, 0, stream>>>(K, L, G, Q, cam, O);
+    if (mixed) k_gather_pp3d<true><<<grid, block, 0, stream>>>(K, L, G, Q, cam, cs, O);
+    else k_gather_pp3d<false><<<grid, block, 0, stream>>>(K, L, G, Q, cam, cs, O);
 }
 
 }  // namespace upbp

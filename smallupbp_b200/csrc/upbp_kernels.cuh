@@ -29,6 +29,7 @@ struct LightSoA {
     const int4* info;       // path_idx, path_length, flags, medium_id
     const upbp_mis* mis;    // MisData
     const int32_t* path_ends;
+    const struct LightSum* sums;  // mixed mode: FP64 partial sums of the light walks
     int64_t n;
 };
 
@@ -160,12 +161,19 @@ void launch_permute_pieces(const int32_t* perm, int n, const float4* pa, const f
                            const Box* boxes, float4* opa, float4* opb, float4* opc, Box* oboxes, cudaStream_t stream);
 void launch_box_leaf_boxes(const Box* boxes, int n, int leaf, Box* leaf_boxes, cudaStream_t stream);
 
+struct CamSum;
 void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,
-                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream);
-void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
-                        const SegQueriesDev& Q, const upbp_mis* cam, const Outputs& O, int block,
+                        const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
                         cudaStream_t stream);
+void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
+                        const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block,
+                        bool mixed, cudaStream_t stream);
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,
-                        const upbp_mis* cam, const Outputs& O, int block, cudaStream_t stream);
+                        const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
+                        cudaStream_t stream);
+void launch_light_sums(const upbp_mis* mis, const int32_t* path_ends, int n_paths, uint32_t tech, uint32_t qbt,
+                       uint32_t pbt, struct LightSum* out, cudaStream_t s);
+void launch_cam_sums(const upbp_mis* cam, const int64_t* begin, const int32_t* path_length, int64_t n, uint32_t tech,
+                     uint32_t qbt, uint32_t pbt, CamSum* out, cudaStream_t s);
 
 }  // namespace upbp

@@ -55,3 +55,32 @@ def test_deterministic_candidates_and_stable_image(stage):
     for k in ("count_pb2d", "hash_pb2d", "count_bb1d", "hash_bb1d", "count_pp3d", "hash_pp3d", "pp3d"):
         np.testing.assert_array_equal(a[k], b[k])
     assert G.image_rel_l2(a["image"], b["image"]) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
+def test_mixed_mode_candidates_and_contributions(stage, path):
+    # Mixed mode: same FP32 candidate predicates (bit-exact sets), FP64 MIS partial sums and an FP64
+    # closest-approach solve for near-parallel beam pairs.  Against the FP32 reference the
+    # per-query contributions agree within 1e-4 except where the reference's own FP32 geometry
+    # cancels; the image agrees within 1e-4 rel L2.
+    w, r = G.load(path)
+    g = run(stage, w, engine.MODE_MIXED)
+    for est in ("pb2d", "bb1d", "pp3d"):
+        np.testing.assert_array_equal(g["hash_" + est], r["hash_" + est], err_msg=est)
+    for est, rk in (("pb2d", "pb2d"), ("bb1d", "bb1d_brute"), ("pp3d", "pp3d")):
+        err = G.rel_errors(g[est].astype(np.float64), r[rk].astype(np.float64))
+        assert (err <= G.RTOL).mean() >= 0.995, (est, float(err.max()))
+    assert G.image_rel_l2(g["image"], r["image"]) <= 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
+def test_image_error_against_fp64_oracle(stage, path):
+    # Both modes within 1e-3 image rel L2 of the FP64 oracle (same candidates, FP64 arithmetic).
+    from oracle import port
+    w, _ = G.load(path)
+    o64 = port.run(w, fp64=True)
+    for mode in (engine.MODE_PLAIN, engine.MODE_MIXED):
+        g = run(stage, w, mode)
+        assert G.image_rel_l2(g["image"], o64["image"]) <= 1e-3

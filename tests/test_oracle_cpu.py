@@ -65,3 +65,13 @@ def test_reference_grid_differs_from_brute_force_only_rarely(path):
     _, r = G.load(path)
     err = G.rel_errors(r["bb1d"].astype(np.float64), r["bb1d_brute"].astype(np.float64))
     assert (err > G.RTOL).mean() <= 0.01
+
+
+@pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
+def test_fp64_oracle_same_candidates_and_close_image(path):
+    # The FP64 oracle evaluates the same candidates (FP32 predicates) with FP64 arithmetic.
+    w, r = G.load(path)
+    o = port.run(w, fp64=True)
+    for est in ("pb2d", "bb1d", "pp3d"):
+        np.testing.assert_array_equal(o["hash_" + est], r["hash_" + est], err_msg=est)
+    assert G.image_rel_l2(o["image"], r["image"]) <= 1e-5
