@@ -238,8 +238,18 @@ const char* upbp_last_error(const upbp_ctx* ctx);
 
 /* Evaluation mode (UPBP_MODE_*). */
 int upbp_set_mode(upbp_ctx* ctx, int mode);
-/* Tunables picked by the autotuner: leaf size of the LBVHs and the gather block size. */
-int upbp_set_tuning(upbp_ctx* ctx, int pb2d_leaf, int bb1d_leaf, int block_threads);
+/* Tunables (picked by smallupbp_b200.autotune): LBVH leaf sizes (powers of two), the block size
+ * of the thread-per-query gathers, the BB1D beam-piece length in beam radii, and the BB1D
+ * gather variant (0: thread per query, 1: warp-cooperative persistent work queue). */
+typedef struct upbp_tuning {
+    int32_t pb2d_leaf;
+    int32_t bb1d_leaf;
+    int32_t block_threads;
+    float beam_piece_radii;
+    int32_t bb1d_kernel;
+} upbp_tuning;
+int upbp_set_tuning(upbp_ctx* ctx, const upbp_tuning* tuning);
+int upbp_get_tuning(const upbp_ctx* ctx, upbp_tuning* tuning);
 /* CUDA stream (cudaStream_t as void*) used by all later calls; NULL = the context's own stream. */
 int upbp_set_stream(upbp_ctx* ctx, void* stream);
 

@@ -59,6 +59,11 @@ class PointQueries(C.Structure):
                 ("path_length", i32p), ("throughput", f32p), ("pixel", i32p), ("cam_mis_begin", i64p)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("pb2d_leaf", C.c_int32), ("bb1d_leaf", C.c_int32), ("block_threads", C.c_int32),
+                ("beam_piece_radii", C.c_float), ("bb1d_kernel", C.c_int32)]
+
+
 class QueryStats(C.Structure):
     _fields_ = [("count_pb2d", u32p), ("hash_pb2d", u64p), ("count_bb1d", u32p), ("hash_bb1d", u64p),
                 ("count_pp3d", u32p), ("hash_pp3d", u64p)]

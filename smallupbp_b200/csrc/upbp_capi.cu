@@ -84,6 +84,9 @@ struct upbp_ctx {
     // temp storage for CUB
     DBuf cub_tmp;
     // outputs
+    DBuf work, status;
+    int num_sms = 0;
+    int bb1d_kernel = 1;  // 0: thread per query, 1: warp-cooperative persistent
     DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
     bool built = false;
     int build_launches = 0, eval_launches = 0;
@@ -168,6 +171,7 @@ DMedium derive_medium(const upbp_medium& m)
     d.mfp = has_att ? 1.0f / mx : INFINITY;
     d.g = m.mean_cosine;
     d.cont = m.continuation_prob;
+    d.gray = (d.st[0] == d.st[1] && d.st[1] == d.st[2]) ? 1 : 0;
     return d;
 }
 
@@ -540,7 +544,18 @@ void do_evaluate(upbp_ctx* c)
         S.n = c->n_beams;
         Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                   c->hash_bb1d.as<unsigned long long>(), tested + 1};
-        launch_gather_bb1d(K, L, B, S, Q, cam, cs_seg, O, c->block, mixed, s);
+        if (c->bb1d_kernel == 1) {
+            if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
+            ensure(c, c->work, sizeof(unsigned int) * 4);
+            ensure(c, c->status, sizeof(int) * 4);
+            ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
+            ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
+            const int grid = c->num_sms * bb1d_warp_blocks_per_sm(mixed);
+            launch_bb1d_warp(K, L, B, S, Q, cam, cs_seg, O, grid, mixed, c->work.as<unsigned int>(),
+                             c->status.as<int>(), s);
+        } else {
+            launch_gather_bb1d(K, L, B, S, Q, cam, cs_seg, O, c->block, mixed, s);
+        }
         c->eval_launches += 1;
     }
     ck(c, cudaEventRecord(c->ev[5], s), "event");
@@ -611,7 +626,7 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->bm_parent_leaf, &c->bm_leaf_boxes, &c->bm_node_boxes, &c->bm_flagsbuf, &c->cub_tmp,
                    &c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->image, &c->cnt_pb2d, &c->cnt_bb1d, &c->cnt_pp3d,
                    &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested, &c->light_sums, &c->cam_sums_seg,
-                   &c->cam_sums_pt};
+                   &c->cam_sums_pt, &c->work, &c->status};
     for (DBuf* b : all) free_buf(*b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
@@ -631,18 +646,37 @@ int upbp_set_mode(upbp_ctx* c, int mode)
     });
 }
 
-int upbp_set_tuning(upbp_ctx* c, int pb2d_leaf, int bb1d_leaf, int block_threads)
+static bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+int upbp_set_tuning(upbp_ctx* c, const upbp_tuning* tu)
 {
     return guarded(c, [&] {
-        if (pb2d_leaf < 1 || pb2d_leaf > 64 || bb1d_leaf < 1 || bb1d_leaf > 64)
-            fail(c, UPBP_ERR_INVALID_ARG, "leaf sizes must be in [1, 64]");
-        if (block_threads < 32 || block_threads > 256 || (block_threads % 32))
+        if (!tu) fail(c, UPBP_ERR_INVALID_ARG, "tuning is NULL");
+        if (!pow2_in(tu->pb2d_leaf, 1, 64) || !pow2_in(tu->bb1d_leaf, 1, 64))
+            fail(c, UPBP_ERR_INVALID_ARG, "leaf sizes must be powers of two in [1, 64]");
+        if (tu->block_threads < 32 || tu->block_threads > 256 || (tu->block_threads % 32))
             fail(c, UPBP_ERR_INVALID_ARG, "block_threads must be a multiple of 32 in [32, 256]");
-        c->pb2d_leaf = pb2d_leaf;
-        c->bb1d_leaf = bb1d_leaf;
-        c->block = block_threads;
+        if (!(tu->beam_piece_radii >= 1.f && tu->beam_piece_radii <= 1024.f))
+            fail(c, UPBP_ERR_INVALID_ARG, "beam_piece_radii must be in [1, 1024]");
+        if (tu->bb1d_kernel != 0 && tu->bb1d_kernel != 1) fail(c, UPBP_ERR_INVALID_ARG, "bb1d_kernel must be 0 or 1");
+        c->pb2d_leaf = tu->pb2d_leaf;
+        c->bb1d_leaf = tu->bb1d_leaf;
+        c->block = tu->block_threads;
+        c->piece_len_r = tu->beam_piece_radii;
+        c->bb1d_kernel = tu->bb1d_kernel;
         c->built = false;
     });
+}
+
+int upbp_get_tuning(const upbp_ctx* c, upbp_tuning* tu)
+{
+    if (!c || !tu) return UPBP_ERR_INVALID_ARG;
+    tu->pb2d_leaf = c->pb2d_leaf;
+    tu->bb1d_leaf = c->bb1d_leaf;
+    tu->block_threads = c->block;
+    tu->beam_piece_radii = c->piece_len_r;
+    tu->bb1d_kernel = c->bb1d_kernel;
+    return UPBP_OK;
 }
 
 int upbp_set_stream(upbp_ctx* c, void* stream)

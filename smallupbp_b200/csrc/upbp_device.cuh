@@ -68,11 +68,16 @@ struct DMedium {
     int min_idx;    // mMinAttenuationCoefIndex
     float mfp;      // mMFP
     int has_scat;   // kHasScattering
+    int gray;       // sigma_t equal in all channels: one exp per attenuation
 };
 
 // EvalAttenuation(dist) = exp(-sigma_t * dist) per channel (Media.hxx:216-229)
 __device__ __forceinline__ Rgb eval_att(const DMedium& m, float dist)
 {
+    if (m.gray) {
+        const float a = expf(-m.st[0] * dist);
+        return Rgb{a, a, a};
+    }
     return Rgb{expf(-m.st[0] * dist), expf(-m.st[1] * dist), expf(-m.st[2] * dist)};
 }
 template <typename R>

@@ -490,6 +490,167 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
     if (O.tested) atomicAdd(O.tested, tested);
 }
 
+// ----------------------------------------------------------------- warp-cooperative traversal
+// One warp per query.  Each step pops up to 32 BVH nodes from the warp's shared-memory stack
+// (one per lane), tests both child boxes, pushes internal hits (ballot + prefix counts) and
+// appends leaf hits to the warp's leaf list; once 32 leaves are gathered (or the traversal is
+// done) the warp tests the leaves' primitives 32 at a time, consecutive primitives to
+// consecutive lanes.  Returns false if the stack overflowed (the status word records it).
+constexpr int kWarpStack = 1024;
+constexpr int kWarpLeaves = 96;
+constexpr unsigned kFull = 0xffffffffu;
+
+template <class PrimFn>
+__device__ __forceinline__ bool warp_traverse(const BNode* __restrict__ nodes, int n_leaves, int n_prims, int leaf_shift,
+                                              V3 o, V3 inv, float tmin, float tmax, int* stack, int* leaves, int lane,
+                                              PrimFn&& prim)
+{
+    if (n_leaves <= 0) return true;
+    const unsigned lt = (1u << lane) - 1u;
+    int sp = 0, nleaf = 0;
+    bool ok = true;
+    if (n_leaves == 1) {
+        if (lane == 0) leaves[0] = 0;
+        nleaf = 1;
+    } else {
+        if (lane == 0) stack[0] = 0;
+        sp = 1;
+    }
+    __syncwarp();
+    while (sp > 0 || nleaf > 0) {
+        if (sp > 0 && nleaf < 32) {
+            const int take = min(sp, 32);
+            const int node = lane < take ? stack[sp - 1 - lane] : -1;
+            sp -= take;
+            __syncwarp();
+            bool hl = false, hr = false;
+            int cl = 0, cr = 0;
+            if (node >= 0) {
+                const float4 a = __ldg(&nodes[node].a);
+                const float4 b = __ldg(&nodes[node].b);
+                const float4 c = __ldg(&nodes[node].c);
+                const int4 d = __ldg(&nodes[node].d);
+                hl = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, tmin, tmax);
+                hr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv, tmin, tmax);
+                cl = d.x;
+                cr = d.y;
+            }
+            const bool pl = hl && cl >= 0, pr = hr && cr >= 0, ll = hl && cl < 0, lr = hr && cr < 0;
+            const unsigned bpl = __ballot_sync(kFull, pl), bpr = __ballot_sync(kFull, pr);
+            const unsigned bll = __ballot_sync(kFull, ll), blr = __ballot_sync(kFull, lr);
+            const int npush = __popc(bpl) + __popc(bpr);
+            if (sp + npush > kWarpStack) {
+                ok = false;  // cannot happen for the tree depths of a 30-bit Morton build
+                break;
+            }
+            const int ppos = sp + __popc(bpl & lt) + __popc(bpr & lt);
+            if (pl) stack[ppos] = cl;
+            if (pr) stack[ppos + (pl ? 1 : 0)] = cr;
+            sp += npush;
+            const int lpos = nleaf + __popc(bll & lt) + __popc(blr & lt);
+            if (ll) leaves[lpos] = ~cl;
+            if (lr) leaves[lpos + (ll ? 1 : 0)] = ~cr;
+            nleaf += __popc(bll) + __popc(blr);
+            __syncwarp();
+        }
+        if (nleaf >= 32 || (sp == 0 && nleaf > 0)) {
+            const int total = nleaf << leaf_shift;
+            for (int base = 0; base < total; base += 32) {
+                const int idx = base + lane;
+                if (idx < total) {
+                    const int p = (leaves[idx >> leaf_shift] << leaf_shift) + (idx & ((1 << leaf_shift) - 1));
+                    if (p < n_prims) prim(p);
+                }
+            }
+            nleaf = 0;
+            __syncwarp();
+        }
+    }
+    return ok;
+}
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// BB1D, warp per query, persistent: warps draw query indices from an atomic counter.
+template <bool kMixed, int kWarps>
+__global__ void __launch_bounds__(kWarps * 32) k_bb1d_warp(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+                                                          const BeamBVH B, const BeamSoA Bs, const SegQueriesDev Q,
+                                                          const upbp_mis* __restrict__ cam,
+                                                          const CamSum* __restrict__ cs, const Outputs O,
+                                                          unsigned int* __restrict__ work, int* __restrict__ status)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    __shared__ int s_stack[kWarps][kWarpStack];
+    __shared__ int s_leaves[kWarps][kWarpLeaves];
+    stage_media(K, media);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int* stack = s_stack[warp];
+    int* leaves = s_leaves[warp];
+    const int leaf_shift = __ffs(B.leaf) - 1;
+    for (;;) {
+        unsigned qq = 0;
+        if (lane == 0) qq = atomicAdd(work, 1u);
+        const int64_t q = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (q >= Q.n) break;
+        Rgb acc = rgb(0.f);
+        unsigned long long cnt = 0, h = 0, tested = 0;
+        if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D) && B.n > 0) {
+            SegCtx s;
+            init_seg_ctx<kMixed>(s, K, Q, cam, cs, q);
+            const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
+            acc = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
+                Rgb part = rgb(0.f);
+                const int mid = (int)(&m - media);
+                const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps,
+                                              s.dmax + K.eps, stack, leaves, lane, [&](int i) {
+                    const float4 pc = __ldg(&B.pc[i]);
+                    if (__float_as_int(pc.w) != mid) return;  // mMedium == medium (PhotonBeam.hxx:390)
+                    const float4 pa = __ldg(&B.pa[i]);
+                    const float4 pb = __ldg(&B.pb[i]);
+                    ++tested;
+                    float dist, sinT, t1, t2;
+                    if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f,
+                                        pa.w, pc.y, &dist, &sinT, &t1, &t2))
+                        return;
+                    if (!(t2 >= pb.w && t2 < pc.x)) return;  // this piece owns t2
+                    const int beam = __float_as_int(pc.z);
+                    const float radius = __ldg(&Bs.radius[beam]);
+                    if (radius < dist) return;  // PhotonBeam.hxx:411-413
+                    ++cnt;
+                    h += mix64((unsigned long long)beam);
+                    part = part + bb1d_contrib<kMixed>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z),
+                                                       v3(pb.x, pb.y, pb.z), radius, dist, sinT, t1, t2);
+                });
+                if (!ok && lane == 0) atomicOr(status, 1);
+                return part;
+            });
+        }
+        const float r = warp_sum(acc.r), g = warp_sum(acc.g), b = warp_sum(acc.b);
+        cnt = warp_sum_u64(cnt);
+        h = warp_sum_u64(h);
+        tested = warp_sum_u64(tested);
+        if (lane == 0) {
+            O.rgb[3 * q + 0] = r;
+            O.rgb[3 * q + 1] = g;
+            O.rgb[3 * q + 2] = b;
+            if (O.count) O.count[q] = (uint32_t)cnt;
+            if (O.hash) O.hash[q] = h;
+            const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+            splat(O.image, Q.pixel[q], thr * K.P.norm_bb1d * Rgb{r, g, b});
+            if (O.tested) atomicAdd(O.tested, tested);
+        }
+    }
+}
+
 // HashGrid::GetCellIndex (Misc/HashGrid.hxx:198-206)
 __device__ __forceinline__ uint32_t hash_cell(int x, int y, int z, int cells)
 {
@@ -619,6 +780,23 @@ void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH&
     const int grid = (int)((Q.n + block - 1) / block);
     if (mixed) k_gather_bb1d<true><<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, cs, O);
     else k_gather_bb1d<false><<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, cs, O);
+}
+
+int bb1d_warp_blocks_per_sm(bool mixed)
+{
+    int nb = 0;
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<true, 4>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<false, 4>, 128, 0);
+    return nb > 0 ? nb : 1;
+}
+
+void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
+                      const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
+                      bool mixed, unsigned int* work, int* status, cudaStream_t stream)
+{
+    if (Q.n <= 0) return;
+    if (mixed) k_bb1d_warp<true, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status);
+    else k_bb1d_warp<false, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status);
 }
 
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,

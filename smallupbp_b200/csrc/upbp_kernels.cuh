@@ -168,6 +168,10 @@ void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBV
 void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
                         const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block,
                         bool mixed, cudaStream_t stream);
+int bb1d_warp_blocks_per_sm(bool mixed);
+void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
+                      const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
+                      bool mixed, unsigned int* work, int* status, cudaStream_t stream);
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,
                         const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
                         cudaStream_t stream);

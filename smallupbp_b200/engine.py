@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libupbp_b20
 MODE_PLAIN, MODE_MIXED = 0, 1
 
 EXPORTS = (
-    "upbp_ctx_create", "upbp_ctx_destroy", "upbp_last_error", "upbp_set_mode", "upbp_set_tuning",
+    "upbp_ctx_create", "upbp_ctx_destroy", "upbp_last_error", "upbp_set_mode", "upbp_set_tuning", "upbp_get_tuning",
     "upbp_set_stream", "upbp_set_media", "upbp_set_params", "upbp_set_light_vertices", "upbp_set_beams",
     "upbp_build", "upbp_set_camera_mis", "upbp_set_segment_queries", "upbp_set_point_queries", "upbp_evaluate",
     "upbp_read_segment_results", "upbp_read_point_results", "upbp_read_query_stats", "upbp_clear_image",
@@ -60,7 +60,8 @@ def lib():
         l.upbp_last_error.argtypes = [vp]
         l.upbp_last_error.restype = C.c_char_p
         l.upbp_set_mode.argtypes = [vp, C.c_int]
-        l.upbp_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        l.upbp_set_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
+        l.upbp_get_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
         l.upbp_set_stream.argtypes = [vp, vp]
         l.upbp_set_media.argtypes = [vp, C.POINTER(abi.Medium), C.c_int32]
         l.upbp_set_params.argtypes = [vp, C.POINTER(abi.Params)]
@@ -126,8 +127,19 @@ class EstimatorStage:
     def set_mode(self, mode: int):
         self._ck(self._l.upbp_set_mode(self._ctx, mode))
 
-    def set_tuning(self, pb2d_leaf: int, bb1d_leaf: int, block_threads: int):
-        self._ck(self._l.upbp_set_tuning(self._ctx, pb2d_leaf, bb1d_leaf, block_threads))
+    def set_tuning(self, **kw):
+        """Update any of pb2d_leaf, bb1d_leaf, block_threads, beam_piece_radii, bb1d_kernel."""
+        t = self.get_tuning()
+        for k, v in kw.items():
+            if not hasattr(t, k):
+                raise KeyError(k)
+            setattr(t, k, v)
+        self._ck(self._l.upbp_set_tuning(self._ctx, C.byref(t)))
+
+    def get_tuning(self) -> "abi.Tuning":
+        t = abi.Tuning()
+        self._ck(self._l.upbp_get_tuning(self._ctx, C.byref(t)))
+        return t
 
     def set_stream(self, stream_ptr: int):
         self._ck(self._l.upbp_set_stream(self._ctx, C.c_void_p(stream_ptr)))

@@ -84,3 +84,19 @@ def test_image_error_against_fp64_oracle(stage, path):
     for mode in (engine.MODE_PLAIN, engine.MODE_MIXED):
         g = run(stage, w, mode)
         assert G.image_rel_l2(g["image"], o64["image"]) <= 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [0, 1], ids=["thread_per_query", "warp_persistent"])
+@pytest.mark.parametrize("leaf", [1, 4, 16])
+def test_bb1d_kernel_variants_same_candidates(stage, kernel, leaf):
+    # Both BB1D gathers and every leaf size / piece length find the reference's candidate set.
+    w, r = G.load(G.FIXTURES[-1])
+    stage.set_tuning(bb1d_kernel=kernel, bb1d_leaf=leaf, beam_piece_radii=4.0 if leaf == 16 else 8.0)
+    try:
+        g = run(stage, w)
+        np.testing.assert_array_equal(g["count_bb1d"], r["count_bb1d"])
+        np.testing.assert_array_equal(g["hash_bb1d"], r["hash_bb1d"])
+        G.assert_close(g["bb1d"], r["bb1d_brute"], "BB1D")
+    finally:
+        stage.set_tuning(bb1d_kernel=1, bb1d_leaf=4, beam_piece_radii=8.0)
