@@ -78,6 +78,10 @@ struct upbp_ctx {
         pc_boxes2, pc_codes, pc_codes_sorted, pc_perm, pc_perm_sorted, bbox_pc;
     int n_pieces = 0;
     DBuf bm_leaf_codes, bm_nodes, bm_parent_int, bm_parent_leaf, bm_leaf_boxes, bm_node_boxes, bm_flagsbuf;
+    DBuf pc_pay;  // mixed mode: beam payload packed per piece
+    // query order (Morton code of the query span's midpoint)
+    DBuf q_keys, q_keys_sorted, q_iota, q_order;
+    bool order_queries = true;
     int bm_n_leaves = 0;
     // mixed mode: FP64 partial sums of the MIS walks
     DBuf light_sums, cam_sums_seg, cam_sums_pt;
@@ -390,6 +394,13 @@ void do_build(upbp_ctx* c)
         build_lbvh(c, c->pc_codes_sorted.as<uint32_t>(), np, leaf, c->bm_leaf_codes, c->bm_nodes, c->bm_parent_int,
                    c->bm_parent_leaf, c->bm_leaf_boxes, c->bm_node_boxes, c->bm_flagsbuf, c->bm_n_leaves);
         c->build_launches += 10;
+        if (c->mode == UPBP_MODE_MIXED) {
+            ensure(c, c->pc_pay, sizeof(PiecePayload) * np);
+            launch_piece_payload(c->pc_c2.as<float4>(), np, c->bm_thr4.as<float4>(), c->bm_pdf4.as<float4>(),
+                                 c->bm_link.as<int2>(), c->bm_radius.as<float>(), c->lv_info4.as<int4>(),
+                                 c->lv_mis.as<upbp_mis>(), c->light_sums.as<LightSum>(), c->pc_pay.as<PiecePayload>(), s);
+            c->build_launches += 1;
+        }
     }
     ck(c, cudaEventRecord(c->ev[1], s), "event");
     ck(c, cudaGetLastError(), "build launch");
@@ -514,6 +525,27 @@ void do_evaluate(upbp_ctx* c)
     }
     ck(c, cudaEventRecord(c->ev[3], s), "event");
     const SegQueriesDev Q = seg_dev(c);
+    // Order the segment queries along a Morton curve of their midpoints, so that the warps in
+    // flight traverse neighbouring parts of the LBVHs (L2 reuse).
+    const int32_t* order = nullptr;
+    const bool have_bbox = c->n_pieces > 0 || c->n_ph > 0;
+    if (c->order_queries && nq > 1 && have_bbox) {
+        ensure(c, c->q_keys, sizeof(uint32_t) * nq);
+        ensure(c, c->q_keys_sorted, sizeof(uint32_t) * nq);
+        ensure(c, c->q_iota, sizeof(int32_t) * nq);
+        ensure(c, c->q_order, sizeof(int32_t) * nq);
+        launch_query_keys(Q, c->n_pieces > 0 ? c->bbox_pc.as<float>() : c->bbox_ph.as<float>(),
+                          c->q_keys.as<uint32_t>(), c->q_iota.as<int32_t>(), s);
+        size_t b = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, b, c->q_keys.as<uint32_t>(), c->q_keys_sorted.as<uint32_t>(),
+                                        c->q_iota.as<int32_t>(), c->q_order.as<int32_t>(), (int)nq, 0, 30, s);
+        ensure(c, c->cub_tmp, b);
+        ck(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, b, c->q_keys.as<uint32_t>(), c->q_keys_sorted.as<uint32_t>(),
+                                              c->q_iota.as<int32_t>(), c->q_order.as<int32_t>(), (int)nq, 0, 30, s),
+           "SortPairs");
+        order = c->q_order.as<int32_t>();
+        c->eval_launches += 5;
+    }
     if (nq > 0) {
         PhotonBVH B{};
         B.pos = c->pb_pos.as<float4>();
@@ -523,7 +555,7 @@ void do_evaluate(upbp_ctx* c)
         B.n_leaves = c->pb_n_leaves;
         Outputs O{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
                   c->hash_pb2d.as<unsigned long long>(), tested + 0};
-        launch_gather_pb2d(K, L, B, Q, cam, cs_seg, O, c->block, mixed, s);
+        launch_gather_pb2d(K, L, B, Q, cam, cs_seg, O, c->block, mixed, s, order);
         c->eval_launches += 1;
     }
     ck(c, cudaEventRecord(c->ev[4], s), "event");
@@ -534,6 +566,7 @@ void do_evaluate(upbp_ctx* c)
         B.pc = c->pc_c2.as<float4>();
         B.nodes = c->bm_nodes.as<BNode>();
         B.n = c->n_pieces;
+        B.pay = mixed ? c->pc_pay.as<PiecePayload>() : nullptr;
         B.leaf = std::max(1, c->bb1d_leaf);
         B.n_leaves = c->bm_n_leaves;
         BeamSoA S{};
@@ -552,7 +585,7 @@ void do_evaluate(upbp_ctx* c)
             ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
             const int grid = c->num_sms * bb1d_warp_blocks_per_sm(mixed);
             launch_bb1d_warp(K, L, B, S, Q, cam, cs_seg, O, grid, mixed, c->work.as<unsigned int>(),
-                             c->status.as<int>(), s);
+                             c->status.as<int>(), order, s);
         } else {
             launch_gather_bb1d(K, L, B, S, Q, cam, cs_seg, O, c->block, mixed, s);
         }
@@ -626,7 +659,8 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->bm_parent_leaf, &c->bm_leaf_boxes, &c->bm_node_boxes, &c->bm_flagsbuf, &c->cub_tmp,
                    &c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->image, &c->cnt_pb2d, &c->cnt_bb1d, &c->cnt_pp3d,
                    &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested, &c->light_sums, &c->cam_sums_seg,
-                   &c->cam_sums_pt, &c->work, &c->status};
+                   &c->cam_sums_pt, &c->work, &c->status, &c->pc_pay, &c->q_keys, &c->q_keys_sorted, &c->q_iota,
+                   &c->q_order};
     for (DBuf* b : all) free_buf(*b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);

@@ -127,9 +127,10 @@ struct SegCtx {
     float last_pdf_w_inv;
     uint32_t ray_flags;        // beamType | estimatorTechniques
     const upbp_mis* cam;
-    // mixed mode: camera entry L-1 and the FP64 suffix of the camera walk
-    upbp_mis e;
-    CamSum cs;
+    // mixed mode: camera entry L-1 and the FP64 suffix of the camera walk (the warp kernel keeps
+    // them in shared memory: they are the same for the whole warp)
+    const upbp_mis* e;
+    const CamSum* cs;
 };
 
 __device__ __forceinline__ void fill_cand(upbp_mis& c, const upbp_params& P, float pdf_a_inv, float rsp_inv,
@@ -195,7 +196,7 @@ __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const Light
     const upbp_mis lvm = load_mis(Lv.mis + lv);
     if (kMixed) {
         const double wc = camera_weight_fast(s.L, cand, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
-                                             camRevPdfW * rsr / distSq, s.e, 1.0f / rsr, s.cs, s.ray_flags,
+                                             camRevPdfW * rsr / distSq, *s.e, 1.0f / rsr, *s.cs, s.ray_flags,
                                              P.query_beam_type, P.photon_beam_type);
         const LightSum ls = Lv.sums[lv];
         const double wl = (double)last * (ls.a + (double)camDirPdfW * ls.c);
@@ -308,8 +309,8 @@ __device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const Light
     const bool onDeltaLight = (lvm.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (lvm.flags & UPBP_MIS_IS_DELTA);
     const float ntl = onDeltaLight ? 0.f : bsdfDirPdfW * rsrB * fabsf(lvm.cos_theta_out) / distSqB;
     if (kMixed) {
-        const double wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ, s.e,
-                                             1.0f / rsrQ, s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
+        const double wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ, *s.e,
+                                             1.0f / rsrQ, *s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
         const LightSum ls = Lv.sums[lvi];
         double inner = (double)ls.bptb;
         if (!(s.ray_flags & UPBP_PREVIOUS)) inner += (double)ntl * (ls.d + ls.e * (double)(1.0f / rsrB));
@@ -324,6 +325,73 @@ __device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const Light
                                            P.photon_beam_type, s.ray_flags, Lv.path_ends, lview, &brec);
     const float w = 1.f / (wLight + wCamera);
     return w * unweighted;
+}
+
+// PhotonBeam::accumulate2 (mixed mode) with the beam's payload packed per piece.
+__device__ Rgb bb1d_contrib_packed(const GatherConsts& K, const DMedium& m, const SegCtx& s, const PiecePayload& py,
+                                   V3 bo, V3 bdir, float dist, float sinTheta, float t1, float t2)
+{
+    const upbp_params& P = K.P;
+    const int lvbits = __float_as_int(py.lv.w);
+    const int pl = lvbits & 0x3fffffff;
+    const bool finite = (lvbits >> 30) & 1;
+    if ((uint32_t)(pl + 1 + s.L) > P.max_path_length || (uint32_t)(pl + 1 + s.L) < P.min_path_length) return rgb(0.f);
+    {
+        const float c = s.d.x * bdir.x + s.d.y * bdir.y + s.d.z * bdir.z;
+        if (1.f - c * c < 1e-2f) closest_approach_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
+    }
+    if (s.L == 1 && t1 < P.min_dist_to_med) return rgb(0.f);
+    const float radius = py.lv.z;
+    const uint32_t bflags = (uint32_t)__float_as_int(py.thr.w);
+    const uint32_t brsf = (uint32_t)__float_as_int(py.pdf.w);
+    Rgb att = eval_att(m, t1 - s.dmin);
+    const float pfdQ = comp(att, m.min_idx);
+    if (s.ray_flags & UPBP_SHORT_BEAM) att = att / pfdQ;
+    float rspQ = m.min_st * pfdQ;
+    float rsrQ = (s.rsf & UPBP_ORIGIN_IN_MEDIUM) ? rspQ : pfdQ;
+    const float ratioQ = 1.0f / m.min_st;
+    const Rgb batt = eval_att(m, t2);
+    att = att * batt;
+    const float pfdB = comp(batt, m.min_idx);
+    if (bflags & UPBP_SHORT_BEAM) att = att / pfdB;
+    float rspB = m.min_st * pfdB;
+    float rsrB = (brsf & UPBP_ORIGIN_IN_MEDIUM) ? rspB : pfdB;
+    const float ratioB = ratioQ;
+    if (!rgb_positive(att)) return rgb(0.f);
+    rspQ *= s.rs_pdf;
+    rsrQ *= s.rs_rev_pdf;
+    rspB *= py.pdf.x;
+    rsrB *= py.pdf.y;
+    float sinDummy;
+    const float phase = hg_pdf(neg3(s.d), neg3(bdir), m.g, &sinDummy);
+    if (phase <= 0.f) return rgb(0.f);
+    const float bsdfPdfW = phase * m.cont;
+    const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
+    const Rgb unweighted = (Rgb{py.thr.x, py.thr.y, py.thr.z} * ss * att * phase *
+                            (1.f - dist * dist / (radius * radius))) * 3.f / (4.f * radius * sinTheta);
+    if (rgb_black_or_neg(unweighted)) return rgb(0.f);
+    const float distSqQ = t1 * t1;
+    const float rspInvQ = 1.0f / rspQ;
+    upbp_mis cand;
+    fill_cand(cand, P, s.last_pdf_w_inv * distSqQ * rspInvQ, rspInvQ, ratioQ, 1.0f, UPBP_MIS_IN_MEDIUM_WITH_BEAMS);
+    const float distSqB = finite ? t2 * t2 : 1.0f;
+    const float rspInvB = 1.0f / rspB;
+    const float brecPdfAInv = py.pdf.z * distSqB * rspInvB;
+    const float sinT = (s.ray_flags & UPBP_NO_SINE_IN_WEIGHTS) ? 1.0f : sinTheta;
+    const float f = cand.bb1d_factor;
+    float last;
+    if (s.ray_flags & UPBP_SHORT_BEAM)
+        last = (bflags & UPBP_SHORT_BEAM) ? (float)(1.0 / (double)(ratioQ * ratioB * f * sinT))
+                                          : rspB / (ratioQ * f * sinT);
+    else
+        last = (bflags & UPBP_SHORT_BEAM) ? rspQ / (ratioB * f * sinT) : rspQ * rspB / (f * sinT);
+    const double wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfPdfW * rsrQ / distSqQ, *s.e,
+                                         1.0f / rsrQ, *s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
+    const float ntl = bsdfPdfW * rsrB * py.lv.x / distSqB;
+    double inner = (double)py.lv.y;
+    if (!(s.ray_flags & UPBP_PREVIOUS)) inner += (double)ntl * (py.mis.x + py.mis.y * (double)(1.0f / rsrB));
+    const double wl = (double)last * (double)brecPdfAInv * inner;
+    return (float)(1.0 / (wl + wc)) * unweighted;
 }
 
 // ----------------------------------------------------------------- segment loop
@@ -373,7 +441,8 @@ __device__ __forceinline__ Rgb segment_loop(const GatherConsts& K, const DMedium
 
 template <bool kMixed>
 __device__ __forceinline__ void init_seg_ctx(SegCtx& s, const GatherConsts& K, const SegQueriesDev& Q,
-                                             const upbp_mis* cam, const CamSum* cs, int64_t q)
+                                             const upbp_mis* cam, const CamSum* cs, int64_t q, upbp_mis* e_store,
+                                             CamSum* cs_store, bool leader = true)
 {
     s.o = v3(Q.origin[3 * q], Q.origin[3 * q + 1], Q.origin[3 * q + 2]);
     s.d = v3(Q.direction[3 * q], Q.direction[3 * q + 1], Q.direction[3 * q + 2]);
@@ -381,9 +450,11 @@ __device__ __forceinline__ void init_seg_ctx(SegCtx& s, const GatherConsts& K, c
     s.last_pdf_w_inv = Q.last_pdf_w_inv[q];
     s.ray_flags = K.P.query_beam_type | K.P.techniques;
     s.cam = cam + Q.cam_mis_begin[q];
-    if (kMixed) {
-        if (s.L >= 2) s.e = load_mis(s.cam + s.L - 1);
-        s.cs = cs[q];
+    s.e = e_store;
+    s.cs = cs_store;
+    if (kMixed && leader) {
+        if (s.L >= 2) *e_store = load_mis(s.cam + s.L - 1);
+        *cs_store = cs[q];
     }
 }
 
@@ -404,18 +475,21 @@ template <bool kMixed>
 __global__ void __launch_bounds__(256) k_gather_pb2d(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                      const PhotonBVH B, const SegQueriesDev Q,
                                                      const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
-                                                     const Outputs O)
+                                                     const Outputs O, const int32_t* __restrict__ order)
 {
     __shared__ DMedium media[UPBP_MAX_MEDIA];
     stage_media(K, media);
-    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (q >= Q.n) return;
+    const int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (item >= Q.n) return;
+    const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
     uint32_t cnt = 0;
     unsigned long long h = 0, tested = 0;
     Rgb res = rgb(0.f);
     if ((Q.flags[q] & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && B.n > 0) {
         SegCtx s;
-        init_seg_ctx<kMixed>(s, K, Q, cam, cs, q);
+        upbp_mis e_store;
+        CamSum cs_store;
+        init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &e_store, &cs_store);
         const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
         const float r2 = K.P.radius_pb2d * K.P.radius_pb2d;
         res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
@@ -456,7 +530,9 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
     Rgb res = rgb(0.f);
     if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D) && B.n > 0) {
         SegCtx s;
-        init_seg_ctx<kMixed>(s, K, Q, cam, cs, q);
+        upbp_mis e_store;
+        CamSum cs_store;
+        init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &e_store, &cs_store);
         const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
         res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
             Rgb acc = rgb(0.f);
@@ -582,15 +658,18 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 
 // BB1D, warp per query, persistent: warps draw query indices from an atomic counter.
 template <bool kMixed, int kWarps>
-__global__ void __launch_bounds__(kWarps * 32) k_bb1d_warp(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+__global__ void __launch_bounds__(kWarps * 32, 5) k_bb1d_warp(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                           const BeamBVH B, const BeamSoA Bs, const SegQueriesDev Q,
                                                           const upbp_mis* __restrict__ cam,
                                                           const CamSum* __restrict__ cs, const Outputs O,
-                                                          unsigned int* __restrict__ work, int* __restrict__ status)
+                                                          unsigned int* __restrict__ work, int* __restrict__ status,
+                                                          const int32_t* __restrict__ order)
 {
     __shared__ DMedium media[UPBP_MAX_MEDIA];
     __shared__ int s_stack[kWarps][kWarpStack];
     __shared__ int s_leaves[kWarps][kWarpLeaves];
+    __shared__ upbp_mis s_e[kWarps];
+    __shared__ CamSum s_cs[kWarps];
     stage_media(K, media);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int* stack = s_stack[warp];
@@ -599,13 +678,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_bb1d_warp(const __grid_constant
     for (;;) {
         unsigned qq = 0;
         if (lane == 0) qq = atomicAdd(work, 1u);
-        const int64_t q = (int64_t)__shfl_sync(kFull, qq, 0);
-        if (q >= Q.n) break;
+        const int64_t item = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (item >= Q.n) break;
+        const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
         Rgb acc = rgb(0.f);
         unsigned long long cnt = 0, h = 0, tested = 0;
         if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D) && B.n > 0) {
             SegCtx s;
-            init_seg_ctx<kMixed>(s, K, Q, cam, cs, q);
+            init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &s_e[warp], &s_cs[warp], lane == 0);
+            __syncwarp();
             const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
             acc = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
                 Rgb part = rgb(0.f);
@@ -623,12 +704,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_bb1d_warp(const __grid_constant
                         return;
                     if (!(t2 >= pb.w && t2 < pc.x)) return;  // this piece owns t2
                     const int beam = __float_as_int(pc.z);
-                    const float radius = __ldg(&Bs.radius[beam]);
+                    const float radius = kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[beam]);
                     if (radius < dist) return;  // PhotonBeam.hxx:411-413
                     ++cnt;
                     h += mix64((unsigned long long)beam);
-                    part = part + bb1d_contrib<kMixed>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z),
-                                                       v3(pb.x, pb.y, pb.z), radius, dist, sinT, t1, t2);
+                    if (kMixed) {
+                        const PiecePayload py = B.pay[i];
+                        part = part + bb1d_contrib_packed(K, m, s, py, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
+                                                          dist, sinT, t1, t2);
+                    } else {
+                        part = part + bb1d_contrib<false>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z),
+                                                          v3(pb.x, pb.y, pb.z), radius, dist, sinT, t1, t2);
+                    }
                 });
                 if (!ok && lane == 0) atomicOr(status, 1);
                 return part;
@@ -764,12 +851,12 @@ __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ Gat
 
 void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,
                         const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
-                        cudaStream_t stream)
+                        cudaStream_t stream, const int32_t* order)
 {
     if (Q.n <= 0) return;
     const int grid = (int)((Q.n + block - 1) / block);
-    if (mixed) k_gather_pb2d<true><<<grid, block, 0, stream>>>(K, L, B, Q, cam, cs, O);
-    else k_gather_pb2d<false><<<grid, block, 0, stream>>>(K, L, B, Q, cam, cs, O);
+    if (mixed) k_gather_pb2d<true><<<grid, block, 0, stream>>>(K, L, B, Q, cam, cs, O, order);
+    else k_gather_pb2d<false><<<grid, block, 0, stream>>>(K, L, B, Q, cam, cs, O, order);
 }
 
 void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
@@ -792,11 +879,73 @@ int bb1d_warp_blocks_per_sm(bool mixed)
 
 void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
                       const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
-                      bool mixed, unsigned int* work, int* status, cudaStream_t stream)
+                      bool mixed, unsigned int* work, int* status, const int32_t* order, cudaStream_t stream)
 {
     if (Q.n <= 0) return;
-    if (mixed) k_bb1d_warp<true, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status);
-    else k_bb1d_warp<false, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status);
+    if (mixed) k_bb1d_warp<true, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+    else k_bb1d_warp<false, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+}
+
+namespace {
+__global__ void k_piece_payload(const float4* __restrict__ pc, int n, const float4* __restrict__ bm_thr,
+                                const float4* __restrict__ bm_pdf, const int2* __restrict__ bm_link,
+                                const float* __restrict__ bm_radius, const int4* __restrict__ lv_info,
+                                const upbp_mis* __restrict__ lv_mis, const LightSum* __restrict__ sums,
+                                PiecePayload* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int beam = __float_as_int(pc[i].z);
+    const int lv = bm_link[beam].x;
+    const upbp_mis m = load_mis(lv_mis + lv);
+    const int4 info = lv_info[lv];
+    const bool onDelta = (m.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (m.flags & UPBP_MIS_IS_DELTA);
+    const LightSum ls = sums[lv];
+    PiecePayload p;
+    p.thr = bm_thr[beam];
+    p.pdf = bm_pdf[beam];
+    const int bits = (info.y & 0x3fffffff) | (((info.z & UPBP_LV_IS_FINITE) ? 1 : 0) << 30);
+    p.lv = make_float4(onDelta ? 0.f : fabsf(m.cos_theta_out), ls.bptb, bm_radius[beam], __int_as_float(bits));
+    p.mis = make_double2(ls.d, ls.e);
+    out[i] = p;
+}
+
+// Morton code of the middle of a segment query's span (10 bits per axis in the given box).
+__global__ void k_query_keys(const SegQueriesDev Q, const float* __restrict__ bb, uint32_t* keys, int32_t* iota)
+{
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= Q.n) return;
+    const int sb = Q.seg_begin[q], sc = Q.seg_count[q];
+    const float t = sc > 0 ? 0.5f * (Q.seg_dist_min[sb] + Q.seg_dist_max[sb + sc - 1]) : 0.f;
+    const float tm = isfinite(t) ? t : (sc > 0 ? Q.seg_dist_min[sb] : 0.f);
+    float p[3];
+    for (int c = 0; c < 3; ++c) p[c] = Q.origin[3 * q + c] + Q.direction[3 * q + c] * tm;
+    uint32_t code = 0;
+    uint32_t ix[3];
+    for (int c = 0; c < 3; ++c) {
+        const float ext = bb[3 + c] - bb[c];
+        const float u = ext > 0.f ? (p[c] - bb[c]) / ext : 0.f;
+        ix[c] = (uint32_t)fminf(fmaxf(u * 1024.f, 0.f), 1023.f);
+    }
+    for (int b = 9; b >= 0; --b)
+        code = (code << 3) | (((ix[0] >> b) & 1u) << 2) | (((ix[1] >> b) & 1u) << 1) | ((ix[2] >> b) & 1u);
+    keys[q] = code;
+    iota[q] = (int32_t)q;
+}
+}  // namespace
+
+void launch_piece_payload(const float4* pc, int n, const float4* bm_thr, const float4* bm_pdf, const int2* bm_link,
+                          const float* bm_radius, const int4* lv_info, const upbp_mis* lv_mis, const LightSum* sums,
+                          PiecePayload* out, cudaStream_t stream)
+{
+    if (n > 0)
+        k_piece_payload<<<(n + 255) / 256, 256, 0, stream>>>(pc, n, bm_thr, bm_pdf, bm_link, bm_radius, lv_info, lv_mis,
+                                                             sums, out);
+}
+
+void launch_query_keys(const SegQueriesDev& Q, const float* bbox, uint32_t* keys, int32_t* iota, cudaStream_t stream)
+{
+    if (Q.n > 0) k_query_keys<<<(int)((Q.n + 255) / 256), 256, 0, stream>>>(Q, bbox, keys, iota);
 }
 
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,

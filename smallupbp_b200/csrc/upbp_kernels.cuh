@@ -42,12 +42,22 @@ struct PhotonBVH {
     int n_leaves;
 };
 
+// Payload of the beam a piece belongs to, packed per piece (mixed mode): everything an accepted
+// candidate reads besides the piece geometry, so it comes from the lines the warp just tested.
+struct __align__(16) PiecePayload {
+    float4 thr;   // beam throughput at origin rgb, beam flags (int bits)
+    float4 pdf;   // beam ray_sample_pdf, ray_sample_rev_pdf, last_pdf_w_inv, ray_sampling_flags (int bits)
+    float4 lv;    // light vertex |cos_theta_out| (0 on a delta light), bptb, radius, path_length | finite << 30
+    double2 mis;  // light vertex FP64 partial sums d, e (LightSum)
+};
+
 // Beam pieces (BB1D) in leaf order.  Piece = beam sub-interval [t_lo, t_hi).
 struct BeamBVH {
     const float4* pa;    // beam origin xyz, beam length
     const float4* pb;    // beam direction xyz, t_lo
     const float4* pc;    // t_hi, max radius^2, beam id (int bits), medium (int bits)
     const BNode* nodes;
+    const PiecePayload* pay;  // mixed mode, per piece
     int n;
     int leaf;
     int n_leaves;
@@ -164,14 +174,18 @@ void launch_box_leaf_boxes(const Box* boxes, int n, int leaf, Box* leaf_boxes, c
 struct CamSum;
 void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,
                         const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
-                        cudaStream_t stream);
+                        cudaStream_t stream, const int32_t* order = nullptr);
 void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
                         const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block,
                         bool mixed, cudaStream_t stream);
+void launch_piece_payload(const float4* pc, int n, const float4* bm_thr, const float4* bm_pdf, const int2* bm_link,
+                          const float* bm_radius, const int4* lv_info, const upbp_mis* lv_mis,
+                          const struct LightSum* sums, PiecePayload* out, cudaStream_t stream);
+void launch_query_keys(const SegQueriesDev& Q, const float* bbox, uint32_t* keys, int32_t* iota, cudaStream_t stream);
 int bb1d_warp_blocks_per_sm(bool mixed);
 void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
                       const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
-                      bool mixed, unsigned int* work, int* status, cudaStream_t stream);
+                      bool mixed, unsigned int* work, int* status, const int32_t* order, cudaStream_t stream);
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,
                         const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
                         cudaStream_t stream);
