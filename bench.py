@@ -156,7 +156,7 @@ def input_bytes(w) -> int:
 
 def run_b200(args, cfg, rank, world, local_rank):
     import torch
-    from smallupbp_b200 import abi, engine, workload as W
+    from smallupbp_b200 import abi, engine, multi, workload as W
 
     torch.cuda.set_device(local_rank)
     dev = local_rank
@@ -168,8 +168,7 @@ def run_b200(args, cfg, rank, world, local_rank):
     n_iter = max(1, min(args.iterations, args.steps))
     t0 = time.time()
     works = []
-    for j in range(n_iter):
-        it = rank + world * j
+    for it in multi.rank_iterations(rank, world, n_iter):
         works.append(W.generate(cfg, iteration=it))
     gen_s = time.time() - t0
     stream = torch.cuda.Stream(device=dev)
@@ -228,13 +227,8 @@ def run_b200(args, cfg, rank, world, local_rank):
     # max over ranks, total units over ranks
     ms_max, units_total = ms, done_units
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        u = torch.tensor([float(done_units)], device="cuda")
-        dist.all_reduce(u)
-        units_total = int(u.item())
+        ms_max = multi.max_over_ranks(ms, "cuda")
+        units_total = int(multi.sum_over_ranks(done_units, "cuda"))
     value = units_total / (ms_max / 1000.0)
 
     # candidate statistics (outside the timed region) for the roofline
@@ -285,10 +279,7 @@ def run_b200(args, cfg, rank, world, local_rank):
         torch.cuda.synchronize()
         e_ms = e0.elapsed_time(e1)
         if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+            e_ms = multi.max_over_ranks(e_ms, "cuda")
         e2e = {"value": e_units * args.steps * world / (e_ms / 1000.0), "unit": "queries/s",
                "h2d_bytes_per_step": input_bytes(works[0]), "d2h_bytes_per_step": npix * 3 * 4,
                "ms_per_step": e_ms / args.steps}
