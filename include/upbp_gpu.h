@@ -292,6 +292,24 @@ int upbp_last_launch_count(const upbp_ctx* ctx, int* build_launches, int* evalua
 /* Average duration (ms) of the last evaluate's dominant gather kernel, measured with CUDA events. */
 int upbp_last_timings(const upbp_ctx* ctx, float* build_ms, float* pp3d_ms, float* pb2d_ms, float* bb1d_ms);
 
+/* Allocation-free PP3D evaluation.  No counterpart in the reference: its HashGrid::Build and
+ * HashGrid::Process with UPBP::RangeQuery (plain FP32 mode) for callers that cannot allocate
+ * device memory -- a renderer plug-in inside a host application that owns the device memory
+ * budget, code running during CUDA graph capture, or an embedded caller that reserves all
+ * memory up front.  All pointers inside lv / pq and cam_mis / out_rgb ([pq->n][3]) are device
+ * pointers the caller owns; nothing is allocated.  The scratch memory is one fixed array of
+ * about 18 MiB inside the library, held on every GPU that loads it until the process exits;
+ * it limits lv->n to UPBP_NOALLOC_MAX_LIGHT_VERTICES and params->hash_cells to
+ * UPBP_NOALLOC_MAX_HASH_CELLS (larger sizes return UPBP_ERR_CAPACITY).  The first call on a
+ * device looks up that device's scratch address, so make the first call before any stream
+ * capture.  Every call shares the scratch array: calls that overlap on the GPU (other
+ * streams, other host threads) race, so serialise them.  stream = cudaStream_t or NULL. */
+#define UPBP_NOALLOC_MAX_LIGHT_VERTICES (1 << 17)
+#define UPBP_NOALLOC_MAX_HASH_CELLS (1 << 17)
+int upbp_pp3d_evaluate_noalloc(const upbp_params* params, const upbp_medium* media, int32_t n_media,
+                               const upbp_light_vertices* lv, const upbp_mis* cam_mis,
+                               const upbp_point_queries* pq, float* out_rgb, void* stream);
+
 /* Releases the per-iteration structures; replaces EmbreeBre::destroy and
  * PhotonBeamsEvaluator::destroy (UPBP.hxx:1172-1181).  Device buffers are
  * kept for reuse by the next iteration. */
