@@ -48,12 +48,20 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="cube1024")
-    ap.add_argument("--mode", default="plain", choices=["mixed", "plain"])
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--iterations", type=int, default=2, help="distinct iteration workloads cycled per rank")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="time forward + adjoint (dL/d sigma_a, sigma_s, g) of an L2 image loss instead")
+    ap.add_argument("--dropin", action="store_true",
+                    help="the plain FP32 drop-in: thread-per-query BB1D gather, plain mode, default tuning")
+    a = ap.parse_args()
+    if a.dropin:
+        a.mode, a.no_autotune = "plain", True
+    return a
 
 
 def dist_env():
@@ -169,19 +177,31 @@ def run_b200(args, cfg, rank, world, local_rank):
     t0 = time.time()
     works = []
     for it in multi.rank_iterations(rank, world, n_iter):
-        works.append(W.generate(cfg, iteration=it))
+        works.append(W.make(cfg, iteration=it))
     gen_s = time.time() - t0
     stream = torch.cuda.Stream(device=dev)
     npix = cfg.width * cfg.height
     img_t = torch.zeros(npix * 3, dtype=torch.float32, device="cuda")
-    stages = []
+    stages, all_structs = [], []
     for w in works:
         st = engine.EstimatorStage(dev, mode)
         st.set_stream(stream.cuda_stream)
         s = abi.make_structs(w)
         st.load(w, s)
         st.set_queries(w, s)
+        if args.dropin:
+            st.set_tuning(bb1d_kernel=0)
         stages.append(st)
+        all_structs.append(s)
+    tuning = {"best": {k: getattr(stages[0].get_tuning(), k) for k, _ in abi.Tuning._fields_}, "autotuned": False}
+    if not args.no_autotune:
+        from smallupbp_b200 import autotune
+        t_at = time.time()
+        with torch.cuda.stream(stream):
+            best, rep = autotune.autotune(stages[0], all_structs[0][0])
+        for st in stages[1:]:
+            st.set_tuning(**best)
+        tuning = {"best": best, "autotuned": True, "trials": rep["trials"], "seconds": time.time() - t_at}
     units = [len(w["sq_path_length"]) + len(w["pq_path_length"]) for w in works]
 
     def step(i):
@@ -239,6 +259,7 @@ def run_b200(args, cfg, rank, world, local_rank):
     stats = st0.query_stats()
     nq, npq = len(works[0]["sq_path_length"]), len(works[0]["pq_path_length"])
     acc = {k: int(stats["count_" + k].astype(np.int64).sum()) for k in ("pb2d", "bb1d", "pp3d")}
+    tested = st0.tested_counts()
     alg = {"pp3d": BYTES_PER_QUERY * npq + BYTES_PER_POINT_CAND * acc["pp3d"],
            "pb2d": BYTES_PER_QUERY * nq + BYTES_PER_POINT_CAND * acc["pb2d"],
            "bb1d": BYTES_PER_QUERY * nq + BYTES_PER_BB1D * acc["bb1d"]}
@@ -261,6 +282,7 @@ def run_b200(args, cfg, rank, world, local_rank):
         pw = pinned_copy(works[0])
         st = engine.EstimatorStage(dev, mode)
         st.set_stream(stream.cuda_stream)
+        st.set_tuning(**tuning["best"])
         host_img = torch.empty(npix * 3, dtype=torch.float32).pin_memory()
         s = abi.make_structs(pw)
         e_units = units[0]
@@ -312,13 +334,16 @@ def run_b200(args, cfg, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f32" if args.mode == "plain" else "f32+f64",
         "data": "synthetic: seeded UPBP light/camera passes (Philox) in the %s scene; no dataset" % cfg.name,
-        "config": dict(workload_desc(cfg), mode=args.mode, iterations_cycled=n_iter,
+        "config": dict(workload_desc(cfg), mode=args.mode + (" drop-in (thread per query)" if args.dropin else ""),
+                       iterations_cycled=n_iter,
                        queries_per_iteration={"segment": nq, "point": npq},
                        photons=int((works[0]["lv_flags"] & 1).sum()), beams=len(works[0]["beam_length"]),
-                       parallelism="dp%d (one iteration per rank, framebuffer all-reduce)" % world),
+                       parallelism="dp%d (one iteration per rank, framebuffer all-reduce)" % world,
+                       tuning=tuning),
         "ms_per_iteration": ms_max / args.steps,
         "kernels_ms": avg,
         "accepted_candidates": acc,
+        "tested_candidates": tested,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg[dom]},
@@ -373,7 +398,7 @@ def run_reference(args, cfg, rank, world):
     from smallupbp_b200 import workload as W
     if not ref.available():
         return {"impl": "reference", "unavailable": "oracle/_ref (reference built from its sources) is not present"}
-    w = W.generate(cfg, iteration=0)
+    w = W.make(cfg, iteration=0)
     cores = os.cpu_count() or 1
     threads = cores
     try:
@@ -410,6 +435,75 @@ def run_reference(args, cfg, rank, world):
     }
 
 
+def run_adjoint(args, cfg, rank, world, local_rank):
+    """Differentiable estimator: one step = forward (mixed mode) + adjoint of the L2 loss against a
+    target rendered with sigma_s = 0.7, sigma_a = 0.05, g = 0.5 (from sigma_s = 0.5, sigma_a = 0.1,
+    g = 0.3), gradients with respect to the grey sigma_a, sigma_s and g of the scene's medium."""
+    import torch
+    from smallupbp_b200 import autograd, engine, workload as W
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = W.make(cfg, iteration=rank)
+    stream = torch.cuda.Stream(device=dev)
+    st = engine.EstimatorStage(local_rank, engine.MODE_MIXED)
+    st.set_stream(stream.cuda_stream)
+    media = np.array(w["media"], copy=True)
+    medium = 1
+    units = len(w["sq_path_length"]) + len(w["pq_path_length"])
+
+    def grey(v, grad=False):
+        return torch.full((3,), v, dtype=torch.float64, device=dev, requires_grad=grad)
+
+    with torch.cuda.stream(stream):
+        st.run(w)
+        torch.cuda.reset_peak_memory_stats(dev)
+        tgt = autograd.render(st, media, medium, grey(0.05), grey(0.7), torch.tensor(0.5, dtype=torch.float64,
+                                                                                       device=dev)).detach().clone()
+
+        def step():
+            sa, ss = grey(0.1, True), grey(0.5, True)
+            g = torch.tensor(0.3, dtype=torch.float64, device=dev, requires_grad=True)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            img = autograd.render(st, media, medium, sa, ss, g)
+            loss = ((img.double() - tgt.double()) ** 2).sum()
+            e1.record(stream)
+            loss.backward()
+            e2.record(stream)
+            return e0, e1, e2, (sa.grad.sum().item(), ss.grad.sum().item(), g.grad.item()), loss.item()
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        fwd, bwd = [], []
+        ev_first = ev_last = None
+        for _ in range(args.steps):
+            e0, e1, e2, grads, loss = step()
+            torch.cuda.synchronize(dev)
+            fwd.append(e0.elapsed_time(e1))
+            bwd.append(e1.elapsed_time(e2))
+            ev_first = ev_first or e0
+            ev_last = e2
+        total_ms = ev_first.elapsed_time(ev_last)
+    peak = st.device_bytes() + torch.cuda.max_memory_allocated(dev)
+    st.close()
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC + " (forward + adjoint)", "value": units * args.steps / (total_ms / 1000.0), "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (adjoint f64 duals)",
+        "data": "synthetic: seeded UPBP light/camera passes (Philox) in the %s scene; no dataset" % cfg.name,
+        "config": dict(workload_desc(cfg), mode="mixed forward + dual-number adjoint",
+                       loss="sum (I - I_target)^2, target sigma_s=0.7 sigma_a=0.05 g=0.5, at sigma_s=0.5 "
+                            "sigma_a=0.1 g=0.3"),
+        "adjoint": {"forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
+                    "peak_device_bytes": int(peak), "loss": loss,
+                    "grad": {"sigma_a": grads[0], "sigma_s": grads[1], "g": grads[2]}},
+    }
+
+
 def main():
     args = parse()
     rank, world, local_rank = dist_env()
@@ -417,6 +511,8 @@ def main():
     cfg = W.config(args.config)
     if args.impl == "reference":
         line = run_reference(args, cfg, rank, world)
+    elif args.adjoint:
+        line = run_adjoint(args, cfg, rank, world, local_rank)
     else:
         line = run_b200(args, cfg, rank, world, local_rank)
     if rank == 0 and line is not None:

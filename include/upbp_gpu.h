@@ -85,6 +85,8 @@ extern "C" {
 /* evaluation modes */
 #define UPBP_MODE_PLAIN 0 /* all-FP32, MIS walks the stored subpaths per candidate (reference order) */
 #define UPBP_MODE_MIXED 1 /* FP32 bulk, FP64 near-parallel BB1D solve and FP64 MIS suffix sums */
+#define UPBP_MODE_FP64 2  /* FP64 oracle on the GPU: the same FP32 candidate predicates, candidate
+                                * geometry re-solved in FP64, all contribution and MIS arithmetic FP64 */
 
 /* ---- records ------------------------------------------------------------ */
 
@@ -240,7 +242,8 @@ const char* upbp_last_error(const upbp_ctx* ctx);
 int upbp_set_mode(upbp_ctx* ctx, int mode);
 /* Tunables (picked by smallupbp_b200.autotune): LBVH leaf sizes (powers of two), the block size
  * of the thread-per-query gathers, the BB1D beam-piece length in beam radii, and the BB1D
- * gather variant (0: thread per query, 1: warp-cooperative persistent work queue). */
+ * gather variant (0: thread per query, 1: warp-cooperative persistent work queue at 5 blocks of
+ * 4 warps per SM, 2: the same kernel compiled for 6 blocks per SM). */
 typedef struct upbp_tuning {
     int32_t pb2d_leaf;
     int32_t bb1d_leaf;
@@ -285,6 +288,21 @@ int upbp_evaluate(upbp_ctx* ctx);
 int upbp_read_segment_results(upbp_ctx* ctx, float* pb2d_rgb, float* bb1d_rgb); /* [n][3] each, may be NULL */
 int upbp_read_point_results(upbp_ctx* ctx, float* pp3d_rgb);                    /* [n][3] */
 int upbp_read_query_stats(upbp_ctx* ctx, const upbp_query_stats* stats);
+/* Adjoint of the estimator sum with respect to the parameters of media[medium]: given
+ * grad_image = dL/d(framebuffer) ([H*W][3] floats, host or device pointer), writes
+ * grad[0..6] = dL/d(sigma_a r,g,b, sigma_s r,g,b, g) for the structures and queries of the last
+ * build / upload, holding the candidate sets and the choice of the minimal sigma_t component
+ * fixed.  Transmittance is recomputed, not stored.  Needs UPBP_MODE_MIXED or UPBP_MODE_FP64.
+ * No counterpart in the reference (it has no derivatives); this is the backward of the
+ * differentiable estimator (smallupbp_b200.autograd). */
+int upbp_adjoint(upbp_ctx* ctx, const float* grad_image, int32_t medium, double* grad);
+
+/* Device memory the context holds (its grow-only buffers), in bytes. */
+int upbp_device_bytes(const upbp_ctx* ctx, uint64_t* bytes);
+
+/* Candidates tested by the last evaluate, summed over all queries: [0] PB2D photons, [1] BB1D beam
+ * pieces, [2] PP3D photons (diagnostics of culling quality; accepted counts are in the query stats). */
+int upbp_read_tested_counts(upbp_ctx* ctx, uint64_t* tested);
 int upbp_clear_image(upbp_ctx* ctx);
 int upbp_read_image(upbp_ctx* ctx, float* rgb); /* [H*W][3] accumulated */
 /* Device-side counters: number of kernels launched by the last upbp_build and upbp_evaluate. */

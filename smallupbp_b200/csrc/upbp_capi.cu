@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "upbp_generic_api.cuh"
 #include "upbp_kernels.cuh"
 #include "upbp_mis_prep.cuh"
 
@@ -44,6 +45,7 @@ struct upbp_ctx {
     upbp_params P{};
     bool have_params = false;
     std::vector<DMedium> media;
+    std::vector<upbp_medium> media_raw;
     size_t bytes = 0;
 
     // inputs
@@ -89,6 +91,9 @@ struct upbp_ctx {
     DBuf cub_tmp;
     // outputs
     DBuf work, status;
+    DBuf grad_img, grad_acc;  // adjoint: dL/d framebuffer, dL/d medium parameters
+    int* status_host = nullptr;   // page-locked copy of status[0] after the last evaluate
+    bool status_pending = false;  // status_host holds the last BB1D launch's flag
     int num_sms = 0;
     int bb1d_kernel = 1;  // 0: thread per query, 1: warp-cooperative persistent
     DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
@@ -120,6 +125,15 @@ void ck(upbp_ctx* c, cudaError_t e, const char* what)
         }
         fail(c, UPBP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
     }
+}
+
+// After a synchronisation of the context's stream: the BB1D warp gather sets status[0] when a
+// query's traversal stack would overflow; its candidate set is then incomplete, which is an error.
+void check_status(upbp_ctx* c)
+{
+    if (c->status_pending && c->status_host && *c->status_host != 0)
+        fail(c, UPBP_ERR_CAPACITY, "BB1D traversal stack overflow in the last evaluate: a candidate set is "
+                                   "incomplete (use a larger bb1d_leaf or beam_piece_radii)");
 }
 
 void ensure(upbp_ctx* c, DBuf& b, size_t bytes)
@@ -245,7 +259,7 @@ void do_build(upbp_ctx* c)
                        c->lv_dir4.as<float4>(), c->lv_thr4.as<float4>(), c->lv_info4.as<int4>(),
                        c->lv_inmed.as<uint32_t>(), s);
     c->build_launches += 1;
-    if (c->mode == UPBP_MODE_MIXED && n > 0) {
+    if (c->mode != UPBP_MODE_PLAIN && n > 0) {
         ensure(c, c->light_sums, sizeof(LightSum) * n);
         // the PB2D / BB1D walks see beamType | techniques, PP3D the techniques: same terms
         launch_light_sums(c->lv_mis.as<upbp_mis>(), c->path_ends.as<int32_t>(), c->n_paths, P.techniques,
@@ -394,7 +408,7 @@ void do_build(upbp_ctx* c)
         build_lbvh(c, c->pc_codes_sorted.as<uint32_t>(), np, leaf, c->bm_leaf_codes, c->bm_nodes, c->bm_parent_int,
                    c->bm_parent_leaf, c->bm_leaf_boxes, c->bm_node_boxes, c->bm_flagsbuf, c->bm_n_leaves);
         c->build_launches += 10;
-        if (c->mode == UPBP_MODE_MIXED) {
+        if (c->mode != UPBP_MODE_PLAIN) {
             ensure(c, c->pc_pay, sizeof(PiecePayload) * np);
             launch_piece_payload(c->pc_c2.as<float4>(), np, c->bm_thr4.as<float4>(), c->bm_pdf4.as<float4>(),
                                  c->bm_link.as<int2>(), c->bm_radius.as<float>(), c->lv_info4.as<int4>(),
@@ -427,7 +441,7 @@ LightSoA light_soa(upbp_ctx* c)
     L.info = c->lv_info4.as<int4>();
     L.mis = c->lv_mis.as<upbp_mis>();
     L.path_ends = c->path_ends.as<int32_t>();
-    L.sums = c->mode == UPBP_MODE_MIXED ? c->light_sums.as<LightSum>() : nullptr;
+    L.sums = c->mode != UPBP_MODE_PLAIN ? c->light_sums.as<LightSum>() : nullptr;
     L.n = c->n_lv;
     return L;
 }
@@ -455,11 +469,121 @@ SegQueriesDev seg_dev(upbp_ctx* c)
     return Q;
 }
 
+HashGridDev hash_dev(upbp_ctx* c)
+{
+    HashGridDev G{};
+    G.pos = c->hg_pos.as<float4>();
+    G.start = c->hg_start.as<int32_t>();
+    G.end = c->hg_end.as<int32_t>();
+    for (int k = 0; k < 3; ++k) {
+        G.bbox_min[k] = c->hg_bbox[k];
+        G.bbox_max[k] = c->hg_bbox[3 + k];
+    }
+    G.inv_cell = c->hg_inv_cell;
+    G.r2 = c->P.radius_pp3d * c->P.radius_pp3d;
+    G.cells = std::max(1, c->P.hash_cells);
+    G.n = (c->P.techniques & UPBP_PP3D) ? c->n_ph : 0;
+    return G;
+}
+
+PointQueriesDev point_dev(upbp_ctx* c)
+{
+    PointQueriesDev Q{};
+    Q.position = c->pq_pos.as<float>();
+    Q.dir_fix = c->pq_dir.as<float>();
+    Q.medium_id = c->pq_med.as<int32_t>();
+    Q.path_length = c->pq_plen.as<int32_t>();
+    Q.throughput = c->pq_thr.as<float>();
+    Q.pixel = c->pq_pixel.as<int32_t>();
+    Q.cam_mis_begin = c->pq_cam_begin.as<int64_t>();
+    Q.n = c->n_pq;
+    return Q;
+}
+
+PhotonBVH photon_bvh(upbp_ctx* c)
+{
+    PhotonBVH B{};
+    B.pos = c->pb_pos.as<float4>();
+    B.nodes = c->pb_nodes.as<BNode>();
+    B.n = (c->P.techniques & UPBP_PB2D) ? c->n_ph : 0;
+    B.leaf = std::max(1, c->pb2d_leaf);
+    B.n_leaves = c->pb_n_leaves;
+    return B;
+}
+
+BeamBVH beam_bvh(upbp_ctx* c)
+{
+    BeamBVH B{};
+    B.pa = c->pc_a2.as<float4>();
+    B.pb = c->pc_b2.as<float4>();
+    B.pc = c->pc_c2.as<float4>();
+    B.nodes = c->bm_nodes.as<BNode>();
+    B.n = c->n_pieces;
+    B.pay = c->mode != UPBP_MODE_PLAIN ? c->pc_pay.as<PiecePayload>() : nullptr;
+    B.leaf = std::max(1, c->bb1d_leaf);
+    B.n_leaves = c->bm_n_leaves;
+    return B;
+}
+
+// FP64 suffix sums of the camera walks, per segment query and per point query.
+void prepare_cam_sums(upbp_ctx* c, cudaStream_t s, const CamSum** cs_seg, const CamSum** cs_pt)
+{
+    const int64_t nq = c->n_sq, np = c->n_pq;
+    const upbp_mis* cam = c->cam_mis.as<upbp_mis>();
+    ensure(c, c->cam_sums_seg, sizeof(CamSum) * std::max<int64_t>(nq, 1));
+    ensure(c, c->cam_sums_pt, sizeof(CamSum) * std::max<int64_t>(np, 1));
+    const uint32_t tq = c->P.query_beam_type | c->P.techniques;
+    launch_cam_sums(cam, c->sq_cam_begin.as<int64_t>(), c->sq_plen.as<int32_t>(), nq, tq, c->P.query_beam_type,
+                    c->P.photon_beam_type, c->cam_sums_seg.as<CamSum>(), s);
+    launch_cam_sums(cam, c->pq_cam_begin.as<int64_t>(), c->pq_plen.as<int32_t>(), np, c->P.techniques,
+                    c->P.query_beam_type, c->P.photon_beam_type, c->cam_sums_pt.as<CamSum>(), s);
+    *cs_seg = c->cam_sums_seg.as<CamSum>();
+    *cs_pt = c->cam_sums_pt.as<CamSum>();
+    c->eval_launches += 2;
+}
+
+// The generic-precision gathers (FP64 evaluation, adjoint) over the context's structures.
+gen::GenLaunch generic_launch(upbp_ctx* c, const CamSum* cs_seg, const CamSum* cs_pt, int grad_medium)
+{
+    gen::GenLaunch A{};
+    A.K = make_consts(c);
+    A.G.n_media = (int)c->media_raw.size();
+    for (int i = 0; i < A.G.n_media; ++i) A.G.raw[i] = c->media_raw[i];
+    A.G.grad_medium = grad_medium;
+    A.L = light_soa(c);
+    A.photons = photon_bvh(c);
+    A.beams = beam_bvh(c);
+    A.hash = hash_dev(c);
+    A.sq = seg_dev(c);
+    A.pq = point_dev(c);
+    A.cam = c->cam_mis.as<upbp_mis>();
+    A.cs_seg = cs_seg;
+    A.cs_pt = cs_pt;
+    if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
+    ensure(c, c->work, sizeof(unsigned int) * 4);
+    ensure(c, c->status, sizeof(int) * 4);
+    ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, c->stream), "memset");
+    ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, c->stream), "memset");
+    A.work = c->work.as<unsigned int>();
+    A.status = c->status.as<int>();
+    A.bb1d_grid = c->num_sms * gen::generic_bb1d_blocks_per_sm(grad_medium >= 0);
+    return A;
+}
+
+void record_status(upbp_ctx* c, cudaStream_t s)
+{
+    if (!c->status_host) ck(c, cudaHostAlloc((void**)&c->status_host, sizeof(int), cudaHostAllocDefault),
+                            "cudaHostAlloc");
+    ck(c, cudaMemcpyAsync(c->status_host, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "status");
+    c->status_pending = true;
+}
+
 void do_evaluate(upbp_ctx* c)
 {
     if (!c->built) fail(c, UPBP_ERR_NOT_BUILT, "upbp_build was not called");
     cudaStream_t s = c->stream;
     c->eval_launches = 0;
+    c->status_pending = false;
     const GatherConsts K = make_consts(c);
     const LightSoA L = light_soa(c);
     const int64_t nq = c->n_sq, np = c->n_pq;
@@ -483,41 +607,28 @@ void do_evaluate(upbp_ctx* c)
     const bool mixed = c->mode == UPBP_MODE_MIXED;
     const CamSum* cs_seg = nullptr;
     const CamSum* cs_pt = nullptr;
-    if (mixed) {
-        ensure(c, c->cam_sums_seg, sizeof(CamSum) * std::max<int64_t>(nq, 1));
-        ensure(c, c->cam_sums_pt, sizeof(CamSum) * std::max<int64_t>(np, 1));
-        const uint32_t tq = c->P.query_beam_type | c->P.techniques;
-        launch_cam_sums(cam, c->sq_cam_begin.as<int64_t>(), c->sq_plen.as<int32_t>(), nq, tq, c->P.query_beam_type,
-                        c->P.photon_beam_type, c->cam_sums_seg.as<CamSum>(), s);
-        launch_cam_sums(cam, c->pq_cam_begin.as<int64_t>(), c->pq_plen.as<int32_t>(), np, c->P.techniques,
-                        c->P.query_beam_type, c->P.photon_beam_type, c->cam_sums_pt.as<CamSum>(), s);
-        cs_seg = c->cam_sums_seg.as<CamSum>();
-        cs_pt = c->cam_sums_pt.as<CamSum>();
-        c->eval_launches += 2;
+    if (c->mode != UPBP_MODE_PLAIN) prepare_cam_sums(c, s, &cs_seg, &cs_pt);
+    if (c->mode == UPBP_MODE_FP64) {
+        // FP64 oracle on the GPU: the same candidates, FP64 geometry, contributions and MIS
+        gen::GenLaunch A = generic_launch(c, cs_seg, cs_pt, -1);
+        A.out_pp3d = gen::GenOut{c->out_pp3d.as<float>(), img, c->cnt_pp3d.as<uint32_t>(),
+                                 c->hash_pp3d.as<unsigned long long>(), nullptr, nullptr};
+        A.out_pb2d = gen::GenOut{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
+                                 c->hash_pb2d.as<unsigned long long>(), nullptr, nullptr};
+        A.out_bb1d = gen::GenOut{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
+                                 c->hash_bb1d.as<unsigned long long>(), nullptr, nullptr};
+        for (int k = 2; k <= 4; ++k) ck(c, cudaEventRecord(c->ev[k], s), "event");
+        gen::launch_generic(A, false, s);
+        record_status(c, s);
+        c->eval_launches += 3;
+        ck(c, cudaEventRecord(c->ev[5], s), "event");
+        ck(c, cudaGetLastError(), "generic gather launch");
+        return;
     }
     ck(c, cudaEventRecord(c->ev[2], s), "event");
     if (np > 0) {
-        HashGridDev G{};
-        G.pos = c->hg_pos.as<float4>();
-        G.start = c->hg_start.as<int32_t>();
-        G.end = c->hg_end.as<int32_t>();
-        for (int k = 0; k < 3; ++k) {
-            G.bbox_min[k] = c->hg_bbox[k];
-            G.bbox_max[k] = c->hg_bbox[3 + k];
-        }
-        G.inv_cell = c->hg_inv_cell;
-        G.r2 = c->P.radius_pp3d * c->P.radius_pp3d;
-        G.cells = std::max(1, c->P.hash_cells);
-        G.n = (c->P.techniques & UPBP_PP3D) ? c->n_ph : 0;
-        PointQueriesDev Q{};
-        Q.position = c->pq_pos.as<float>();
-        Q.dir_fix = c->pq_dir.as<float>();
-        Q.medium_id = c->pq_med.as<int32_t>();
-        Q.path_length = c->pq_plen.as<int32_t>();
-        Q.throughput = c->pq_thr.as<float>();
-        Q.pixel = c->pq_pixel.as<int32_t>();
-        Q.cam_mis_begin = c->pq_cam_begin.as<int64_t>();
-        Q.n = np;
+        const HashGridDev G = hash_dev(c);
+        const PointQueriesDev Q = point_dev(c);
         Outputs O{c->out_pp3d.as<float>(), img, c->cnt_pp3d.as<uint32_t>(),
                   c->hash_pp3d.as<unsigned long long>(), tested + 2};
         launch_gather_pp3d(K, L, G, Q, cam, cs_pt, O, c->block, mixed, s);
@@ -547,12 +658,7 @@ void do_evaluate(upbp_ctx* c)
         c->eval_launches += 5;
     }
     if (nq > 0) {
-        PhotonBVH B{};
-        B.pos = c->pb_pos.as<float4>();
-        B.nodes = c->pb_nodes.as<BNode>();
-        B.n = (c->P.techniques & UPBP_PB2D) ? c->n_ph : 0;
-        B.leaf = std::max(1, c->pb2d_leaf);
-        B.n_leaves = c->pb_n_leaves;
+        const PhotonBVH B = photon_bvh(c);
         Outputs O{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
                   c->hash_pb2d.as<unsigned long long>(), tested + 0};
         launch_gather_pb2d(K, L, B, Q, cam, cs_seg, O, c->block, mixed, s, order);
@@ -560,15 +666,7 @@ void do_evaluate(upbp_ctx* c)
     }
     ck(c, cudaEventRecord(c->ev[4], s), "event");
     if (nq > 0) {
-        BeamBVH B{};
-        B.pa = c->pc_a2.as<float4>();
-        B.pb = c->pc_b2.as<float4>();
-        B.pc = c->pc_c2.as<float4>();
-        B.nodes = c->bm_nodes.as<BNode>();
-        B.n = c->n_pieces;
-        B.pay = mixed ? c->pc_pay.as<PiecePayload>() : nullptr;
-        B.leaf = std::max(1, c->bb1d_leaf);
-        B.n_leaves = c->bm_n_leaves;
+        const BeamBVH B = beam_bvh(c);
         BeamSoA S{};
         S.thr = c->bm_thr4.as<float4>();
         S.pdf = c->bm_pdf4.as<float4>();
@@ -577,15 +675,16 @@ void do_evaluate(upbp_ctx* c)
         S.n = c->n_beams;
         Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                   c->hash_bb1d.as<unsigned long long>(), tested + 1};
-        if (c->bb1d_kernel == 1) {
+        if (c->bb1d_kernel >= 1) {
             if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
             ensure(c, c->work, sizeof(unsigned int) * 4);
             ensure(c, c->status, sizeof(int) * 4);
             ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
             ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
-            const int grid = c->num_sms * bb1d_warp_blocks_per_sm(mixed);
+            const int grid = c->num_sms * bb1d_warp_blocks_per_sm(mixed, c->bb1d_kernel);
             launch_bb1d_warp(K, L, B, S, Q, cam, cs_seg, O, grid, mixed, c->work.as<unsigned int>(),
-                             c->status.as<int>(), order, s);
+                             c->status.as<int>(), order, s, c->bb1d_kernel);
+            record_status(c, s);
         } else {
             launch_gather_bb1d(K, L, B, S, Q, cam, cs_seg, O, c->block, mixed, s);
         }
@@ -660,8 +759,9 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->image, &c->cnt_pb2d, &c->cnt_bb1d, &c->cnt_pp3d,
                    &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested, &c->light_sums, &c->cam_sums_seg,
                    &c->cam_sums_pt, &c->work, &c->status, &c->pc_pay, &c->q_keys, &c->q_keys_sorted, &c->q_iota,
-                   &c->q_order};
+                   &c->q_order, &c->grad_img, &c->grad_acc};
     for (DBuf* b : all) free_buf(*b);
+    if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -674,7 +774,8 @@ const char* upbp_last_error(const upbp_ctx* c) { return c ? c->err.c_str() : "nu
 int upbp_set_mode(upbp_ctx* c, int mode)
 {
     return guarded(c, [&] {
-        if (mode != UPBP_MODE_PLAIN && mode != UPBP_MODE_MIXED) fail(c, UPBP_ERR_INVALID_ARG, "unknown mode %d", mode);
+        if (mode != UPBP_MODE_PLAIN && mode != UPBP_MODE_MIXED && mode != UPBP_MODE_FP64)
+            fail(c, UPBP_ERR_INVALID_ARG, "unknown mode %d", mode);
         if (mode != c->mode) c->built = false;
         c->mode = mode;
     });
@@ -692,7 +793,7 @@ int upbp_set_tuning(upbp_ctx* c, const upbp_tuning* tu)
             fail(c, UPBP_ERR_INVALID_ARG, "block_threads must be a multiple of 32 in [32, 256]");
         if (!(tu->beam_piece_radii >= 1.f && tu->beam_piece_radii <= 1024.f))
             fail(c, UPBP_ERR_INVALID_ARG, "beam_piece_radii must be in [1, 1024]");
-        if (tu->bb1d_kernel != 0 && tu->bb1d_kernel != 1) fail(c, UPBP_ERR_INVALID_ARG, "bb1d_kernel must be 0 or 1");
+        if (tu->bb1d_kernel < 0 || tu->bb1d_kernel > 2) fail(c, UPBP_ERR_INVALID_ARG, "bb1d_kernel must be 0, 1 or 2");
         c->pb2d_leaf = tu->pb2d_leaf;
         c->bb1d_leaf = tu->bb1d_leaf;
         c->block = tu->block_threads;
@@ -723,6 +824,7 @@ int upbp_set_media(upbp_ctx* c, const upbp_medium* media, int32_t n)
     return guarded(c, [&] {
         if (!media || n <= 0 || n > UPBP_MAX_MEDIA) fail(c, UPBP_ERR_INVALID_ARG, "n_media must be in [1, %d]", UPBP_MAX_MEDIA);
         c->media.clear();
+        c->media_raw.assign(media, media + n);
         for (int i = 0; i < n; ++i) c->media.push_back(derive_medium(media[i]));
     });
 }
@@ -855,6 +957,7 @@ int upbp_read_segment_results(upbp_ctx* c, float* pb2d, float* bb1d)
         if (pb2d && bytes) ck(c, cudaMemcpyAsync(pb2d, c->out_pb2d.p, bytes, cudaMemcpyDefault, c->stream), "read");
         if (bb1d && bytes) ck(c, cudaMemcpyAsync(bb1d, c->out_bb1d.p, bytes, cudaMemcpyDefault, c->stream), "read");
         ck(c, cudaStreamSynchronize(c->stream), "sync");
+        check_status(c);
     });
 }
 
@@ -864,6 +967,7 @@ int upbp_read_point_results(upbp_ctx* c, float* pp3d)
         const size_t bytes = sizeof(float) * 3 * (size_t)c->n_pq;
         if (pp3d && bytes) ck(c, cudaMemcpyAsync(pp3d, c->out_pp3d.p, bytes, cudaMemcpyDefault, c->stream), "read");
         ck(c, cudaStreamSynchronize(c->stream), "sync");
+        check_status(c);
     });
 }
 
@@ -882,6 +986,64 @@ int upbp_read_query_stats(upbp_ctx* c, const upbp_query_stats* st)
         rd(st->count_pp3d, c->cnt_pp3d, 4 * np);
         rd(st->hash_pp3d, c->hash_pp3d, 8 * np);
         ck(c, cudaStreamSynchronize(c->stream), "sync");
+        check_status(c);
+    });
+}
+
+int upbp_adjoint(upbp_ctx* c, const float* grad_image, int32_t medium, double* grad)
+{
+    return guarded(c, [&] {
+        if (!grad_image || !grad) fail(c, UPBP_ERR_INVALID_ARG, "grad_image and grad must not be NULL");
+        if (medium < 0 || medium >= (int)c->media_raw.size()) fail(c, UPBP_ERR_INVALID_ARG, "medium out of range");
+        if (!c->built) fail(c, UPBP_ERR_NOT_BUILT, "upbp_build was not called");
+        if (c->mode == UPBP_MODE_PLAIN)
+            fail(c, UPBP_ERR_INVALID_ARG, "the adjoint needs UPBP_MODE_MIXED or UPBP_MODE_FP64 structures");
+        cudaStream_t s = c->stream;
+        c->eval_launches = 0;
+        c->status_pending = false;
+        const size_t npix = (size_t)std::max(0, c->P.image_width) * (size_t)std::max(0, c->P.image_height);
+        ensure(c, c->grad_img, sizeof(float) * 3 * std::max<size_t>(npix, 1));
+        if (npix)
+            ck(c, cudaMemcpyAsync(c->grad_img.p, grad_image, sizeof(float) * 3 * npix, cudaMemcpyDefault, s),
+               "grad_image");
+        ensure(c, c->grad_acc, sizeof(double) * 8);
+        ck(c, cudaMemsetAsync(c->grad_acc.p, 0, sizeof(double) * 8, s), "memset");
+        const CamSum* cs_seg = nullptr;
+        const CamSum* cs_pt = nullptr;
+        prepare_cam_sums(c, s, &cs_seg, &cs_pt);
+        gen::GenLaunch A = generic_launch(c, cs_seg, cs_pt, medium);
+        const gen::GenOut O{nullptr, nullptr, nullptr, nullptr, c->grad_img.as<float>(), c->grad_acc.as<double>()};
+        A.out_pp3d = A.out_pb2d = A.out_bb1d = O;
+        gen::launch_generic(A, true, s);
+        c->eval_launches += 3;
+        record_status(c, s);
+        ck(c, cudaGetLastError(), "adjoint launch");
+        double h[8];
+        ck(c, cudaMemcpyAsync(h, c->grad_acc.p, sizeof(double) * 8, cudaMemcpyDeviceToHost, s), "read grad");
+        ck(c, cudaStreamSynchronize(s), "sync");
+        check_status(c);
+        for (int i = 0; i < 7; ++i) grad[i] = h[i];
+    });
+}
+
+int upbp_device_bytes(const upbp_ctx* c, uint64_t* bytes)
+{
+    if (!c || !bytes) return UPBP_ERR_INVALID_ARG;
+    *bytes = (uint64_t)c->bytes;
+    return UPBP_OK;
+}
+
+int upbp_read_tested_counts(upbp_ctx* c, uint64_t* tested)
+{
+    return guarded(c, [&] {
+        if (!tested) fail(c, UPBP_ERR_INVALID_ARG, "tested is NULL");
+        unsigned long long h[4] = {0, 0, 0, 0};
+        if (c->tested.p) {
+            ck(c, cudaMemcpyAsync(h, c->tested.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "read tested");
+            ck(c, cudaStreamSynchronize(c->stream), "sync");
+        check_status(c);
+        }
+        for (int i = 0; i < 3; ++i) tested[i] = (uint64_t)h[i];
     });
 }
 
@@ -901,6 +1063,7 @@ int upbp_read_image(upbp_ctx* c, float* rgb)
         const size_t npix = (size_t)std::max(0, c->P.image_width) * (size_t)std::max(0, c->P.image_height);
         if (npix) ck(c, cudaMemcpyAsync(rgb, c->image.p, sizeof(float) * 3 * npix, cudaMemcpyDefault, c->stream), "read image");
         ck(c, cudaStreamSynchronize(c->stream), "sync");
+        check_status(c);
     });
 }
 
@@ -917,6 +1080,7 @@ int upbp_last_timings(const upbp_ctx* cc, float* build_ms, float* pp3d_ms, float
     upbp_ctx* c = const_cast<upbp_ctx*>(cc);
     return guarded(c, [&] {
         ck(c, cudaStreamSynchronize(c->stream), "sync");
+        check_status(c);
         float v = 0.f;
         if (build_ms) { cudaEventElapsedTime(&v, c->ev[0], c->ev[1]); *build_ms = v; }
         if (pp3d_ms) { cudaEventElapsedTime(&v, c->ev[2], c->ev[3]); *pp3d_ms = v; }

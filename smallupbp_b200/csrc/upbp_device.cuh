@@ -158,6 +158,56 @@ __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float 
     return true;
 }
 
+// Which piece of a beam takes a candidate that test_beam_beam accepted.  The predicate does not
+// depend on the piece (it tests the whole beam), but its t2 = (t1 + d1.O1 - d1.O2) / (d1.d2) is
+// ill-conditioned for nearly perpendicular pairs, and t1, t2 for nearly parallel ones, so the
+// FP32 t2 can lie far from the true closest point -- in a piece whose box the query never
+// crosses.  The owner is the piece containing the point of the beam segment [0, len] closest to
+// the query segment [dmin, dmax], computed in FP64; every piece computes the same point, and the
+// query crosses the owner's box whenever the pair is geometrically within the radius (plus the
+// box slack).  Where the FP32 t1 and t2 are provably within m = 1e-4 * scale of the exact line
+// solution -- |c| (1 - c^2) > 0.04 with c = d1.d2 bounds their rounding error by about
+// 2.5e-5 * scale (measured over 2M random pairs in the unit cube) -- and away from the ends of
+// their ranges, the FP32 t2 decides without the FP64 solve.
+__device__ __forceinline__ double owner_param_f64(V3 O1, V3 d1, float dminf, float dmaxf, V3 O2, V3 d2, float lenf)
+{
+    const double wx = (double)O1.x - O2.x, wy = (double)O1.y - O2.y, wz = (double)O1.z - O2.z;
+    const double ax = d1.x, ay = d1.y, az = d1.z, bx = d2.x, by = d2.y, bz = d2.z;
+    const double aa = ax * ax + ay * ay + az * az, cc = bx * bx + by * by + bz * bz, b = ax * bx + ay * by + az * bz;
+    const double dd = ax * wx + ay * wy + az * wz, ee = bx * wx + by * wy + bz * wz;
+    const double den = aa * cc - b * b;
+    const double dmin = dminf, dmax = dmaxf, len = lenf;
+    double t = dmin;
+    if (den > 1e-300) {
+        const double inv = 1.0 / den;
+        t = (b * ee - cc * dd) * inv;
+        const double u = (aa * ee - b * dd) * inv;
+        if (t >= dmin && t <= dmax && u >= 0.0 && u <= len) return u;  // closest points inside both
+    }
+    t = fmin(fmax(t, dmin), dmax);
+    double u = fmin(fmax((b * t + ee) / cc, 0.0), len);
+    t = fmin(fmax((b * u - dd) / aa, dmin), dmax);
+    u = fmin(fmax((b * t + ee) / cc, 0.0), len);
+    return u;
+}
+
+__device__ __forceinline__ bool piece_owns(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len, float t_lo,
+                                           float t_hi, float t1, float t2)
+{
+    const float c = fabsf(d1.x * d2.x + d1.y * d2.y + d1.z * d2.z);
+    if (c * (1.f - c * c) > 0.04f) {
+        const float scale = fmaxf(fmaxf(fmaxf(fabsf(O1.x), fabsf(O1.y)), fmaxf(fabsf(O1.z), fabsf(O2.x))),
+                                  fmaxf(fmaxf(fabsf(O2.y), fabsf(O2.z)), fmaxf(fmaxf(len, fabsf(dmax)), 1.f)));
+        const float m = 1e-4f * scale;
+        if (t1 > dmin + m && t1 < dmax - m && t2 > m && t2 < len - m) {
+            if (t2 >= t_lo + m && t2 < t_hi - m) return true;
+            if (t2 < t_lo - m || t2 >= t_hi + m) return false;
+        }
+    }
+    const double u = owner_param_f64(O1, d1, dmin, dmax, O2, d2, len);
+    return u >= (double)t_lo && (u < (double)t_hi || t_hi >= len);
+}
+
 // ------------------------------------------------------------------ MIS walks
 __device__ __forceinline__ bool mis_spec(const upbp_mis& m) { return (m.flags & UPBP_MIS_IS_SPECULAR) != 0; }
 

@@ -12,75 +12,11 @@
 
 #include "upbp_kernels.cuh"
 #include "upbp_mis_prep.cuh"
+#include "upbp_traverse.cuh"
 
 namespace upbp {
 
 namespace {
-
-__device__ __forceinline__ void stage_media(const GatherConsts& K, DMedium* s)
-{
-    for (int i = threadIdx.x; i < K.n_media; i += blockDim.x) s[i] = K.media[i];
-    __syncthreads();
-}
-
-__device__ __forceinline__ bool slab(float lx, float ly, float lz, float hx, float hy, float hz, V3 o, V3 inv,
-                                     float tmin, float tmax)
-{
-    const float tx0 = (lx - o.x) * inv.x, tx1 = (hx - o.x) * inv.x;
-    const float ty0 = (ly - o.y) * inv.y, ty1 = (hy - o.y) * inv.y;
-    const float tz0 = (lz - o.z) * inv.z, tz1 = (hz - o.z) * inv.z;
-    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
-    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
-    return tn <= tf;
-}
-
-__device__ __forceinline__ float safe_inv(float d) { return 1.f / (d == 0.f ? copysignf(1e-30f, d) : d); }
-
-// Stack traversal of a BVH2 with child boxes; calls leaf(k) for every leaf whose box the
-// segment [tmin, tmax] overlaps.  Returns false on stack overflow (reported through the
-// status word; the 30-bit Morton build never gets that deep).
-template <class LeafFn>
-__device__ __forceinline__ bool traverse(const BNode* __restrict__ nodes, int n_leaves, V3 o, V3 inv, float tmin,
-                                         float tmax, LeafFn&& leaf)
-{
-    if (n_leaves <= 0) return true;
-    if (n_leaves == 1) {
-        leaf(0);
-        return true;
-    }
-    constexpr int kStack = 96;
-    int stack[kStack];
-    int sp = 0;
-    stack[sp++] = 0;
-    while (sp > 0) {
-        const int node = stack[--sp];
-        const float4 a = __ldg(&nodes[node].a);
-        const float4 b = __ldg(&nodes[node].b);
-        const float4 c = __ldg(&nodes[node].c);
-        const int4 d = __ldg(&nodes[node].d);
-        const bool hl = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, tmin, tmax);
-        const bool hr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv, tmin, tmax);
-        if (hl) {
-            if (d.x < 0) leaf(~d.x);
-            else if (sp < kStack) stack[sp++] = d.x;
-            else return false;
-        }
-        if (hr) {
-            if (d.y < 0) leaf(~d.y);
-            else if (sp < kStack) stack[sp++] = d.y;
-            else return false;
-        }
-    }
-    return true;
-}
-
-__device__ __forceinline__ void splat(float* image, int px, Rgb v)
-{
-    if (!image || px < 0) return;
-    atomicAdd(&image[3 * px + 0], v.r);
-    atomicAdd(&image[3 * px + 1], v.g);
-    atomicAdd(&image[3 * px + 2], v.b);
-}
 
 // Camera MisData as the reference array holds it during an estimator call at path length L:
 // entries < L-1 from the snapshot, entry L-1 from the snapshot with mRaySampleRevPdfInv set by
@@ -549,7 +485,9 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                     if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
                                         pc.y, &dist, &sinT, &t1, &t2))
                         continue;
-                    if (!(t2 >= pb.w && t2 < pc.x)) continue;  // this piece owns t2
+                    if (!piece_owns(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pb.w,
+                                    pc.x, t1, t2))
+                        continue;
                     const int beam = __float_as_int(pc.z);
                     const float radius = __ldg(&Bs.radius[beam]);
                     if (radius < dist) continue;  // PhotonBeam.hxx:411-413
@@ -566,99 +504,20 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
     if (O.tested) atomicAdd(O.tested, tested);
 }
 
-// ----------------------------------------------------------------- warp-cooperative traversal
-// One warp per query.  Each step pops up to 32 BVH nodes from the warp's shared-memory stack
-// (one per lane), tests both child boxes, pushes internal hits (ballot + prefix counts) and
-// appends leaf hits to the warp's leaf list; once 32 leaves are gathered (or the traversal is
-// done) the warp tests the leaves' primitives 32 at a time, consecutive primitives to
-// consecutive lanes.  Returns false if the stack overflowed (the status word records it).
-constexpr int kWarpStack = 1024;
-constexpr int kWarpLeaves = 96;
-constexpr unsigned kFull = 0xffffffffu;
+// Accepted candidates of one warp waiting for evaluation: the piece and its closest approach.
+constexpr int kCandQueue = 64;
+struct CandQueue {
+    int piece[kCandQueue];
+    float4 geo[kCandQueue];  // dist, sin(theta), t1 (query), t2 (beam)
+};
 
-template <class PrimFn>
-__device__ __forceinline__ bool warp_traverse(const BNode* __restrict__ nodes, int n_leaves, int n_prims, int leaf_shift,
-                                              V3 o, V3 inv, float tmin, float tmax, int* stack, int* leaves, int lane,
-                                              PrimFn&& prim)
-{
-    if (n_leaves <= 0) return true;
-    const unsigned lt = (1u << lane) - 1u;
-    int sp = 0, nleaf = 0;
-    bool ok = true;
-    if (n_leaves == 1) {
-        if (lane == 0) leaves[0] = 0;
-        nleaf = 1;
-    } else {
-        if (lane == 0) stack[0] = 0;
-        sp = 1;
-    }
-    __syncwarp();
-    while (sp > 0 || nleaf > 0) {
-        if (sp > 0 && nleaf < 32) {
-            const int take = min(sp, 32);
-            const int node = lane < take ? stack[sp - 1 - lane] : -1;
-            sp -= take;
-            __syncwarp();
-            bool hl = false, hr = false;
-            int cl = 0, cr = 0;
-            if (node >= 0) {
-                const float4 a = __ldg(&nodes[node].a);
-                const float4 b = __ldg(&nodes[node].b);
-                const float4 c = __ldg(&nodes[node].c);
-                const int4 d = __ldg(&nodes[node].d);
-                hl = slab(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, tmin, tmax);
-                hr = slab(b.z, b.w, c.x, c.y, c.z, c.w, o, inv, tmin, tmax);
-                cl = d.x;
-                cr = d.y;
-            }
-            const bool pl = hl && cl >= 0, pr = hr && cr >= 0, ll = hl && cl < 0, lr = hr && cr < 0;
-            const unsigned bpl = __ballot_sync(kFull, pl), bpr = __ballot_sync(kFull, pr);
-            const unsigned bll = __ballot_sync(kFull, ll), blr = __ballot_sync(kFull, lr);
-            const int npush = __popc(bpl) + __popc(bpr);
-            if (sp + npush > kWarpStack) {
-                ok = false;  // cannot happen for the tree depths of a 30-bit Morton build
-                break;
-            }
-            const int ppos = sp + __popc(bpl & lt) + __popc(bpr & lt);
-            if (pl) stack[ppos] = cl;
-            if (pr) stack[ppos + (pl ? 1 : 0)] = cr;
-            sp += npush;
-            const int lpos = nleaf + __popc(bll & lt) + __popc(blr & lt);
-            if (ll) leaves[lpos] = ~cl;
-            if (lr) leaves[lpos + (ll ? 1 : 0)] = ~cr;
-            nleaf += __popc(bll) + __popc(blr);
-            __syncwarp();
-        }
-        if (nleaf >= 32 || (sp == 0 && nleaf > 0)) {
-            const int total = nleaf << leaf_shift;
-            for (int base = 0; base < total; base += 32) {
-                const int idx = base + lane;
-                if (idx < total) {
-                    const int p = (leaves[idx >> leaf_shift] << leaf_shift) + (idx & ((1 << leaf_shift) - 1));
-                    if (p < n_prims) prim(p);
-                }
-            }
-            nleaf = 0;
-            __syncwarp();
-        }
-    }
-    return ok;
-}
-
-__device__ __forceinline__ float warp_sum(float v)
-{
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
-}
-__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
-{
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
-}
-
-// BB1D, warp per query, persistent: warps draw query indices from an atomic counter.
-template <bool kMixed, int kWarps>
-__global__ void __launch_bounds__(kWarps * 32, 5) k_bb1d_warp(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+// BB1D, warp per query, persistent: warps draw query indices from an atomic counter.  The lanes
+// test 32 beam pieces at a time; the accepted ones go to the warp's candidate queue, and whenever
+// it holds 32 they are evaluated one per lane, so the contribution (transmittance, phase
+// function, MIS weight) runs with every lane busy although only a fraction of the tested pieces
+// is accepted.
+template <bool kMixed, int kWarps, int kMinBlocks>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bb1d_warp(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                           const BeamBVH B, const BeamSoA Bs, const SegQueriesDev Q,
                                                           const upbp_mis* __restrict__ cam,
                                                           const CamSum* __restrict__ cs, const Outputs O,
@@ -668,12 +527,15 @@ __global__ void __launch_bounds__(kWarps * 32, 5) k_bb1d_warp(const __grid_const
     __shared__ DMedium media[UPBP_MAX_MEDIA];
     __shared__ int s_stack[kWarps][kWarpStack];
     __shared__ int s_leaves[kWarps][kWarpLeaves];
+    __shared__ CandQueue s_queue[kWarps];
     __shared__ upbp_mis s_e[kWarps];
     __shared__ CamSum s_cs[kWarps];
     stage_media(K, media);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     int* stack = s_stack[warp];
     int* leaves = s_leaves[warp];
+    CandQueue& cq = s_queue[warp];
     const int leaf_shift = __ffs(B.leaf) - 1;
     for (;;) {
         unsigned qq = 0;
@@ -691,32 +553,65 @@ __global__ void __launch_bounds__(kWarps * 32, 5) k_bb1d_warp(const __grid_const
             acc = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
                 Rgb part = rgb(0.f);
                 const int mid = (int)(&m - media);
-                const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps,
-                                              s.dmax + K.eps, stack, leaves, lane, [&](int i) {
-                    const float4 pc = __ldg(&B.pc[i]);
-                    if (__float_as_int(pc.w) != mid) return;  // mMedium == medium (PhotonBeam.hxx:390)
+                int qn = 0;  // entries in the candidate queue (warp-uniform)
+                // evaluates queue entry e (one lane, one accepted candidate)
+                auto eval = [&](int e) {
+                    const int i = cq.piece[e];
+                    const float4 g = cq.geo[e];
                     const float4 pa = __ldg(&B.pa[i]);
                     const float4 pb = __ldg(&B.pb[i]);
-                    ++tested;
-                    float dist, sinT, t1, t2;
-                    if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f,
-                                        pa.w, pc.y, &dist, &sinT, &t1, &t2))
-                        return;
-                    if (!(t2 >= pb.w && t2 < pc.x)) return;  // this piece owns t2
-                    const int beam = __float_as_int(pc.z);
-                    const float radius = kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[beam]);
-                    if (radius < dist) return;  // PhotonBeam.hxx:411-413
-                    ++cnt;
-                    h += mix64((unsigned long long)beam);
                     if (kMixed) {
                         const PiecePayload py = B.pay[i];
                         part = part + bb1d_contrib_packed(K, m, s, py, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                                          dist, sinT, t1, t2);
+                                                          g.x, g.y, g.z, g.w);
                     } else {
+                        const int beam = __float_as_int(__ldg(&B.pc[i]).z);
                         part = part + bb1d_contrib<false>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z),
-                                                          v3(pb.x, pb.y, pb.z), radius, dist, sinT, t1, t2);
+                                                          v3(pb.x, pb.y, pb.z), __ldg(&Bs.radius[beam]), g.x, g.y,
+                                                          g.z, g.w);
+                    }
+                };
+                const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps,
+                                              s.dmax + K.eps, stack, leaves, lane, [&](int i) {
+                    bool hit = false;
+                    float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f;
+                    if (i >= 0) {
+                        const float4 pc = __ldg(&B.pc[i]);
+                        if (__float_as_int(pc.w) == mid) {  // mMedium == medium (PhotonBeam.hxx:390)
+                            const float4 pa = __ldg(&B.pa[i]);
+                            const float4 pb = __ldg(&B.pb[i]);
+                            ++tested;
+                            if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
+                                               v3(pb.x, pb.y, pb.z), 0.f, pa.w, pc.y, &dist, &sinT, &t1, &t2) &&
+                                piece_owns(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w,
+                                           pb.w, pc.x, t1, t2)) {
+                                const int beam = __float_as_int(pc.z);
+                                const float radius = kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[beam]);
+                                if (!(radius < dist)) {  // PhotonBeam.hxx:411-413
+                                    hit = true;
+                                    ++cnt;
+                                    h += mix64((unsigned long long)beam);
+                                }
+                            }
+                        }
+                    }
+                    const unsigned vote = __ballot_sync(kFull, hit);
+                    if (vote == 0u) return;
+                    if (hit) {
+                        const int pos = qn + __popc(vote & lt);
+                        cq.piece[pos] = i;
+                        cq.geo[pos] = make_float4(dist, sinT, t1, t2);
+                    }
+                    qn += __popc(vote);
+                    __syncwarp();
+                    if (qn >= 32) {  // the newest 32 entries, one per lane
+                        eval(qn - 32 + lane);
+                        qn -= 32;
+                        __syncwarp();
                     }
                 });
+                if (lane < qn) eval(lane);
+                __syncwarp();
                 if (!ok && lane == 0) atomicOr(status, 1);
                 return part;
             });
@@ -736,13 +631,6 @@ __global__ void __launch_bounds__(kWarps * 32, 5) k_bb1d_warp(const __grid_const
             if (O.tested) atomicAdd(O.tested, tested);
         }
     }
-}
-
-// HashGrid::GetCellIndex (Misc/HashGrid.hxx:198-206)
-__device__ __forceinline__ uint32_t hash_cell(int x, int y, int z, int cells)
-{
-    const uint32_t ux = (uint32_t)x, uy = (uint32_t)y, uz = (uint32_t)z;
-    return ((ux * 73856093u) ^ (uy * 19349663u) ^ (uz * 83492791u)) % (uint32_t)cells;
 }
 
 template <bool kMixed>
@@ -869,21 +757,36 @@ void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH&
     else k_gather_bb1d<false><<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, cs, O);
 }
 
-int bb1d_warp_blocks_per_sm(bool mixed)
+// Two instantiations of the warp kernel differ only in the occupancy the compiler is asked to
+// reach: 5 blocks of 4 warps per SM (up to 96 registers) or 6 (up to 80 registers, more warps to
+// hide load latency, some spills); the tuning's bb1d_kernel picks 1 or 2.
+template <bool kMixed>
+static int blocks_for(int variant)
 {
     int nb = 0;
-    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<true, 4>, 128, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<false, 4>, 128, 0);
+    if (variant == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 6>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 5>, 128, 0);
     return nb > 0 ? nb : 1;
+}
+
+int bb1d_warp_blocks_per_sm(bool mixed, int variant)
+{
+    return mixed ? blocks_for<true>(variant) : blocks_for<false>(variant);
 }
 
 void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
                       const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
-                      bool mixed, unsigned int* work, int* status, const int32_t* order, cudaStream_t stream)
+                      bool mixed, unsigned int* work, int* status, const int32_t* order, cudaStream_t stream,
+                      int variant)
 {
     if (Q.n <= 0) return;
-    if (mixed) k_bb1d_warp<true, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
-    else k_bb1d_warp<false, 4><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+    if (variant == 2) {
+        if (mixed) k_bb1d_warp<true, 4, 6><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+        else k_bb1d_warp<false, 4, 6><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+    } else {
+        if (mixed) k_bb1d_warp<true, 4, 5><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+        else k_bb1d_warp<false, 4, 5><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+    }
 }
 
 namespace {

@@ -27,7 +27,7 @@ from . import abi
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libupbp_b200.so")
 
-MODE_PLAIN, MODE_MIXED = 0, 1
+MODE_PLAIN, MODE_MIXED, MODE_FP64 = 0, 1, 2
 
 EXPORTS = (
     "upbp_ctx_create", "upbp_ctx_destroy", "upbp_last_error", "upbp_set_mode", "upbp_set_tuning", "upbp_get_tuning",
@@ -35,6 +35,7 @@ EXPORTS = (
     "upbp_build", "upbp_set_camera_mis", "upbp_set_segment_queries", "upbp_set_point_queries", "upbp_evaluate",
     "upbp_read_segment_results", "upbp_read_point_results", "upbp_read_query_stats", "upbp_clear_image",
     "upbp_read_image", "upbp_last_launch_count", "upbp_last_timings", "upbp_destroy_structures",
+    "upbp_read_tested_counts", "upbp_adjoint", "upbp_device_bytes",
 )
 
 
@@ -80,6 +81,9 @@ def lib():
         l.upbp_last_launch_count.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         l.upbp_last_timings.argtypes = [vp] + [C.POINTER(C.c_float)] * 4
         l.upbp_destroy_structures.argtypes = [vp]
+        l.upbp_read_tested_counts.argtypes = [vp, abi.u64p]
+        l.upbp_adjoint.argtypes = [vp, abi.f32p, C.c_int32, C.POINTER(C.c_double)]
+        l.upbp_device_bytes.argtypes = [vp, abi.u64p]
         for name in EXPORTS:
             if name != "upbp_last_error":
                 getattr(l, name).restype = C.c_int
@@ -192,6 +196,34 @@ class EstimatorStage:
         st = abi.QueryStats(**{k: abi.ptr(v) for k, v in out.items()})
         self._ck(self._l.upbp_read_query_stats(self._ctx, C.byref(st)))
         return out
+
+    def device_bytes(self) -> int:
+        out = np.zeros(1, np.uint64)
+        self._ck(self._l.upbp_device_bytes(self._ctx, abi.ptr(out)))
+        return int(out[0])
+
+    def pixels(self) -> int:
+        return self._npix
+
+    def set_media(self, media: np.ndarray):
+        """Replace the media table (``workload.MEDIUM_DTYPE`` records); the structures stay built."""
+        m = np.ascontiguousarray(media, dtype=abi.MEDIUM_DTYPE)
+        arr = (abi.Medium * len(m)).from_buffer_copy(m.tobytes())
+        self._media_keep = arr
+        self._ck(self._l.upbp_set_media(self._ctx, arr, len(m)))
+
+    def adjoint(self, grad_image_ptr: int, medium: int) -> np.ndarray:
+        """dL/d(sigma_a rgb, sigma_s rgb, g) of ``medium`` given dL/d framebuffer at ``grad_image_ptr``
+        ([H*W][3] float32, host or device address)."""
+        out = (C.c_double * 7)()
+        self._ck(self._l.upbp_adjoint(self._ctx, C.cast(C.c_void_p(grad_image_ptr), abi.f32p), medium, out))
+        return np.array(list(out), np.float64)
+
+    def tested_counts(self):
+        """Candidates tested by the last evaluate: {"pb2d": photons, "bb1d": beam pieces, "pp3d": photons}."""
+        out = np.zeros(3, np.uint64)
+        self._ck(self._l.upbp_read_tested_counts(self._ctx, abi.ptr(out)))
+        return {"pb2d": int(out[0]), "bb1d": int(out[1]), "pp3d": int(out[2])}
 
     def image(self):
         img = np.zeros((self._npix, 3), np.float32)

@@ -149,6 +149,10 @@ def config(name: str) -> SceneConfig:
         return nested_boxes_scene()
     if name == "diff512":      # differentiable-estimator scene: 512^2, 262,144 light paths
         return cube_scene("diff512", 512, 512, 262_144, 6, 0.01)
+    if name == "beamstress":   # BB1D closest-approach stress: 2M beams x 2M query rays (see beam_stress)
+        ss = 1.6
+        return SceneConfig("beamstress", [CLEAR, Medium((0.4,) * 3, (ss,) * 3, 0.3, 0.8)], [((0, 0, 0), (1, 1, 1), 1)],
+                           64, 64, 4096, 6, 0.002)
     if name.startswith("cube") and "x" in name[4:]:
         # cube<W>x<N_L>, e.g. cube64x4096 (small parity cases)
         w, nl = name[4:].split("x")
@@ -713,3 +717,80 @@ def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float]
     out["pq_pixel"] = cat(PQ, "pixel", np.int32)
     out["pq_cam_mis_begin"] = cat(PQ, "cam_begin", np.int64)
     out["cam_mis"] = np.concatenate(CR) if CR else np.zeros(0, MIS_DTYPE)
+
+
+# ----------------------------------------------------------------------------------------------
+# Closest-approach precision stress (beam-beam geometry only)
+
+def _stress_directions(rng: np.random.Generator, n: int, parallel_fraction: float, max_angle: float):
+    """Unit directions: a ``parallel_fraction`` share within ``max_angle`` (uniform angle) of +z, the
+    rest uniform on the sphere."""
+    par = rng.random(n) < parallel_fraction
+    theta = np.where(par, rng.random(n) * max_angle, np.arccos(1.0 - 2.0 * rng.random(n)))
+    phi = 2.0 * math.pi * rng.random(n)
+    st = np.sin(theta)
+    d = np.stack([st * np.cos(phi), st * np.sin(phi), np.cos(theta)], axis=1)
+    return d, par
+
+
+def beam_stress(n_beams: int, n_queries: int, radius: float = 0.002, sigma_t: float = 2.0,
+                parallel_fraction: float = 0.5, max_angle: float = 1e-4, seed: int = 1234,
+                base_light_paths: int = 4096, base_size: int = 64) -> Dict[str, np.ndarray]:
+    """BB1D closest-approach stress workload: ``n_beams`` photon beams and ``n_queries`` query rays
+    with origins uniform in [0,1]^3, half of both (``parallel_fraction``) within ``max_angle`` rad of
+    a common axis and half isotropic, lengths exponential with rate ``sigma_t``, radius ``radius``.
+
+    The geometry is the stress; every other record comes from one ordinary cube iteration (radius
+    ``radius``, medium with sigma_t = ``sigma_t``), whose beam and query records are reused
+    cyclically: beam throughputs, pdfs, flags and light-vertex links (so the light-side MIS records
+    stay valid), and the queries' camera MIS snapshots, path lengths, throughputs and pixels.  Each
+    query becomes one full segment [0, length) in the medium with only BB1D enabled; there are no
+    point queries.
+    """
+    ss = 0.8 * sigma_t
+    med = Medium((sigma_t - ss,) * 3, (ss,) * 3, 0.3, 0.8)
+    cfg = SceneConfig("stress_base", [CLEAR, med], [((0, 0, 0), (1, 1, 1), 1)], base_size, base_size,
+                      base_light_paths, 6, radius, seed=seed)
+    w = generate(cfg, 0)
+    rng = np.random.Generator(np.random.Philox(key=seed + 7919))
+    nb0, nq0 = len(w["beam_length"]), len(w["sq_path_length"])
+    if nb0 == 0 or nq0 == 0:
+        raise ValueError("base iteration has no beams or no segment queries")
+    bi = np.arange(n_beams) % nb0
+    for k in [k for k in w if k.startswith("beam_")]:
+        w[k] = np.ascontiguousarray(w[k][bi])
+    w["beam_origin"] = rng.random((n_beams, 3)).astype(np.float32)
+    d, _ = _stress_directions(rng, n_beams, parallel_fraction, max_angle)
+    w["beam_direction"] = d.astype(np.float32)
+    w["beam_length"] = (-np.log1p(-rng.random(n_beams)) / sigma_t).astype(np.float32)
+    w["beam_medium_id"] = np.ones(n_beams, np.int32)
+
+    qi = np.arange(n_queries) % nq0
+    for k in ("sq_path_length", "sq_last_pdf_w_inv", "sq_throughput", "sq_pixel", "sq_cam_mis_begin"):
+        w[k] = np.ascontiguousarray(w[k][qi])
+    w["sq_flags"] = ((w["sq_flags"][qi] & Q_ORIGIN_IN_MEDIUM) | Q_BB1D).astype(np.uint32)
+    w["sq_origin"] = rng.random((n_queries, 3)).astype(np.float32)
+    d, _ = _stress_directions(rng, n_queries, parallel_fraction, max_angle)
+    w["sq_direction"] = d.astype(np.float32)
+    w["sq_seg_begin"] = np.arange(n_queries, dtype=np.int32)
+    w["sq_seg_count"] = np.ones(n_queries, np.int32)
+    length = (-np.log1p(-rng.random(n_queries)) / sigma_t).astype(np.float32)
+    w["seg_dist_min"] = np.zeros(n_queries, np.float32)
+    w["seg_dist_max"] = length
+    w["seg_pdf"] = np.exp(-sigma_t * length.astype(np.float64)).astype(np.float32)
+    w["seg_rev_pdf"] = w["seg_pdf"].copy()
+    w["seg_attenuation"] = np.repeat(w["seg_pdf"][:, None], 3, axis=1).astype(np.float32)
+    w["seg_medium"] = np.ones(n_queries, np.int32)
+    for k in ("pq_position", "pq_dir_fix", "pq_throughput"):
+        w[k] = np.zeros((0, 3), np.float32)
+    for k, dt in (("pq_medium_id", np.int32), ("pq_path_length", np.int32), ("pq_pixel", np.int32),
+                  ("pq_cam_mis_begin", np.int64)):
+        w[k] = np.zeros(0, dt)
+    return w
+
+
+def make(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
+    """The estimator-stage inputs of one iteration of configuration ``cfg``."""
+    if cfg.name == "beamstress":
+        return beam_stress(2_000_000, 2_000_000, radius=cfg.radius, seed=cfg.seed + iteration)
+    return generate(cfg, iteration)

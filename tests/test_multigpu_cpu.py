@@ -102,7 +102,8 @@ def test_two_ranks_combine_to_the_serial_framebuffer(tmp_path):
     want = (((per[0] + per[2]) / 2 + (per[1] + per[3]) / 2) / 2).reshape(-1)
     assert np.abs(want).max() > 0
     for img in imgs:
-        np.testing.assert_allclose(img, want, rtol=1e-12, atol=1e-15)
+        # the framebuffers are FP32 sums: compared at FP32 precision
+        np.testing.assert_allclose(img, want, rtol=1e-6, atol=1e-12)
     for s in stats:
         assert s[0] == 20.0          # max over ranks
         assert s[1] == total         # units over ranks
@@ -112,4 +113,4 @@ def test_rank_without_iterations_does_not_count(tmp_path):
     imgs, _ = _launch(2, 1, tmp_path)  # rank 1 runs nothing, as an unused renderer
     want = _image(0).reshape(-1)
     for img in imgs:
-        np.testing.assert_allclose(img, want, rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(img, want, rtol=1e-6, atol=1e-12)
