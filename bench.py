@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
+    ap.add_argument("--no-graph", action="store_true", help="direct calls instead of the captured CUDA graph")
     ap.add_argument("--adjoint", action="store_true",
                     help="time forward + adjoint (dL/d sigma_a, sigma_s, g) of an L2 image loss instead")
     ap.add_argument("--dropin", action="store_true",
@@ -204,11 +205,16 @@ def run_b200(args, cfg, rank, world, local_rank):
         tuning = {"best": best, "autotuned": True, "trials": rep["trials"], "seconds": time.time() - t_at}
     units = [len(w["sq_path_length"]) + len(w["pq_path_length"]) for w in works]
 
+    graphs = set()
+
     def step(i):
         st = stages[i % n_iter]
-        st.build()
-        st.clear_image()
-        st.evaluate()
+        if id(st) in graphs:
+            st.launch_graph()  # clear + build + evaluate, captured after the warm-up
+        else:
+            st.build()
+            st.clear_image()
+            st.evaluate()
         if world > 1:
             import torch.distributed as dist
             st.read_image_into(img_t.data_ptr())
@@ -218,6 +224,14 @@ def run_b200(args, cfg, rank, world, local_rank):
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
             step(i)
+        if not args.no_graph:
+            for st in stages:
+                try:
+                    st.capture_graph()
+                except engine.UpbpError:  # not evaluated during the warm-up
+                    st.build(); st.clear_image(); st.evaluate()
+                    st.capture_graph()
+                graphs.add(id(st))
     torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
@@ -264,9 +278,13 @@ def run_b200(args, cfg, rank, world, local_rank):
            "pb2d": BYTES_PER_QUERY * nq + BYTES_PER_POINT_CAND * acc["pb2d"],
            "bb1d": BYTES_PER_QUERY * nq + BYTES_PER_BB1D * acc["bb1d"]}
     avg = {k: statistics.mean(v) for k, v in kern.items()}
+    if tuning["best"].get("bb1d_kernel", 1) >= 3:
+        # one persistent kernel evaluates PB2D and BB1D: its phase (bb1d_ms) carries both
+        alg["bb1d"] += alg.pop("pb2d")
+        alg["pb2d"] = 0
     dom = max(("pp3d", "pb2d", "bb1d"), key=lambda k: avg[k + "_ms"])
     peak, peak_kind = measured_peak()
-    achieved = alg[dom] / (avg[dom + "_ms"] / 1000.0) / 1e9
+    achieved = alg[dom] / (avg[dom + "_ms"] / 1000.0) / 1e9 if avg[dom + "_ms"] > 0 else None
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (dom, cfg.name))
     if os.path.exists(tfile):
@@ -339,13 +357,13 @@ def run_b200(args, cfg, rank, world, local_rank):
                        queries_per_iteration={"segment": nq, "point": npq},
                        photons=int((works[0]["lv_flags"] & 1).sum()), beams=len(works[0]["beam_length"]),
                        parallelism="dp%d (one iteration per rank, framebuffer all-reduce)" % world,
-                       tuning=tuning),
+                       tuning=tuning, cuda_graph=not args.no_graph),
         "ms_per_iteration": ms_max / args.steps,
         "kernels_ms": avg,
         "accepted_candidates": acc,
         "tested_candidates": tested,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "unit": "GB/s", "frac": achieved / peak if achieved is not None else None, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg[dom]},
         "cpu_baseline": cpu,
         "e2e": e2e,

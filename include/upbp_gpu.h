@@ -62,6 +62,9 @@ extern "C" {
 #define UPBP_PREVIOUS 256u
 #define UPBP_COMPATIBLE 512u
 #define UPBP_BB1D_PREVIOUS 1024u
+#define UPBP_BP2D 65536u /* extension, not a reference technique (above every reference flag; 2048 is
+                         * SPECULAR_ONLY): B-P2D, photon beams x camera medium points with a 2-D
+                         * kernel, as a standalone estimator with MIS weight 1 */
 #define UPBP_ORIGIN_IN_MEDIUM 1u /* AbstractMedium::kOriginInMedium */
 #define UPBP_END_IN_MEDIUM 2u    /* AbstractMedium::kEndInMedium */
 
@@ -243,7 +246,9 @@ int upbp_set_mode(upbp_ctx* ctx, int mode);
 /* Tunables (picked by smallupbp_b200.autotune): LBVH leaf sizes (powers of two), the block size
  * of the thread-per-query gathers, the BB1D beam-piece length in beam radii, and the BB1D
  * gather variant (0: thread per query, 1: warp-cooperative persistent work queue at 5 blocks of
- * 4 warps per SM, 2: the same kernel compiled for 6 blocks per SM). */
+ * 4 warps per SM, 2: the same kernel compiled for 6 blocks per SM, 3 and 4: one persistent
+ * work-queue kernel for all camera segments that evaluates PB2D and BB1D per query, at 5 or 6
+ * blocks per SM; the PB2D phase of upbp_last_timings is then 0 and the BB1D phase covers both). */
 typedef struct upbp_tuning {
     int32_t pb2d_leaf;
     int32_t bb1d_leaf;
@@ -288,6 +293,15 @@ int upbp_evaluate(upbp_ctx* ctx);
 int upbp_read_segment_results(upbp_ctx* ctx, float* pb2d_rgb, float* bb1d_rgb); /* [n][3] each, may be NULL */
 int upbp_read_point_results(upbp_ctx* ctx, float* pp3d_rgb);                    /* [n][3] */
 int upbp_read_query_stats(upbp_ctx* ctx, const upbp_query_stats* stats);
+/* CUDA graph of one iteration's estimator stage: upbp_capture_graph records clear image + build
+ * + evaluate for the inputs of the last upbp_build / upbp_evaluate (which must have run, so that
+ * every buffer is sized and the photon and beam-piece counts are known) without executing it;
+ * upbp_launch_graph replays it on the context's stream, asynchronously, with the same results
+ * as those three calls.  Any upload, upbp_set_* or reallocation discards the graph (launch then
+ * returns UPBP_ERR_NOT_BUILT).  The stream must not be the legacy default stream. */
+int upbp_capture_graph(upbp_ctx* ctx);
+int upbp_launch_graph(upbp_ctx* ctx);
+
 /* Adjoint of the estimator sum with respect to the parameters of media[medium]: given
  * grad_image = dL/d(framebuffer) ([H*W][3] floats, host or device pointer), writes
  * grad[0..6] = dL/d(sigma_a r,g,b, sigma_s r,g,b, g) for the structures and queries of the last
@@ -297,13 +311,19 @@ int upbp_read_query_stats(upbp_ctx* ctx, const upbp_query_stats* stats);
  * differentiable estimator (smallupbp_b200.autograd). */
 int upbp_adjoint(upbp_ctx* ctx, const float* grad_image, int32_t medium, double* grad);
 
+/* B-P2D results of the last evaluate (extension; needs UPBP_BP2D in params.techniques): per
+ * point query the contribution [n][3] (before throughput and normalisation), the number of
+ * accepted beams and the order-independent hash of their indices.  Any pointer may be NULL.
+ * The point-query phase of upbp_last_timings (pp3d_ms) includes the B-P2D gather. */
+int upbp_read_bp2d_results(upbp_ctx* ctx, float* rgb, uint32_t* count, uint64_t* hash);
+
 /* Device memory the context holds (its grow-only buffers), in bytes. */
 int upbp_device_bytes(const upbp_ctx* ctx, uint64_t* bytes);
 
 /* Candidates tested by the last evaluate, summed over all queries: [0] PB2D photons, [1] BB1D beam
  * pieces, [2] PP3D photons (diagnostics of culling quality; accepted counts are in the query stats). */
 int upbp_read_tested_counts(upbp_ctx* ctx, uint64_t* tested);
-int upbp_clear_image(upbp_ctx* ctx);
+int upbp_clear_image(upbp_ctx* ctx); /* zeroes the framebuffer and the per-query results */
 int upbp_read_image(upbp_ctx* ctx, float* rgb); /* [H*W][3] accumulated */
 /* Device-side counters: number of kernels launched by the last upbp_build and upbp_evaluate. */
 int upbp_last_launch_count(const upbp_ctx* ctx, int* build_launches, int* evaluate_launches);

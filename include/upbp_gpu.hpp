@@ -185,6 +185,27 @@ public:
         return img;
     }
 
+    /* B-P2D contributions per point ticket (extension, UPBP_BP2D in the techniques). */
+    void bp2d_results(std::vector<float>& bp2d_rgb)
+    {
+        bp2d_rgb.resize(3 * pq_path_length_.size());
+        check(upbp_read_bp2d_results(ctx_, bp2d_rgb.data(), nullptr, nullptr));
+    }
+
+    /* dL/d(sigma_a rgb, sigma_s rgb, g) of media[medium] for dL/d framebuffer (H*W*3 floats), after
+     * evaluate() in UPBP_MODE_MIXED or UPBP_MODE_FP64 (no counterpart in the reference). */
+    std::vector<double> adjoint(const std::vector<float>& grad_image, int medium)
+    {
+        std::vector<double> g(7);
+        check(upbp_adjoint(ctx_, grad_image.data(), medium, g.data()));
+        return g;
+    }
+
+    /* Record build + evaluate of the current recording as a CUDA graph (after one evaluate()), and
+     * replay it (asynchronously; results as from build() + evaluate()). */
+    void capture_graph() { check(upbp_capture_graph(ctx_)); }
+    void launch_graph() { check(upbp_launch_graph(ctx_)); }
+
     /* End of the iteration: EmbreeBre::destroy / PhotonBeamsEvaluator::destroy and a new recording. */
     void clear()
     {

@@ -55,3 +55,25 @@ def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False) -> Dict[s
         raise RuntimeError("upbp_oracle_run failed (%d)" % rc)
     del keep
     return out
+
+
+def bp2d(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False) -> Dict[str, np.ndarray]:
+    """B-P2D (extension) of workload ``w`` with the C restatement: per point query rgb, count, hash,
+    and the framebuffer of the B-P2D contributions alone."""
+    s, keep = abi.make_structs(w)
+    l = lib(fp64)
+    f = l.upbp_oracle_bp2d
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Medium), C.c_int32, C.POINTER(abi.Beams),
+                  C.POINTER(abi.PointQueries), C.c_int64, abi.f32p, abi.u32p, abi.u64p, abi.f32p]
+    npq = s["pq"].n
+    p = s["params"]
+    out = {"bp2d": np.zeros((npq, 3), np.float32), "count_bp2d": np.zeros(npq, np.uint32),
+           "hash_bp2d": np.zeros(npq, np.uint64), "image": np.zeros((p.image_width * p.image_height, 3), np.float32)}
+    P = abi.ptr
+    rc = f(C.byref(p), s["media"], s["n_media"], C.byref(s["beams"]), C.byref(s["pq"]), stride, P(out["bp2d"]),
+           P(out["count_bp2d"]), P(out["hash_bp2d"]), P(out["image"]))
+    if rc != 0:
+        raise RuntimeError("upbp_oracle_bp2d failed (%d)" % rc)
+    del keep
+    return out

@@ -810,3 +810,84 @@ int upbp_oracle_run(const upbp_params* P, const upbp_medium* media, int32_t n_me
     if (have_grid) { free(g.start); free(g.end); free(g.idx); }
     return 0;
 }
+
+/* ---------------------------------------------------------------- B-P2D (extension) */
+/*
+ * Beam x point, 2-D kernel: photon beams queried at the camera medium vertices (the PP3D
+ * queries).  The reference has no B-P2D estimator, so this is the definition the CUDA path is
+ * checked against (parity unpinned by the reference):
+ *   candidate  the beam's ray [0, len) passes within r = radius_bb1d of the point, tested with
+ *              testIntersectionBre (Bre.cxx:199-223) with the beam as the ray and the query point
+ *              as the photon (FP32, reference operation order), beam medium == point medium;
+ *   value      beam throughput x exp(-sigma_t t) (divided by the free-flight pdf of the minimum
+ *              component for SHORT beams, as accumulate2 does on the beam side) x sigma_s x
+ *              HG phase(camera dir_fix, -beam dir) x (1 - d^2 / r^2) / (pi r^2 / 2);
+ *   weight     1: the reference's MIS records carry no B-P2D terms, so B-P2D is a standalone
+ *              estimator outside the UPBP combination;
+ *   image      += camera throughput x norm_bb1d (1 / light paths) x value.
+ * Point queries with index % stride == 0; any output pointer may be NULL.
+ */
+int upbp_oracle_bp2d(const upbp_params* P, const upbp_medium* media, int32_t n_media, const upbp_beams* bm,
+                     const upbp_point_queries* pq, int64_t stride, float* bp2d_rgb, uint32_t* cnt, uint64_t* hash,
+                     float* image)
+{
+    medium M[ORACLE_MAX_MEDIA];
+    int64_t q;
+    int i;
+    if (!P || !media || n_media <= 0 || n_media > ORACLE_MAX_MEDIA || !bm || !pq || stride < 1) return -1;
+    for (i = 0; i < n_media; ++i) M[i] = make_medium(&media[i]);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (q = 0; q < pq->n; q += stride) {
+        const int px = pq->pixel[q];
+        const v3f x = Vf(pq->position + 3 * q);
+        const v3 cfix = V(pq->dir_fix + 3 * q);
+        const int mid = pq->medium_id[q];
+        const medium* m = &M[mid];
+        const float r = P->radius_bb1d, r2 = r * r;
+        rgb v = cs(0.f);
+        uint32_t c = 0;
+        uint64_t h = 0;
+        int64_t b;
+        int k;
+        if ((P->techniques & UPBP_BP2D) && m->has_scat) {
+            for (b = 0; b < bm->n; ++b) {
+                float tf, d2f;
+                real t, d2, pfd, phase, sinT, kernel;
+                rgb att, val;
+                if (bm->medium_id[b] != mid) continue;
+                if (!test_bre(Vf(bm->origin + 3 * b), Vf(bm->direction + 3 * b), 0.f, bm->length[b], x, r2, &tf, &d2f))
+                    continue;
+                ++c;
+                h += mix64((uint64_t)b);
+                t = tf;
+                d2 = d2f;
+                if (IS_F64) { /* re-solve the foot point in FP64 */
+                    const v3 o = V(bm->origin + 3 * b), d = V(bm->direction + 3 * b), p = V(pq->position + 3 * q);
+                    v3 qv;
+                    t = dot(sub(p, o), d);
+                    qv.x = o.x + d.x * t - p.x; qv.y = o.y + d.y * t - p.y; qv.z = o.z + d.z * t - p.z;
+                    d2 = dot(qv, qv);
+                }
+                att = eval_att(m, t);
+                pfd = comp(att, m->min_idx);
+                if (bm->flags[b] & UPBP_SHORT_BEAM) att = cdiv(att, pfd);
+                if (!c_positive(att)) continue;
+                phase = hg_pdf(cfix, neg(V(bm->direction + 3 * b)), m->g, &sinT);
+                if (phase <= 0) continue;
+                kernel = (1 - d2 / (real)r2) / ((real)r2 * (IS_F64 ? (real)3.14159265358979323846 : (real)PI_F) * (real)0.5);
+                if (!is_pos(kernel)) continue;
+                val = cscale(cmul(cmul(C3(bm->throughput + 3 * b), att), Cr(m->ss)), phase * kernel);
+                v = cadd(v, val);
+            }
+        }
+        if (bp2d_rgb) { bp2d_rgb[3 * q] = v.r; bp2d_rgb[3 * q + 1] = v.g; bp2d_rgb[3 * q + 2] = v.b; }
+        if (cnt) cnt[q] = c;
+        if (hash) hash[q] = h;
+        if (image && px >= 0)
+            for (k = 0; k < 3; ++k) {
+#pragma omp atomic
+                image[3 * px + k] += pq->throughput[3 * q + k] * P->norm_bb1d * comp(v, k);
+            }
+    }
+    return 0;
+}

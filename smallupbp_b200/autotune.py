@@ -4,14 +4,15 @@ The knobs (``upbp_tuning`` in ``include/upbp_gpu.h``):
 
 * ``bb1d_leaf`` and ``beam_piece_radii`` shape the BB1D beam-piece LBVH: shorter pieces and
   smaller leaves give tighter boxes (fewer tested pieces per query) at the price of more nodes;
-* ``bb1d_kernel`` 1 or 2 picks the occupancy the warp-cooperative BB1D gather is compiled for
-  (5 or 6 blocks of 4 warps per SM);
+* ``bb1d_kernel`` picks the segment gathers: 1 or 2 the warp-cooperative BB1D kernel compiled for
+  5 or 6 blocks of 4 warps per SM (PB2D in its own kernel), 3 or 4 one persistent kernel for all
+  camera segments doing PB2D and BB1D per query;
 * ``pb2d_leaf`` is the photon count per PB2D LBVH leaf;
 * ``block_threads`` is the block shape (queries per block) of the thread-per-query PB2D and PP3D
   gathers.
 
-The tuner searches the grids on the caller's own workload, every candidate timed by the
-library's per-kernel CUDA events, best of ``repeats``.  The workload stays resident; only the
+The tuner searches the grids on the caller's own workload, one stage of knobs at a time, every
+candidate timed by the library's CUDA events (the whole estimator stage), best of ``repeats``.  The workload stays resident; only the
 structures are rebuilt.  Results are plain dicts, so a
 caller can store them (``save``/``load``) and skip the search next time for the same workload
 signature.
@@ -24,8 +25,12 @@ import os
 from typing import Dict, Iterable, List, Optional, Tuple
 
 
-BB1D_SPACE = {"bb1d_leaf": (2, 4, 8), "beam_piece_radii": (2.0, 3.0, 4.0, 6.0), "bb1d_kernel": (1, 2)}
-PB2D_SPACE = {"pb2d_leaf": (4, 8, 16), "block_threads": (128, 256)}
+# searched one stage at a time (coordinate descent), each stage a grid over its knobs
+STAGES = (
+    {"bb1d_kernel": (1, 2, 3, 4)},
+    {"bb1d_leaf": (2, 4, 8), "beam_piece_radii": (3.0, 4.0, 6.0)},
+    {"pb2d_leaf": (4, 8, 16), "block_threads": (128, 256)},
+)
 
 
 def _grid(space: Dict[str, Iterable]) -> List[Dict]:
@@ -55,32 +60,27 @@ def _time(stage, repeats: int) -> Dict[str, float]:
     return best
 
 
-def autotune(stage, structs, repeats: int = 2, bb1d_space: Optional[Dict] = None,
-             pb2d_space: Optional[Dict] = None) -> Tuple[Dict, Dict]:
+def autotune(stage, structs, repeats: int = 2, stages=STAGES) -> Tuple[Dict, Dict]:
     """Search the knobs for the workload already loaded into ``stage`` (``EstimatorStage``).
 
-    The BB1D and PB2D knobs are disjoint and each gather's time depends only on its own, so one
-    trial times a BB1D candidate and a PB2D candidate together (the shorter list is cycled).
-    Each estimator is scored by its gather time; the builds are a few percent of the step.
-    Leaves the best tuning set on ``stage`` (built) and returns ``(best, report)``.
+    Coordinate descent over ``stages``: each stage times every point of its grid with the best
+    values found so far for the other knobs and keeps the fastest.  A candidate's score is the
+    whole estimator stage (builds + all gathers) from the library's CUDA events, because the
+    fused segment kernel moves PB2D time into the BB1D phase.  Leaves the best tuning set on
+    ``stage`` (built) and returns ``(best, report)``.
     """
     base = stage.get_tuning()
     best = {k: getattr(base, k) for k, _ in base._fields_}
-    bb = _grid(bb1d_space or BB1D_SPACE)
-    pb = _grid(pb2d_space or PB2D_SPACE)
     trials = []
-    score_bb, score_pb = [], []
-    for i in range(max(len(bb), len(pb))):
-        cand = dict(bb[i % len(bb)], **pb[i % len(pb)])
-        stage.set_tuning(**dict(best, **cand))
-        t = _time(stage, repeats)
-        trials.append(dict(cand, **t))
-        if i < len(bb):
-            score_bb.append((t["bb1d_ms"], bb[i]))
-        if i < len(pb):
-            score_pb.append((t["pb2d_ms"], pb[i]))
-    best.update(min(score_bb, key=lambda x: x[0])[1])
-    best.update(min(score_pb, key=lambda x: x[0])[1])
+    for space in stages:
+        scores = []
+        for cand in _grid(space):
+            stage.set_tuning(**dict(best, **cand))
+            t = _time(stage, repeats)
+            total = t["build_ms"] + t["pp3d_ms"] + t["pb2d_ms"] + t["bb1d_ms"]
+            trials.append(dict(cand, total_ms=total, **t))
+            scores.append((total, cand))
+        best.update(min(scores, key=lambda x: x[0])[1])
     stage.set_tuning(**best)
     stage.build()
     return best, {"signature": signature(structs), "best": best, "trials": trials}

@@ -93,9 +93,15 @@ struct upbp_ctx {
     DBuf work, status;
     DBuf grad_img, grad_acc;  // adjoint: dL/d framebuffer, dL/d medium parameters
     int* status_host = nullptr;   // page-locked copy of status[0] after the last evaluate
+    // CUDA graph of clear + build + evaluate for the current inputs (upbp_capture_graph)
+    cudaGraphExec_t graph_exec = nullptr;
+    bool replay = false;     // capturing: reuse the last build's counts, allocate nothing, no host syncs
+    bool evaluated = false;  // an evaluate ran after the last build (every buffer is sized)
+    bool graph_status = false;  // the graph copies the BB1D traversal status back
     bool status_pending = false;  // status_host holds the last BB1D launch's flag
     int num_sms = 0;
     int bb1d_kernel = 1;  // 0: thread per query, 1: warp-cooperative persistent
+    DBuf out_bp2d, cnt_bp2d, hash_bp2d;  // B-P2D (extension) per point query
     DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
     bool built = false;
     int build_launches = 0, eval_launches = 0;
@@ -136,9 +142,27 @@ void check_status(upbp_ctx* c)
                                    "incomplete (use a larger bb1d_leaf or beam_piece_radii)");
 }
 
+// Timing event; inside a graph capture it must be an external event record node, or the
+// captured record would only order the graph's own nodes and never time anything.
+void mark(upbp_ctx* c, int k, cudaStream_t s)
+{
+    ck(c, c->replay ? cudaEventRecordWithFlags(c->ev[k], s, cudaEventRecordExternal) : cudaEventRecord(c->ev[k], s),
+       "event");
+}
+
+void drop_graph(upbp_ctx* c)
+{
+    if (c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        c->graph_exec = nullptr;
+    }
+}
+
 void ensure(upbp_ctx* c, DBuf& b, size_t bytes)
 {
     if (bytes <= b.cap) return;
+    if (c->replay) fail(c, UPBP_ERR_INVALID_ARG, "graph capture needs buffers sized by a build and an evaluate");
+    drop_graph(c);  // a reallocation moves a buffer the graph may hold
     if (b.p) {
         ck(c, cudaFreeAsync(b.p, c->stream), "cudaFreeAsync");
         c->bytes -= b.cap;
@@ -243,7 +267,7 @@ void do_build(upbp_ctx* c)
     if (c->media.empty()) fail(c, UPBP_ERR_INVALID_ARG, "upbp_set_media was not called");
     cudaStream_t s = c->stream;
     c->build_launches = 0;
-    ck(c, cudaEventRecord(c->ev[0], s), "event");
+    mark(c, 0, s);
     const upbp_params& P = c->P;
     const int64_t n = c->n_lv;
     // ---- light vertices
@@ -267,7 +291,7 @@ void do_build(upbp_ctx* c)
         c->build_launches += 1;
     }
     // ---- photons = light vertices in media (stable compaction keeps light-vertex order)
-    c->n_ph = 0;
+    if (!c->replay) c->n_ph = 0;
     if (n > 0) {
         ensure(c, c->bbox_partial, sizeof(int32_t) * 8 + sizeof(float) * 6 * 1024);
         int32_t* d_nsel = c->bbox_partial.as<int32_t>();
@@ -284,10 +308,12 @@ void do_build(upbp_ctx* c)
                "DeviceSelect");
             c->build_launches += 2;
         }
-        int32_t h_nsel = 0;
-        ck(c, cudaMemcpyAsync(&h_nsel, d_nsel, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "copy n_sel");
-        ck(c, cudaStreamSynchronize(s), "sync");
-        c->n_ph = h_nsel;
+        if (!c->replay) {  // a replay reuses the count of the build it repeats
+            int32_t h_nsel = 0;
+            ck(c, cudaMemcpyAsync(&h_nsel, d_nsel, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "copy n_sel");
+            ck(c, cudaStreamSynchronize(s), "sync");
+            c->n_ph = h_nsel;
+        }
     }
     const int nph = c->n_ph;
     const int blocks = std::max(1, std::min(1024, (nph + 255) / 256));
@@ -296,7 +322,8 @@ void do_build(upbp_ctx* c)
         float* partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
         launch_bbox_partial(c->lv_pos4.as<float4>(), c->ph_lv.as<int32_t>(), nph, partial, blocks, s);
         launch_bbox_final(partial, blocks, c->bbox_ph.as<float>(), s);
-        ck(c, cudaMemcpyAsync(c->hg_bbox, c->bbox_ph.p, sizeof(float) * 6, cudaMemcpyDeviceToHost, s), "bbox");
+        if (!c->replay)
+            ck(c, cudaMemcpyAsync(c->hg_bbox, c->bbox_ph.p, sizeof(float) * 6, cudaMemcpyDeviceToHost, s), "bbox");
         c->build_launches += 2;
     }
     // ---- PP3D hash grid (HashGrid::Build, Misc/HashGrid.hxx:47-126)
@@ -339,7 +366,8 @@ void do_build(upbp_ctx* c)
                    c->pb_parent_leaf, c->pb_leaf_boxes, c->pb_node_boxes, c->pb_flags, c->pb_n_leaves);
         c->build_launches += 3;
     }
-    // ---- BB1D beams: pieces + LBVH
+    // ---- BB1D beams: pieces + LBVH (a replay keeps the piece count of the build it repeats)
+    const int replay_pieces = c->n_pieces;
     c->n_pieces = 0;
     c->bm_n_leaves = 0;
     const int64_t nb = c->n_beams;
@@ -365,10 +393,13 @@ void do_build(upbp_ctx* c)
         ck(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, b, c->bm_counts.as<int32_t>(), c->bm_offsets.as<int32_t>(),
                                             (int)(nb + 1), s),
            "ExclusiveSum");
-        int32_t total = 0;
-        ck(c, cudaMemcpyAsync(&total, c->bm_offsets.as<int32_t>() + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, s),
-           "copy pieces");
-        ck(c, cudaStreamSynchronize(s), "sync");
+        int32_t total = replay_pieces;
+        if (!c->replay) {
+            ck(c, cudaMemcpyAsync(&total, c->bm_offsets.as<int32_t>() + nb, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                  s),
+               "copy pieces");
+            ck(c, cudaStreamSynchronize(s), "sync");
+        }
         const int np = total;
         c->n_pieces = np;
         ensure(c, c->pc_a, sizeof(float4) * np);
@@ -416,9 +447,10 @@ void do_build(upbp_ctx* c)
             c->build_launches += 1;
         }
     }
-    ck(c, cudaEventRecord(c->ev[1], s), "event");
+    mark(c, 1, s);
     ck(c, cudaGetLastError(), "build launch");
     c->built = true;
+    if (!c->replay) c->evaluated = false;
 }
 
 GatherConsts make_consts(upbp_ctx* c)
@@ -525,6 +557,17 @@ BeamBVH beam_bvh(upbp_ctx* c)
     return B;
 }
 
+BeamSoA beam_soa(upbp_ctx* c)
+{
+    BeamSoA S{};
+    S.thr = c->bm_thr4.as<float4>();
+    S.pdf = c->bm_pdf4.as<float4>();
+    S.link = c->bm_link.as<int2>();
+    S.radius = c->bm_radius.as<float>();
+    S.n = c->n_beams;
+    return S;
+}
+
 // FP64 suffix sums of the camera walks, per segment query and per point query.
 void prepare_cam_sums(upbp_ctx* c, cudaStream_t s, const CamSum** cs_seg, const CamSum** cs_pt)
 {
@@ -553,6 +596,7 @@ gen::GenLaunch generic_launch(upbp_ctx* c, const CamSum* cs_seg, const CamSum* c
     A.L = light_soa(c);
     A.photons = photon_bvh(c);
     A.beams = beam_bvh(c);
+    A.bs = beam_soa(c);
     A.hash = hash_dev(c);
     A.sq = seg_dev(c);
     A.pq = point_dev(c);
@@ -598,6 +642,12 @@ void do_evaluate(upbp_ctx* c)
     ensure(c, c->hash_pb2d, sizeof(uint64_t) * std::max<int64_t>(nq, 1));
     ensure(c, c->hash_bb1d, sizeof(uint64_t) * std::max<int64_t>(nq, 1));
     ensure(c, c->hash_pp3d, sizeof(uint64_t) * std::max<int64_t>(np, 1));
+    const bool bp2d = (c->P.techniques & UPBP_BP2D) && np > 0 && c->n_pieces > 0;
+    if (bp2d) {
+        ensure(c, c->out_bp2d, sizeof(float) * 3 * np);
+        ensure(c, c->cnt_bp2d, sizeof(uint32_t) * np);
+        ensure(c, c->hash_bp2d, sizeof(uint64_t) * np);
+    }
     ensure(c, c->tested, sizeof(unsigned long long) * 4);
     ck(c, cudaMemsetAsync(c->tested.p, 0, sizeof(unsigned long long) * 4, s), "memset");
     const upbp_mis* cam = c->cam_mis.as<upbp_mis>();
@@ -617,15 +667,19 @@ void do_evaluate(upbp_ctx* c)
                                  c->hash_pb2d.as<unsigned long long>(), nullptr, nullptr};
         A.out_bb1d = gen::GenOut{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                                  c->hash_bb1d.as<unsigned long long>(), nullptr, nullptr};
-        for (int k = 2; k <= 4; ++k) ck(c, cudaEventRecord(c->ev[k], s), "event");
+        if (bp2d)
+            A.out_bp2d = gen::GenOut{c->out_bp2d.as<float>(), img, c->cnt_bp2d.as<uint32_t>(),
+                                     c->hash_bp2d.as<unsigned long long>(), nullptr, nullptr};
+        for (int k = 2; k <= 4; ++k) mark(c, k, s);
         gen::launch_generic(A, false, s);
         record_status(c, s);
         c->eval_launches += 3;
-        ck(c, cudaEventRecord(c->ev[5], s), "event");
+        mark(c, 5, s);
         ck(c, cudaGetLastError(), "generic gather launch");
+        c->evaluated = true;
         return;
     }
-    ck(c, cudaEventRecord(c->ev[2], s), "event");
+    mark(c, 2, s);
     if (np > 0) {
         const HashGridDev G = hash_dev(c);
         const PointQueriesDev Q = point_dev(c);
@@ -633,8 +687,14 @@ void do_evaluate(upbp_ctx* c)
                   c->hash_pp3d.as<unsigned long long>(), tested + 2};
         launch_gather_pp3d(K, L, G, Q, cam, cs_pt, O, c->block, mixed, s);
         c->eval_launches += 1;
+        if (bp2d) {
+            const Outputs Ob{c->out_bp2d.as<float>(), img, c->cnt_bp2d.as<uint32_t>(),
+                             c->hash_bp2d.as<unsigned long long>(), tested + 3};
+            launch_gather_bp2d(K, beam_bvh(c), beam_soa(c), Q, Ob, c->block, s);
+            c->eval_launches += 1;
+        }
     }
-    ck(c, cudaEventRecord(c->ev[3], s), "event");
+    mark(c, 3, s);
     const SegQueriesDev Q = seg_dev(c);
     // Order the segment queries along a Morton curve of their midpoints, so that the warps in
     // flight traverse neighbouring parts of the LBVHs (L2 reuse).
@@ -657,14 +717,15 @@ void do_evaluate(upbp_ctx* c)
         order = c->q_order.as<int32_t>();
         c->eval_launches += 5;
     }
-    if (nq > 0) {
+    const bool fused = c->bb1d_kernel >= 3;  // PB2D and BB1D in the one persistent segment kernel
+    if (nq > 0 && !fused) {
         const PhotonBVH B = photon_bvh(c);
         Outputs O{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
                   c->hash_pb2d.as<unsigned long long>(), tested + 0};
         launch_gather_pb2d(K, L, B, Q, cam, cs_seg, O, c->block, mixed, s, order);
         c->eval_launches += 1;
     }
-    ck(c, cudaEventRecord(c->ev[4], s), "event");
+    mark(c, 4, s);
     if (nq > 0) {
         const BeamBVH B = beam_bvh(c);
         BeamSoA S{};
@@ -675,7 +736,19 @@ void do_evaluate(upbp_ctx* c)
         S.n = c->n_beams;
         Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                   c->hash_bb1d.as<unsigned long long>(), tested + 1};
-        if (c->bb1d_kernel >= 1) {
+        if (fused) {
+            if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
+            ensure(c, c->work, sizeof(unsigned int) * 4);
+            ensure(c, c->status, sizeof(int) * 4);
+            ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
+            ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
+            const Outputs Opb{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
+                              c->hash_pb2d.as<unsigned long long>(), tested + 0};
+            const int grid = c->num_sms * segments_warp_blocks_per_sm(mixed, c->bb1d_kernel);
+            launch_segments_warp(K, L, photon_bvh(c), B, S, Q, cam, cs_seg, Opb, O, grid, mixed,
+                                 c->work.as<unsigned int>(), c->status.as<int>(), order, s, c->bb1d_kernel);
+            record_status(c, s);
+        } else if (c->bb1d_kernel >= 1) {
             if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
             ensure(c, c->work, sizeof(unsigned int) * 4);
             ensure(c, c->status, sizeof(int) * 4);
@@ -690,8 +763,9 @@ void do_evaluate(upbp_ctx* c)
         }
         c->eval_launches += 1;
     }
-    ck(c, cudaEventRecord(c->ev[5], s), "event");
+    mark(c, 5, s);
     ck(c, cudaGetLastError(), "gather launch");
+    c->evaluated = true;
 }
 
 template <class F>
@@ -741,6 +815,7 @@ int upbp_ctx_destroy(upbp_ctx* c)
     if (!c) return UPBP_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    drop_graph(c);
     DBuf* all[] = {&c->lv_pos_in, &c->lv_thr_in, &c->lv_dir_in, &c->lv_cont_in, &c->lv_pidx_in, &c->lv_plen_in,
                    &c->lv_med_in, &c->lv_flags_in, &c->lv_mis, &c->path_ends, &c->b_origin, &c->b_dir, &c->b_len,
                    &c->b_thr_in, &c->b_flags_in, &c->b_rsp_in, &c->b_rsr_in, &c->b_rsf_in, &c->b_lpw_in,
@@ -759,7 +834,7 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->image, &c->cnt_pb2d, &c->cnt_bb1d, &c->cnt_pp3d,
                    &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested, &c->light_sums, &c->cam_sums_seg,
                    &c->cam_sums_pt, &c->work, &c->status, &c->pc_pay, &c->q_keys, &c->q_keys_sorted, &c->q_iota,
-                   &c->q_order, &c->grad_img, &c->grad_acc};
+                   &c->q_order, &c->grad_img, &c->grad_acc, &c->out_bp2d, &c->cnt_bp2d, &c->hash_bp2d};
     for (DBuf* b : all) free_buf(*b);
     if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)
@@ -774,6 +849,7 @@ const char* upbp_last_error(const upbp_ctx* c) { return c ? c->err.c_str() : "nu
 int upbp_set_mode(upbp_ctx* c, int mode)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (mode != UPBP_MODE_PLAIN && mode != UPBP_MODE_MIXED && mode != UPBP_MODE_FP64)
             fail(c, UPBP_ERR_INVALID_ARG, "unknown mode %d", mode);
         if (mode != c->mode) c->built = false;
@@ -786,6 +862,7 @@ static bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (
 int upbp_set_tuning(upbp_ctx* c, const upbp_tuning* tu)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (!tu) fail(c, UPBP_ERR_INVALID_ARG, "tuning is NULL");
         if (!pow2_in(tu->pb2d_leaf, 1, 64) || !pow2_in(tu->bb1d_leaf, 1, 64))
             fail(c, UPBP_ERR_INVALID_ARG, "leaf sizes must be powers of two in [1, 64]");
@@ -793,7 +870,7 @@ int upbp_set_tuning(upbp_ctx* c, const upbp_tuning* tu)
             fail(c, UPBP_ERR_INVALID_ARG, "block_threads must be a multiple of 32 in [32, 256]");
         if (!(tu->beam_piece_radii >= 1.f && tu->beam_piece_radii <= 1024.f))
             fail(c, UPBP_ERR_INVALID_ARG, "beam_piece_radii must be in [1, 1024]");
-        if (tu->bb1d_kernel < 0 || tu->bb1d_kernel > 2) fail(c, UPBP_ERR_INVALID_ARG, "bb1d_kernel must be 0, 1 or 2");
+        if (tu->bb1d_kernel < 0 || tu->bb1d_kernel > 4) fail(c, UPBP_ERR_INVALID_ARG, "bb1d_kernel must be in [0, 4]");
         c->pb2d_leaf = tu->pb2d_leaf;
         c->bb1d_leaf = tu->bb1d_leaf;
         c->block = tu->block_threads;
@@ -816,12 +893,13 @@ int upbp_get_tuning(const upbp_ctx* c, upbp_tuning* tu)
 
 int upbp_set_stream(upbp_ctx* c, void* stream)
 {
-    return guarded(c, [&] { c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream; });
+    return guarded(c, [&] { drop_graph(c); c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream; });
 }
 
 int upbp_set_media(upbp_ctx* c, const upbp_medium* media, int32_t n)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (!media || n <= 0 || n > UPBP_MAX_MEDIA) fail(c, UPBP_ERR_INVALID_ARG, "n_media must be in [1, %d]", UPBP_MAX_MEDIA);
         c->media.clear();
         c->media_raw.assign(media, media + n);
@@ -832,6 +910,7 @@ int upbp_set_media(upbp_ctx* c, const upbp_medium* media, int32_t n)
 int upbp_set_params(upbp_ctx* c, const upbp_params* p)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (!p) fail(c, UPBP_ERR_INVALID_ARG, "params is NULL");
         if (p->max_path_length + 1 > UPBP_MAX_CAM) fail(c, UPBP_ERR_INVALID_ARG, "max_path_length too large");
         if (!(p->radius_pp3d > 0) || !(p->radius_pb2d > 0) || !(p->radius_bb1d > 0))
@@ -849,6 +928,7 @@ int upbp_set_params(upbp_ctx* c, const upbp_params* p)
 int upbp_set_light_vertices(upbp_ctx* c, const upbp_light_vertices* lv)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (!lv || lv->n < 0 || lv->n > (int64_t)INT32_MAX || lv->n_paths < 0)
             fail(c, UPBP_ERR_INVALID_ARG, "bad light vertex count");
         const int64_t n = lv->n;
@@ -871,6 +951,7 @@ int upbp_set_light_vertices(upbp_ctx* c, const upbp_light_vertices* lv)
 int upbp_set_beams(upbp_ctx* c, const upbp_beams* b)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (!b || b->n < 0 || b->n > (int64_t)(1 << 28)) fail(c, UPBP_ERR_INVALID_ARG, "bad beam count");
         const int64_t n = b->n;
         upload(c, c->b_origin, b->origin, 3 * n, "beam origin");
@@ -897,6 +978,7 @@ int upbp_build(upbp_ctx* c)
 int upbp_set_camera_mis(upbp_ctx* c, const upbp_mis* rec, int64_t n)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (n < 0) fail(c, UPBP_ERR_INVALID_ARG, "negative camera record count");
         upload(c, c->cam_mis, rec, n, "camera mis");
         c->n_cam = n;
@@ -906,6 +988,7 @@ int upbp_set_camera_mis(upbp_ctx* c, const upbp_mis* rec, int64_t n)
 int upbp_set_segment_queries(upbp_ctx* c, const upbp_segment_queries* q)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (!q || q->n < 0 || q->n_segments < 0) fail(c, UPBP_ERR_INVALID_ARG, "bad segment query counts");
         const int64_t n = q->n, s = q->n_segments;
         upload(c, c->sq_origin, q->origin, 3 * n, "origin");
@@ -932,6 +1015,7 @@ int upbp_set_segment_queries(upbp_ctx* c, const upbp_segment_queries* q)
 int upbp_set_point_queries(upbp_ctx* c, const upbp_point_queries* q)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         if (!q || q->n < 0) fail(c, UPBP_ERR_INVALID_ARG, "bad point query count");
         const int64_t n = q->n;
         upload(c, c->pq_pos, q->position, 3 * n, "position");
@@ -948,6 +1032,49 @@ int upbp_set_point_queries(upbp_ctx* c, const upbp_point_queries* q)
 int upbp_evaluate(upbp_ctx* c)
 {
     return guarded(c, [&] { do_evaluate(c); });
+}
+
+int upbp_capture_graph(upbp_ctx* c)
+{
+    return guarded(c, [&] {
+        if (!c->built || !c->evaluated)
+            fail(c, UPBP_ERR_NOT_BUILT, "capture needs upbp_build and upbp_evaluate of the current inputs first");
+        drop_graph(c);
+        cudaStream_t s = c->stream;
+        if (s == nullptr) fail(c, UPBP_ERR_INVALID_ARG, "graph capture needs a non-default stream");
+        const size_t npix = (size_t)std::max(0, c->P.image_width) * (size_t)std::max(0, c->P.image_height);
+        ck(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        c->replay = true;
+        cudaGraph_t g = nullptr;
+        try {
+            if (npix) ck(c, cudaMemsetAsync(c->image.p, 0, sizeof(float) * 3 * npix, s), "memset image");
+            do_build(c);
+            do_evaluate(c);
+        } catch (...) {
+            c->replay = false;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        c->replay = false;
+        ck(c, cudaStreamEndCapture(s, &g), "cudaStreamEndCapture");
+        cudaGraphExec_t e = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&e, g, 0);
+        cudaGraphDestroy(g);
+        ck(c, ie, "cudaGraphInstantiate");
+        c->graph_exec = e;
+        c->graph_status = c->status_pending;
+    });
+}
+
+int upbp_launch_graph(upbp_ctx* c)
+{
+    return guarded(c, [&] {
+        if (!c->graph_exec) fail(c, UPBP_ERR_NOT_BUILT, "no graph: inputs changed or upbp_capture_graph not called");
+        ck(c, cudaGraphLaunch(c->graph_exec, c->stream), "cudaGraphLaunch");
+        c->status_pending = c->graph_status;
+    });
 }
 
 int upbp_read_segment_results(upbp_ctx* c, float* pb2d, float* bb1d)
@@ -1013,7 +1140,7 @@ int upbp_adjoint(upbp_ctx* c, const float* grad_image, int32_t medium, double* g
         prepare_cam_sums(c, s, &cs_seg, &cs_pt);
         gen::GenLaunch A = generic_launch(c, cs_seg, cs_pt, medium);
         const gen::GenOut O{nullptr, nullptr, nullptr, nullptr, c->grad_img.as<float>(), c->grad_acc.as<double>()};
-        A.out_pp3d = A.out_pb2d = A.out_bb1d = O;
+        A.out_pp3d = A.out_pb2d = A.out_bb1d = A.out_bp2d = O;
         gen::launch_generic(A, true, s);
         c->eval_launches += 3;
         record_status(c, s);
@@ -1023,6 +1150,24 @@ int upbp_adjoint(upbp_ctx* c, const float* grad_image, int32_t medium, double* g
         ck(c, cudaStreamSynchronize(s), "sync");
         check_status(c);
         for (int i = 0; i < 7; ++i) grad[i] = h[i];
+    });
+}
+
+int upbp_read_bp2d_results(upbp_ctx* c, float* rgb, uint32_t* count, uint64_t* hash)
+{
+    return guarded(c, [&] {
+        const size_t np = (size_t)c->n_pq;
+        if (np == 0) return;
+        if (!(c->P.techniques & UPBP_BP2D) || !c->out_bp2d.p || c->out_bp2d.cap < sizeof(float) * 3 * np)
+            fail(c, UPBP_ERR_NOT_BUILT, "no B-P2D results: UPBP_BP2D is not in the techniques of the last evaluate");
+        auto rd = [&](void* dst, const DBuf& src, size_t bytes) {
+            if (dst) ck(c, cudaMemcpyAsync(dst, src.p, bytes, cudaMemcpyDefault, c->stream), "read bp2d");
+        };
+        rd(rgb, c->out_bp2d, sizeof(float) * 3 * np);
+        rd(count, c->cnt_bp2d, sizeof(uint32_t) * np);
+        rd(hash, c->hash_bp2d, sizeof(uint64_t) * np);
+        ck(c, cudaStreamSynchronize(c->stream), "sync");
+        check_status(c);
     });
 }
 
@@ -1053,6 +1198,10 @@ int upbp_clear_image(upbp_ctx* c)
         const size_t npix = (size_t)std::max(0, c->P.image_width) * (size_t)std::max(0, c->P.image_height);
         ensure(c, c->image, sizeof(float) * 3 * std::max<size_t>(npix, 1));
         ck(c, cudaMemsetAsync(c->image.p, 0, sizeof(float) * 3 * npix, c->stream), "memset image");
+        // and the per-query results of the last evaluate (the next evaluate overwrites them)
+        for (DBuf* b : {&c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->out_bp2d, &c->cnt_pb2d, &c->cnt_bb1d,
+                        &c->cnt_pp3d, &c->cnt_bp2d, &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->hash_bp2d})
+            if (b->p) ck(c, cudaMemsetAsync(b->p, 0, b->cap, c->stream), "memset results");
     });
 }
 
@@ -1093,6 +1242,7 @@ int upbp_last_timings(const upbp_ctx* cc, float* build_ms, float* pp3d_ms, float
 int upbp_destroy_structures(upbp_ctx* c)
 {
     return guarded(c, [&] {
+        drop_graph(c);
         c->built = false;
         c->n_ph = 0;
         c->pb_n_leaves = 0;

@@ -191,8 +191,9 @@ __device__ __forceinline__ double owner_param_f64(V3 O1, V3 d1, float dminf, flo
     return u;
 }
 
-__device__ __forceinline__ bool piece_owns(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len, float t_lo,
-                                           float t_hi, float t1, float t2)
+// 1: this piece owns the candidate, 0: it does not, -1: undecided in FP32 (use piece_owns_f64).
+__device__ __forceinline__ int piece_owns_fast(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
+                                               float t_lo, float t_hi, float t1, float t2)
 {
     const float c = fabsf(d1.x * d2.x + d1.y * d2.y + d1.z * d2.z);
     if (c * (1.f - c * c) > 0.04f) {
@@ -200,12 +201,25 @@ __device__ __forceinline__ bool piece_owns(V3 O1, V3 d1, float dmin, float dmax,
                                   fmaxf(fmaxf(fabsf(O2.y), fabsf(O2.z)), fmaxf(fmaxf(len, fabsf(dmax)), 1.f)));
         const float m = 1e-4f * scale;
         if (t1 > dmin + m && t1 < dmax - m && t2 > m && t2 < len - m) {
-            if (t2 >= t_lo + m && t2 < t_hi - m) return true;
-            if (t2 < t_lo - m || t2 >= t_hi + m) return false;
+            if (t2 >= t_lo + m && t2 < t_hi - m) return 1;
+            if (t2 < t_lo - m || t2 >= t_hi + m) return 0;
         }
     }
+    return -1;
+}
+
+__device__ __forceinline__ bool piece_owns_f64(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
+                                               float t_lo, float t_hi)
+{
     const double u = owner_param_f64(O1, d1, dmin, dmax, O2, d2, len);
     return u >= (double)t_lo && (u < (double)t_hi || t_hi >= len);
+}
+
+__device__ __forceinline__ bool piece_owns(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len, float t_lo,
+                                           float t_hi, float t1, float t2)
+{
+    const int f = piece_owns_fast(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi, t1, t2);
+    return f >= 0 ? f == 1 : piece_owns_f64(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi);
 }
 
 // ------------------------------------------------------------------ MIS walks

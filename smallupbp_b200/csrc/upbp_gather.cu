@@ -511,11 +511,162 @@ struct CandQueue {
     float4 geo[kCandQueue];  // dist, sin(theta), t1 (query), t2 (beam)
 };
 
-// BB1D, warp per query, persistent: warps draw query indices from an atomic counter.  The lanes
-// test 32 beam pieces at a time; the accepted ones go to the warp's candidate queue, and whenever
-// it holds 32 they are evaluated one per lane, so the contribution (transmittance, phase
-// function, MIS weight) runs with every lane busy although only a fraction of the tested pieces
-// is accepted.
+// Per-warp scratch of the warp-cooperative gathers (shared memory).
+struct WarpScratch {
+    int* stack;
+    int* leaves;
+    CandQueue* cq;
+    int lane;
+    unsigned lt;  // lanes below this one
+};
+
+// BB1D of one query by one warp: the lanes test 32 beam pieces at a time; the accepted ones go to
+// the warp's candidate queue, and whenever it holds 32 they are evaluated one per lane, so the
+// contribution (transmittance, phase function, MIS weight) runs with every lane busy although
+// only a fraction of the tested pieces is accepted.  Returns this lane's share of the result.
+template <bool kMixed>
+__device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMedium* media, const LightSoA& Lv,
+                                               const BeamBVH& B, const BeamSoA& Bs, const SegQueriesDev& Q,
+                                               int64_t q, SegCtx& s, V3 inv, const WarpScratch& ws,
+                                               unsigned long long& cnt, unsigned long long& h,
+                                               unsigned long long& tested, int* status)
+{
+    const int lane = ws.lane;
+    const unsigned lt = ws.lt;
+    CandQueue& cq = *ws.cq;
+    const int leaf_shift = __ffs(B.leaf) - 1;
+    return segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
+        Rgb part = rgb(0.f);
+        const int mid = (int)(&m - media);
+        int qn = 0;  // entries in the candidate queue (warp-uniform)
+        // evaluates queue entry e (one lane, one accepted candidate); an entry stored as ~piece
+        // still needs the FP64 ownership decision, taken here with all lanes busy
+        auto eval = [&](int e) {
+            int i = cq.piece[e];
+            const bool undecided = i < 0;
+            if (undecided) i = ~i;
+            const float4 g = cq.geo[e];
+            const float4 pa = __ldg(&B.pa[i]);
+            const float4 pb = __ldg(&B.pb[i]);
+            const float4 pc = __ldg(&B.pc[i]);
+            if (undecided &&
+                !piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pb.w, pc.x))
+                return;
+            ++cnt;
+            h += mix64((unsigned long long)__float_as_int(pc.z));
+            if (kMixed) {
+                const PiecePayload py = B.pay[i];
+                part = part + bb1d_contrib_packed(K, m, s, py, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), g.x, g.y,
+                                                  g.z, g.w);
+            } else {
+                const int beam = __float_as_int(pc.z);
+                part = part + bb1d_contrib<false>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
+                                                  __ldg(&Bs.radius[beam]), g.x, g.y, g.z, g.w);
+            }
+        };
+        const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps, s.dmax + K.eps,
+                                      ws.stack, ws.leaves, lane, [&](int i) {
+            bool hit = false;
+            int entry = 0;
+            float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f;
+            if (i >= 0) {
+                const float4 pc = __ldg(&B.pc[i]);
+                if (__float_as_int(pc.w) == mid) {  // mMedium == medium (PhotonBeam.hxx:390)
+                    const float4 pa = __ldg(&B.pa[i]);
+                    const float4 pb = __ldg(&B.pb[i]);
+                    ++tested;
+                    if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f,
+                                       pa.w, pc.y, &dist, &sinT, &t1, &t2)) {
+                        const float radius = kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[__float_as_int(pc.z)]);
+                        if (!(radius < dist)) {  // PhotonBeam.hxx:411-413
+                            const int own = piece_owns_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
+                                                            v3(pb.x, pb.y, pb.z), pa.w, pb.w, pc.x, t1, t2);
+                            hit = own != 0;
+                            entry = own > 0 ? i : ~i;
+                        }
+                    }
+                }
+            }
+            const unsigned vote = __ballot_sync(kFull, hit);
+            if (vote == 0u) return;
+            if (hit) {
+                const int pos = qn + __popc(vote & lt);
+                cq.piece[pos] = entry;
+                cq.geo[pos] = make_float4(dist, sinT, t1, t2);
+            }
+            qn += __popc(vote);
+            __syncwarp();
+            if (qn >= 32) {  // the newest 32 entries, one per lane
+                eval(qn - 32 + lane);
+                qn -= 32;
+                __syncwarp();
+            }
+        });
+        if (lane < qn) eval(lane);
+        __syncwarp();
+        if (!ok && lane == 0) atomicOr(status, 1);
+        return part;
+    });
+}
+
+// PB2D of one query by one warp over the photon LBVH, with the same candidate queue.
+template <bool kMixed>
+__device__ __forceinline__ Rgb pb2d_query_warp(const GatherConsts& K, const DMedium* media, const LightSoA& Lv,
+                                               const PhotonBVH& P, const SegQueriesDev& Q, int64_t q, SegCtx& s,
+                                               V3 inv, const WarpScratch& ws, unsigned long long& cnt,
+                                               unsigned long long& h, unsigned long long& tested, int* status)
+{
+    const int lane = ws.lane;
+    const unsigned lt = ws.lt;
+    CandQueue& cq = *ws.cq;
+    const int leaf_shift = __ffs(P.leaf) - 1;
+    const float r2 = K.P.radius_pb2d * K.P.radius_pb2d;
+    return segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
+        Rgb part = rgb(0.f);
+        int qn = 0;
+        auto eval = [&](int e) {
+            const float4 g = cq.geo[e];
+            part = part + pb2d_contrib<kMixed>(K, m, Lv, s, cq.piece[e], g.x, g.y);
+        };
+        const bool ok = warp_traverse(P.nodes, P.n_leaves, P.n, leaf_shift, s.o, inv, s.dmin - K.eps, s.dmax + K.eps,
+                                      ws.stack, ws.leaves, lane, [&](int i) {
+            bool hit = false;
+            float t = 0.f, d2 = 0.f;
+            int lv = 0;
+            if (i >= 0) {
+                const float4 p = __ldg(&P.pos[i]);
+                ++tested;
+                if (test_bre(s.o, s.d, s.dmin, s.dmax, v3(p.x, p.y, p.z), r2, &t, &d2)) {
+                    lv = __float_as_int(p.w);
+                    hit = true;
+                    ++cnt;
+                    h += mix64((unsigned long long)lv);
+                }
+            }
+            const unsigned vote = __ballot_sync(kFull, hit);
+            if (vote == 0u) return;
+            if (hit) {
+                const int pos = qn + __popc(vote & lt);
+                cq.piece[pos] = lv;
+                cq.geo[pos] = make_float4(t, d2, 0.f, 0.f);
+            }
+            qn += __popc(vote);
+            __syncwarp();
+            if (qn >= 32) {
+                eval(qn - 32 + lane);
+                qn -= 32;
+                __syncwarp();
+            }
+        });
+        if (lane < qn) eval(lane);
+        __syncwarp();
+        if (!ok && lane == 0) atomicOr(status, 1);
+        return part;
+    });
+}
+
+// BB1D, warp per query, persistent: warps draw query indices (in Morton order of the query
+// midpoints) from an atomic counter.
 template <bool kMixed, int kWarps, int kMinBlocks>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bb1d_warp(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                           const BeamBVH B, const BeamSoA Bs, const SegQueriesDev Q,
@@ -532,11 +683,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bb1d_warp(const __g
     __shared__ CamSum s_cs[kWarps];
     stage_media(K, media);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    int* stack = s_stack[warp];
-    int* leaves = s_leaves[warp];
-    CandQueue& cq = s_queue[warp];
-    const int leaf_shift = __ffs(B.leaf) - 1;
+    const WarpScratch ws{s_stack[warp], s_leaves[warp], &s_queue[warp], lane, (1u << lane) - 1u};
     for (;;) {
         unsigned qq = 0;
         if (lane == 0) qq = atomicAdd(work, 1u);
@@ -550,71 +697,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bb1d_warp(const __g
             init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &s_e[warp], &s_cs[warp], lane == 0);
             __syncwarp();
             const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
-            acc = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
-                Rgb part = rgb(0.f);
-                const int mid = (int)(&m - media);
-                int qn = 0;  // entries in the candidate queue (warp-uniform)
-                // evaluates queue entry e (one lane, one accepted candidate)
-                auto eval = [&](int e) {
-                    const int i = cq.piece[e];
-                    const float4 g = cq.geo[e];
-                    const float4 pa = __ldg(&B.pa[i]);
-                    const float4 pb = __ldg(&B.pb[i]);
-                    if (kMixed) {
-                        const PiecePayload py = B.pay[i];
-                        part = part + bb1d_contrib_packed(K, m, s, py, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                                          g.x, g.y, g.z, g.w);
-                    } else {
-                        const int beam = __float_as_int(__ldg(&B.pc[i]).z);
-                        part = part + bb1d_contrib<false>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z),
-                                                          v3(pb.x, pb.y, pb.z), __ldg(&Bs.radius[beam]), g.x, g.y,
-                                                          g.z, g.w);
-                    }
-                };
-                const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps,
-                                              s.dmax + K.eps, stack, leaves, lane, [&](int i) {
-                    bool hit = false;
-                    float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f;
-                    if (i >= 0) {
-                        const float4 pc = __ldg(&B.pc[i]);
-                        if (__float_as_int(pc.w) == mid) {  // mMedium == medium (PhotonBeam.hxx:390)
-                            const float4 pa = __ldg(&B.pa[i]);
-                            const float4 pb = __ldg(&B.pb[i]);
-                            ++tested;
-                            if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
-                                               v3(pb.x, pb.y, pb.z), 0.f, pa.w, pc.y, &dist, &sinT, &t1, &t2) &&
-                                piece_owns(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w,
-                                           pb.w, pc.x, t1, t2)) {
-                                const int beam = __float_as_int(pc.z);
-                                const float radius = kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[beam]);
-                                if (!(radius < dist)) {  // PhotonBeam.hxx:411-413
-                                    hit = true;
-                                    ++cnt;
-                                    h += mix64((unsigned long long)beam);
-                                }
-                            }
-                        }
-                    }
-                    const unsigned vote = __ballot_sync(kFull, hit);
-                    if (vote == 0u) return;
-                    if (hit) {
-                        const int pos = qn + __popc(vote & lt);
-                        cq.piece[pos] = i;
-                        cq.geo[pos] = make_float4(dist, sinT, t1, t2);
-                    }
-                    qn += __popc(vote);
-                    __syncwarp();
-                    if (qn >= 32) {  // the newest 32 entries, one per lane
-                        eval(qn - 32 + lane);
-                        qn -= 32;
-                        __syncwarp();
-                    }
-                });
-                if (lane < qn) eval(lane);
-                __syncwarp();
-                if (!ok && lane == 0) atomicOr(status, 1);
-                return part;
-            });
+            acc = bb1d_query_warp<kMixed>(K, media, Lv, B, Bs, Q, q, s, inv, ws, cnt, h, tested, status);
         }
         const float r = warp_sum(acc.r), g = warp_sum(acc.g), b = warp_sum(acc.b);
         cnt = warp_sum_u64(cnt);
@@ -629,6 +712,70 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bb1d_warp(const __g
             const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
             splat(O.image, Q.pixel[q], thr * K.P.norm_bb1d * Rgb{r, g, b});
             if (O.tested) atomicAdd(O.tested, tested);
+        }
+    }
+}
+
+// All camera segments of an iteration in one persistent work-queue kernel: a warp takes the next
+// query (Morton order) and evaluates both segment estimators for it, PB2D over the photon LBVH
+// and BB1D over the beam-piece LBVH, with one camera context and one splat per query.
+template <bool kMixed, int kWarps, int kMinBlocks>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_segments_warp(
+    const __grid_constant__ GatherConsts K, const LightSoA Lv, const PhotonBVH P, const BeamBVH B, const BeamSoA Bs,
+    const SegQueriesDev Q, const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs, const Outputs Opb,
+    const Outputs Obb, unsigned int* __restrict__ work, int* __restrict__ status, const int32_t* __restrict__ order)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    __shared__ int s_stack[kWarps][kWarpStack];
+    __shared__ int s_leaves[kWarps][kWarpLeaves];
+    __shared__ CandQueue s_queue[kWarps];
+    __shared__ upbp_mis s_e[kWarps];
+    __shared__ CamSum s_cs[kWarps];
+    stage_media(K, media);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const WarpScratch ws{s_stack[warp], s_leaves[warp], &s_queue[warp], lane, (1u << lane) - 1u};
+    for (;;) {
+        unsigned qq = 0;
+        if (lane == 0) qq = atomicAdd(work, 1u);
+        const int64_t item = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (item >= Q.n) break;
+        const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
+        const uint32_t qf = Q.flags[q];
+        const bool do_pb = (qf & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && P.n > 0;
+        const bool do_bb = (qf & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D) && B.n > 0;
+        Rgb apb = rgb(0.f), abb = rgb(0.f);
+        unsigned long long cpb = 0, hpb = 0, tpb = 0, cbb = 0, hbb = 0, tbb = 0;
+        if (do_pb || do_bb) {
+            SegCtx s;
+            init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &s_e[warp], &s_cs[warp], lane == 0);
+            __syncwarp();
+            const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
+            if (do_pb) apb = pb2d_query_warp<kMixed>(K, media, Lv, P, Q, q, s, inv, ws, cpb, hpb, tpb, status);
+            if (do_bb) abb = bb1d_query_warp<kMixed>(K, media, Lv, B, Bs, Q, q, s, inv, ws, cbb, hbb, tbb, status);
+        }
+        const Rgb vpb{warp_sum(apb.r), warp_sum(apb.g), warp_sum(apb.b)};
+        const Rgb vbb{warp_sum(abb.r), warp_sum(abb.g), warp_sum(abb.b)};
+        cpb = warp_sum_u64(cpb);
+        hpb = warp_sum_u64(hpb);
+        tpb = warp_sum_u64(tpb);
+        cbb = warp_sum_u64(cbb);
+        hbb = warp_sum_u64(hbb);
+        tbb = warp_sum_u64(tbb);
+        if (lane == 0) {
+            Opb.rgb[3 * q + 0] = vpb.r;
+            Opb.rgb[3 * q + 1] = vpb.g;
+            Opb.rgb[3 * q + 2] = vpb.b;
+            Obb.rgb[3 * q + 0] = vbb.r;
+            Obb.rgb[3 * q + 1] = vbb.g;
+            Obb.rgb[3 * q + 2] = vbb.b;
+            if (Opb.count) Opb.count[q] = (uint32_t)cpb;
+            if (Opb.hash) Opb.hash[q] = hpb;
+            if (Obb.count) Obb.count[q] = (uint32_t)cbb;
+            if (Obb.hash) Obb.hash[q] = hbb;
+            const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+            splat(Obb.image, Q.pixel[q], thr * (vpb * K.P.norm_pb2d + vbb * K.P.norm_bb1d));
+            if (Opb.tested) atomicAdd(Opb.tested, tpb);
+            if (Obb.tested) atomicAdd(Obb.tested, tbb);
         }
     }
 }
@@ -735,7 +882,76 @@ __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ Gat
     if (O.tested) atomicAdd(O.tested, tested);
 }
 
+// B-P2D (extension; the reference has no beam x point estimator): photon beams queried at the
+// camera medium vertices with a 2-D kernel, MIS weight 1.  Candidate: testIntersectionBre with
+// the beam as the ray and the query point as the photon; the piece containing the foot point
+// takes it.  Value: beam throughput x transmittance to the foot point (divided by the free-flight
+// pdf for SHORT beams) x sigma_s x HG phase x (1 - d^2/r^2) / (pi r^2 / 2).
+__global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ GatherConsts K, const BeamBVH B,
+                                                     const BeamSoA Bs, const PointQueriesDev Q, const Outputs O)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    stage_media(K, media);
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= Q.n) return;
+    uint32_t cnt = 0;
+    unsigned long long h = 0, tested = 0;
+    Rgb res = rgb(0.f);
+    const V3 x = v3(Q.position[3 * q], Q.position[3 * q + 1], Q.position[3 * q + 2]);
+    const int mid = Q.medium_id[q];
+    const DMedium& m = media[mid];
+    if ((K.P.techniques & UPBP_BP2D) && m.has_scat && B.n > 0) {
+        const V3 cfix = v3(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
+        const float r = K.P.radius_bb1d, r2 = r * r;
+        const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
+        // a zero-length ray at x: the slab test becomes point-in-box
+        traverse(B.nodes, B.n_leaves, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, [&](int leaf) {
+            const int e = min(B.n, (leaf + 1) * B.leaf);
+            for (int i = leaf * B.leaf; i < e; ++i) {
+                const float4 pc = __ldg(&B.pc[i]);
+                if (__float_as_int(pc.w) != mid) continue;
+                const float4 pa = __ldg(&B.pa[i]);
+                const float4 pb = __ldg(&B.pb[i]);
+                ++tested;
+                float t, d2;
+                if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, r2, &t, &d2)) continue;
+                if (!(t >= pb.w && t < pc.x)) continue;  // the piece containing the foot point
+                const int beam = __float_as_int(pc.z);
+                ++cnt;
+                h += mix64((unsigned long long)beam);
+                const float4 bthr = __ldg(&Bs.thr[beam]);
+                Rgb att = eval_att(m, t);
+                const float pfd = comp(att, m.min_idx);
+                if ((uint32_t)__float_as_int(bthr.w) & UPBP_SHORT_BEAM) att = att / pfd;
+                if (!rgb_positive(att)) continue;
+                float sinT;
+                const float phase = hg_pdf(cfix, neg3(v3(pb.x, pb.y, pb.z)), m.g, &sinT);
+                if (phase <= 0.f) continue;
+                const float kernel = (1.f - d2 / r2) / (r2 * UPBP_PI_F * 0.5f);
+                if (!is_pos(kernel)) continue;
+                res = res + Rgb{bthr.x, bthr.y, bthr.z} * att * ss * (phase * kernel);
+            }
+        });
+    }
+    O.rgb[3 * q + 0] = res.r;
+    O.rgb[3 * q + 1] = res.g;
+    O.rgb[3 * q + 2] = res.b;
+    if (O.count) O.count[q] = cnt;
+    if (O.hash) O.hash[q] = h;
+    const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+    splat(O.image, Q.pixel[q], thr * K.P.norm_bb1d * res);
+    if (O.tested) atomicAdd(O.tested, tested);
+}
+
 }  // namespace
+
+void launch_gather_bp2d(const GatherConsts& K, const BeamBVH& B, const BeamSoA& S, const PointQueriesDev& Q,
+                        const Outputs& O, int block, cudaStream_t stream)
+{
+    if (Q.n <= 0) return;
+    const int grid = (int)((Q.n + block - 1) / block);
+    k_gather_bp2d<<<grid, block, 0, stream>>>(K, B, S, Q, O);
+}
 
 void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,
                         const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
@@ -755,6 +971,40 @@ void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH&
     const int grid = (int)((Q.n + block - 1) / block);
     if (mixed) k_gather_bb1d<true><<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, cs, O);
     else k_gather_bb1d<false><<<grid, block, 0, stream>>>(K, L, B, S, Q, cam, cs, O);
+}
+
+// The fused segment kernel at 5 (variant 3) or 6 (variant 4) blocks of 4 warps per SM.
+int segments_warp_blocks_per_sm(bool mixed, int variant)
+{
+    int nb = 0;
+    const bool six = variant == 4;
+    if (mixed) {
+        if (six) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_segments_warp<true, 4, 6>, 128, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_segments_warp<true, 4, 5>, 128, 0);
+    } else {
+        if (six) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_segments_warp<false, 4, 6>, 128, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_segments_warp<false, 4, 5>, 128, 0);
+    }
+    return nb > 0 ? nb : 1;
+}
+
+void launch_segments_warp(const GatherConsts& K, const LightSoA& L, const PhotonBVH& P, const BeamBVH& B,
+                          const BeamSoA& S, const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs,
+                          const Outputs& Opb, const Outputs& Obb, int grid, bool mixed, unsigned int* work,
+                          int* status, const int32_t* order, cudaStream_t stream, int variant)
+{
+    if (Q.n <= 0) return;
+    const bool six = variant == 4;
+#define UPBP_SEG_LAUNCH(M, N) \
+    k_segments_warp<M, 4, N><<<grid, 128, 0, stream>>>(K, L, P, B, S, Q, cam, cs, Opb, Obb, work, status, order)
+    if (mixed) {
+        if (six) UPBP_SEG_LAUNCH(true, 6);
+        else UPBP_SEG_LAUNCH(true, 5);
+    } else {
+        if (six) UPBP_SEG_LAUNCH(false, 6);
+        else UPBP_SEG_LAUNCH(false, 5);
+    }
+#undef UPBP_SEG_LAUNCH
 }
 
 // Two instantiations of the warp kernel differ only in the occupancy the compiler is asked to

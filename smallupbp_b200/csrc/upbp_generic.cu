@@ -553,6 +553,64 @@ __global__ void __launch_bounds__(128) k_gen_pp3d(const __grid_constant__ Gather
                     cnt, h);
 }
 
+// B-P2D (extension, standalone, MIS weight 1) in T: the foot point re-solved in FP64.
+template <class T>
+__global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ GatherConsts K,
+                                                  const __grid_constant__ GenConsts G, const BeamBVH B,
+                                                  const BeamSoA Bs, const PointQueriesDev Q, const GenOut O)
+{
+    __shared__ MedT<T> media[UPBP_MAX_MEDIA];
+    stage_media_t<T>(G, media);
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool valid = q < Q.n;
+    uint32_t cnt = 0;
+    unsigned long long h = 0;
+    RgbT<T> res = rgb_zero<T>();
+    if (valid) {
+        const V3 x = v3(Q.position[3 * q], Q.position[3 * q + 1], Q.position[3 * q + 2]);
+        const int mid = Q.medium_id[q];
+        const MedT<T>& m = media[mid];
+        if ((K.P.techniques & UPBP_BP2D) && m.has_scat && B.n > 0) {
+            const V3d cfix = v3d(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
+            const float r = K.P.radius_bb1d, r2 = r * r;
+            const double r2d = r2;
+            traverse(B.nodes, B.n_leaves, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, [&](int leaf) {
+                const int e = min(B.n, (leaf + 1) * B.leaf);
+                for (int i = leaf * B.leaf; i < e; ++i) {
+                    const float4 pc = __ldg(&B.pc[i]);
+                    if (__float_as_int(pc.w) != mid) continue;
+                    const float4 pa = __ldg(&B.pa[i]);
+                    const float4 pb = __ldg(&B.pb[i]);
+                    float tf, d2f;
+                    if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, r2, &tf, &d2f)) continue;
+                    if (!(tf >= pb.w && tf < pc.x)) continue;
+                    const int beam = __float_as_int(pc.z);
+                    ++cnt;
+                    h += mix64((unsigned long long)beam);
+                    const V3d o = v3d(pa.x, pa.y, pa.z), d = v3d(pb.x, pb.y, pb.z), p = v3d(x);
+                    const double t = dot(sub(p, o), d);
+                    const V3d qv = V3d{o.x + d.x * t - p.x, o.y + d.y * t - p.y, o.z + d.z * t - p.z};
+                    const double d2 = dot(qv, qv);
+                    const float4 bthr = __ldg(&Bs.thr[beam]);
+                    RgbT<T> att = eval_att(m, t);
+                    const T pfd = comp(att, m.min_idx);
+                    if ((uint32_t)__float_as_int(bthr.w) & UPBP_SHORT_BEAM) att = att / pfd;
+                    if (!positive(att)) continue;
+                    double sinT;
+                    const T phase = hg_pdf(cfix, neg(d), m.g, &sinT);
+                    if (!(val(phase) > 0.0)) continue;
+                    const double kernel = (1.0 - d2 / r2d) / (r2d * 3.14159265358979323846 * 0.5);
+                    if (!(kernel > 1e-20)) continue;
+                    res = res + RgbT<T>{att.r * (double)bthr.x, att.g * (double)bthr.y, att.b * (double)bthr.z} *
+                                    RgbT<T>{m.ss[0], m.ss[1], m.ss[2]} * (phase * kernel);
+                }
+            });
+        }
+    }
+    finish_lanes<T>(O, valid, q, res, valid ? Q.pixel[q] : -1, valid ? Q.throughput + 3 * q : nullptr, K.P.norm_bb1d,
+                    cnt, h);
+}
+
 }  // namespace
 
 template <class T>
@@ -561,6 +619,8 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
     if (A.pq.n > 0 && A.hash.n > 0)
         k_gen_pp3d<T><<<(unsigned)((A.pq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.L, A.hash, A.pq, A.cam, A.cs_pt,
                                                                         A.out_pp3d);
+    if (A.pq.n > 0 && A.beams.n > 0 && (A.K.P.techniques & UPBP_BP2D))
+        k_gen_bp2d<T><<<(unsigned)((A.pq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.pq, A.out_bp2d);
     if (A.sq.n > 0 && A.photons.n > 0)
         k_gen_pb2d<T><<<(unsigned)((A.sq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam,
                                                                         A.cs_seg, A.out_pb2d);

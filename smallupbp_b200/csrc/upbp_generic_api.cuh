@@ -31,13 +31,14 @@ struct GenLaunch {
     LightSoA L;
     PhotonBVH photons;
     BeamBVH beams;
+    BeamSoA bs;
     HashGridDev hash;
     SegQueriesDev sq;
     PointQueriesDev pq;
     const upbp_mis* cam;
     const CamSum* cs_seg;
     const CamSum* cs_pt;
-    GenOut out_pb2d, out_bb1d, out_pp3d;
+    GenOut out_pb2d, out_bb1d, out_pp3d, out_bp2d;
     unsigned int* work;  // BB1D work counter (zeroed by the caller)
     int* status;         // BB1D traversal status (zeroed by the caller)
     int bb1d_grid;

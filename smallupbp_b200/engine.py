@@ -35,7 +35,8 @@ EXPORTS = (
     "upbp_build", "upbp_set_camera_mis", "upbp_set_segment_queries", "upbp_set_point_queries", "upbp_evaluate",
     "upbp_read_segment_results", "upbp_read_point_results", "upbp_read_query_stats", "upbp_clear_image",
     "upbp_read_image", "upbp_last_launch_count", "upbp_last_timings", "upbp_destroy_structures",
-    "upbp_read_tested_counts", "upbp_adjoint", "upbp_device_bytes",
+    "upbp_read_tested_counts", "upbp_adjoint", "upbp_device_bytes", "upbp_capture_graph", "upbp_launch_graph",
+    "upbp_read_bp2d_results",
 )
 
 
@@ -84,6 +85,9 @@ def lib():
         l.upbp_read_tested_counts.argtypes = [vp, abi.u64p]
         l.upbp_adjoint.argtypes = [vp, abi.f32p, C.c_int32, C.POINTER(C.c_double)]
         l.upbp_device_bytes.argtypes = [vp, abi.u64p]
+        l.upbp_capture_graph.argtypes = [vp]
+        l.upbp_read_bp2d_results.argtypes = [vp, abi.f32p, abi.u32p, abi.u64p]
+        l.upbp_launch_graph.argtypes = [vp]
         for name in EXPORTS:
             if name != "upbp_last_error":
                 getattr(l, name).restype = C.c_int
@@ -196,6 +200,22 @@ class EstimatorStage:
         st = abi.QueryStats(**{k: abi.ptr(v) for k, v in out.items()})
         self._ck(self._l.upbp_read_query_stats(self._ctx, C.byref(st)))
         return out
+
+    def bp2d_results(self):
+        """B-P2D per point query: (rgb [n][3], accepted count, candidate hash)."""
+        rgb = np.zeros((self._np, 3), np.float32)
+        cnt = np.zeros(self._np, np.uint32)
+        h = np.zeros(self._np, np.uint64)
+        self._ck(self._l.upbp_read_bp2d_results(self._ctx, abi.ptr(rgb), abi.ptr(cnt), abi.ptr(h)))
+        return rgb, cnt, h
+
+    def capture_graph(self):
+        """Record clear + build + evaluate of the current inputs as a CUDA graph (after one build and
+        evaluate of them)."""
+        self._ck(self._l.upbp_capture_graph(self._ctx))
+
+    def launch_graph(self):
+        self._ck(self._l.upbp_launch_graph(self._ctx))
 
     def device_bytes(self) -> int:
         out = np.zeros(1, np.uint64)

@@ -28,6 +28,7 @@ import numpy as np
 # flags, identical to include/upbp_gpu.h (and the reference enums)
 SHORT_BEAM, LONG_BEAM = 1, 2
 BPT, SURF, PP3D, PB2D, BB1D = 4, 8, 16, 32, 64
+BP2D = 65536  # extension: B-P2D (standalone, MIS weight 1); not a reference technique
 NO_SINE_IN_WEIGHTS, PREVIOUS, COMPATIBLE, BB1D_PREVIOUS = 128, 256, 512, 1024
 ORIGIN_IN_MEDIUM, END_IN_MEDIUM = 1, 2
 MIS_IS_DELTA, MIS_ON_LIGHT_SOURCE, MIS_IS_SPECULAR, MIS_IN_MEDIUM_WITH_BEAMS = 1, 2, 4, 8

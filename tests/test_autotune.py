@@ -35,9 +35,11 @@ def test_autotuned_stage_keeps_parity(mode):
     with engine.EstimatorStage(0, mode) as st:
         s = st.load(w)
         st.set_queries(w)
-        best, rep = autotune.autotune(st, s, repeats=1, bb1d_space={"bb1d_leaf": (1, 8), "beam_piece_radii": (4.0, 16.0)},
-                                      pb2d_space={"pb2d_leaf": (4, 16), "block_threads": (64,)})
-        assert len(rep["trials"]) == 4
+        best, rep = autotune.autotune(st, s, repeats=1,
+                                      stages=({"bb1d_kernel": (0, 1, 3)},
+                                              {"bb1d_leaf": (1, 8), "beam_piece_radii": (4.0, 16.0)},
+                                              {"pb2d_leaf": (4, 16), "block_threads": (64,)}))
+        assert len(rep["trials"]) == 3 + 4 + 2
         assert best["bb1d_leaf"] in (1, 8) and best["pb2d_leaf"] in (4, 16)
         t = st.get_tuning()
         assert (t.bb1d_leaf, t.pb2d_leaf, t.block_threads) == (best["bb1d_leaf"], best["pb2d_leaf"], 64)
