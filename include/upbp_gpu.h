@@ -144,6 +144,13 @@ typedef struct upbp_params {
     int32_t hash_cells;         /* PP3D HashGrid::Reserve(pathCountL) */
     int32_t image_width;
     int32_t image_height;
+    /* KNN radii (RadiusCalculation KNN_RADIUS): 0 = constant radius.  k > 0: each PB2D photon's
+     * radius is radius_pb2d * 2 * (distance to its k-th nearest photon, itself included)
+     * (EmbreeBre::build, Bre.cxx:685-725); each beam's start / end radius is
+     * max(2 * (distance from its origin / end to the k-th nearest beam origin) * radius_bb1d, 0.001),
+     * varying linearly along the beam (PhotonBeamsEvaluator::build, PhBeams.cxx:72-123). */
+    int32_t pb2d_knn;           /* mPB2DRadiusKNN when mPB2DRadiusCalculation == KNN_RADIUS, else 0 */
+    int32_t bb1d_knn;           /* mBB1DRadiusKNN when mBB1DRadiusCalculation == KNN_RADIUS, else 0 */
 } upbp_params;
 
 /* Light vertices (mLightVertices): n entries, stored per light path in
@@ -248,7 +255,8 @@ int upbp_set_mode(upbp_ctx* ctx, int mode);
  * gather variant (0: thread per query, 1: warp-cooperative persistent work queue at 5 blocks of
  * 4 warps per SM, 2: the same kernel compiled for 6 blocks per SM, 3 and 4: one persistent
  * work-queue kernel for all camera segments that evaluates PB2D and BB1D per query, at 5 or 6
- * blocks per SM; the PB2D phase of upbp_last_timings is then 0 and the BB1D phase covers both). */
+ * blocks per SM; the PB2D phase of upbp_last_timings is then 0 and the BB1D phase covers both).
+ * Defaults: leaves of 4, 128 threads, pieces of 4 radii, variant 2. */
 typedef struct upbp_tuning {
     int32_t pb2d_leaf;
     int32_t bb1d_leaf;

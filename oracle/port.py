@@ -34,9 +34,20 @@ def lib(fp64: bool = False):
     return _libs[path]
 
 
-def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False) -> Dict[str, np.ndarray]:
-    """Evaluate workload ``w`` with the C restatement (``fp64``: the FP64 oracle build)."""
+def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False, radii=None) -> Dict[str, np.ndarray]:
+    """Evaluate workload ``w`` with the C restatement (``fp64``: the FP64 oracle build).
+
+    ``radii`` = (photon radius^2 per light vertex, beam start radius, beam end radius) replaces the
+    KNN search (used to inject the radii the reference's own builds produced)."""
     s, keep = abi.make_structs(w)
+    l = lib(fp64)
+    l.upbp_oracle_set_radii.restype = None
+    l.upbp_oracle_set_radii.argtypes = [abi.f32p] * 3
+    if radii is not None:
+        radii = [np.ascontiguousarray(a, np.float32) for a in radii]
+        l.upbp_oracle_set_radii(*[abi.ptr(a) for a in radii])
+    else:
+        l.upbp_oracle_set_radii(None, None, None)
     nq, npq = s["sq"].n, s["pq"].n
     p = s["params"]
     out = {"pb2d": np.zeros((nq, 3), np.float32), "bb1d": np.zeros((nq, 3), np.float32),
@@ -51,9 +62,10 @@ def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False) -> Dict[s
                                P(out["bb1d"]), P(out["pp3d"]), P(out["count_pb2d"]), P(out["hash_pb2d"]),
                                P(out["count_bb1d"]), P(out["hash_bb1d"]), P(out["count_pp3d"]), P(out["hash_pp3d"]),
                                P(out["image"]))
+    l.upbp_oracle_set_radii(None, None, None)
     if rc != 0:
         raise RuntimeError("upbp_oracle_run failed (%d)" % rc)
-    del keep
+    del keep, radii
     return out
 
 

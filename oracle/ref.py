@@ -128,3 +128,31 @@ class Session:
             self.close()
         except Exception:
             pass
+
+
+def radii(w: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+    """The photon and beam radii the reference's own builds assign to workload ``w`` (KNN or
+    constant): per light vertex the photon radius^2 (0 for non-photons), per beam the start and end
+    radius and the max radius^2."""
+    s, keep = abi.make_structs(w)
+    l = lib()
+    l.ref_prepare.restype = C.c_void_p
+    l.ref_prepare.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Medium), C.c_int32, C.POINTER(abi.LightVertices),
+                              C.POINTER(abi.Beams), C.POINTER(abi.Mis), C.POINTER(abi.SegmentQueries),
+                              C.POINTER(abi.PointQueries), C.c_int32, C.c_int32]
+    l.ref_radii.restype = C.c_int
+    l.ref_radii.argtypes = [C.c_void_p] + [abi.f32p] * 4
+    l.ref_release.argtypes = [C.c_void_p]
+    h = l.ref_prepare(C.byref(s["params"]), s["media"], s["n_media"], C.byref(s["lv"]), C.byref(s["beams"]),
+                      s["cam_mis"], C.byref(s["sq"]), C.byref(s["pq"]), PB2D | BB1D_BRUTE, 1)
+    if not h:
+        raise RuntimeError("ref_prepare failed")
+    nlv, nb = s["lv"].n, s["beams"].n
+    out = {"ph_r2": np.zeros(nlv, np.float32), "bm_start": np.zeros(nb, np.float32),
+           "bm_end": np.zeros(nb, np.float32), "bm_r2": np.zeros(nb, np.float32)}
+    rc = l.ref_radii(h, *[abi.ptr(out[k]) for k in ("ph_r2", "bm_start", "bm_end", "bm_r2")])
+    l.ref_release(h)
+    del keep
+    if rc != 0:
+        raise RuntimeError("ref_radii failed")
+    return out

@@ -24,10 +24,10 @@
 #if defined(UPBP_REF_USE_BRUTE)
 /* Opaque entry points so the main harness TU (which sees the grid class
  * under the reference name) can drive the brute-force evaluator. */
-void* ref_brute_create(const Scene& scene, PhotonBeamsArray& beams, float radius)
+void* ref_brute_create(const Scene& scene, PhotonBeamsArray& beams, float radius, int knn)
 {
     PhotonBeamsEvaluatorBrute* e = new PhotonBeamsEvaluatorBrute(scene);
-    e->build(beams, CONSTANT_RADIUS, radius, 0, false);
+    e->build(beams, knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, radius, knn, false);
     return e;
 }
 Rgb ref_brute_eval(void* h, BeamType bt, const Ray& ray, const VolumeSegments& segs, uint tech, uint rsf,

@@ -34,3 +34,12 @@ void ref_bre_candidates(const EmbreeBre& bre, const float* origin, const float* 
         }
     }
 }
+
+void ref_bre_radii(const EmbreeBre& bre, const UPBPLightVertex* base, int64_t n, float* r2)
+{
+    for (int64_t i = 0; i < n; ++i) r2[i] = 0.f;
+    for (int i = 0; i < bre.numEmbreePhotons; ++i) {
+        const EmbreePhoton& ph = bre.embreePhotons[i];
+        r2[ph.lightVertex - base] = ph.radiusSqr;
+    }
+}

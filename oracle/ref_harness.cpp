@@ -39,7 +39,8 @@
 #include "ref_harness.h"
 #include "ref_internal.h"
 
-void* ref_brute_create(const Scene& scene, PhotonBeamsArray& beams, float radius);
+void* ref_brute_create(const Scene& scene, PhotonBeamsArray& beams, float radius, int knn);
+void ref_bre_radii(const EmbreeBre& bre, const UPBPLightVertex* base, int64_t n, float* r2);
 Rgb ref_brute_eval(void* h, BeamType bt, const Ray& ray, const VolumeSegments& segs, uint tech, uint rsf,
                    embree::AdditionalRayDataForMis* data);
 Rgb ref_brute_eval_lite(void* h, BeamType bt, const Ray& ray, const LiteVolumeSegments& segs, uint tech, uint rsf,
@@ -112,8 +113,10 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
     const float nl = (float)P.hash_cells;
     w.scene.mCamera.mResolution = Vec2f(1.f, 1.f);
     w.upbp = new UPBP(w.scene, UPBP::kCustom, P.techniques,
-                      P.radius_pp3d, 1.f, P.radius_pp3d, 1.f, P.radius_pb2d, 1.f, CONSTANT_RADIUS, 0,
-                      (BeamType)P.query_beam_type, P.radius_bb1d, 1.f, CONSTANT_RADIUS, 0,
+                      P.radius_pp3d, 1.f, P.radius_pp3d, 1.f, P.radius_pb2d, 1.f,
+                      P.pb2d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.pb2d_knn,
+                      (BeamType)P.query_beam_type, P.radius_bb1d, 1.f,
+                      P.bb1d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.bb1d_knn,
                       (BeamType)P.photon_beam_type, nl, 0.f, nl, nl, P.min_dist_to_med,
                       (size_t)1 << 30, 1234, 1234, false, false);
     UPBP& U = *w.upbp;
@@ -184,12 +187,13 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
         U.mPP3DHashGrid.Build(U.mLightVertices, P.radius_pp3d, PP3D);
     }
     if ((what & (REF_PB2D | REF_CANDIDATES)) && U.mMergeWithLightVerticesPB2D && !U.mLightVertices.empty())
-        U.mPB2DEmbreeBre.build(&U.mLightVertices[0], (int)U.mLightVertices.size(), CONSTANT_RADIUS, P.radius_pb2d,
-                               0, false);
+        U.mPB2DEmbreeBre.build(&U.mLightVertices[0], (int)U.mLightVertices.size(),
+                               P.pb2d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.radius_pb2d, P.pb2d_knn, false);
     if ((what & REF_BB1D_GRID) && U.mMergeWithLightVerticesBB1D && !U.mPhotonBeamsArray.empty())
-        U.mBB1DPhotonBeams.build(U.mPhotonBeamsArray, CONSTANT_RADIUS, P.radius_bb1d, 0, false);
+        U.mBB1DPhotonBeams.build(U.mPhotonBeamsArray, P.bb1d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.radius_bb1d,
+                                 P.bb1d_knn, false);
     if ((what & (REF_BB1D_BRUTE | REF_CANDIDATES)) && U.mMergeWithLightVerticesBB1D && !U.mPhotonBeamsArray.empty())
-        w.brute = ref_brute_create(w.scene, U.mPhotonBeamsArray, P.radius_bb1d);
+        w.brute = ref_brute_create(w.scene, U.mPhotonBeamsArray, P.radius_bb1d, P.bb1d_knn);
 }
 
 void load_camera(UPBP& U, const upbp_mis* cam_mis, int64_t begin, int count)
@@ -317,6 +321,25 @@ extern "C" void* ref_prepare(const upbp_params* params, const upbp_medium* media
 }
 
 extern "C" void ref_release(void* h) { delete static_cast<RefSession*>(h); }
+
+/* The radii the reference's builds assigned (session prepared with PB2D and BB1D_BRUTE):
+ * ph_r2[light vertex] = EmbreePhoton::radiusSqr (0 for vertices that are no photon), and per beam
+ * mStartRadius, mEndRadius, mMaxRadiusSqr.  Any pointer may be NULL. */
+extern "C" int ref_radii(void* h, float* ph_r2, float* bm_start, float* bm_end, float* bm_r2)
+{
+    RefSession* S = static_cast<RefSession*>(h);
+    if (!S || S->worlds.empty() || !S->worlds[0]) return -1;
+    UPBP& U = *S->worlds[0]->upbp;
+    if (ph_r2 && !U.mLightVertices.empty())
+        ref_bre_radii(U.mPB2DEmbreeBre, &U.mLightVertices[0], (int64_t)U.mLightVertices.size(), ph_r2);
+    for (size_t b = 0; b < U.mPhotonBeamsArray.size(); ++b) {
+        const PhotonBeam& pb = U.mPhotonBeamsArray[b];
+        if (bm_start) bm_start[b] = pb.mStartRadius;
+        if (bm_end) bm_end[b] = pb.mEndRadius;
+        if (bm_r2) bm_r2[b] = pb.mMaxRadiusSqr;
+    }
+    return 0;
+}
 
 /* Evaluate queries q = offset + k*stride; returns the wall time in ms through out->gather_ms. */
 extern "C" int ref_eval(void* h, int64_t offset, int64_t stride, ref_outputs* out)

@@ -359,7 +359,103 @@ typedef struct {
     const upbp_beams* bm;
     const upbp_mis* cam;
     int has_beams;
+    float* ph_r2;      /* KNN photon radius^2 per light vertex (NULL: constant radius_pb2d) */
+    float* bm_start;   /* KNN beam start radius, radius change per unit length, max radius^2 */
+    float* bm_change;  /* (NULL: constant radius_bb1d) */
+    float* bm_r2;
 } oracle;
+
+/* ---------------------------------------------------------------- KNN radii */
+/* k-th smallest squared distance from q to the n points pts[idx[i]] (idx NULL: pts[i]).  This is
+ * the dist2[1] that KdTree::KNNQuery leaves for a query with k nearest (Misc/KdTmpl.hxx:600-680):
+ * the root of the max-heap of the k nearest found, each distance ((dx*dx + dy*dy) + dz*dz) in FP32
+ * with d = point - query.  With n <= k the reference's value depends on its tree order; the
+ * largest distance is used then. */
+static float knn_d2(const float* pts, const int64_t* idx, int64_t n, const float* q, int k)
+{
+    float best[256];
+    int nb = 0, a;
+    int64_t i;
+    if (k > 256) k = 256;
+    for (i = 0; i < n; ++i) {
+        const float* p = pts + 3 * (idx ? idx[i] : i);
+        float d1 = p[0] - q[0];
+        float d2 = d1 * d1;
+        d1 = p[1] - q[1];
+        d2 += d1 * d1;
+        d1 = p[2] - q[2];
+        d2 += d1 * d1;
+        if (nb < k) {
+            for (a = nb++; a > 0 && best[a - 1] > d2; --a) best[a] = best[a - 1];
+            best[a] = d2;
+        } else if (d2 < best[k - 1]) {
+            for (a = k - 1; a > 0 && best[a - 1] > d2; --a) best[a] = best[a - 1];
+            best[a] = d2;
+        }
+    }
+    return nb > 0 ? best[nb - 1] : 0.f;
+}
+
+/* Radii given from outside instead of the KNN search (tests inject the radii the reference's own
+ * builds produced, so that everything but the search is compared with the reference).  Per light
+ * vertex photon radius^2; per beam start and end radius.  NULL pointers: compute by KNN. */
+static const float* g_ph_r2;
+static const float* g_bm_start;
+static const float* g_bm_end;
+void upbp_oracle_set_radii(const float* ph_r2, const float* bm_start, const float* bm_end)
+{
+    g_ph_r2 = ph_r2;
+    g_bm_start = bm_start;
+    g_bm_end = bm_end;
+}
+
+/* EmbreeBre::build with KNN_RADIUS (Bre.cxx:685-725): radius = r * (2 * sqrt(d2_k)) over the
+ * photons (light vertices in media); EmbreePhoton::set keeps radius * radius. */
+static float* knn_photon_r2(const upbp_light_vertices* lv, float r, int k)
+{
+    int64_t i, n = 0;
+    int64_t* idx = (int64_t*)malloc(sizeof(int64_t) * (size_t)(lv->n > 0 ? lv->n : 1));
+    float* r2 = (float*)calloc((size_t)(lv->n > 0 ? lv->n : 1), sizeof(float));
+    if (!idx || !r2) { free(idx); free(r2); return NULL; }
+    for (i = 0; i < lv->n; ++i)
+        if (lv->flags[i] & UPBP_LV_IN_MEDIUM) idx[n++] = i;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (i = 0; i < n; ++i) {
+        const int64_t j = idx[i];
+        const float radius = r * (2.0f * sqrtf(knn_d2(lv->position, idx, n, lv->position + 3 * j, k)));
+        r2[j] = radius * radius;
+    }
+    free(idx);
+    return r2;
+}
+
+/* PhotonBeamsEvaluator::build with KNN_RADIUS (PhBeams.cxx:77-123): start / end radius from the
+ * k-th nearest beam origin to the beam's origin / end, max(2 * sqrt(d2_k) * r, 0.001). */
+static int knn_beam_radii(const upbp_beams* bm, float r, int k, float** start, float** change, float** r2)
+{
+    int64_t b;
+    *start = (float*)malloc(sizeof(float) * (size_t)(bm->n > 0 ? bm->n : 1));
+    *change = (float*)malloc(sizeof(float) * (size_t)(bm->n > 0 ? bm->n : 1));
+    *r2 = (float*)malloc(sizeof(float) * (size_t)(bm->n > 0 ? bm->n : 1));
+    if (!*start || !*change || !*r2) return -1;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (b = 0; b < bm->n; ++b) {
+        const float* o = bm->origin + 3 * b;
+        const float* d = bm->direction + 3 * b;
+        const float len = bm->length[b];
+        const float end[3] = {o[0] + d[0] * len, o[1] + d[1] * len, o[2] + d[2] * len};
+        float rs = 2.0f * sqrtf(knn_d2(bm->origin, NULL, bm->n, o, k)) * r;
+        float re = 2.0f * sqrtf(knn_d2(bm->origin, NULL, bm->n, end, k)) * r;
+        float mx;
+        rs = rs > 0.001f ? rs : 0.001f;
+        re = re > 0.001f ? re : 0.001f;
+        mx = rs > re ? rs : re;
+        (*start)[b] = rs;
+        (*r2)[b] = mx * mx;
+        (*change)[b] = (re - rs) / len;
+    }
+    return 0;
+}
 
 typedef struct {
     v3f of, df;   /* query ray, float (predicates) */
@@ -406,7 +502,7 @@ static rgb pb2d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int6
     if (phase <= 0) return cs(0);
     dirPdf = phase * m->cont;
     revPdf = phase * lv->cont_prob[j];
-    r2 = (real)P->radius_pb2d * P->radius_pb2d;
+    r2 = O->ph_r2 ? (real)O->ph_r2[j] : (real)P->radius_pb2d * P->radius_pb2d;
     kernel = (1 - d2 / r2) / (r2 * (IS_F64 ? (real)3.14159265358979323846 : (real)PI_F) * (real)0.5);
     if (!is_pos(kernel)) return cs(0);
     un = cscale(cscale(cmul(cmul(C3(lv->throughput + 3 * j), att), Cr(m->ss)), phase), kernel);
@@ -448,8 +544,9 @@ static void closest_f64(v3 O1, v3 d1, v3 O2, v3 d2, real* dist, real* sinT, real
 
 /* PhotonBeam::accumulate2 after the test and the radius check accepted beam b. */
 static rgb bb1d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int64_t b, real dist, real sinTheta,
-                        real t1, real t2, real radius)
+                        real t1, real t2, real rstart, real rchange)
 {
+    real radius;
     const upbp_params* P = O->P;
     const upbp_beams* B = O->bm;
     const upbp_light_vertices* lv = O->lv;
@@ -463,6 +560,7 @@ static rgb bb1d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int6
     cam_view cv;
     light_view lview;
     if (IS_F64) closest_f64(s->o, s->d, V(B->origin + 3 * b), V(B->direction + 3 * b), &dist, &sinTheta, &t1, &t2);
+    radius = rstart + t2 * rchange;
     if ((uint32_t)(pl + 1 + s->L) > P->max_path_length || (uint32_t)(pl + 1 + s->L) < P->min_path_length) return cs(0);
     if (s->L == 1 && t1 < P->min_dist_to_med) return cs(0);
     att = eval_att(m, t1 - s->dmin);
@@ -552,10 +650,11 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
             s.rsf = UPBP_END_IN_MEDIUM | (i == 0 ? qrsf : 0u);
             if (est == UPBP_PB2D) {
                 const upbp_light_vertices* lv = O->lv;
-                const float r2 = P->radius_pb2d * P->radius_pb2d;
+                const float r2c = P->radius_pb2d * P->radius_pb2d;
                 int64_t j;
                 for (j = 0; j < lv->n; ++j) {
                     float t, d2;
+                    const float r2 = O->ph_r2 ? O->ph_r2[j] : r2c;
                     if (!(lv->flags[j] & UPBP_LV_IN_MEDIUM)) continue;
                     if (!test_bre(s.of, s.df, dminf, dmaxf, Vf(lv->position + 3 * j), r2, &t, &d2)) continue;
                     ++*cnt;
@@ -564,18 +663,20 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
                 }
             } else {
                 const upbp_beams* B = O->bm;
-                const float radius = P->radius_bb1d, r2 = radius * radius;
+                const float rc = P->radius_bb1d, r2c = rc * rc;
                 int64_t b;
                 for (b = 0; b < B->n; ++b) {
-                    float dist, sinT, t1, t2;
+                    float dist, sinT, t1, t2, radius;
+                    const float rs = O->bm_start ? O->bm_start[b] : rc, rd = O->bm_change ? O->bm_change[b] : 0.f;
                     if (&O->media[B->medium_id[b]] != m) continue;
                     if (!test_beam_beam(s.of, s.df, dminf, dmaxf, Vf(B->origin + 3 * b), Vf(B->direction + 3 * b), 0.f,
-                                        B->length[b], r2, &dist, &sinT, &t1, &t2))
+                                        B->length[b], O->bm_r2 ? O->bm_r2[b] : r2c, &dist, &sinT, &t1, &t2))
                         continue;
+                    radius = rs + t2 * rd; /* mStartRadius + t2 * mRadiusChange (PhotonBeam.hxx:411) */
                     if (radius < dist) continue;
                     ++*cnt;
                     *hash += mix64((uint64_t)b);
-                    seg = cadd(seg, bb1d_contrib(O, m, &s, b, dist, sinT, t1, t2, radius));
+                    seg = cadd(seg, bb1d_contrib(O, m, &s, b, dist, sinT, t1, t2, rs, rd));
                 }
             }
         }
@@ -742,6 +843,23 @@ int upbp_oracle_run(const upbp_params* P, const upbp_medium* media, int32_t n_me
     O.bm = bm;
     O.cam = cam;
     O.has_beams = (P->techniques & UPBP_BB1D) && bm && bm->n > 0;
+    if (P->pb2d_knn > 0 && (P->techniques & UPBP_PB2D)) {
+        O.ph_r2 = knn_photon_r2(lv, P->radius_pb2d, P->pb2d_knn);
+        if (!O.ph_r2) return -1;
+        if (g_ph_r2) memcpy(O.ph_r2, g_ph_r2, sizeof(float) * (size_t)lv->n);
+    }
+    if (P->bb1d_knn > 0 && O.has_beams) {
+        if (knn_beam_radii(bm, P->radius_bb1d, P->bb1d_knn, &O.bm_start, &O.bm_change, &O.bm_r2) != 0) return -1;
+        if (g_bm_start && g_bm_end) {
+            int64_t b;
+            for (b = 0; b < bm->n; ++b) {  /* PhBeams.cxx:117-121 from the given start / end */
+                const float rs = g_bm_start[b], re = g_bm_end[b], mx = rs > re ? rs : re;
+                O.bm_start[b] = rs;
+                O.bm_r2[b] = mx * mx;
+                O.bm_change[b] = (re - rs) / bm->length[b];
+            }
+        }
+    }
     if (pq && pq->n > 0 && (P->techniques & UPBP_PP3D)) {
         int64_t nin = 0;
         for (q = 0; q < lv->n; ++q) nin += (lv->flags[q] & UPBP_LV_IN_MEDIUM) != 0;
@@ -808,6 +926,10 @@ int upbp_oracle_run(const upbp_params* P, const upbp_medium* media, int32_t n_me
         }
     }
     if (have_grid) { free(g.start); free(g.end); free(g.idx); }
+    free(O.ph_r2);
+    free(O.bm_start);
+    free(O.bm_change);
+    free(O.bm_r2);
     return 0;
 }
 
@@ -834,8 +956,11 @@ int upbp_oracle_bp2d(const upbp_params* P, const upbp_medium* media, int32_t n_m
     medium M[ORACLE_MAX_MEDIA];
     int64_t q;
     int i;
+    float *bs = NULL, *bc = NULL, *br2 = NULL; /* KNN beam radii */
     if (!P || !media || n_media <= 0 || n_media > ORACLE_MAX_MEDIA || !bm || !pq || stride < 1) return -1;
     for (i = 0; i < n_media; ++i) M[i] = make_medium(&media[i]);
+    if (P->bb1d_knn > 0 && (P->techniques & UPBP_BP2D) && knn_beam_radii(bm, P->radius_bb1d, P->bb1d_knn, &bs, &bc, &br2))
+        return -1;
 #pragma omp parallel for schedule(dynamic, 8)
     for (q = 0; q < pq->n; q += stride) {
         const int px = pq->pixel[q];
@@ -843,7 +968,7 @@ int upbp_oracle_bp2d(const upbp_params* P, const upbp_medium* media, int32_t n_m
         const v3 cfix = V(pq->dir_fix + 3 * q);
         const int mid = pq->medium_id[q];
         const medium* m = &M[mid];
-        const float r = P->radius_bb1d, r2 = r * r;
+        const float r = P->radius_bb1d, r2c = r * r;
         rgb v = cs(0.f);
         uint32_t c = 0;
         uint64_t h = 0;
@@ -854,9 +979,15 @@ int upbp_oracle_bp2d(const upbp_params* P, const upbp_medium* media, int32_t n_m
                 float tf, d2f;
                 real t, d2, pfd, phase, sinT, kernel;
                 rgb att, val;
+                float rt, r2;
                 if (bm->medium_id[b] != mid) continue;
-                if (!test_bre(Vf(bm->origin + 3 * b), Vf(bm->direction + 3 * b), 0.f, bm->length[b], x, r2, &tf, &d2f))
+                /* bound: the beam's largest radius^2; then the radius at the foot point (KNN radii) */
+                if (!test_bre(Vf(bm->origin + 3 * b), Vf(bm->direction + 3 * b), 0.f, bm->length[b], x,
+                              br2 ? br2[b] : r2c, &tf, &d2f))
                     continue;
+                rt = bs ? bs[b] + tf * bc[b] : r;
+                r2 = rt * rt;
+                if (bs && d2f > r2) continue;
                 ++c;
                 h += mix64((uint64_t)b);
                 t = tf;
@@ -889,5 +1020,8 @@ int upbp_oracle_bp2d(const upbp_params* P, const upbp_medium* media, int32_t n_m
                 image[3 * px + k] += pq->throughput[3 * q + k] * P->norm_bb1d * comp(v, k);
             }
     }
+    free(bs);
+    free(bc);
+    free(br2);
     return 0;
 }

@@ -323,10 +323,13 @@ __device__ __forceinline__ float piece_t(int k, int cnt, float len)
     return k >= cnt ? len : __fmul_rn((float)k, __fdiv_rn(len, (float)cnt));
 }
 
+// rstart / rchange / r2max (KNN radii, or NULL for the constant radius): beam radius at t is
+// rstart + t * rchange, the predicate's bound is r2max (PhotonBeam.hxx:238-296, 411).
 __global__ void k_emit_pieces(const float* __restrict__ origin, const float* __restrict__ dir,
                               const float* __restrict__ length, const int32_t* __restrict__ medium, int64_t n,
                               const int32_t* __restrict__ offsets, float piece_len, float radius, float eps,
-                              float4* pa, float4* pb, float4* pc, Box* boxes)
+                              const float* __restrict__ rstart, const float* __restrict__ rchange,
+                              const float* __restrict__ r2max, float4* pa, float4* pb, float4* pc, Box* boxes)
 {
     const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (b >= n) return;
@@ -336,12 +339,15 @@ __global__ void k_emit_pieces(const float* __restrict__ origin, const float* __r
     const int first = offsets[b];
     const int cnt = offsets[b + 1] - first;
     // disc of radius r perpendicular to the beam: extent r*sqrt(1-d_i^2) per axis
-    const float mx = radius * sqrtf(fmaxf(0.f, 1.f - dx * dx)) + eps;
-    const float my = radius * sqrtf(fmaxf(0.f, 1.f - dy * dy)) + eps;
-    const float mz = radius * sqrtf(fmaxf(0.f, 1.f - dz * dz)) + eps;
-    const float r2 = radius * radius;
+    const float ex = sqrtf(fmaxf(0.f, 1.f - dx * dx)), ey = sqrtf(fmaxf(0.f, 1.f - dy * dy));
+    const float ez = sqrtf(fmaxf(0.f, 1.f - dz * dz));
+    const float rs = rstart ? rstart[b] : radius, rc = rchange ? rchange[b] : 0.f;
+    const float r2 = r2max ? r2max[b] : radius * radius;
     for (int k = 0; k < cnt; ++k) {
         const float t0 = piece_t(k, cnt, len), t1 = piece_t(k + 1, cnt, len);
+        // the largest radius on the piece (the radius is linear in t)
+        const float rp = rchange ? fmaxf(rs + t0 * rc, rs + t1 * rc) * 1.000001f : radius;
+        const float mx = rp * ex + eps, my = rp * ey + eps, mz = rp * ez + eps;
         const float ax = ox + dx * t0, ay = oy + dy * t0, az = oz + dz * t0;
         const float bx = ox + dx * t1, by = oy + dy * t1, bz = oz + dz * t1;
         Box bx_;
@@ -453,12 +459,13 @@ void launch_piece_counts(const float* length, int64_t n, float piece_len, int32_
     if (n > 0) k_piece_counts<<<blocks_for(n), kThreads, 0, s>>>(length, n, piece_len, counts);
 }
 void launch_emit_pieces(const float* origin, const float* dir, const float* length, const int32_t* medium, int64_t n,
-                        const int32_t* offsets, float piece_len, float radius, float eps, float4* pa, float4* pb,
-                        float4* pc, Box* boxes, cudaStream_t s)
+                        const int32_t* offsets, float piece_len, float radius, float eps, const float* rstart,
+                        const float* rchange, const float* r2max, float4* pa, float4* pb, float4* pc, Box* boxes,
+                        cudaStream_t s)
 {
     if (n > 0)
         k_emit_pieces<<<blocks_for(n), kThreads, 0, s>>>(origin, dir, length, medium, n, offsets, piece_len, radius,
-                                                         eps, pa, pb, pc, boxes);
+                                                         eps, rstart, rchange, r2max, pa, pb, pc, boxes);
 }
 void launch_morton_boxes(const Box* boxes, int n, const float* bbox, uint32_t* codes, cudaStream_t s)
 {

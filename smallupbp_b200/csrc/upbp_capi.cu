@@ -40,7 +40,7 @@ struct upbp_ctx {
     int pb2d_leaf = 4;
     int bb1d_leaf = 4;
     int block = 128;
-    float piece_len_r = 8.f;  // beam piece length in units of the beam radius
+    float piece_len_r = 4.f;  // beam piece length in units of the beam radius
     std::string err;
     upbp_params P{};
     bool have_params = false;
@@ -81,6 +81,12 @@ struct upbp_ctx {
     int n_pieces = 0;
     DBuf bm_leaf_codes, bm_nodes, bm_parent_int, bm_parent_leaf, bm_leaf_boxes, bm_node_boxes, bm_flagsbuf;
     DBuf pc_pay;  // mixed mode: beam payload packed per piece
+    // KNN radii: per-photon radius^2 (leaf order); per-beam radius change and max radius^2 (the
+    // start radius goes to bm_radius); the LBVH over beam origins for the beam KNN search
+    DBuf pb_r2, bm_rchange, bm_r2max, knn_status;
+    DBuf bo_pos, bo_pts, bo_codes, bo_codes_sorted, bo_idx, bo_idx_sorted, bo_bbox, bo_leaf_codes, bo_nodes,
+        bo_parent_int, bo_parent_leaf, bo_leaf_boxes, bo_node_boxes, bo_flags;
+    int bo_n_leaves = 0;
     // query order (Morton code of the query span's midpoint)
     DBuf q_keys, q_keys_sorted, q_iota, q_order;
     bool order_queries = true;
@@ -100,7 +106,7 @@ struct upbp_ctx {
     bool graph_status = false;  // the graph copies the BB1D traversal status back
     bool status_pending = false;  // status_host holds the last BB1D launch's flag
     int num_sms = 0;
-    int bb1d_kernel = 1;  // 0: thread per query, 1: warp-cooperative persistent
+    int bb1d_kernel = 2;  // 0: thread per query, 1-2: warp-cooperative BB1D, 3-4: fused segment kernel
     DBuf out_bp2d, cnt_bp2d, hash_bp2d;  // B-P2D (extension) per point query
     DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
     bool built = false;
@@ -268,6 +274,12 @@ void do_build(upbp_ctx* c)
     cudaStream_t s = c->stream;
     c->build_launches = 0;
     mark(c, 0, s);
+    const bool knn = (c->P.pb2d_knn > 0 && (c->P.techniques & UPBP_PB2D)) ||
+                     (c->P.bb1d_knn > 0 && (c->P.techniques & UPBP_BB1D));
+    if (knn) {
+        ensure(c, c->knn_status, sizeof(int) * 4);
+        ck(c, cudaMemsetAsync(c->knn_status.p, 0, sizeof(int) * 4, s), "memset");
+    }
     const upbp_params& P = c->P;
     const int64_t n = c->n_lv;
     // ---- light vertices
@@ -365,6 +377,21 @@ void do_build(upbp_ctx* c)
         build_lbvh(c, c->ph_keys_sorted.as<uint32_t>(), nph, leaf, c->pb_leaf_codes, c->pb_nodes, c->pb_parent_int,
                    c->pb_parent_leaf, c->pb_leaf_boxes, c->pb_node_boxes, c->pb_flags, c->pb_n_leaves);
         c->build_launches += 3;
+        if (P.pb2d_knn > 0 && (P.techniques & UPBP_PB2D)) {
+            // KNN photon radii over the LBVH just built (its boxes hold the points), then refit
+            // the boxes to the per-photon spheres
+            ensure(c, c->pb_r2, sizeof(float) * nph);
+            launch_photon_knn_r2(c->pb_pos.as<float4>(), nph, c->pb_nodes.as<BNode>(), c->pb_n_leaves, leaf, P.pb2d_knn,
+                                 P.radius_pb2d, c->pb_r2.as<float>(), c->knn_status.as<int>(), s);
+            launch_photon_leaf_boxes_r2(c->pb_pos.as<float4>(), c->pb_r2.as<float>(), nph, leaf, 1e-5f,
+                                        c->pb_leaf_boxes.as<Box>(), s);
+            const int ni = std::max(1, c->pb_n_leaves - 1);
+            ck(c, cudaMemsetAsync(c->pb_flags.p, 0, sizeof(int32_t) * ni, s), "memset");
+            launch_bottom_up(c->pb_leaf_boxes.as<Box>(), c->pb_n_leaves, c->pb_nodes.as<BNode>(),
+                             c->pb_parent_int.as<int32_t>(), c->pb_parent_leaf.as<int32_t>(),
+                             c->pb_node_boxes.as<Box>(), c->pb_flags.as<int32_t>(), s);
+            c->build_launches += 3;
+        }
     }
     // ---- BB1D beams: pieces + LBVH (a replay keeps the piece count of the build it repeats)
     const int replay_pieces = c->n_pieces;
@@ -381,6 +408,47 @@ void do_build(upbp_ctx* c)
                           c->b_rsr_in.as<float>(), c->b_lpw_in.as<float>(), c->b_rsf_in.as<uint32_t>(),
                           c->b_lv_in.as<int32_t>(), c->b_med_in.as<int32_t>(), nb, r, c->bm_thr4.as<float4>(),
                           c->bm_pdf4.as<float4>(), c->bm_link.as<int2>(), c->bm_radius.as<float>(), s);
+        const float* rchange = nullptr;
+        const float* r2max = nullptr;
+        if (P.bb1d_knn > 0) {
+            // KNN beam radii: an LBVH over the beam origins, two queries per beam
+            const int n = (int)nb;
+            ensure(c, c->bo_pos, sizeof(float4) * n);
+            ensure(c, c->bo_pts, sizeof(float4) * n);
+            ensure(c, c->bo_codes, sizeof(uint32_t) * n);
+            ensure(c, c->bo_codes_sorted, sizeof(uint32_t) * n);
+            ensure(c, c->bo_idx, sizeof(int32_t) * n);
+            ensure(c, c->bo_idx_sorted, sizeof(int32_t) * n);
+            ensure(c, c->bo_bbox, sizeof(float) * 6);
+            ensure(c, c->bm_rchange, sizeof(float) * n);
+            ensure(c, c->bm_r2max, sizeof(float) * n);
+            ensure(c, c->bbox_partial, sizeof(int32_t) * 8 + sizeof(float) * 6 * 1024);
+            launch_beam_origins(c->b_origin.as<float>(), n, c->bo_pos.as<float4>(), s);
+            const int ob = std::max(1, std::min(1024, (n + 255) / 256));
+            float* part = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
+            launch_bbox_partial(c->bo_pos.as<float4>(), nullptr, n, part, ob, s);
+            launch_bbox_final(part, ob, c->bo_bbox.as<float>(), s);
+            k_iota<<<(n + 255) / 256, 256, 0, s>>>(c->bo_idx.as<int32_t>(), n);
+            launch_morton_points(c->bo_pos.as<float4>(), c->bo_idx.as<int32_t>(), n, c->bo_bbox.as<float>(),
+                                 c->bo_codes.as<uint32_t>(), s);
+            sort_pairs(c, c->bo_codes.as<uint32_t>(), c->bo_codes_sorted.as<uint32_t>(), c->bo_idx.as<int32_t>(),
+                       c->bo_idx_sorted.as<int32_t>(), n, 30);
+            launch_gather_photons(c->bo_idx_sorted.as<int32_t>(), c->bo_pos.as<float4>(), n, c->bo_pts.as<float4>(),
+                                  s);
+            constexpr int kOriginLeaf = 4;
+            ensure(c, c->bo_leaf_boxes, sizeof(Box) * ((n + kOriginLeaf - 1) / kOriginLeaf));
+            launch_photon_leaf_boxes(c->bo_pts.as<float4>(), n, kOriginLeaf, 0.f, 1e-6f, c->bo_leaf_boxes.as<Box>(), s);
+            build_lbvh(c, c->bo_codes_sorted.as<uint32_t>(), n, kOriginLeaf, c->bo_leaf_codes, c->bo_nodes,
+                       c->bo_parent_int, c->bo_parent_leaf, c->bo_leaf_boxes, c->bo_node_boxes, c->bo_flags,
+                       c->bo_n_leaves);
+            launch_beam_knn(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(), n,
+                            c->bo_nodes.as<BNode>(), c->bo_n_leaves, c->bo_pts.as<float4>(), kOriginLeaf, P.bb1d_knn,
+                            r, c->bm_radius.as<float>(), c->bm_rchange.as<float>(), c->bm_r2max.as<float>(),
+                            c->knn_status.as<int>(), s);
+            rchange = c->bm_rchange.as<float>();
+            r2max = c->bm_r2max.as<float>();
+            c->build_launches += 12;
+        }
         const float piece_len = std::max(1e-6f, c->piece_len_r * r);
         ensure(c, c->bm_counts, sizeof(int32_t) * (nb + 1));
         ensure(c, c->bm_offsets, sizeof(int32_t) * (nb + 1));
@@ -418,6 +486,7 @@ void do_build(upbp_ctx* c)
         const float eps = 1e-5f + 1e-3f * r;
         launch_emit_pieces(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(),
                            c->b_med_in.as<int32_t>(), nb, c->bm_offsets.as<int32_t>(), piece_len, r, eps,
+                           rchange ? c->bm_radius.as<float>() : nullptr, rchange, r2max,
                            c->pc_a.as<float4>(), c->pc_b.as<float4>(), c->pc_c.as<float4>(), c->pc_boxes.as<Box>(), s);
         const int pblocks = std::max(1, std::min(1024, (np + 255) / 256));
         float* partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
@@ -449,6 +518,12 @@ void do_build(upbp_ctx* c)
     }
     mark(c, 1, s);
     ck(c, cudaGetLastError(), "build launch");
+    if (knn && !c->replay) {  // the KNN searches' traversal stacks must not have overflowed
+        int h = 0;
+        ck(c, cudaMemcpyAsync(&h, c->knn_status.p, sizeof(int), cudaMemcpyDeviceToHost, s), "knn status");
+        ck(c, cudaStreamSynchronize(s), "sync");
+        if (h) fail(c, UPBP_ERR_CAPACITY, "KNN radius search: traversal stack overflow");
+    }
     c->built = true;
     if (!c->replay) c->evaluated = false;
 }
@@ -540,6 +615,7 @@ PhotonBVH photon_bvh(upbp_ctx* c)
     B.n = (c->P.techniques & UPBP_PB2D) ? c->n_ph : 0;
     B.leaf = std::max(1, c->pb2d_leaf);
     B.n_leaves = c->pb_n_leaves;
+    B.r2 = (c->P.pb2d_knn > 0 && (c->P.techniques & UPBP_PB2D) && c->n_ph > 0) ? c->pb_r2.as<float>() : nullptr;
     return B;
 }
 
@@ -564,6 +640,8 @@ BeamSoA beam_soa(upbp_ctx* c)
     S.pdf = c->bm_pdf4.as<float4>();
     S.link = c->bm_link.as<int2>();
     S.radius = c->bm_radius.as<float>();
+    S.rchange = (c->P.bb1d_knn > 0 && c->n_beams > 0 && (c->P.techniques & UPBP_BB1D)) ? c->bm_rchange.as<float>()
+                                                                                          : nullptr;
     S.n = c->n_beams;
     return S;
 }
@@ -728,12 +806,7 @@ void do_evaluate(upbp_ctx* c)
     mark(c, 4, s);
     if (nq > 0) {
         const BeamBVH B = beam_bvh(c);
-        BeamSoA S{};
-        S.thr = c->bm_thr4.as<float4>();
-        S.pdf = c->bm_pdf4.as<float4>();
-        S.link = c->bm_link.as<int2>();
-        S.radius = c->bm_radius.as<float>();
-        S.n = c->n_beams;
+        const BeamSoA S = beam_soa(c);
         Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                   c->hash_bb1d.as<unsigned long long>(), tested + 1};
         if (fused) {
@@ -834,7 +907,10 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->out_pb2d, &c->out_bb1d, &c->out_pp3d, &c->image, &c->cnt_pb2d, &c->cnt_bb1d, &c->cnt_pp3d,
                    &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested, &c->light_sums, &c->cam_sums_seg,
                    &c->cam_sums_pt, &c->work, &c->status, &c->pc_pay, &c->q_keys, &c->q_keys_sorted, &c->q_iota,
-                   &c->q_order, &c->grad_img, &c->grad_acc, &c->out_bp2d, &c->cnt_bp2d, &c->hash_bp2d};
+                   &c->q_order, &c->grad_img, &c->grad_acc, &c->out_bp2d, &c->cnt_bp2d, &c->hash_bp2d,
+                   &c->pb_r2, &c->bm_rchange, &c->bm_r2max, &c->knn_status, &c->bo_pos, &c->bo_pts, &c->bo_codes,
+                   &c->bo_codes_sorted, &c->bo_idx, &c->bo_idx_sorted, &c->bo_bbox, &c->bo_leaf_codes, &c->bo_nodes,
+                   &c->bo_parent_int, &c->bo_parent_leaf, &c->bo_leaf_boxes, &c->bo_node_boxes, &c->bo_flags};
     for (DBuf* b : all) free_buf(*b);
     if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)
@@ -919,6 +995,8 @@ int upbp_set_params(upbp_ctx* c, const upbp_params* p)
             (p->photon_beam_type != UPBP_SHORT_BEAM && p->photon_beam_type != UPBP_LONG_BEAM))
             fail(c, UPBP_ERR_INVALID_ARG, "beam types must be SHORT_BEAM or LONG_BEAM");
         if (p->image_width < 0 || p->image_height < 0) fail(c, UPBP_ERR_INVALID_ARG, "negative image size");
+        if (p->pb2d_knn < 0 || p->pb2d_knn > kMaxKnn || p->bb1d_knn < 0 || p->bb1d_knn > kMaxKnn)
+            fail(c, UPBP_ERR_INVALID_ARG, "KNN counts must be in [0, %d]", kMaxKnn);
         c->P = *p;
         c->have_params = true;
         c->built = false;

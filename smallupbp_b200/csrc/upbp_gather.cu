@@ -93,7 +93,7 @@ __device__ __forceinline__ void fill_cand(upbp_mis& c, const upbp_params& P, flo
 // breIntersectFuncHomogeneous2 after testIntersectionBre accepted photon `lv` at (t, d2).
 template <bool kMixed>
 __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const LightSoA& Lv, const SegCtx& s, int lv,
-                            float t, float d2)
+                            float t, float d2, float r2)
 {
     const upbp_params& P = K.P;
     const int4 info = __ldg(&Lv.info[lv]);
@@ -115,8 +115,7 @@ __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const Light
     if (phase <= 0.f) return rgb(0.f);
     const float camDirPdfW = phase * m.cont;
     const float camRevPdfW = phase * __ldg(&Lv.pos[lv]).w;
-    const float r2 = P.radius_pb2d * P.radius_pb2d;
-    const float kernel = (1.f - d2 / r2) / (r2 * UPBP_PI_F * 0.5f);
+    const float kernel = (1.f - d2 / r2) / (r2 * UPBP_PI_F * 0.5f);  // the photon's radiusSqr
     if (!is_pos(kernel)) return rgb(0.f);
     const float4 th = __ldg(&Lv.thr[lv]);
     const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
@@ -265,7 +264,7 @@ __device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const Light
 
 // PhotonBeam::accumulate2 (mixed mode) with the beam's payload packed per piece.
 __device__ Rgb bb1d_contrib_packed(const GatherConsts& K, const DMedium& m, const SegCtx& s, const PiecePayload& py,
-                                   V3 bo, V3 bdir, float dist, float sinTheta, float t1, float t2)
+                                   V3 bo, V3 bdir, float dist, float sinTheta, float t1, float t2, float radius)
 {
     const upbp_params& P = K.P;
     const int lvbits = __float_as_int(py.lv.w);
@@ -277,7 +276,6 @@ __device__ Rgb bb1d_contrib_packed(const GatherConsts& K, const DMedium& m, cons
         if (1.f - c * c < 1e-2f) closest_approach_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
     }
     if (s.L == 1 && t1 < P.min_dist_to_med) return rgb(0.f);
-    const float radius = py.lv.z;
     const uint32_t bflags = (uint32_t)__float_as_int(py.thr.w);
     const uint32_t brsf = (uint32_t)__float_as_int(py.pdf.w);
     Rgb att = eval_att(m, t1 - s.dmin);
@@ -436,11 +434,12 @@ __global__ void __launch_bounds__(256) k_gather_pb2d(const __grid_constant__ Gat
                     const float4 p = __ldg(&B.pos[i]);
                     ++tested;
                     float t, d2;
-                    if (test_bre(s.o, s.d, s.dmin, s.dmax, v3(p.x, p.y, p.z), r2, &t, &d2)) {
+                    const float r2i = B.r2 ? __ldg(&B.r2[i]) : r2;
+                    if (test_bre(s.o, s.d, s.dmin, s.dmax, v3(p.x, p.y, p.z), r2i, &t, &d2)) {
                         const int lv = __float_as_int(p.w);
                         ++cnt;
                         h += mix64((unsigned long long)lv);
-                        acc = acc + pb2d_contrib<kMixed>(K, m, Lv, s, lv, t, d2);
+                        acc = acc + pb2d_contrib<kMixed>(K, m, Lv, s, lv, t, d2, r2i);
                     }
                 }
             });
@@ -489,7 +488,7 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                                     pc.x, t1, t2))
                         continue;
                     const int beam = __float_as_int(pc.z);
-                    const float radius = __ldg(&Bs.radius[beam]);
+                    const float radius = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t2);
                     if (radius < dist) continue;  // PhotonBeam.hxx:411-413
                     ++cnt;
                     h += mix64((unsigned long long)beam);
@@ -554,14 +553,15 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                 return;
             ++cnt;
             h += mix64((unsigned long long)__float_as_int(pc.z));
+            const int beam = __float_as_int(pc.z);
             if (kMixed) {
                 const PiecePayload py = B.pay[i];
                 part = part + bb1d_contrib_packed(K, m, s, py, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), g.x, g.y,
-                                                  g.z, g.w);
+                                                  g.z, g.w, beam_radius_at(Bs, beam, py.lv.z, g.w));
             } else {
-                const int beam = __float_as_int(pc.z);
                 part = part + bb1d_contrib<false>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                                  __ldg(&Bs.radius[beam]), g.x, g.y, g.z, g.w);
+                                                  beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), g.w), g.x, g.y,
+                                                  g.z, g.w);
             }
         };
         const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps, s.dmax + K.eps,
@@ -577,7 +577,9 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                     ++tested;
                     if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f,
                                        pa.w, pc.y, &dist, &sinT, &t1, &t2)) {
-                        const float radius = kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[__float_as_int(pc.z)]);
+                        const int beam = __float_as_int(pc.z);
+                        const float radius = beam_radius_at(
+                            Bs, beam, kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[beam]), t2);
                         if (!(radius < dist)) {  // PhotonBeam.hxx:411-413
                             const int own = piece_owns_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
                                                             v3(pb.x, pb.y, pb.z), pa.w, pb.w, pc.x, t1, t2);
@@ -626,17 +628,18 @@ __device__ __forceinline__ Rgb pb2d_query_warp(const GatherConsts& K, const DMed
         int qn = 0;
         auto eval = [&](int e) {
             const float4 g = cq.geo[e];
-            part = part + pb2d_contrib<kMixed>(K, m, Lv, s, cq.piece[e], g.x, g.y);
+            part = part + pb2d_contrib<kMixed>(K, m, Lv, s, cq.piece[e], g.x, g.y, g.z);
         };
         const bool ok = warp_traverse(P.nodes, P.n_leaves, P.n, leaf_shift, s.o, inv, s.dmin - K.eps, s.dmax + K.eps,
                                       ws.stack, ws.leaves, lane, [&](int i) {
             bool hit = false;
-            float t = 0.f, d2 = 0.f;
+            float t = 0.f, d2 = 0.f, r2i = r2;
             int lv = 0;
             if (i >= 0) {
                 const float4 p = __ldg(&P.pos[i]);
                 ++tested;
-                if (test_bre(s.o, s.d, s.dmin, s.dmax, v3(p.x, p.y, p.z), r2, &t, &d2)) {
+                if (P.r2) r2i = __ldg(&P.r2[i]);
+                if (test_bre(s.o, s.d, s.dmin, s.dmax, v3(p.x, p.y, p.z), r2i, &t, &d2)) {
                     lv = __float_as_int(p.w);
                     hit = true;
                     ++cnt;
@@ -648,7 +651,7 @@ __device__ __forceinline__ Rgb pb2d_query_warp(const GatherConsts& K, const DMed
             if (hit) {
                 const int pos = qn + __popc(vote & lt);
                 cq.piece[pos] = lv;
-                cq.geo[pos] = make_float4(t, d2, 0.f, 0.f);
+                cq.geo[pos] = make_float4(t, d2, r2i, 0.f);
             }
             qn += __popc(vote);
             __syncwarp();
@@ -902,7 +905,6 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
     const DMedium& m = media[mid];
     if ((K.P.techniques & UPBP_BP2D) && m.has_scat && B.n > 0) {
         const V3 cfix = v3(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
-        const float r = K.P.radius_bb1d, r2 = r * r;
         const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
         // a zero-length ray at x: the slab test becomes point-in-box
         traverse(B.nodes, B.n_leaves, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, [&](int leaf) {
@@ -914,9 +916,12 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
                 const float4 pb = __ldg(&B.pb[i]);
                 ++tested;
                 float t, d2;
-                if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, r2, &t, &d2)) continue;
+                // bound: the beam's largest radius^2; then the radius at the foot point
+                if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pc.y, &t, &d2)) continue;
                 if (!(t >= pb.w && t < pc.x)) continue;  // the piece containing the foot point
                 const int beam = __float_as_int(pc.z);
+                const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t), r2 = rt * rt;
+                if (Bs.rchange && d2 > r2) continue;
                 ++cnt;
                 h += mix64((unsigned long long)beam);
                 const float4 bthr = __ldg(&Bs.thr[beam]);

@@ -107,7 +107,7 @@ __device__ __forceinline__ void init_ctx(SegCtx<T>& s, const GatherConsts& K, co
 // ------------------------------------------------------------------ PB2D (Bre.cxx:293-464)
 template <class T>
 __device__ RgbT<T> pb2d_contrib(const GatherConsts& K, const MedT<T>& m, const LightSoA& Lv, const SegCtx<T>& s,
-                                int lv)
+                                int lv, float r2f)
 {
     const upbp_params& P = K.P;
     const int4 info = __ldg(&Lv.info[lv]);
@@ -135,7 +135,7 @@ __device__ RgbT<T> pb2d_contrib(const GatherConsts& K, const MedT<T>& m, const L
     if (!(val(phase) > 0.0)) return rgb_zero<T>();
     const T camDirPdfW = phase * m.cont;
     const T camRevPdfW = phase * (double)lp.w;
-    const double r2 = (double)P.radius_pb2d * P.radius_pb2d;
+    const double r2 = r2f;  // the photon's radiusSqr
     const double kernel = (1.0 - d2 / r2) / (r2 * 3.14159265358979323846 * 0.5);
     if (!(kernel > 1e-20)) return rgb_zero<T>();
     const float4 th = __ldg(&Lv.thr[lv]);
@@ -183,7 +183,7 @@ __device__ __forceinline__ void closest_f64(V3d O1, V3d d1, V3d O2, V3d d2, doub
 
 template <class T>
 __device__ RgbT<T> bb1d_contrib(const GatherConsts& K, const MedT<T>& m, const SegCtx<T>& s, const PiecePayload& py,
-                                V3d bo, V3d bdir)
+                                V3d bo, V3d bdir, double rchange)
 {
     const upbp_params& P = K.P;
     const int lvbits = __float_as_int(py.lv.w);
@@ -194,7 +194,7 @@ __device__ RgbT<T> bb1d_contrib(const GatherConsts& K, const MedT<T>& m, const S
     double dist, sinTheta, t1, t2;
     closest_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
     if (s.L == 1 && t1 < P.min_dist_to_med) return rgb_zero<T>();
-    const double radius = py.lv.z;
+    const double radius = (double)py.lv.z + t2 * rchange;  // mStartRadius + t2 * mRadiusChange
     const uint32_t bflags = (uint32_t)__float_as_int(py.thr.w);
     const uint32_t brsf = (uint32_t)__float_as_int(py.pdf.w);
     RgbT<T> att = eval_att(m, t1 - s.dmin);
@@ -350,11 +350,12 @@ __global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ Gather
                 for (int i = leaf * B.leaf; i < e; ++i) {
                     const float4 p = __ldg(&B.pos[i]);
                     float t, d2;
-                    if (test_bre(s.of, s.df, dminf, dmaxf, v3(p.x, p.y, p.z), r2, &t, &d2)) {
+                    const float r2i = B.r2 ? __ldg(&B.r2[i]) : r2;
+                    if (test_bre(s.of, s.df, dminf, dmaxf, v3(p.x, p.y, p.z), r2i, &t, &d2)) {
                         const int lv = __float_as_int(p.w);
                         ++cnt;
                         h += mix64((unsigned long long)lv);
-                        acc = acc + pb2d_contrib<T>(K, m, Lv, s, lv);
+                        acc = acc + pb2d_contrib<T>(K, m, Lv, s, lv, r2i);
                     }
                 }
             });
@@ -371,9 +372,10 @@ constexpr int kGenQueue = 64;
 template <class T>
 __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ GatherConsts K,
                                                   const __grid_constant__ GenConsts G, const BeamBVH B,
-                                                  const SegQueriesDev Q, const upbp_mis* __restrict__ cam,
-                                                  const CamSum* __restrict__ cs, const GenOut O,
-                                                  unsigned int* __restrict__ work, int* __restrict__ status)
+                                                  const BeamSoA Bs, const SegQueriesDev Q,
+                                                  const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
+                                                  const GenOut O, unsigned int* __restrict__ work,
+                                                  int* __restrict__ status)
 {
     constexpr int kWarps = 4;
     __shared__ MedT<T> media[UPBP_MAX_MEDIA];
@@ -406,7 +408,8 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                     const float4 pa = __ldg(&B.pa[i]);
                     const float4 pb = __ldg(&B.pb[i]);
                     const PiecePayload py = B.pay[i];
-                    part = part + bb1d_contrib<T>(K, m, s, py, v3d(pa.x, pa.y, pa.z), v3d(pb.x, pb.y, pb.z));
+                    const double rchg = Bs.rchange ? (double)__ldg(&Bs.rchange[__float_as_int(__ldg(&B.pc[i]).z)]) : 0.0;
+                    part = part + bb1d_contrib<T>(K, m, s, py, v3d(pa.x, pa.y, pa.z), v3d(pb.x, pb.y, pb.z), rchg);
                 };
                 const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.of, inv, dminf - K.eps,
                                               dmaxf + K.eps, stack, leaves, lane, [&](int i) {
@@ -421,7 +424,7 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                                                0.f, pa.w, pc.y, &dist, &sinT, &t1, &t2) &&
                                 piece_owns(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w,
                                            pb.w, pc.x, t1, t2) &&
-                                !(__ldg(&B.pay[i].lv.z) < dist)) {
+                                !(beam_radius_at(Bs, __float_as_int(pc.z), __ldg(&B.pay[i].lv.z), t2) < dist)) {
                                 hit = true;
                                 ++cnt;
                                 h += mix64((unsigned long long)__float_as_int(pc.z));
@@ -572,8 +575,6 @@ __global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ Gather
         const MedT<T>& m = media[mid];
         if ((K.P.techniques & UPBP_BP2D) && m.has_scat && B.n > 0) {
             const V3d cfix = v3d(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
-            const float r = K.P.radius_bb1d, r2 = r * r;
-            const double r2d = r2;
             traverse(B.nodes, B.n_leaves, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, [&](int leaf) {
                 const int e = min(B.n, (leaf + 1) * B.leaf);
                 for (int i = leaf * B.leaf; i < e; ++i) {
@@ -582,9 +583,12 @@ __global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ Gather
                     const float4 pa = __ldg(&B.pa[i]);
                     const float4 pb = __ldg(&B.pb[i]);
                     float tf, d2f;
-                    if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, r2, &tf, &d2f)) continue;
+                    if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pc.y, &tf, &d2f)) continue;
                     if (!(tf >= pb.w && tf < pc.x)) continue;
                     const int beam = __float_as_int(pc.z);
+                    const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), tf), r2 = rt * rt;
+                    if (Bs.rchange && d2f > r2) continue;
+                    const double r2d = r2;
                     ++cnt;
                     h += mix64((unsigned long long)beam);
                     const V3d o = v3d(pa.x, pa.y, pa.z), d = v3d(pb.x, pb.y, pb.z), p = v3d(x);
@@ -625,7 +629,7 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
         k_gen_pb2d<T><<<(unsigned)((A.sq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam,
                                                                         A.cs_seg, A.out_pb2d);
     if (A.sq.n > 0 && A.beams.n > 0)
-        k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.sq, A.cam, A.cs_seg, A.out_bb1d, A.work,
+        k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.sq, A.cam, A.cs_seg, A.out_bb1d, A.work,
                                                   A.status);
 }
 

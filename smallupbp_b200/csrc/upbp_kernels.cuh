@@ -37,6 +37,7 @@ struct LightSoA {
 struct PhotonBVH {
     const float4* pos;   // xyz, light-vertex index (int bits)
     const BNode* nodes;  // n_leaves - 1 internal nodes, root 0
+    const float* r2;     // KNN radii: photon radius^2 in leaf order (NULL: radius_pb2d^2)
     int n;
     int leaf;
     int n_leaves;
@@ -68,9 +69,16 @@ struct BeamSoA {
     const float4* thr;   // throughput at origin rgb, flags (int bits)
     const float4* pdf;   // ray_sample_pdf, ray_sample_rev_pdf, last_pdf_w_inv, ray_sampling_flags (int bits)
     const int2* link;    // light vertex, medium
-    const float* radius; // start radius (constant-radius build)
+    const float* radius; // start radius (the constant radius, or the KNN start radius)
+    const float* rchange; // KNN radii: radius change per unit length (NULL: constant radius)
     int64_t n;
 };
+
+// Radius of a beam at t (PhotonBeam.hxx:411: mStartRadius + t * mRadiusChange).
+__device__ __forceinline__ float beam_radius_at(const BeamSoA& S, int beam, float start, float t)
+{
+    return S.rchange ? __fadd_rn(start, __fmul_rn(t, __ldg(&S.rchange[beam]))) : start;
+}
 
 // PP3D hash grid (Misc/HashGrid.hxx), photons sorted by bucket, stable in light-vertex order.
 struct HashGridDev {
@@ -131,7 +139,17 @@ struct GatherConsts {
     float eps;           // conservative box slack for traversal
 };
 
+constexpr int kMaxKnn = 64;  // largest k of the KNN radii
+
 // ---- launches (all asynchronous on `stream`) ----------------------------------------
+void launch_photon_knn_r2(const float4* pts, int n, const BNode* nodes, int n_leaves, int leaf, int k, float r,
+                          float* r2, int* status, cudaStream_t stream);
+void launch_photon_leaf_boxes_r2(const float4* pos, const float* r2, int n, int leaf, float eps, Box* leaf_boxes,
+                                 cudaStream_t stream);
+void launch_beam_origins(const float* origin, int n, float4* out, cudaStream_t stream);
+void launch_beam_knn(const float* origin, const float* dir, const float* length, int n, const BNode* nodes,
+                     int n_leaves, const float4* pts, int leaf, int k, float r, float* rstart, float* rchange,
+                     float* r2max, int* status, cudaStream_t stream);
 void launch_pack_lights(const float* pos, const float* thr, const float* dir, const float* cont,
                         const int32_t* path_idx, const int32_t* path_length, const int32_t* medium,
                         const uint32_t* flags, int64_t n, float4* o_pos, float4* o_dir, float4* o_thr, int4* o_info,
@@ -162,9 +180,10 @@ void launch_pack_beams(const float* thr, const uint32_t* flags, const float* rsp
                        const uint32_t* rsf, const int32_t* lv, const int32_t* medium, int64_t n, float radius,
                        float4* o_thr, float4* o_pdf, int2* o_link, float* o_radius, cudaStream_t stream);
 void launch_piece_counts(const float* length, int64_t n, float piece_len, int32_t* counts, cudaStream_t stream);
-void launch_emit_pieces(const float* origin, const float* dir, const float* length, const int32_t* medium,
-                        int64_t n, const int32_t* offsets, float piece_len, float radius, float eps,
-                        float4* pa, float4* pb, float4* pc, Box* boxes, cudaStream_t stream);
+void launch_emit_pieces(const float* origin, const float* dir, const float* length, const int32_t* medium, int64_t n,
+                        const int32_t* offsets, float piece_len, float radius, float eps, const float* rstart,
+                        const float* rchange, const float* r2max, float4* pa, float4* pb, float4* pc, Box* boxes,
+                        cudaStream_t stream);
 void launch_bbox_boxes_partial(const Box* boxes, int n, float* partial, int blocks, cudaStream_t stream);
 void launch_morton_boxes(const Box* boxes, int n, const float* bbox, uint32_t* codes, cudaStream_t stream);
 void launch_permute_pieces(const int32_t* perm, int n, const float4* pa, const float4* pb, const float4* pc,

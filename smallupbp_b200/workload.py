@@ -55,6 +55,7 @@ PARAMS_FIELDS = (
     ("norm_pp3d", "<f4"), ("norm_pb2d", "<f4"), ("norm_bb1d", "<f4"),
     ("bb1d_min_mfp", "<f4"), ("min_dist_to_med", "<f4"),
     ("hash_cells", "<i4"), ("image_width", "<i4"), ("image_height", "<i4"),
+    ("pb2d_knn", "<i4"), ("bb1d_knn", "<i4"),
 )
 PARAMS_DTYPE = np.dtype(list(PARAMS_FIELDS))
 
@@ -118,6 +119,8 @@ class SceneConfig:
     min_path_length: int = 0
     min_dist_to_med: float = 0.0
     bb1d_storage_factor: float = 0.0
+    pb2d_knn: int = 0   # KNN photon radius (0: constant radius)
+    bb1d_knn: int = 0   # KNN beam radius (0: constant radius)
     seed: int = 1234
 
 
@@ -554,6 +557,8 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     prm["hash_cells"] = NL
     prm["image_width"] = cfg.width
     prm["image_height"] = cfg.height
+    prm["pb2d_knn"] = cfg.pb2d_knn
+    prm["bb1d_knn"] = cfg.bb1d_knn
     out["params"] = prm
     return out
 

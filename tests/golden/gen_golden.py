@@ -6,7 +6,7 @@ the reference harness (oracle/_ref/libupbp_ref.so, built from the reference sour
 oracle/build_ref.py):  per-query PB2D / BB1D (grid and brute force) / PP3D contributions,
 per-query candidate counts and hashes, and the splatted image.
 
-Run from the repository root:  python tests/golden/gen_golden.py
+Run from the repository root:  python tests/golden/gen_golden.py [fixture names]
 """
 from __future__ import annotations
 
@@ -32,7 +32,9 @@ CASES = [
     ("cube_previous", "cube24x1536", dict(techniques=W.PP3D | W.PB2D | W.BB1D | W.PREVIOUS | W.BB1D_PREVIOUS, seed=9)),
     ("boxes_all", "boxes", dict()),
     ("cube_wide_radius", "cube24x1536", dict(radius=0.08, seed=21)),
+    ("cube_knn_radius", "cube24x1536", dict(radius=0.25, pb2d_knn=8, bb1d_knn=6, seed=31)),
 ]
+
 
 
 def scene(name: str, overrides: dict) -> W.SceneConfig:
@@ -45,8 +47,10 @@ def scene(name: str, overrides: dict) -> W.SceneConfig:
     return cfg
 
 
-def main():
+def main(names=None):
     for fname, cname, over in CASES:
+        if names and fname not in names:
+            continue
         cfg = scene(cname, over)
         w = W.generate(cfg)
         o = ref.run(w, threads=8)
@@ -54,6 +58,9 @@ def main():
         for k in ("pb2d", "bb1d", "bb1d_brute", "pp3d", "count_pb2d", "hash_pb2d", "count_bb1d", "hash_bb1d",
                   "count_pp3d", "hash_pp3d", "image"):
             out["ref_" + k] = o[k]
+        if cfg.pb2d_knn > 0 or cfg.bb1d_knn > 0:  # the radii the reference's KNN search produced
+            rr = ref.radii(w)
+            out["ref_ph_r2"], out["ref_bm_start"], out["ref_bm_end"] = rr["ph_r2"], rr["bm_start"], rr["bm_end"]
         path = os.path.join(HERE, fname + ".npz")
         np.savez_compressed(path, **out)
         print("%-22s lv=%d beams=%d sq=%d pq=%d  cand pb2d=%d bb1d=%d pp3d=%d  %.0f KB" % (
@@ -62,4 +69,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

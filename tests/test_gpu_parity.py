@@ -29,7 +29,7 @@ def run(stage, w, mode=engine.MODE_PLAIN):
 @pytest.mark.gpu
 @pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
 def test_candidate_sets_bit_exact(stage, path):
-    w, r = G.load(path)
+    w, r = G.expected(path)
     g = run(stage, w)
     for est in ("pb2d", "bb1d", "pp3d"):
         np.testing.assert_array_equal(g["count_" + est], r["count_" + est], err_msg=est + " candidate counts")
@@ -39,7 +39,7 @@ def test_candidate_sets_bit_exact(stage, path):
 @pytest.mark.gpu
 @pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
 def test_contributions_plain_fp32(stage, path):
-    w, r = G.load(path)
+    w, r = G.expected(path)
     g = run(stage, w)
     G.assert_close(g["pb2d"], r["pb2d"], "PB2D")
     G.assert_close(g["bb1d"], r["bb1d_brute"], "BB1D vs brute-force reference")
@@ -64,7 +64,7 @@ def test_mixed_mode_candidates_and_contributions(stage, path):
     # closest-approach solve for near-parallel beam pairs.  Against the FP32 reference the
     # per-query contributions agree within 1e-4 except where the reference's own FP32 geometry
     # cancels; the image agrees within 1e-4 rel L2.
-    w, r = G.load(path)
+    w, r = G.expected(path)
     g = run(stage, w, engine.MODE_MIXED)
     for est in ("pb2d", "bb1d", "pp3d"):
         np.testing.assert_array_equal(g["hash_" + est], r["hash_" + est], err_msg=est)
@@ -87,16 +87,49 @@ def test_image_error_against_fp64_oracle(stage, path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel", [0, 1], ids=["thread_per_query", "warp_persistent"])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4],
+                         ids=["thread_per_query", "warp5", "warp6", "segments5", "segments6"])
 @pytest.mark.parametrize("leaf", [1, 4, 16])
 def test_bb1d_kernel_variants_same_candidates(stage, kernel, leaf):
-    # Both BB1D gathers and every leaf size / piece length find the reference's candidate set.
+    # Every BB1D gather variant and every leaf size / piece length finds the reference's
+    # candidate set (and the fused segment kernel the PB2D one as well).
     w, r = G.load(G.FIXTURES[-1])
     stage.set_tuning(bb1d_kernel=kernel, bb1d_leaf=leaf, beam_piece_radii=4.0 if leaf == 16 else 8.0)
     try:
         g = run(stage, w)
         np.testing.assert_array_equal(g["count_bb1d"], r["count_bb1d"])
         np.testing.assert_array_equal(g["hash_bb1d"], r["hash_bb1d"])
+        np.testing.assert_array_equal(g["count_pb2d"], r["count_pb2d"])
+        np.testing.assert_array_equal(g["hash_pb2d"], r["hash_pb2d"])
         G.assert_close(g["bb1d"], r["bb1d_brute"], "BB1D")
+        G.assert_close(g["pb2d"], r["pb2d"], "PB2D")
     finally:
-        stage.set_tuning(bb1d_kernel=1, bb1d_leaf=4, beam_piece_radii=8.0)
+        stage.set_tuning(bb1d_kernel=2, bb1d_leaf=4, beam_piece_radii=4.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [engine.MODE_PLAIN, engine.MODE_MIXED], ids=["plain", "mixed"])
+def test_knn_radii_bit_exact_with_exact_knn_oracle(stage, mode):
+    # KNN radii at a size where photons and beam origins span many LBVH leaves: the CUDA KNN
+    # search must find the exact k-th nearest distance the oracle computes, so candidate sets
+    # match bit for bit (PB2D, BB1D and B-P2D).
+    from oracle import port
+    from smallupbp_b200 import workload as W
+
+    cfg = W.config("cube64x4096")
+    cfg.radius, cfg.pb2d_knn, cfg.bb1d_knn = 0.3, 10, 7
+    w = W.generate(cfg)
+    w["params"]["techniques"] |= W.BP2D
+    o = port.run(w)
+    ob = port.bp2d(w)
+    g = run(stage, w, mode)
+    for est in ("pb2d", "bb1d", "pp3d"):
+        np.testing.assert_array_equal(g["count_" + est], o["count_" + est], err_msg=est)
+        np.testing.assert_array_equal(g["hash_" + est], o["hash_" + est], err_msg=est)
+    if mode == engine.MODE_PLAIN:
+        G.assert_close(g["pb2d"], o["pb2d"], "PB2D (KNN)")
+        G.assert_close(g["bb1d"], o["bb1d"], "BB1D (KNN)")
+    rgb, cnt, h = stage.bp2d_results()
+    np.testing.assert_array_equal(cnt, ob["count_bp2d"])
+    np.testing.assert_array_equal(h, ob["hash_bp2d"])
+    assert G.image_rel_l2(g["image"], o["image"] + ob["image"]) <= 1e-4
