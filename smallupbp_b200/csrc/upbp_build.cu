@@ -356,8 +356,8 @@ __global__ void k_emit_pieces(const float* __restrict__ origin, const float* __r
         bx_.lo[2] = fminf(az, bz) - mz; bx_.hi[2] = fmaxf(az, bz) + mz;
         const int p = first + k;
         pa[p] = make_float4(ox, oy, oz, len);
-        pb[p] = make_float4(dx, dy, dz, t0);
-        pc[p] = make_float4(t1, r2, __int_as_float((int)b), __int_as_float(medium[b]));
+        pb[p] = make_float4(dx, dy, dz, r2);
+        pc[p] = make_float4(t0, t1, __int_as_float((int)b), __int_as_float(medium[b]));
         boxes[p] = bx_;
     }
 }

@@ -482,10 +482,10 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                     ++tested;
                     float dist, sinT, t1, t2;
                     if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
-                                        pc.y, &dist, &sinT, &t1, &t2))
+                                        pb.w, &dist, &sinT, &t1, &t2))
                         continue;
-                    if (!piece_owns(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pb.w,
-                                    pc.x, t1, t2))
+                    if (!piece_owns(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pc.x,
+                                    pc.y, t1, t2))
                         continue;
                     const int beam = __float_as_int(pc.z);
                     const float radius = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t2);
@@ -549,7 +549,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
             const float4 pb = __ldg(&B.pb[i]);
             const float4 pc = __ldg(&B.pc[i]);
             if (undecided &&
-                !piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pb.w, pc.x))
+                !piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y))
                 return;
             ++cnt;
             h += mix64((unsigned long long)__float_as_int(pc.z));
@@ -570,22 +570,24 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
             int entry = 0;
             float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f;
             if (i >= 0) {
-                const float4 pc = __ldg(&B.pc[i]);
-                if (__float_as_int(pc.w) == mid) {  // mMedium == medium (PhotonBeam.hxx:390)
-                    const float4 pa = __ldg(&B.pa[i]);
-                    const float4 pb = __ldg(&B.pb[i]);
-                    ++tested;
-                    if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f,
-                                       pa.w, pc.y, &dist, &sinT, &t1, &t2)) {
+                // the predicate reads only pa and pb; pc (piece interval, beam, medium) is loaded for
+                // the pieces that pass it
+                const float4 pa = __ldg(&B.pa[i]);
+                const float4 pb = __ldg(&B.pb[i]);
+                ++tested;
+                if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
+                                   pb.w, &dist, &sinT, &t1, &t2)) {
+                    const float4 pc = __ldg(&B.pc[i]);
+                    const int own = __float_as_int(pc.w) == mid  // mMedium == medium (PhotonBeam.hxx:390)
+                                        ? piece_owns_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
+                                                          v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y, t1, t2)
+                                        : 0;
+                    if (own != 0) {  // this piece may take it: the radius test (PhotonBeam.hxx:411-413)
                         const int beam = __float_as_int(pc.z);
                         const float radius = beam_radius_at(
                             Bs, beam, kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[beam]), t2);
-                        if (!(radius < dist)) {  // PhotonBeam.hxx:411-413
-                            const int own = piece_owns_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
-                                                            v3(pb.x, pb.y, pb.z), pa.w, pb.w, pc.x, t1, t2);
-                            hit = own != 0;
-                            entry = own > 0 ? i : ~i;
-                        }
+                        hit = !(radius < dist);
+                        entry = own > 0 ? i : ~i;
                     }
                 }
             }
@@ -917,8 +919,8 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
                 ++tested;
                 float t, d2;
                 // bound: the beam's largest radius^2; then the radius at the foot point
-                if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pc.y, &t, &d2)) continue;
-                if (!(t >= pb.w && t < pc.x)) continue;  // the piece containing the foot point
+                if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &t, &d2)) continue;
+                if (!(t >= pc.x && t < pc.y)) continue;  // the piece containing the foot point
                 const int beam = __float_as_int(pc.z);
                 const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t), r2 = rt * rt;
                 if (Bs.rchange && d2 > r2) continue;

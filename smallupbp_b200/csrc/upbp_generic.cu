@@ -421,9 +421,9 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                             const float4 pb = __ldg(&B.pb[i]);
                             float dist, sinT, t1, t2;
                             if (test_beam_beam(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                               0.f, pa.w, pc.y, &dist, &sinT, &t1, &t2) &&
+                                               0.f, pa.w, pb.w, &dist, &sinT, &t1, &t2) &&
                                 piece_owns(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w,
-                                           pb.w, pc.x, t1, t2) &&
+                                           pc.x, pc.y, t1, t2) &&
                                 !(beam_radius_at(Bs, __float_as_int(pc.z), __ldg(&B.pay[i].lv.z), t2) < dist)) {
                                 hit = true;
                                 ++cnt;
@@ -583,8 +583,8 @@ __global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ Gather
                     const float4 pa = __ldg(&B.pa[i]);
                     const float4 pb = __ldg(&B.pb[i]);
                     float tf, d2f;
-                    if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pc.y, &tf, &d2f)) continue;
-                    if (!(tf >= pb.w && tf < pc.x)) continue;
+                    if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &tf, &d2f)) continue;
+                    if (!(tf >= pc.x && tf < pc.y)) continue;
                     const int beam = __float_as_int(pc.z);
                     const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), tf), r2 = rt * rt;
                     if (Bs.rchange && d2f > r2) continue;

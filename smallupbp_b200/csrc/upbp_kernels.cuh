@@ -55,8 +55,8 @@ struct __align__(16) PiecePayload {
 // Beam pieces (BB1D) in leaf order.  Piece = beam sub-interval [t_lo, t_hi).
 struct BeamBVH {
     const float4* pa;    // beam origin xyz, beam length
-    const float4* pb;    // beam direction xyz, t_lo
-    const float4* pc;    // t_hi, max radius^2, beam id (int bits), medium (int bits)
+    const float4* pb;    // beam direction xyz, max radius^2   (pa, pb: all the predicate reads)
+    const float4* pc;    // t_lo, t_hi, beam id (int bits), medium (int bits)
     const BNode* nodes;
     const PiecePayload* pay;  // mixed mode, per piece
     int n;
