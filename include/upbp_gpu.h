@@ -356,6 +356,81 @@ int upbp_pp3d_evaluate_noalloc(const upbp_params* params, const upbp_medium* med
                                const upbp_light_vertices* lv, const upbp_mis* cam_mis,
                                const upbp_point_queries* pq, float* out_rgb, void* stream);
 
+/* ---- device-side light and camera passes -------------------------------- */
+
+/* The estimator stage's inputs can also be produced on the device: the light pass of
+ * UPBP::RunIteration (Renderers/UPBP.hxx:501-674, with UPBP::AddBeams :1783-1870) and its camera
+ * pass (:742-1160), for scenes of nested axis-aligned boxes of homogeneous media with imaginary
+ * boundaries, an area quad light and a pinhole camera.  The passes compute in FP64.  Random
+ * numbers are per path: Philox4x64-10 with key (seed, iteration) and counter (path or pixel index,
+ * bounce, block, stream 0 = light / 1 = camera), four uniforms (x >> 11) * 2^-53 per counter.
+ * Light path p draws its emission from block 0 of bounce 0 (position x, position z, two
+ * direction samples); the ray of bounce L (leaving vertex L-1) draws the free flight of its k-th
+ * medium segment from block 1 + k / 4, word k % 4, and the scattering at vertex L its phase
+ * function and Russian roulette samples from block 0, words 0-2.  Camera paths draw the pixel
+ * jitter from block 0 of bounce 0, words 0-1, and bounce as light paths do. */
+#define UPBP_MAX_BOXES 8
+#define UPBP_SCENE_MAX_MEDIA 16
+
+typedef struct upbp_scene_medium {
+    double absorption[3];
+    double scattering[3];
+    double mean_cosine;
+    double continuation_prob;
+} upbp_scene_medium;
+
+/* Box i+1 lies inside box i; a point takes the medium of the last box that contains it (bounds
+ * included) and medium 0 outside every box.  The light is a square of side light_size centred on
+ * the top face (y = box_hi[0][1]) of box 0, emitting with a cosine distribution downwards, with
+ * radiance light_intensity.  The camera at camera_pos looks along +z, x right and y up, with a
+ * horizontal field of view fov_deg over width pixels.  width, height, max_path_length and
+ * techniques must equal the upbp_params given to upbp_set_params, which must come first (the
+ * records take its MIS factors). */
+typedef struct upbp_scene {
+    int32_t n_media;
+    upbp_scene_medium media[UPBP_SCENE_MAX_MEDIA];
+    int32_t n_boxes;
+    double box_lo[UPBP_MAX_BOXES][3];
+    double box_hi[UPBP_MAX_BOXES][3];
+    int32_t box_medium[UPBP_MAX_BOXES];
+    double camera_pos[3];
+    double fov_deg;
+    int32_t width;
+    int32_t height;
+    int32_t light_paths;        /* N_L */
+    int32_t max_path_length;    /* at most 16 */
+    double light_size;
+    double light_intensity;
+    uint32_t techniques;        /* UPBP_PB2D decides where beams are stored (bb1d_min_mfp) */
+    uint32_t query_beam_type;   /* UPBP_SHORT_BEAM / UPBP_LONG_BEAM */
+    uint32_t photon_beam_type;
+    double beam_length_cap;     /* cap on LONG photon beams beyond MaxBeamLength; +inf for none */
+    double min_dist_to_med;     /* mMinDistToMed: no PP3D query at a first camera vertex closer than this */
+    double bb1d_min_mfp;        /* mBB1DMinMFP */
+    uint64_t seed;
+} upbp_scene;
+
+/* Trace the light sub-paths of iteration `iteration` on the device and store their light vertices
+ * and photon beams in the context, as upbp_set_light_vertices and upbp_set_beams would: vertex
+ * records per path in increasing path length, beams per path in the order AddBeams emits them. */
+int upbp_trace_light_paths(upbp_ctx* ctx, const upbp_scene* scene, uint32_t iteration);
+/* Trace the camera sub-paths (one per pixel) of iteration `iteration` on the device and store the
+ * estimator calls they make, as upbp_set_camera_mis, upbp_set_segment_queries and
+ * upbp_set_point_queries would: per pixel in call order, for each camera path length the segment
+ * query, then the point query, each with its snapshot of the camera MIS records. */
+int upbp_trace_camera_paths(upbp_ctx* ctx, const upbp_scene* scene, uint32_t iteration);
+/* Copy one stored input array to dst (host or device memory; capacity in bytes).  name is one of
+ * the C ABI's record arrays: lv_position, lv_throughput, lv_dir_fix, lv_cont_prob, lv_path_idx,
+ * lv_path_length, lv_medium_id, lv_flags, lv_mis, lv_path_ends, beam_origin, beam_direction,
+ * beam_length, beam_throughput, beam_flags, beam_ray_sample_pdf, beam_ray_sample_rev_pdf,
+ * beam_ray_sampling_flags, beam_last_pdf_w_inv, beam_medium_id, beam_light_vertex, cam_mis,
+ * sq_origin, sq_direction, sq_seg_begin, sq_seg_count, sq_flags, sq_path_length,
+ * sq_last_pdf_w_inv, sq_throughput, sq_pixel, sq_cam_mis_begin, seg_dist_min, seg_dist_max,
+ * seg_pdf, seg_rev_pdf, seg_attenuation, seg_medium, pq_position, pq_dir_fix, pq_medium_id,
+ * pq_path_length, pq_throughput, pq_pixel, pq_cam_mis_begin.  *bytes receives the array's size;
+ * dst may be NULL to query it. */
+int upbp_read_input(upbp_ctx* ctx, const char* name, void* dst, int64_t capacity_bytes, int64_t* bytes);
+
 /* Releases the per-iteration structures; replaces EmbreeBre::destroy and
  * PhotonBeamsEvaluator::destroy (UPBP.hxx:1172-1181).  Device buffers are
  * kept for reuse by the next iteration. */

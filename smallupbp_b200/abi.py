@@ -69,6 +69,56 @@ class QueryStats(C.Structure):
                 ("count_pp3d", u32p), ("hash_pp3d", u64p)]
 
 
+MAX_BOXES, SCENE_MAX_MEDIA = 8, 16
+
+
+class SceneMedium(C.Structure):
+    _fields_ = [("absorption", C.c_double * 3), ("scattering", C.c_double * 3), ("mean_cosine", C.c_double),
+                ("continuation_prob", C.c_double)]
+
+
+class Scene(C.Structure):
+    _fields_ = [("n_media", C.c_int32), ("media", SceneMedium * SCENE_MAX_MEDIA), ("n_boxes", C.c_int32),
+                ("box_lo", (C.c_double * 3) * MAX_BOXES), ("box_hi", (C.c_double * 3) * MAX_BOXES),
+                ("box_medium", C.c_int32 * MAX_BOXES), ("camera_pos", C.c_double * 3), ("fov_deg", C.c_double),
+                ("width", C.c_int32), ("height", C.c_int32), ("light_paths", C.c_int32),
+                ("max_path_length", C.c_int32), ("light_size", C.c_double), ("light_intensity", C.c_double),
+                ("techniques", C.c_uint32), ("query_beam_type", C.c_uint32), ("photon_beam_type", C.c_uint32),
+                ("beam_length_cap", C.c_double), ("min_dist_to_med", C.c_double), ("bb1d_min_mfp", C.c_double),
+                ("seed", C.c_uint64)]
+
+
+def scene_struct(cfg) -> Scene:
+    """upbp_scene of a :class:`smallupbp_b200.workload.SceneConfig` (the scene the host generator traces)."""
+    from .workload import iteration_constants
+    if len(cfg.boxes) > MAX_BOXES or len(cfg.media) > SCENE_MAX_MEDIA:
+        raise ValueError("scene too large for upbp_scene")
+    sc = Scene()
+    sc.n_media = len(cfg.media)
+    for i, m in enumerate(cfg.media):
+        sc.media[i].absorption[:] = [float(x) for x in m.absorption]
+        sc.media[i].scattering[:] = [float(x) for x in m.scattering]
+        sc.media[i].mean_cosine = float(m.mean_cosine)
+        sc.media[i].continuation_prob = float(m.continuation_prob)
+    sc.n_boxes = len(cfg.boxes)
+    for b, (lo, hi, mid) in enumerate(cfg.boxes):
+        sc.box_lo[b][:] = [float(x) for x in lo]
+        sc.box_hi[b][:] = [float(x) for x in hi]
+        sc.box_medium[b] = mid
+    sc.camera_pos[:] = [float(x) for x in cfg.camera_pos]
+    sc.fov_deg = cfg.fov_deg
+    sc.width, sc.height = cfg.width, cfg.height
+    sc.light_paths = cfg.light_paths
+    sc.max_path_length = cfg.max_path_length
+    sc.light_size, sc.light_intensity = cfg.light_size, cfg.light_intensity
+    sc.techniques, sc.query_beam_type, sc.photon_beam_type = cfg.techniques, cfg.query_beam_type, cfg.photon_beam_type
+    sc.beam_length_cap = cfg.beam_length_cap
+    sc.min_dist_to_med = cfg.min_dist_to_med
+    sc.bb1d_min_mfp = iteration_constants(cfg)["bb1d_min_mfp"]
+    sc.seed = cfg.seed
+    return sc
+
+
 assert C.sizeof(Mis) == 60
 assert C.sizeof(Medium) == MEDIUM_DTYPE.itemsize
 assert C.sizeof(Params) == PARAMS_DTYPE.itemsize

@@ -26,6 +26,11 @@ def nvcc() -> str:
     raise FileNotFoundError("nvcc not found")
 
 
+# Per-file flags: the device-side light and camera passes reproduce the host generator's FP64
+# operation order, so no multiply-add may be contracted there.
+FILE_FLAGS = {"upbp_trace.cu": ["-fmad=false"]}
+
+
 def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
@@ -37,7 +42,8 @@ def build(verbose: bool = False, extra=()) -> str:
     os.makedirs(objdir, exist_ok=True)
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + list(extra) + ["-I", CSRC, "-c", src, "-o", obj]
+        cmd = [nvcc()] + ARCH + NVCC_FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + list(extra) + [
+            "-I", CSRC, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         procs.append((subprocess.Popen(cmd), cmd))

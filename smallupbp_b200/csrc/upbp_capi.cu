@@ -13,6 +13,7 @@
 #include "upbp_generic_api.cuh"
 #include "upbp_kernels.cuh"
 #include "upbp_mis_prep.cuh"
+#include "upbp_trace.cuh"
 
 using namespace upbp;
 
@@ -108,6 +109,7 @@ struct upbp_ctx {
     int num_sms = 0;
     int bb1d_kernel = 2;  // 0: thread per query, 1-2: warp-cooperative BB1D, 3-4: fused segment kernel
     DBuf out_bp2d, cnt_bp2d, hash_bp2d;  // B-P2D (extension) per point query
+    DBuf tr_cnt, tr_off, tr_status;  // device-side light / camera passes: per-path record counts and offsets
     DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
     bool built = false;
     int build_launches = 0, eval_launches = 0;
@@ -910,7 +912,8 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->q_order, &c->grad_img, &c->grad_acc, &c->out_bp2d, &c->cnt_bp2d, &c->hash_bp2d,
                    &c->pb_r2, &c->bm_rchange, &c->bm_r2max, &c->knn_status, &c->bo_pos, &c->bo_pts, &c->bo_codes,
                    &c->bo_codes_sorted, &c->bo_idx, &c->bo_idx_sorted, &c->bo_bbox, &c->bo_leaf_codes, &c->bo_nodes,
-                   &c->bo_parent_int, &c->bo_parent_leaf, &c->bo_leaf_boxes, &c->bo_node_boxes, &c->bo_flags};
+                   &c->bo_parent_int, &c->bo_parent_leaf, &c->bo_leaf_boxes, &c->bo_node_boxes, &c->bo_flags,
+                   &c->tr_cnt, &c->tr_off, &c->tr_status};
     for (DBuf* b : all) free_buf(*b);
     if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)
@@ -1104,6 +1107,266 @@ int upbp_set_point_queries(upbp_ctx* c, const upbp_point_queries* q)
         upload(c, c->pq_pixel, q->pixel, n, "pixel");
         upload(c, c->pq_cam_begin, q->cam_mis_begin, n, "cam_mis_begin");
         c->n_pq = n;
+    });
+}
+
+namespace {
+
+// Per-path counts (count pass) -> exclusive offsets -> totals on the host.  `k` arrays of n ints
+// live in tr_cnt / tr_off, each followed by a zero so that offset[n] is the total.
+void trace_offsets(upbp_ctx* c, int k, int64_t n, int64_t* totals)
+{
+    cudaStream_t s = c->stream;
+    int* cnt = c->tr_cnt.as<int>();
+    int* off = c->tr_off.as<int>();
+    const size_t tb = trace::scan_temp_bytes((int)(n + 1));
+    ensure(c, c->cub_tmp, tb);
+    for (int j = 0; j < k; ++j) {
+        ck(c, cudaMemsetAsync(cnt + j * (n + 1) + n, 0, sizeof(int), s), "memset");
+        trace::exclusive_scan(cnt + j * (n + 1), off + j * (n + 1), (int)(n + 1), c->cub_tmp.p, c->cub_tmp.cap, s);
+        ck(c, cudaGetLastError(), "scan");
+    }
+    std::vector<int> t(k);
+    for (int j = 0; j < k; ++j)
+        ck(c, cudaMemcpyAsync(&t[j], off + j * (n + 1) + n, sizeof(int), cudaMemcpyDeviceToHost, s), "copy totals");
+    ck(c, cudaStreamSynchronize(s), "sync");
+    for (int j = 0; j < k; ++j) {
+        if (t[j] < 0) fail(c, UPBP_ERR_CAPACITY, "traced record count overflows 32 bits");
+        totals[j] = t[j];
+    }
+}
+
+// After a write pass: every path wrote exactly the records its count pass sized.
+void check_trace_status(upbp_ctx* c, const char* pass)
+{
+    int st = 0;
+    ck(c, cudaMemcpyAsync(&st, c->tr_status.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, c->stream), pass);
+    ck(c, cudaStreamSynchronize(c->stream), pass);
+    if (st) fail(c, UPBP_ERR_CUDA, "%s: a path's write pass differed from its count pass", pass);
+}
+
+trace::TraceScene trace_scene(upbp_ctx* c, const upbp_scene* sc, uint32_t iteration)
+{
+    if (!sc) fail(c, UPBP_ERR_INVALID_ARG, "scene is NULL");
+    if (!c->have_params) fail(c, UPBP_ERR_INVALID_ARG, "upbp_set_params must precede the device-side passes");
+    trace::TraceScene S;
+    if (const char* e = trace::make_scene(*sc, c->P, iteration, &S)) fail(c, UPBP_ERR_INVALID_ARG, "scene: %s", e);
+    return S;
+}
+
+}  // namespace
+
+int upbp_trace_light_paths(upbp_ctx* c, const upbp_scene* sc, uint32_t iteration)
+{
+    return guarded(c, [&] {
+        drop_graph(c);
+        const trace::TraceScene S = trace_scene(c, sc, iteration);
+        const int64_t n = S.light_paths;
+        // every path holds at most max_path_length vertices and (max_path_length - 1) * 2 n_boxes beams
+        if (n * S.max_path_length * (2 * S.n_boxes) >= (int64_t)INT32_MAX)
+            fail(c, UPBP_ERR_CAPACITY, "too many light paths for 32-bit record offsets");
+        cudaStream_t s = c->stream;
+        ensure(c, c->tr_cnt, sizeof(int) * 2 * (n + 1));
+        ensure(c, c->tr_off, sizeof(int) * 2 * (n + 1));
+        trace::LightOut O{};
+        O.v_count = c->tr_cnt.as<int>();
+        O.b_count = O.v_count + (n + 1);
+        trace::launch_light(S, false, O, s);
+        ck(c, cudaGetLastError(), "light pass (count)");
+        int64_t tot[2];
+        trace_offsets(c, 2, n, tot);
+        const int64_t nv = tot[0], nb = tot[1];
+        ensure(c, c->lv_pos_in, sizeof(float) * 3 * nv);
+        ensure(c, c->lv_thr_in, sizeof(float) * 3 * nv);
+        ensure(c, c->lv_dir_in, sizeof(float) * 3 * nv);
+        ensure(c, c->lv_cont_in, sizeof(float) * nv);
+        ensure(c, c->lv_pidx_in, sizeof(int32_t) * nv);
+        ensure(c, c->lv_plen_in, sizeof(int32_t) * nv);
+        ensure(c, c->lv_med_in, sizeof(int32_t) * nv);
+        ensure(c, c->lv_flags_in, sizeof(uint32_t) * nv);
+        ensure(c, c->lv_mis, sizeof(upbp_mis) * nv);
+        ensure(c, c->path_ends, sizeof(int32_t) * n);
+        ensure(c, c->b_origin, sizeof(float) * 3 * nb);
+        ensure(c, c->b_dir, sizeof(float) * 3 * nb);
+        ensure(c, c->b_len, sizeof(float) * nb);
+        ensure(c, c->b_thr_in, sizeof(float) * 3 * nb);
+        ensure(c, c->b_flags_in, sizeof(uint32_t) * nb);
+        ensure(c, c->b_rsp_in, sizeof(float) * nb);
+        ensure(c, c->b_rsr_in, sizeof(float) * nb);
+        ensure(c, c->b_rsf_in, sizeof(uint32_t) * nb);
+        ensure(c, c->b_lpw_in, sizeof(float) * nb);
+        ensure(c, c->b_med_in, sizeof(int32_t) * nb);
+        ensure(c, c->b_lv_in, sizeof(int32_t) * nb);
+        O.v_off = c->tr_off.as<int>();
+        O.b_off = O.v_off + (n + 1);
+        O.pos = c->lv_pos_in.as<float>();
+        O.thr = c->lv_thr_in.as<float>();
+        O.dir = c->lv_dir_in.as<float>();
+        O.cont = c->lv_cont_in.as<float>();
+        O.pidx = c->lv_pidx_in.as<int>();
+        O.plen = c->lv_plen_in.as<int>();
+        O.med = c->lv_med_in.as<int>();
+        O.flags = c->lv_flags_in.as<uint32_t>();
+        O.mis = c->lv_mis.as<upbp_mis>();
+        O.path_ends = c->path_ends.as<int>();
+        O.b_origin = c->b_origin.as<float>();
+        O.b_dir = c->b_dir.as<float>();
+        O.b_len = c->b_len.as<float>();
+        O.b_thr = c->b_thr_in.as<float>();
+        O.b_flags = c->b_flags_in.as<uint32_t>();
+        O.b_rsp = c->b_rsp_in.as<float>();
+        O.b_rsr = c->b_rsr_in.as<float>();
+        O.b_rsf = c->b_rsf_in.as<uint32_t>();
+        O.b_lpw = c->b_lpw_in.as<float>();
+        O.b_med = c->b_med_in.as<int>();
+        O.b_lv = c->b_lv_in.as<int>();
+        ensure(c, c->tr_status, sizeof(int));
+        ck(c, cudaMemsetAsync(c->tr_status.p, 0, sizeof(int), s), "memset");
+        O.status = c->tr_status.as<int>();
+        trace::launch_light(S, true, O, s);
+        ck(c, cudaGetLastError(), "light pass (write)");
+        check_trace_status(c, "light pass");
+        c->n_lv = nv;
+        c->n_paths = (int32_t)n;
+        c->n_beams = nb;
+        c->built = false;
+    });
+}
+
+int upbp_trace_camera_paths(upbp_ctx* c, const upbp_scene* sc, uint32_t iteration)
+{
+    return guarded(c, [&] {
+        drop_graph(c);
+        const trace::TraceScene S = trace_scene(c, sc, iteration);
+        const int64_t n = (int64_t)S.width * S.height;
+        // per pixel at most max_path_length segment queries of 2 n_boxes segments, and camera
+        // records sum over L of (2 L + 1)
+        const int64_t per_pixel = (int64_t)S.max_path_length * (2 * S.n_boxes + 2 * S.max_path_length + 2);
+        if (n * per_pixel >= (int64_t)INT32_MAX)
+            fail(c, UPBP_ERR_CAPACITY, "too many pixels for 32-bit record offsets");
+        cudaStream_t s = c->stream;
+        ensure(c, c->tr_cnt, sizeof(int) * 4 * (n + 1));
+        ensure(c, c->tr_off, sizeof(int) * 4 * (n + 1));
+        trace::CameraOut O{};
+        O.q_count = c->tr_cnt.as<int>();
+        O.s_count = O.q_count + (n + 1);
+        O.p_count = O.s_count + (n + 1);
+        O.c_count = O.p_count + (n + 1);
+        trace::launch_camera(S, false, O, s);
+        ck(c, cudaGetLastError(), "camera pass (count)");
+        int64_t tot[4];
+        trace_offsets(c, 4, n, tot);
+        const int64_t nq = tot[0], ns = tot[1], np = tot[2], nc = tot[3];
+        ensure(c, c->sq_origin, sizeof(float) * 3 * nq);
+        ensure(c, c->sq_dir, sizeof(float) * 3 * nq);
+        ensure(c, c->sq_seg_begin, sizeof(int32_t) * nq);
+        ensure(c, c->sq_seg_count, sizeof(int32_t) * nq);
+        ensure(c, c->sq_flags, sizeof(uint32_t) * nq);
+        ensure(c, c->sq_plen, sizeof(int32_t) * nq);
+        ensure(c, c->sq_lpw, sizeof(float) * nq);
+        ensure(c, c->sq_thr, sizeof(float) * 3 * nq);
+        ensure(c, c->sq_pixel, sizeof(int32_t) * nq);
+        ensure(c, c->sq_cam_begin, sizeof(int64_t) * nq);
+        ensure(c, c->seg_dmin, sizeof(float) * ns);
+        ensure(c, c->seg_dmax, sizeof(float) * ns);
+        ensure(c, c->seg_pdf, sizeof(float) * ns);
+        ensure(c, c->seg_rev, sizeof(float) * ns);
+        ensure(c, c->seg_att, sizeof(float) * 3 * ns);
+        ensure(c, c->seg_med, sizeof(int32_t) * ns);
+        ensure(c, c->pq_pos, sizeof(float) * 3 * np);
+        ensure(c, c->pq_dir, sizeof(float) * 3 * np);
+        ensure(c, c->pq_med, sizeof(int32_t) * np);
+        ensure(c, c->pq_plen, sizeof(int32_t) * np);
+        ensure(c, c->pq_thr, sizeof(float) * 3 * np);
+        ensure(c, c->pq_pixel, sizeof(int32_t) * np);
+        ensure(c, c->pq_cam_begin, sizeof(int64_t) * np);
+        ensure(c, c->cam_mis, sizeof(upbp_mis) * nc);
+        O.q_off = c->tr_off.as<int>();
+        O.s_off = O.q_off + (n + 1);
+        O.p_off = O.s_off + (n + 1);
+        O.c_off = O.p_off + (n + 1);
+        O.sq_origin = c->sq_origin.as<float>();
+        O.sq_dir = c->sq_dir.as<float>();
+        O.sq_seg_begin = c->sq_seg_begin.as<int>();
+        O.sq_seg_count = c->sq_seg_count.as<int>();
+        O.sq_flags = c->sq_flags.as<uint32_t>();
+        O.sq_plen = c->sq_plen.as<int>();
+        O.sq_lpw = c->sq_lpw.as<float>();
+        O.sq_thr = c->sq_thr.as<float>();
+        O.sq_pixel = c->sq_pixel.as<int>();
+        O.sq_cam_begin = c->sq_cam_begin.as<int64_t>();
+        O.seg_dmin = c->seg_dmin.as<float>();
+        O.seg_dmax = c->seg_dmax.as<float>();
+        O.seg_pdf = c->seg_pdf.as<float>();
+        O.seg_rev = c->seg_rev.as<float>();
+        O.seg_att = c->seg_att.as<float>();
+        O.seg_med = c->seg_med.as<int>();
+        O.pq_pos = c->pq_pos.as<float>();
+        O.pq_dir = c->pq_dir.as<float>();
+        O.pq_med = c->pq_med.as<int>();
+        O.pq_plen = c->pq_plen.as<int>();
+        O.pq_thr = c->pq_thr.as<float>();
+        O.pq_pixel = c->pq_pixel.as<int>();
+        O.pq_cam_begin = c->pq_cam_begin.as<int64_t>();
+        O.cam = c->cam_mis.as<upbp_mis>();
+        ensure(c, c->tr_status, sizeof(int));
+        ck(c, cudaMemsetAsync(c->tr_status.p, 0, sizeof(int), s), "memset");
+        O.status = c->tr_status.as<int>();
+        trace::launch_camera(S, true, O, s);
+        ck(c, cudaGetLastError(), "camera pass (write)");
+        check_trace_status(c, "camera pass");
+        c->n_sq = nq;
+        c->n_seg = ns;
+        c->n_pq = np;
+        c->n_cam = nc;
+    });
+}
+
+int upbp_read_input(upbp_ctx* c, const char* name, void* dst, int64_t capacity, int64_t* bytes)
+{
+    return guarded(c, [&] {
+        if (!name) fail(c, UPBP_ERR_INVALID_ARG, "name is NULL");
+        struct Entry {
+            const char* name;
+            DBuf* buf;
+            int64_t bytes;
+        };
+        const int64_t nv = c->n_lv, nb = c->n_beams, nq = c->n_sq, ns = c->n_seg, np = c->n_pq;
+        const Entry table[] = {
+            {"lv_position", &c->lv_pos_in, 12 * nv}, {"lv_throughput", &c->lv_thr_in, 12 * nv},
+            {"lv_dir_fix", &c->lv_dir_in, 12 * nv}, {"lv_cont_prob", &c->lv_cont_in, 4 * nv},
+            {"lv_path_idx", &c->lv_pidx_in, 4 * nv}, {"lv_path_length", &c->lv_plen_in, 4 * nv},
+            {"lv_medium_id", &c->lv_med_in, 4 * nv}, {"lv_flags", &c->lv_flags_in, 4 * nv},
+            {"lv_mis", &c->lv_mis, (int64_t)sizeof(upbp_mis) * nv}, {"lv_path_ends", &c->path_ends, 4 * (int64_t)c->n_paths},
+            {"beam_origin", &c->b_origin, 12 * nb}, {"beam_direction", &c->b_dir, 12 * nb},
+            {"beam_length", &c->b_len, 4 * nb}, {"beam_throughput", &c->b_thr_in, 12 * nb},
+            {"beam_flags", &c->b_flags_in, 4 * nb}, {"beam_ray_sample_pdf", &c->b_rsp_in, 4 * nb},
+            {"beam_ray_sample_rev_pdf", &c->b_rsr_in, 4 * nb}, {"beam_ray_sampling_flags", &c->b_rsf_in, 4 * nb},
+            {"beam_last_pdf_w_inv", &c->b_lpw_in, 4 * nb}, {"beam_medium_id", &c->b_med_in, 4 * nb},
+            {"beam_light_vertex", &c->b_lv_in, 4 * nb}, {"cam_mis", &c->cam_mis, (int64_t)sizeof(upbp_mis) * c->n_cam},
+            {"sq_origin", &c->sq_origin, 12 * nq}, {"sq_direction", &c->sq_dir, 12 * nq},
+            {"sq_seg_begin", &c->sq_seg_begin, 4 * nq}, {"sq_seg_count", &c->sq_seg_count, 4 * nq},
+            {"sq_flags", &c->sq_flags, 4 * nq}, {"sq_path_length", &c->sq_plen, 4 * nq},
+            {"sq_last_pdf_w_inv", &c->sq_lpw, 4 * nq}, {"sq_throughput", &c->sq_thr, 12 * nq},
+            {"sq_pixel", &c->sq_pixel, 4 * nq}, {"sq_cam_mis_begin", &c->sq_cam_begin, 8 * nq},
+            {"seg_dist_min", &c->seg_dmin, 4 * ns}, {"seg_dist_max", &c->seg_dmax, 4 * ns},
+            {"seg_pdf", &c->seg_pdf, 4 * ns}, {"seg_rev_pdf", &c->seg_rev, 4 * ns},
+            {"seg_attenuation", &c->seg_att, 12 * ns}, {"seg_medium", &c->seg_med, 4 * ns},
+            {"pq_position", &c->pq_pos, 12 * np}, {"pq_dir_fix", &c->pq_dir, 12 * np},
+            {"pq_medium_id", &c->pq_med, 4 * np}, {"pq_path_length", &c->pq_plen, 4 * np},
+            {"pq_throughput", &c->pq_thr, 12 * np}, {"pq_pixel", &c->pq_pixel, 4 * np},
+            {"pq_cam_mis_begin", &c->pq_cam_begin, 8 * np},
+        };
+        for (const Entry& e : table) {
+            if (std::strcmp(e.name, name) != 0) continue;
+            if (bytes) *bytes = e.bytes;
+            if (!dst || e.bytes == 0) return;
+            if (capacity < e.bytes) fail(c, UPBP_ERR_INVALID_ARG, "%s needs %lld bytes", name, (long long)e.bytes);
+            ck(c, cudaMemcpyAsync(dst, e.buf->p, (size_t)e.bytes, cudaMemcpyDefault, c->stream), name);
+            ck(c, cudaStreamSynchronize(c->stream), "sync");
+            return;
+        }
+        fail(c, UPBP_ERR_INVALID_ARG, "unknown input array %s", name);
     });
 }
 

@@ -36,8 +36,27 @@ EXPORTS = (
     "upbp_read_segment_results", "upbp_read_point_results", "upbp_read_query_stats", "upbp_clear_image",
     "upbp_read_image", "upbp_last_launch_count", "upbp_last_timings", "upbp_destroy_structures",
     "upbp_read_tested_counts", "upbp_adjoint", "upbp_device_bytes", "upbp_capture_graph", "upbp_launch_graph",
-    "upbp_read_bp2d_results",
+    "upbp_read_bp2d_results", "upbp_trace_light_paths", "upbp_trace_camera_paths", "upbp_read_input",
 )
+
+# the record arrays of the C ABI: name -> (dtype, values per record); upbp_read_input reads them back
+INPUT_ARRAYS = {
+    "lv_position": ("<f4", 3), "lv_throughput": ("<f4", 3), "lv_dir_fix": ("<f4", 3), "lv_cont_prob": ("<f4", 0),
+    "lv_path_idx": ("<i4", 0), "lv_path_length": ("<i4", 0), "lv_medium_id": ("<i4", 0), "lv_flags": ("<u4", 0),
+    "lv_mis": (None, 0), "lv_path_ends": ("<i4", 0),
+    "beam_origin": ("<f4", 3), "beam_direction": ("<f4", 3), "beam_length": ("<f4", 0),
+    "beam_throughput": ("<f4", 3), "beam_flags": ("<u4", 0), "beam_ray_sample_pdf": ("<f4", 0),
+    "beam_ray_sample_rev_pdf": ("<f4", 0), "beam_ray_sampling_flags": ("<u4", 0),
+    "beam_last_pdf_w_inv": ("<f4", 0), "beam_medium_id": ("<i4", 0), "beam_light_vertex": ("<i4", 0),
+    "cam_mis": (None, 0),
+    "sq_origin": ("<f4", 3), "sq_direction": ("<f4", 3), "sq_seg_begin": ("<i4", 0), "sq_seg_count": ("<i4", 0),
+    "sq_flags": ("<u4", 0), "sq_path_length": ("<i4", 0), "sq_last_pdf_w_inv": ("<f4", 0),
+    "sq_throughput": ("<f4", 3), "sq_pixel": ("<i4", 0), "sq_cam_mis_begin": ("<i8", 0),
+    "seg_dist_min": ("<f4", 0), "seg_dist_max": ("<f4", 0), "seg_pdf": ("<f4", 0), "seg_rev_pdf": ("<f4", 0),
+    "seg_attenuation": ("<f4", 3), "seg_medium": ("<i4", 0),
+    "pq_position": ("<f4", 3), "pq_dir_fix": ("<f4", 3), "pq_medium_id": ("<i4", 0), "pq_path_length": ("<i4", 0),
+    "pq_throughput": ("<f4", 3), "pq_pixel": ("<i4", 0), "pq_cam_mis_begin": ("<i8", 0),
+}
 
 
 class UpbpError(RuntimeError):
@@ -88,6 +107,9 @@ def lib():
         l.upbp_capture_graph.argtypes = [vp]
         l.upbp_read_bp2d_results.argtypes = [vp, abi.f32p, abi.u32p, abi.u64p]
         l.upbp_launch_graph.argtypes = [vp]
+        l.upbp_trace_light_paths.argtypes = [vp, C.POINTER(abi.Scene), C.c_uint32]
+        l.upbp_trace_camera_paths.argtypes = [vp, C.POINTER(abi.Scene), C.c_uint32]
+        l.upbp_read_input.argtypes = [vp, C.c_char_p, vp, C.c_int64, C.POINTER(C.c_int64)]
         for name in EXPORTS:
             if name != "upbp_last_error":
                 getattr(l, name).restype = C.c_int
@@ -175,6 +197,44 @@ class EstimatorStage:
         self._ck(self._l.upbp_set_point_queries(self._ctx, C.byref(s["pq"])))
         self._nq = s["sq"].n
         self._np = s["pq"].n
+
+    def trace(self, cfg, iteration: int = 0):
+        """The light and camera passes of iteration ``iteration`` of scene ``cfg`` (a
+        :class:`workload.SceneConfig`) on the device: sets the media and params as the host
+        generator does, then traces the light sub-paths and the camera sub-paths into the context.
+        Follow with :meth:`build`, :meth:`clear_image` and :meth:`evaluate`."""
+        from . import workload as W
+        media, params = W.stage_constants(cfg, iteration)
+        self.set_media(media)
+        prm = abi.Params.from_buffer_copy(np.ascontiguousarray(params).tobytes())
+        self._params_keep = prm
+        self._ck(self._l.upbp_set_params(self._ctx, C.byref(prm)))
+        sc = abi.scene_struct(cfg)
+        self._ck(self._l.upbp_trace_light_paths(self._ctx, C.byref(sc), iteration))
+        self._ck(self._l.upbp_trace_camera_paths(self._ctx, C.byref(sc), iteration))
+        self._npix = cfg.width * cfg.height
+        self._nq = self.input_bytes("sq_pixel") // 4
+        self._np = self.input_bytes("pq_pixel") // 4
+        return self
+
+    def input_bytes(self, name: str) -> int:
+        n = C.c_int64()
+        self._ck(self._l.upbp_read_input(self._ctx, name.encode(), None, 0, C.byref(n)))
+        return n.value
+
+    def read_inputs(self, names=None) -> Dict[str, np.ndarray]:
+        """Copy stored input arrays back (as the workload dict names and shapes them)."""
+        from .workload import MIS_DTYPE
+        out = {}
+        for name in names or INPUT_ARRAYS:
+            dt, width = INPUT_ARRAYS[name]
+            dtype = MIS_DTYPE if dt is None else np.dtype(dt)
+            nbytes = self.input_bytes(name)
+            a = np.zeros(nbytes // dtype.itemsize, dtype)
+            if nbytes:
+                self._ck(self._l.upbp_read_input(self._ctx, name.encode(), C.c_void_p(a.ctypes.data), nbytes, None))
+            out[name] = a.reshape(-1, width) if width else a
+        return out
 
     def clear_image(self):
         self._ck(self._l.upbp_clear_image(self._ctx))

@@ -16,6 +16,19 @@ camera passes (``UPBP.hxx:600-645, 940-975, 1908-1969``).
 No public dataset is involved; the inputs are generated from a Philox
 counter-based generator with a fixed seed.  Both the oracle and the CUDA path
 consume the same arrays (layout of ``include/upbp_gpu.h``).
+
+Random numbers are per path: Philox4x64-10 (Salmon et al., "Parallel random
+numbers: as easy as 1, 2, 3", SC'11) with key (seed, iteration) and counter
+(path or pixel index, bounce, block, stream) gives four uniforms
+``(x >> 11) * 2^-53`` per counter.  Light path p: the emission draws are block 0
+of bounce 0 (position x, position z, two direction samples); the ray of bounce L
+(from vertex L-1) takes its free-flight draws for medium segment k from block
+1 + k // 4, word k % 4, and the scattering at vertex L its phase-function and
+Russian-roulette draws from block 0, words 0-2.  Camera path of pixel p: the
+pixel jitter is block 0 of bounce 0, words 0-1; bounces as for light paths.
+Every path therefore draws the same numbers whatever the others do, and the
+device-side light and camera passes (``upbp_trace_light_paths`` /
+``upbp_trace_camera_paths``) trace the same paths.
 """
 from __future__ import annotations
 
@@ -61,6 +74,52 @@ PARAMS_DTYPE = np.dtype(list(PARAMS_FIELDS))
 
 EPS_COSINE = 1e-6
 INV_PI = 1.0 / math.pi
+
+
+LIGHT_STREAM, CAMERA_STREAM = 0, 1
+_PHILOX_M = (np.uint64(0xD2E7470EE14C6C93), np.uint64(0xCA5A826395121157))
+_PHILOX_W = (np.uint64(0x9E3779B97F4A7C15), np.uint64(0xBB67AE8584CAA73B))
+_MASK32 = np.uint64(0xFFFFFFFF)
+_S32 = np.uint64(32)
+
+
+def _mulhilo64(a: np.ndarray, b: np.uint64):
+    """(high, low) 64-bit halves of the 128-bit product a * b, elementwise."""
+    a0, a1 = a & _MASK32, a >> _S32
+    b0, b1 = b & _MASK32, b >> _S32
+    p00, p01, p10, p11 = a0 * b0, a0 * b1, a1 * b0, a1 * b1
+    mid = (p00 >> _S32) + (p01 & _MASK32) + (p10 & _MASK32)
+    return p11 + (p01 >> _S32) + (p10 >> _S32) + (mid >> _S32), a * b
+
+
+def philox4x64(counter, key):
+    """Philox4x64-10 block function: counter = 4 uint64 arrays, key = 2 uint64 -> 4 uint64 arrays."""
+    c = [np.asarray(x, np.uint64) for x in counter]
+    k0, k1 = np.uint64(key[0]), np.uint64(key[1])
+    with np.errstate(over="ignore"):
+        for rnd in range(10):
+            if rnd:
+                k0, k1 = k0 + _PHILOX_W[0], k1 + _PHILOX_W[1]
+            hi0, lo0 = _mulhilo64(c[0], _PHILOX_M[0])
+            hi1, lo1 = _mulhilo64(c[2], _PHILOX_M[1])
+            c = [hi1 ^ c[1] ^ k0, lo1, hi0 ^ c[3] ^ k1, lo0]
+    return c
+
+
+def uniforms(key, stream: int, ids: np.ndarray, bounce: int, block: int) -> np.ndarray:
+    """(n, 4) uniforms in [0, 1) of counter (ids, bounce, block, stream) under key (seed, iteration)."""
+    ids = np.asarray(ids, np.uint64)
+    z = np.zeros_like(ids)
+    words = philox4x64((ids, z + np.uint64(bounce), z + np.uint64(block), z + np.uint64(stream)), key)
+    return np.stack([(w >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0) for w in words], axis=1)
+
+
+def flight_uniforms(key, stream: int, ids: np.ndarray, bounce: int, n_segments: int) -> np.ndarray:
+    """(n, n_segments) free-flight uniforms of one bounce: segment k is word k % 4 of block 1 + k // 4."""
+    blocks = [uniforms(key, stream, ids, bounce, 1 + b) for b in range((n_segments + 3) // 4)]
+    if not blocks:
+        return np.zeros((len(ids), 0))
+    return np.concatenate(blocks, axis=1)[:, :n_segments]
 
 
 @dataclasses.dataclass
@@ -197,12 +256,13 @@ def _medium_at(cfg: SceneConfig, p: np.ndarray) -> np.ndarray:
     return m
 
 
-def _trace(cfg: SceneConfig, rng: np.random.Generator, o: np.ndarray, d: np.ndarray, origin_in_medium: np.ndarray):
+def _trace(cfg: SceneConfig, u: np.ndarray, o: np.ndarray, d: np.ndarray, origin_in_medium: np.ndarray):
     """Scene::Intersect for imaginary-boundary media, vectorised over rays.
 
     The ray is split at every box face into medium segments; a free-flight distance is sampled in
     each scattering medium in order (HomogeneousMedium::SampleRay, Scene/Media.hxx:240-290) until
-    one scatters.  Returns a dict of (n, K) arrays: ``full`` marks the VolumeSegments (up to the
+    one scatters; ``u`` (n, K) holds the free-flight uniforms of the K possible segments.  Returns
+    a dict of (n, K) arrays: ``full`` marks the VolumeSegments (up to the
     scattering point, clear-medium segments included), ``lite`` the LiteVolumeSegments (every
     scattering medium on the ray), with distances, pdfs, attenuation and medium ids, plus the
     scattering distance per ray (inf when the ray leaves the scene).
@@ -220,7 +280,7 @@ def _trace(cfg: SceneConfig, rng: np.random.Generator, o: np.ndarray, d: np.ndar
     st_tab = np.array([m.sigma_t for m in cfg.media])                 # (M, 3)
     smin_tab = np.array([m.min_pos_sigma_t for m in cfg.media])
     scat_tab = np.array([m.has_scattering for m in cfg.media])
-    u = rng.random((n, K))
+    assert u.shape == (n, K)
     np.seterr(invalid="ignore")
     alive = np.ones(n, bool)
     full = np.zeros((n, K), bool)
@@ -256,10 +316,8 @@ def _trace(cfg: SceneConfig, rng: np.random.Generator, o: np.ndarray, d: np.ndar
                 lite=lite, scatter_t=scatter_t)
 
 
-def _hg_sample(rng: np.random.Generator, wfix: np.ndarray, g: np.ndarray):
+def _hg_sample(u1: np.ndarray, u2: np.ndarray, wfix: np.ndarray, g: np.ndarray):
     """PhaseFunction::Sample (Path/PhaseFunction.hxx:82-137): returns (direction, pdf, sinTheta)."""
-    n = wfix.shape[0]
-    u1, u2 = rng.random(n), rng.random(n)
     iso = np.abs(g) < 1e-3
     g2 = g * g
     twog = g + g
@@ -331,7 +389,7 @@ def _last_full_medium(tr, sel: np.ndarray) -> np.ndarray:
 
 def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     """Run the light and camera passes of one iteration and return the estimator-stage inputs."""
-    rng = np.random.Generator(np.random.Philox(key=cfg.seed + iteration))
+    key = (cfg.seed, iteration)
     k = iteration_constants(cfg, iteration)
     tech = cfg.techniques
     merge_pb2d = bool(tech & PB2D)
@@ -347,9 +405,10 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     area = cfg.light_size * cfg.light_size
     lo_box, hi_box = np.asarray(cfg.boxes[0][0], float), np.asarray(cfg.boxes[0][1], float)
     cx, cz = 0.5 * (lo_box[0] + hi_box[0]), 0.5 * (lo_box[2] + hi_box[2])
-    pos0 = np.stack([cx - half + cfg.light_size * rng.random(NL), np.full(NL, hi_box[1]),
-                     cz - half + cfg.light_size * rng.random(NL)], axis=1)
-    u1, u2 = rng.random(NL), rng.random(NL)
+    ue = uniforms(key, LIGHT_STREAM, np.arange(NL), 0, 0)
+    pos0 = np.stack([cx - half + cfg.light_size * ue[:, 0], np.full(NL, hi_box[1]),
+                     cz - half + cfg.light_size * ue[:, 1]], axis=1)
+    u1, u2 = ue[:, 2], ue[:, 3]
     r_ = np.sqrt(u1)
     phi = 2 * math.pi * u2
     cos_l = np.maximum(np.sqrt(np.maximum(0.0, 1 - u1)), EPS_COSINE)   # SampleCosHemisphereW around -y
@@ -380,7 +439,7 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     L = 1
     while act.size and maxL > 1:
         o, d = origin[act], direction[act]
-        tr = _trace(cfg, rng, o, d, oim[act])
+        tr = _trace(cfg, flight_uniforms(key, LIGHT_STREAM, act, L, 2 * len(cfg.boxes)), o, d, oim[act])
         K = tr["K"]
         # ---- UPBP::AddBeams (UPBP.hxx:1783-1870) for the ray of this segment
         bl = []
@@ -474,8 +533,9 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
             break
         # ---- SampleScattering (UPBP.hxx:1908-1969): HG direction, Russian roulette
         gvals = T["g"][mid[rows]]
-        wnew, pdfw, sin_t = _hg_sample(rng, -d[sc[rows]], gvals)
-        rr = rng.random(rows.size)
+        us = uniforms(key, LIGHT_STREAM, pth[rows], L, 0)
+        wnew, pdfw, sin_t = _hg_sample(us[:, 0], us[:, 1], -d[sc[rows]], gvals)
+        rr = us[:, 2]
         cont = T["cont"][mid[rows]]
         keep = ~((cont == 0) | ((cont < 1) & (rr > cont)))
         rows, wnew, pdfw, sin_t, cont = rows[keep], wnew[keep], pdfw[keep], sin_t[keep], cont[keep]
@@ -532,12 +592,19 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
                           ("last_pdf_w_inv", np.float32, 0), ("medium_id", np.int32, 0), ("light_vertex", np.int32, 0)):
             out["beam_" + f] = np.zeros((0, 3) if sh else 0, dt)
 
-    _camera_pass(cfg, rng, k, T, out)
+    _camera_pass(cfg, key, k, T, out)
+    out["media"], out["params"] = stage_constants(cfg, iteration)
+    return out
 
+
+def stage_constants(cfg: SceneConfig, iteration: int = 0):
+    """The media table and the per-iteration params of the estimator stage (no tracing)."""
+    k = iteration_constants(cfg, iteration)
+    tech = cfg.techniques
+    NL = cfg.light_paths
     med = np.zeros(len(cfg.media), MEDIUM_DTYPE)
     for mi, m in enumerate(cfg.media):
         med[mi] = (m.absorption, m.scattering, m.mean_cosine, m.continuation_prob)
-    out["media"] = med
     prm = np.zeros(1, PARAMS_DTYPE)
     prm["techniques"] = tech
     prm["query_beam_type"] = cfg.query_beam_type
@@ -559,14 +626,14 @@ def generate(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     prm["image_height"] = cfg.height
     prm["pb2d_knn"] = cfg.pb2d_knn
     prm["bb1d_knn"] = cfg.bb1d_knn
-    out["params"] = prm
-    return out
+    return med, prm
 
 
-def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float], T, out: Dict[str, np.ndarray]):
+def _camera_pass(cfg: SceneConfig, key, k: Dict[str, float], T, out: Dict[str, np.ndarray]):
     """Camera sub-paths (UPBP.hxx:742-1160): one segment query per traced ray that crosses a scattering
     medium and one PP3D point query per camera medium vertex, each with the snapshot of
-    mCameraVerticesMisData at the call."""
+    mCameraVerticesMisData at the call.  The records are stored per pixel in call order: for
+    each camera path length L, the segment query, then the point query (and their snapshots)."""
     W_, H_ = cfg.width, cfg.height
     npix = W_ * H_
     tech = cfg.techniques
@@ -577,8 +644,9 @@ def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float]
     tan_half = math.tan(math.radians(cfg.fov_deg) * 0.5)
     ipd = W_ / (2.0 * tan_half)
     pix = np.arange(npix)
-    sx = (pix % W_ + rng.random(npix)) - W_ * 0.5
-    sy = (pix // W_ + rng.random(npix)) - H_ * 0.5
+    uj = uniforms(key, CAMERA_STREAM, pix, 0, 0)
+    sx = (pix % W_ + uj[:, 0]) - W_ * 0.5
+    sy = (pix // W_ + uj[:, 1]) - H_ * 0.5
     d_all = np.stack([sx, -sy, np.full(npix, ipd)], axis=1)
     d_all /= np.linalg.norm(d_all, axis=1, keepdims=True)
     cos_cam = d_all[:, 2]
@@ -599,9 +667,10 @@ def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float]
     CR: List[np.ndarray] = []
     n_cam = 0
     n_seg = 0
+    kstride = 2 * (maxL + 2)  # record order key: pixel, path length, segment before point query
     L = 1
     while act.size:
-        tr = _trace(cfg, rng, o, d, oim)
+        tr = _trace(cfg, flight_uniforms(key, CAMERA_STREAM, act, L, 2 * len(cfg.boxes)), o, d, oim)
         sc_mask = np.isfinite(tr["scatter_t"])
         use_lite = sc_mask & (cfg.query_beam_type == LONG_BEAM)
         seg_mask = np.where(use_lite[:, None], tr["lite"], tr["full"])
@@ -629,7 +698,7 @@ def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float]
             CR.append(snap)
             Q.append(dict(origin=o[qr], direction=d[qr], seg_begin=begin, seg_count=cnt, flags=qf,
                           path_length=np.full(qr.size, L), lpw=lpw[qr], thr=thr[qr], pixel=act[qr],
-                          cam_begin=n_cam + np.arange(qr.size) * L))
+                          cam_begin=n_cam + np.arange(qr.size) * L, key=act[qr].astype(np.int64) * kstride + 2 * L))
             n_cam += snap.size
         # scattering events: camera vertex in a medium
         sc = np.nonzero(sc_mask)[0]
@@ -670,11 +739,13 @@ def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float]
                 snap = table[sc[r], :L + 1].reshape(-1)
                 CR.append(snap)
                 PQ.append(dict(position=hit[r], dir_fix=-d[sc[r]], medium=mid[r], path_length=np.full(r.size, L),
-                               thr=nthr[r], pixel=act[sc[r]], cam_begin=n_cam + np.arange(r.size) * (L + 1)))
+                               thr=nthr[r], pixel=act[sc[r]], cam_begin=n_cam + np.arange(r.size) * (L + 1),
+                               key=act[sc[r]].astype(np.int64) * kstride + 2 * L + 1))
                 n_cam += snap.size
         # SampleScattering at the camera vertex
-        wnew, pdfw, sin_t = _hg_sample(rng, -d[sc], T["g"][mid])
-        rr = rng.random(sc.size)
+        us = uniforms(key, CAMERA_STREAM, act[sc], L, 0)
+        wnew, pdfw, sin_t = _hg_sample(us[:, 0], us[:, 1], -d[sc], T["g"][mid])
+        rr = us[:, 2]
         cont = T["cont"][mid]
         keep = ~((cont == 0) | ((cont < 1) & (rr > cont)))
         sc, mid, wnew, pdfw, sin_t, cont, hit = sc[keep], mid[keep], wnew[keep], pdfw[keep], sin_t[keep], cont[keep], hit[keep]
@@ -697,32 +768,51 @@ def _camera_pass(cfg: SceneConfig, rng: np.random.Generator, k: Dict[str, float]
 
     cat = lambda lst, f, dt: (np.concatenate([x[f] for x in lst]) if lst else np.zeros(0)).astype(dt)
     nq = sum(len(x["flags"]) for x in Q)
-    out["sq_origin"] = cat(Q, "origin", np.float32).reshape(nq, 3)
-    out["sq_direction"] = cat(Q, "direction", np.float32).reshape(nq, 3)
-    out["sq_seg_begin"] = cat(Q, "seg_begin", np.int32)
-    out["sq_seg_count"] = cat(Q, "seg_count", np.int32)
-    out["sq_flags"] = cat(Q, "flags", np.uint32)
-    out["sq_path_length"] = cat(Q, "path_length", np.int32)
-    out["sq_last_pdf_w_inv"] = cat(Q, "lpw", np.float32)
-    out["sq_throughput"] = cat(Q, "thr", np.float32).reshape(nq, 3)
-    out["sq_pixel"] = cat(Q, "pixel", np.int32)
-    out["sq_cam_mis_begin"] = cat(Q, "cam_begin", np.int64)
-    ns = sum(len(x["dmin"]) for x in S)
-    out["seg_dist_min"] = cat(S, "dmin", np.float32)
-    out["seg_dist_max"] = cat(S, "dmax", np.float32)
-    out["seg_pdf"] = cat(S, "pdf", np.float32)
-    out["seg_rev_pdf"] = cat(S, "rev", np.float32)
-    out["seg_attenuation"] = cat(S, "att", np.float32).reshape(ns, 3)
-    out["seg_medium"] = cat(S, "med", np.int32)
     npq = sum(len(x["pixel"]) for x in PQ)
-    out["pq_position"] = cat(PQ, "position", np.float32).reshape(npq, 3)
-    out["pq_dir_fix"] = cat(PQ, "dir_fix", np.float32).reshape(npq, 3)
-    out["pq_medium_id"] = cat(PQ, "medium", np.int32)
-    out["pq_path_length"] = cat(PQ, "path_length", np.int32)
-    out["pq_throughput"] = cat(PQ, "thr", np.float32).reshape(npq, 3)
-    out["pq_pixel"] = cat(PQ, "pixel", np.int32)
-    out["pq_cam_mis_begin"] = cat(PQ, "cam_begin", np.int64)
-    out["cam_mis"] = np.concatenate(CR) if CR else np.zeros(0, MIS_DTYPE)
+    # per-pixel call order (the records were produced bounce by bounce)
+    qkey, pqkey = cat(Q, "key", np.int64), cat(PQ, "key", np.int64)
+    oq, opq = np.argsort(qkey, kind="stable"), np.argsort(pqkey, kind="stable")
+    cam_all = np.concatenate(CR) if CR else np.zeros(0, MIS_DTYPE)
+    bkey = np.concatenate([qkey, pqkey])
+    blen = np.concatenate([cat(Q, "path_length", np.int64), cat(PQ, "path_length", np.int64) + 1])
+    bbeg = np.concatenate([cat(Q, "cam_begin", np.int64), cat(PQ, "cam_begin", np.int64)])
+    ob = np.argsort(bkey, kind="stable")
+    nb_sorted = np.concatenate([[0], np.cumsum(blen[ob])[:-1]]).astype(np.int64) if ob.size else np.zeros(0, np.int64)
+    new_beg = np.empty_like(nb_sorted)
+    new_beg[ob] = nb_sorted
+    out["cam_mis"] = cam_all[np.repeat(bbeg[ob] - nb_sorted, blen[ob]) + np.arange(int(blen.sum()))]
+    sbeg, scnt = cat(Q, "seg_begin", np.int64)[oq], cat(Q, "seg_count", np.int64)[oq]
+    nsb = np.concatenate([[0], np.cumsum(scnt)[:-1]]).astype(np.int64) if nq else np.zeros(0, np.int64)
+    sidx = np.repeat(sbeg - nsb, scnt) + np.arange(int(scnt.sum()))
+    qcat = lambda f, dt: cat(Q, f, dt)[oq]
+    q3 = lambda f: (np.concatenate([x[f] for x in Q])[oq] if Q else np.zeros((0, 3))).astype(np.float32).reshape(nq, 3)
+    out["sq_origin"] = q3("origin")
+    out["sq_direction"] = q3("direction")
+    out["sq_seg_begin"] = nsb.astype(np.int32)
+    out["sq_seg_count"] = scnt.astype(np.int32)
+    out["sq_flags"] = qcat("flags", np.uint32)
+    out["sq_path_length"] = qcat("path_length", np.int32)
+    out["sq_last_pdf_w_inv"] = qcat("lpw", np.float32)
+    out["sq_throughput"] = q3("thr")
+    out["sq_pixel"] = qcat("pixel", np.int32)
+    out["sq_cam_mis_begin"] = new_beg[:nq][oq].astype(np.int64)
+    ns = int(scnt.sum())
+    scat = lambda f, dt: cat(S, f, dt)[sidx]
+    out["seg_dist_min"] = scat("dmin", np.float32)
+    out["seg_dist_max"] = scat("dmax", np.float32)
+    out["seg_pdf"] = scat("pdf", np.float32)
+    out["seg_rev_pdf"] = scat("rev", np.float32)
+    out["seg_attenuation"] = (np.concatenate([x["att"] for x in S])[sidx] if S else np.zeros((0, 3))).astype(np.float32).reshape(ns, 3)
+    out["seg_medium"] = scat("med", np.int32)
+    pcat = lambda f, dt: cat(PQ, f, dt)[opq]
+    p3 = lambda f: (np.concatenate([x[f] for x in PQ])[opq] if PQ else np.zeros((0, 3))).astype(np.float32).reshape(npq, 3)
+    out["pq_position"] = p3("position")
+    out["pq_dir_fix"] = p3("dir_fix")
+    out["pq_medium_id"] = pcat("medium", np.int32)
+    out["pq_path_length"] = pcat("path_length", np.int32)
+    out["pq_throughput"] = p3("thr")
+    out["pq_pixel"] = pcat("pixel", np.int32)
+    out["pq_cam_mis_begin"] = new_beg[nq:][opq].astype(np.int64)
 
 
 # ----------------------------------------------------------------------------------------------
