@@ -17,6 +17,7 @@ Prints ONE JSON line on rank 0.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -53,6 +54,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-device-passes", action="store_true",
+                    help="skip the iteration traced on the device (light + camera passes, build, evaluate)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
     ap.add_argument("--no-graph", action="store_true", help="direct calls instead of the captured CUDA graph")
     ap.add_argument("--adjoint", action="store_true",
@@ -325,6 +328,11 @@ def run_b200(args, cfg, rank, world, local_rank):
                "ms_per_step": e_ms / args.steps}
         st.close()
 
+    # whole iteration on the device: light and camera passes, build, evaluate, image read back
+    device_passes = None
+    if not args.no_device_passes and cfg.name != "beamstress":
+        device_passes = run_device_passes(args, cfg, dev, mode, stream, tuning, npix, rank, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(works[0], args.cpu_seconds)
@@ -370,8 +378,56 @@ def run_b200(args, cfg, rank, world, local_rank):
         "gpu_launches": int(sum(launches)),
         "clocks": clock,
         "generate_s": gen_s,
+        "device_passes": device_passes,
     }
     return line
+
+
+def run_device_passes(args, cfg, dev, mode, stream, tuning, npix, rank, world):
+    """Iterations traced on the device (upbp_trace_light_paths + upbp_trace_camera_paths), then
+    built and evaluated, the framebuffer read back to page-locked host memory: the estimator
+    stage with no host-side generation and no upload."""
+    import torch
+    from smallupbp_b200 import engine
+    st = engine.EstimatorStage(dev, mode)
+    st.set_stream(stream.cuda_stream)
+    st.set_tuning(**tuning["best"])
+    host_img = torch.empty(npix * 3, dtype=torch.float32).pin_memory()
+    n_it = max(1, args.iterations)
+    queries = []
+    with torch.cuda.stream(stream):
+        for i in range(max(1, args.warmup)):
+            st.trace(cfg, rank + world * (i % n_it)); st.build(); st.clear_image(); st.evaluate()
+            st.read_image_into(host_img.data_ptr())
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        trace_ms = 0.0
+        ev[0].record(stream)
+        for i in range(args.steps):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            st.trace(cfg, rank + world * (i % n_it))
+            t1.record(stream)
+            st.build(); st.clear_image(); st.evaluate()
+            st.read_image_into(host_img.data_ptr())
+            queries.append(st._nq + st._np)
+            torch.cuda.synchronize()
+            trace_ms += t0.elapsed_time(t1)
+        ev[1].record(stream)
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1])
+    st.close()
+    if world > 1:
+        from smallupbp_b200 import multi
+        ms = multi.max_over_ranks(ms, "cuda")
+    from smallupbp_b200 import abi
+    scene_bytes = ctypes.sizeof(abi.Scene) + ctypes.sizeof(abi.Params) + len(cfg.media) * ctypes.sizeof(abi.Medium)
+    return {"value": sum(queries) * world / (ms / 1000.0), "unit": "queries/s", "ms_per_iteration": ms / args.steps,
+            "trace_ms_per_iteration": trace_ms / args.steps, "h2d_bytes_per_step": scene_bytes,
+            "d2h_bytes_per_step": npix * 3 * 4,
+            "note": "light and camera sub-paths traced on the GPU (the host generator's records, bit for bit), "
+                    "then build + evaluate; only the scene description and params cross from the host"}
 
 
 def cpu_baseline(w, seconds: float) -> dict:
