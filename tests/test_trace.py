@@ -156,3 +156,14 @@ def test_traced_iteration_evaluates_like_the_uploaded_one(mode):
     for a, b, what in zip(seg, want_seg, ("PB2D", "BB1D")):
         G.assert_close(a, b, what)
     assert G.image_rel_l2(img, want_img) < 1e-5
+
+
+@pytest.mark.gpu
+def test_device_passes_at_full_size():
+    """cube512 (262,144 light paths, 512x512 pixels): every array as the generator's."""
+    cfg = W.config("cube512")
+    want = W.generate(cfg, 2)
+    with engine.EstimatorStage(0, engine.MODE_MIXED) as st:
+        got = st.trace(cfg, 2).read_inputs()
+    assert len(got["lv_path_idx"]) > 300_000 and len(got["sq_pixel"]) > 200_000
+    compare_inputs(got, want, LIGHT + CAMERA)
