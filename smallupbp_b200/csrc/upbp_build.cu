@@ -54,32 +54,6 @@ __global__ void k_bbox_partial(const float4* __restrict__ pts, const int32_t* __
         for (int c = 0; c < 6; ++c) partial[6 * blockIdx.x + c] = s[c][0];
 }
 
-__global__ void k_bbox_boxes_partial(const Box* __restrict__ boxes, int n, float* partial)
-{
-    __shared__ float s[6][kThreads];
-    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const Box b = boxes[i];
-        for (int c = 0; c < 3; ++c) {
-            const float m = 0.5f * (b.lo[c] + b.hi[c]);
-            lo[c] = fminf(lo[c], m);
-            hi[c] = fmaxf(hi[c], m);
-        }
-    }
-    for (int c = 0; c < 3; ++c) { s[c][threadIdx.x] = lo[c]; s[3 + c][threadIdx.x] = hi[c]; }
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w)
-            for (int c = 0; c < 3; ++c) {
-                s[c][threadIdx.x] = fminf(s[c][threadIdx.x], s[c][threadIdx.x + w]);
-                s[3 + c][threadIdx.x] = fmaxf(s[3 + c][threadIdx.x], s[3 + c][threadIdx.x + w]);
-            }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        for (int c = 0; c < 6; ++c) partial[6 * blockIdx.x + c] = s[c][0];
-}
-
 __global__ void k_bbox_final(const float* partial, int blocks, float* out)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -154,14 +128,6 @@ __global__ void k_morton_points(const float4* __restrict__ lv_pos, const int32_t
     if (i >= n) return;
     const float4 p = lv_pos[ph_lv[i]];
     codes[i] = morton3(p.x, p.y, p.z, bbox);
-}
-
-__global__ void k_morton_boxes(const Box* __restrict__ boxes, int n, const float* __restrict__ bbox, uint32_t* codes)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const Box b = boxes[i];
-    codes[i] = morton3(0.5f * (b.lo[0] + b.hi[0]), 0.5f * (b.lo[1] + b.hi[1]), 0.5f * (b.lo[2] + b.hi[2]), bbox);
 }
 
 __global__ void k_gather_photons(const int32_t* __restrict__ lv_sorted, const float4* __restrict__ lv_pos, int n,
@@ -323,56 +289,102 @@ __device__ __forceinline__ float piece_t(int k, int cnt, float len)
     return k >= cnt ? len : __fmul_rn((float)k, __fdiv_rn(len, (float)cnt));
 }
 
-// rstart / rchange / r2max (KNN radii, or NULL for the constant radius): beam radius at t is
-// rstart + t * rchange, the predicate's bound is r2max (PhotonBeam.hxx:238-296, 411).
-__global__ void k_emit_pieces(const float* __restrict__ origin, const float* __restrict__ dir,
-                              const float* __restrict__ length, const int32_t* __restrict__ medium, int64_t n,
-                              const int32_t* __restrict__ offsets, float piece_len, float radius, float eps,
-                              const float* __restrict__ rstart, const float* __restrict__ rchange,
-                              const float* __restrict__ r2max, float4* pa, float4* pb, float4* pc, Box* boxes)
+// Beam of piece p: offsets (nb + 1 entries, every beam has at least one piece) are strictly
+// increasing, so the beam is the last one whose first piece is <= p.
+__device__ __forceinline__ int piece_beam(const int32_t* __restrict__ offsets, int64_t nb, int p)
 {
-    const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (b >= n) return;
+    int lo = 0, hi = (int)nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&offsets[mid]) <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Bounding box of the beam segments (both end points of every beam): the frame of the pieces'
+// Morton codes.
+__global__ void k_bbox_beams_partial(const float* __restrict__ origin, const float* __restrict__ dir,
+                                     const float* __restrict__ length, int64_t n, float* partial)
+{
+    __shared__ float s[6][kThreads];
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float len = length[i];
+        for (int c = 0; c < 3; ++c) {
+            const float a = origin[3 * i + c], b = a + dir[3 * i + c] * len;
+            lo[c] = fminf(lo[c], fminf(a, b));
+            hi[c] = fmaxf(hi[c], fmaxf(a, b));
+        }
+    }
+    for (int c = 0; c < 3; ++c) { s[c][threadIdx.x] = lo[c]; s[3 + c][threadIdx.x] = hi[c]; }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int c = 0; c < 3; ++c) {
+                s[c][threadIdx.x] = fminf(s[c][threadIdx.x], s[c][threadIdx.x + w]);
+                s[3 + c][threadIdx.x] = fmaxf(s[3 + c][threadIdx.x], s[3 + c][threadIdx.x + w]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 6; ++c) partial[6 * blockIdx.x + c] = s[c][0];
+}
+
+// Morton code of every piece's midpoint (one thread per piece); perm = the identity.
+__global__ void k_piece_codes(const float* __restrict__ origin, const float* __restrict__ dir,
+                              const float* __restrict__ length, int64_t nb, const int32_t* __restrict__ offsets,
+                              int np, const float* __restrict__ bbox, uint32_t* codes, int32_t* perm)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const int b = piece_beam(offsets, nb, p);
+    const int first = offsets[b], cnt = offsets[b + 1] - first, k = p - first;
+    const float len = length[b];
+    const float t0 = piece_t(k, cnt, len), t1 = piece_t(k + 1, cnt, len), tm = 0.5f * (t0 + t1);
+    codes[p] = morton3(origin[3 * b] + dir[3 * b] * tm, origin[3 * b + 1] + dir[3 * b + 1] * tm,
+                       origin[3 * b + 2] + dir[3 * b + 2] * tm, bbox);
+    perm[p] = p;
+}
+
+// The records of the pieces in Morton order (one thread per sorted position): piece perm[i] of
+// its beam, at position i.  rstart / rchange / r2max (KNN radii, or NULL for the constant radius):
+// beam radius at t is rstart + t * rchange, the predicate's bound is r2max (PhotonBeam.hxx:238-296,
+// 411).
+__global__ void k_emit_sorted(const float* __restrict__ origin, const float* __restrict__ dir,
+                              const float* __restrict__ length, const int32_t* __restrict__ medium, int64_t nb,
+                              const int32_t* __restrict__ offsets, const int32_t* __restrict__ perm, int np,
+                              float radius, float eps, const float* __restrict__ rstart,
+                              const float* __restrict__ rchange, const float* __restrict__ r2max, float4* pa,
+                              float4* pb, float4* pc, Box* boxes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const int p = perm[i];
+    const int b = piece_beam(offsets, nb, p);
+    const int first = offsets[b], cnt = offsets[b + 1] - first, k = p - first;
     const float ox = origin[3 * b], oy = origin[3 * b + 1], oz = origin[3 * b + 2];
     const float dx = dir[3 * b], dy = dir[3 * b + 1], dz = dir[3 * b + 2];
     const float len = length[b];
-    const int first = offsets[b];
-    const int cnt = offsets[b + 1] - first;
     // disc of radius r perpendicular to the beam: extent r*sqrt(1-d_i^2) per axis
     const float ex = sqrtf(fmaxf(0.f, 1.f - dx * dx)), ey = sqrtf(fmaxf(0.f, 1.f - dy * dy));
     const float ez = sqrtf(fmaxf(0.f, 1.f - dz * dz));
     const float rs = rstart ? rstart[b] : radius, rc = rchange ? rchange[b] : 0.f;
     const float r2 = r2max ? r2max[b] : radius * radius;
-    for (int k = 0; k < cnt; ++k) {
-        const float t0 = piece_t(k, cnt, len), t1 = piece_t(k + 1, cnt, len);
-        // the largest radius on the piece (the radius is linear in t)
-        const float rp = rchange ? fmaxf(rs + t0 * rc, rs + t1 * rc) * 1.000001f : radius;
-        const float mx = rp * ex + eps, my = rp * ey + eps, mz = rp * ez + eps;
-        const float ax = ox + dx * t0, ay = oy + dy * t0, az = oz + dz * t0;
-        const float bx = ox + dx * t1, by = oy + dy * t1, bz = oz + dz * t1;
-        Box bx_;
-        bx_.lo[0] = fminf(ax, bx) - mx; bx_.hi[0] = fmaxf(ax, bx) + mx;
-        bx_.lo[1] = fminf(ay, by) - my; bx_.hi[1] = fmaxf(ay, by) + my;
-        bx_.lo[2] = fminf(az, bz) - mz; bx_.hi[2] = fmaxf(az, bz) + mz;
-        const int p = first + k;
-        pa[p] = make_float4(ox, oy, oz, len);
-        pb[p] = make_float4(dx, dy, dz, r2);
-        pc[p] = make_float4(t0, t1, __int_as_float((int)b), __int_as_float(medium[b]));
-        boxes[p] = bx_;
-    }
-}
-
-__global__ void k_permute_pieces(const int32_t* __restrict__ perm, int n, const float4* __restrict__ pa,
-                                 const float4* __restrict__ pb, const float4* __restrict__ pc,
-                                 const Box* __restrict__ boxes, float4* opa, float4* opb, float4* opc, Box* oboxes)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int s = perm[i];
-    opa[i] = pa[s];
-    opb[i] = pb[s];
-    opc[i] = pc[s];
-    oboxes[i] = boxes[s];
+    const float t0 = piece_t(k, cnt, len), t1 = piece_t(k + 1, cnt, len);
+    // the largest radius on the piece (the radius is linear in t)
+    const float rp = rchange ? fmaxf(rs + t0 * rc, rs + t1 * rc) * 1.000001f : radius;
+    const float mx = rp * ex + eps, my = rp * ey + eps, mz = rp * ez + eps;
+    const float ax = ox + dx * t0, ay = oy + dy * t0, az = oz + dz * t0;
+    const float bx = ox + dx * t1, by = oy + dy * t1, bz = oz + dz * t1;
+    Box bx_;
+    bx_.lo[0] = fminf(ax, bx) - mx; bx_.hi[0] = fmaxf(ax, bx) + mx;
+    bx_.lo[1] = fminf(ay, by) - my; bx_.hi[1] = fmaxf(ay, by) + my;
+    bx_.lo[2] = fminf(az, bz) - mz; bx_.hi[2] = fmaxf(az, bz) + mz;
+    pa[i] = make_float4(ox, oy, oz, len);
+    pb[i] = make_float4(dx, dy, dz, r2);
+    pc[i] = make_float4(t0, t1, __int_as_float(b), __int_as_float(medium[b]));
+    boxes[i] = bx_;
 }
 
 }  // namespace
@@ -390,10 +402,6 @@ void launch_pack_lights(const float* pos, const float* thr, const float* dir, co
 void launch_bbox_partial(const float4* pts, const int32_t* idx, int n, float* partial, int blocks, cudaStream_t s)
 {
     k_bbox_partial<<<blocks, kThreads, 0, s>>>(pts, idx, n, partial);
-}
-void launch_bbox_boxes_partial(const Box* boxes, int n, float* partial, int blocks, cudaStream_t s)
-{
-    k_bbox_boxes_partial<<<blocks, kThreads, 0, s>>>(boxes, n, partial);
 }
 void launch_bbox_final(const float* partial, int blocks, float* out, cudaStream_t s)
 {
@@ -458,23 +466,24 @@ void launch_piece_counts(const float* length, int64_t n, float piece_len, int32_
 {
     if (n > 0) k_piece_counts<<<blocks_for(n), kThreads, 0, s>>>(length, n, piece_len, counts);
 }
-void launch_emit_pieces(const float* origin, const float* dir, const float* length, const int32_t* medium, int64_t n,
-                        const int32_t* offsets, float piece_len, float radius, float eps, const float* rstart,
-                        const float* rchange, const float* r2max, float4* pa, float4* pb, float4* pc, Box* boxes,
-                        cudaStream_t s)
+void launch_bbox_beams_partial(const float* origin, const float* dir, const float* length, int64_t n, float* partial,
+                               int blocks, cudaStream_t s)
 {
-    if (n > 0)
-        k_emit_pieces<<<blocks_for(n), kThreads, 0, s>>>(origin, dir, length, medium, n, offsets, piece_len, radius,
-                                                         eps, rstart, rchange, r2max, pa, pb, pc, boxes);
+    k_bbox_beams_partial<<<blocks, kThreads, 0, s>>>(origin, dir, length, n, partial);
 }
-void launch_morton_boxes(const Box* boxes, int n, const float* bbox, uint32_t* codes, cudaStream_t s)
+void launch_piece_codes(const float* origin, const float* dir, const float* length, int64_t nb, const int32_t* offsets,
+                        int np, const float* bbox, uint32_t* codes, int32_t* perm, cudaStream_t s)
 {
-    if (n > 0) k_morton_boxes<<<blocks_for(n), kThreads, 0, s>>>(boxes, n, bbox, codes);
+    if (np > 0) k_piece_codes<<<blocks_for(np), kThreads, 0, s>>>(origin, dir, length, nb, offsets, np, bbox, codes, perm);
 }
-void launch_permute_pieces(const int32_t* perm, int n, const float4* pa, const float4* pb, const float4* pc,
-                           const Box* boxes, float4* opa, float4* opb, float4* opc, Box* oboxes, cudaStream_t s)
+void launch_emit_sorted(const float* origin, const float* dir, const float* length, const int32_t* medium, int64_t nb,
+                        const int32_t* offsets, const int32_t* perm, int np, float radius, float eps,
+                        const float* rstart, const float* rchange, const float* r2max, float4* pa, float4* pb,
+                        float4* pc, Box* boxes, cudaStream_t s)
 {
-    if (n > 0) k_permute_pieces<<<blocks_for(n), kThreads, 0, s>>>(perm, n, pa, pb, pc, boxes, opa, opb, opc, oboxes);
+    if (np > 0)
+        k_emit_sorted<<<blocks_for(np), kThreads, 0, s>>>(origin, dir, length, medium, nb, offsets, perm, np, radius,
+                                                          eps, rstart, rchange, r2max, pa, pb, pc, boxes);
 }
 
 }  // namespace upbp

@@ -77,7 +77,7 @@ struct upbp_ctx {
     DBuf pb_pos, pb_leaf_codes, pb_nodes, pb_parent_int, pb_parent_leaf, pb_leaf_boxes, pb_node_boxes, pb_flags;
     int pb_n_leaves = 0;
     // beams
-    DBuf bm_thr4, bm_pdf4, bm_link, bm_radius, bm_counts, bm_offsets, pc_a, pc_b, pc_c, pc_boxes, pc_a2, pc_b2, pc_c2,
+    DBuf bm_thr4, bm_pdf4, bm_link, bm_radius, bm_counts, bm_offsets, pc_a2, pc_b2, pc_c2,
         pc_boxes2, pc_codes, pc_codes_sorted, pc_perm, pc_perm_sorted, bbox_pc;
     int n_pieces = 0;
     DBuf bm_leaf_codes, bm_nodes, bm_parent_int, bm_parent_leaf, bm_leaf_boxes, bm_node_boxes, bm_flagsbuf;
@@ -472,10 +472,6 @@ void do_build(upbp_ctx* c)
         }
         const int np = total;
         c->n_pieces = np;
-        ensure(c, c->pc_a, sizeof(float4) * np);
-        ensure(c, c->pc_b, sizeof(float4) * np);
-        ensure(c, c->pc_c, sizeof(float4) * np);
-        ensure(c, c->pc_boxes, sizeof(Box) * np);
         ensure(c, c->pc_a2, sizeof(float4) * np);
         ensure(c, c->pc_b2, sizeof(float4) * np);
         ensure(c, c->pc_c2, sizeof(float4) * np);
@@ -485,31 +481,32 @@ void do_build(upbp_ctx* c)
         ensure(c, c->pc_perm, sizeof(int32_t) * np);
         ensure(c, c->pc_perm_sorted, sizeof(int32_t) * np);
         ensure(c, c->bbox_pc, sizeof(float) * 6);
-        const float eps = 1e-5f + 1e-3f * r;
-        launch_emit_pieces(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(),
-                           c->b_med_in.as<int32_t>(), nb, c->bm_offsets.as<int32_t>(), piece_len, r, eps,
-                           rchange ? c->bm_radius.as<float>() : nullptr, rchange, r2max,
-                           c->pc_a.as<float4>(), c->pc_b.as<float4>(), c->pc_c.as<float4>(), c->pc_boxes.as<Box>(), s);
-        const int pblocks = std::max(1, std::min(1024, (np + 255) / 256));
-        float* partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
+        // Morton codes of the pieces' midpoints in the box of the beam segments, sorted; the piece
+        // records are then written directly in that order
+        const int bblocks = (int)std::max<int64_t>(1, std::min<int64_t>(1024, (nb + 255) / 256));
         ensure(c, c->bbox_partial, sizeof(int32_t) * 8 + sizeof(float) * 6 * 1024);
-        partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
-        launch_bbox_boxes_partial(c->pc_boxes.as<Box>(), np, partial, pblocks, s);
-        launch_bbox_final(partial, pblocks, c->bbox_pc.as<float>(), s);
-        launch_morton_boxes(c->pc_boxes.as<Box>(), np, c->bbox_pc.as<float>(), c->pc_codes.as<uint32_t>(), s);
-        k_iota<<<(np + 255) / 256, 256, 0, s>>>(c->pc_perm.as<int32_t>(), np);
+        float* partial = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
+        launch_bbox_beams_partial(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(), nb, partial,
+                                  bblocks, s);
+        launch_bbox_final(partial, bblocks, c->bbox_pc.as<float>(), s);
+        launch_piece_codes(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(), nb,
+                           c->bm_offsets.as<int32_t>(), np, c->bbox_pc.as<float>(), c->pc_codes.as<uint32_t>(),
+                           c->pc_perm.as<int32_t>(), s);
         sort_pairs(c, c->pc_codes.as<uint32_t>(), c->pc_codes_sorted.as<uint32_t>(), c->pc_perm.as<int32_t>(),
                    c->pc_perm_sorted.as<int32_t>(), np, 30);
-        launch_permute_pieces(c->pc_perm_sorted.as<int32_t>(), np, c->pc_a.as<float4>(), c->pc_b.as<float4>(),
-                              c->pc_c.as<float4>(), c->pc_boxes.as<Box>(), c->pc_a2.as<float4>(),
-                              c->pc_b2.as<float4>(), c->pc_c2.as<float4>(), c->pc_boxes2.as<Box>(), s);
+        const float eps = 1e-5f + 1e-3f * r;
+        launch_emit_sorted(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(),
+                           c->b_med_in.as<int32_t>(), nb, c->bm_offsets.as<int32_t>(), c->pc_perm_sorted.as<int32_t>(),
+                           np, r, eps, rchange ? c->bm_radius.as<float>() : nullptr, rchange, r2max,
+                           c->pc_a2.as<float4>(), c->pc_b2.as<float4>(), c->pc_c2.as<float4>(), c->pc_boxes2.as<Box>(),
+                           s);
         const int leaf = std::max(1, c->bb1d_leaf);
         const int nl = (np + leaf - 1) / leaf;
         ensure(c, c->bm_leaf_boxes, sizeof(Box) * nl);
         launch_box_leaf_boxes(c->pc_boxes2.as<Box>(), np, leaf, c->bm_leaf_boxes.as<Box>(), s);
         build_lbvh(c, c->pc_codes_sorted.as<uint32_t>(), np, leaf, c->bm_leaf_codes, c->bm_nodes, c->bm_parent_int,
                    c->bm_parent_leaf, c->bm_leaf_boxes, c->bm_node_boxes, c->bm_flagsbuf, c->bm_n_leaves);
-        c->build_launches += 10;
+        c->build_launches += 8;
         if (c->mode != UPBP_MODE_PLAIN) {
             ensure(c, c->pc_pay, sizeof(PiecePayload) * np);
             launch_piece_payload(c->pc_c2.as<float4>(), np, c->bm_thr4.as<float4>(), c->bm_pdf4.as<float4>(),
@@ -902,7 +899,7 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->ph_keys, &c->ph_keys_sorted, &c->bbox_partial, &c->bbox_ph, &c->hg_start, &c->hg_end,
                    &c->hg_pos, &c->pb_pos, &c->pb_leaf_codes, &c->pb_nodes, &c->pb_parent_int, &c->pb_parent_leaf,
                    &c->pb_leaf_boxes, &c->pb_node_boxes, &c->pb_flags, &c->bm_thr4, &c->bm_pdf4, &c->bm_link,
-                   &c->bm_radius, &c->bm_counts, &c->bm_offsets, &c->pc_a, &c->pc_b, &c->pc_c, &c->pc_boxes,
+                   &c->bm_radius, &c->bm_counts, &c->bm_offsets,
                    &c->pc_a2, &c->pc_b2, &c->pc_c2, &c->pc_boxes2, &c->pc_codes, &c->pc_codes_sorted, &c->pc_perm,
                    &c->pc_perm_sorted, &c->bbox_pc, &c->bm_leaf_codes, &c->bm_nodes, &c->bm_parent_int,
                    &c->bm_parent_leaf, &c->bm_leaf_boxes, &c->bm_node_boxes, &c->bm_flagsbuf, &c->cub_tmp,

@@ -180,14 +180,14 @@ void launch_pack_beams(const float* thr, const uint32_t* flags, const float* rsp
                        const uint32_t* rsf, const int32_t* lv, const int32_t* medium, int64_t n, float radius,
                        float4* o_thr, float4* o_pdf, int2* o_link, float* o_radius, cudaStream_t stream);
 void launch_piece_counts(const float* length, int64_t n, float piece_len, int32_t* counts, cudaStream_t stream);
-void launch_emit_pieces(const float* origin, const float* dir, const float* length, const int32_t* medium, int64_t n,
-                        const int32_t* offsets, float piece_len, float radius, float eps, const float* rstart,
-                        const float* rchange, const float* r2max, float4* pa, float4* pb, float4* pc, Box* boxes,
-                        cudaStream_t stream);
-void launch_bbox_boxes_partial(const Box* boxes, int n, float* partial, int blocks, cudaStream_t stream);
-void launch_morton_boxes(const Box* boxes, int n, const float* bbox, uint32_t* codes, cudaStream_t stream);
-void launch_permute_pieces(const int32_t* perm, int n, const float4* pa, const float4* pb, const float4* pc,
-                           const Box* boxes, float4* opa, float4* opb, float4* opc, Box* oboxes, cudaStream_t stream);
+void launch_bbox_beams_partial(const float* origin, const float* dir, const float* length, int64_t n, float* partial,
+                               int blocks, cudaStream_t s);
+void launch_piece_codes(const float* origin, const float* dir, const float* length, int64_t nb, const int32_t* offsets,
+                        int np, const float* bbox, uint32_t* codes, int32_t* perm, cudaStream_t s);
+void launch_emit_sorted(const float* origin, const float* dir, const float* length, const int32_t* medium, int64_t nb,
+                        const int32_t* offsets, const int32_t* perm, int np, float radius, float eps,
+                        const float* rstart, const float* rchange, const float* r2max, float4* pa, float4* pb,
+                        float4* pc, Box* boxes, cudaStream_t s);
 void launch_box_leaf_boxes(const Box* boxes, int n, int leaf, Box* leaf_boxes, cudaStream_t stream);
 
 struct CamSum;
