@@ -7,6 +7,8 @@ The knobs (``upbp_tuning`` in ``include/upbp_gpu.h``):
 * ``bb1d_kernel`` picks the segment gathers: 1 or 2 the warp-cooperative BB1D kernel compiled for
   5 or 6 blocks of 4 warps per SM (PB2D in its own kernel), 3 or 4 one persistent kernel for all
   camera segments doing PB2D and BB1D per query;
+* ``pb2d_kernel`` picks the PB2D gather when it runs on its own: 0 one thread per query, 1 one
+  warp per query from a persistent work queue;
 * ``pb2d_leaf`` is the photon count per PB2D LBVH leaf;
 * ``block_threads`` is the block shape (queries per block) of the thread-per-query PB2D and PP3D
   gathers.
@@ -29,7 +31,7 @@ from typing import Dict, Iterable, List, Optional, Tuple
 STAGES = (
     {"bb1d_kernel": (1, 2, 3, 4)},
     {"bb1d_leaf": (2, 4, 8), "beam_piece_radii": (3.0, 4.0, 6.0)},
-    {"pb2d_leaf": (4, 8, 16), "block_threads": (128, 256)},
+    {"pb2d_kernel": (0, 1), "pb2d_leaf": (4, 8, 16), "block_threads": (128, 256)},
 )
 
 

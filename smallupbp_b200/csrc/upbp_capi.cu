@@ -108,6 +108,7 @@ struct upbp_ctx {
     bool status_pending = false;  // status_host holds the last BB1D launch's flag
     int num_sms = 0;
     int bb1d_kernel = 2;  // 0: thread per query, 1-2: warp-cooperative BB1D, 3-4: fused segment kernel
+    int pb2d_kernel = 1;  // PB2D on its own: 0 thread per query, 1 warp-cooperative persistent
     DBuf out_bp2d, cnt_bp2d, hash_bp2d;  // B-P2D (extension) per point query
     DBuf tr_cnt, tr_off, tr_status;  // device-side light / camera passes: per-path record counts and offsets
     DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
@@ -795,11 +796,26 @@ void do_evaluate(upbp_ctx* c)
         c->eval_launches += 5;
     }
     const bool fused = c->bb1d_kernel >= 3;  // PB2D and BB1D in the one persistent segment kernel
+    if (nq > 0 && c->bb1d_kernel >= 1) {
+        // persistent warp kernels: work counters (BB1D or the fused kernel: [0], PB2D: [1]) and the
+        // traversal status word they share
+        if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
+        ensure(c, c->work, sizeof(unsigned int) * 4);
+        ensure(c, c->status, sizeof(int) * 4);
+        ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
+        ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
+    }
     if (nq > 0 && !fused) {
         const PhotonBVH B = photon_bvh(c);
         Outputs O{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
                   c->hash_pb2d.as<unsigned long long>(), tested + 0};
-        launch_gather_pb2d(K, L, B, Q, cam, cs_seg, O, c->block, mixed, s, order);
+        if (c->pb2d_kernel == 1 && c->bb1d_kernel >= 1) {
+            const int grid = c->num_sms * pb2d_warp_blocks_per_sm(mixed);
+            launch_pb2d_warp(K, L, B, Q, cam, cs_seg, O, grid, mixed, c->work.as<unsigned int>() + 1,
+                             c->status.as<int>(), order, s);
+        } else {
+            launch_gather_pb2d(K, L, B, Q, cam, cs_seg, O, c->block, mixed, s, order);
+        }
         c->eval_launches += 1;
     }
     mark(c, 4, s);
@@ -809,11 +825,6 @@ void do_evaluate(upbp_ctx* c)
         Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                   c->hash_bb1d.as<unsigned long long>(), tested + 1};
         if (fused) {
-            if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
-            ensure(c, c->work, sizeof(unsigned int) * 4);
-            ensure(c, c->status, sizeof(int) * 4);
-            ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
-            ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
             const Outputs Opb{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
                               c->hash_pb2d.as<unsigned long long>(), tested + 0};
             const int grid = c->num_sms * segments_warp_blocks_per_sm(mixed, c->bb1d_kernel);
@@ -821,11 +832,6 @@ void do_evaluate(upbp_ctx* c)
                                  c->work.as<unsigned int>(), c->status.as<int>(), order, s, c->bb1d_kernel);
             record_status(c, s);
         } else if (c->bb1d_kernel >= 1) {
-            if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
-            ensure(c, c->work, sizeof(unsigned int) * 4);
-            ensure(c, c->status, sizeof(int) * 4);
-            ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
-            ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
             const int grid = c->num_sms * bb1d_warp_blocks_per_sm(mixed, c->bb1d_kernel);
             launch_bb1d_warp(K, L, B, S, Q, cam, cs_seg, O, grid, mixed, c->work.as<unsigned int>(),
                              c->status.as<int>(), order, s, c->bb1d_kernel);
@@ -947,11 +953,13 @@ int upbp_set_tuning(upbp_ctx* c, const upbp_tuning* tu)
         if (!(tu->beam_piece_radii >= 1.f && tu->beam_piece_radii <= 1024.f))
             fail(c, UPBP_ERR_INVALID_ARG, "beam_piece_radii must be in [1, 1024]");
         if (tu->bb1d_kernel < 0 || tu->bb1d_kernel > 4) fail(c, UPBP_ERR_INVALID_ARG, "bb1d_kernel must be in [0, 4]");
+        if (tu->pb2d_kernel < 0 || tu->pb2d_kernel > 1) fail(c, UPBP_ERR_INVALID_ARG, "pb2d_kernel must be 0 or 1");
         c->pb2d_leaf = tu->pb2d_leaf;
         c->bb1d_leaf = tu->bb1d_leaf;
         c->block = tu->block_threads;
         c->piece_len_r = tu->beam_piece_radii;
         c->bb1d_kernel = tu->bb1d_kernel;
+        c->pb2d_kernel = tu->pb2d_kernel;
         c->built = false;
     });
 }
@@ -964,6 +972,7 @@ int upbp_get_tuning(const upbp_ctx* c, upbp_tuning* tu)
     tu->block_threads = c->block;
     tu->beam_piece_radii = c->piece_len_r;
     tu->bb1d_kernel = c->bb1d_kernel;
+    tu->pb2d_kernel = c->pb2d_kernel;
     return UPBP_OK;
 }
 

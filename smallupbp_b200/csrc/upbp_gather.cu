@@ -721,6 +721,59 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bb1d_warp(const __g
     }
 }
 
+// PB2D, warp per query, persistent (the BB1D kernel's scheme over the photon LBVH): the lanes
+// test 32 photons at a time and evaluate the accepted ones 32 at a time from the candidate queue.
+template <bool kMixed, int kWarps, int kMinBlocks>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_pb2d_warp(const __grid_constant__ GatherConsts K,
+                                                                     const LightSoA Lv, const PhotonBVH P,
+                                                                     const SegQueriesDev Q,
+                                                                     const upbp_mis* __restrict__ cam,
+                                                                     const CamSum* __restrict__ cs, const Outputs O,
+                                                                     unsigned int* __restrict__ work,
+                                                                     int* __restrict__ status,
+                                                                     const int32_t* __restrict__ order)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    __shared__ int s_stack[kWarps][kWarpStack];
+    __shared__ int s_leaves[kWarps][kWarpLeaves];
+    __shared__ CandQueue s_queue[kWarps];
+    __shared__ upbp_mis s_e[kWarps];
+    __shared__ CamSum s_cs[kWarps];
+    stage_media(K, media);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const WarpScratch ws{s_stack[warp], s_leaves[warp], &s_queue[warp], lane, (1u << lane) - 1u};
+    for (;;) {
+        unsigned qq = 0;
+        if (lane == 0) qq = atomicAdd(work, 1u);
+        const int64_t item = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (item >= Q.n) break;
+        const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
+        Rgb acc = rgb(0.f);
+        unsigned long long cnt = 0, h = 0, tested = 0;
+        if ((Q.flags[q] & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && P.n > 0) {
+            SegCtx s;
+            init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &s_e[warp], &s_cs[warp], lane == 0);
+            __syncwarp();
+            const V3 inv = v3(safe_inv(s.d.x), safe_inv(s.d.y), safe_inv(s.d.z));
+            acc = pb2d_query_warp<kMixed>(K, media, Lv, P, Q, q, s, inv, ws, cnt, h, tested, status);
+        }
+        const float r = warp_sum(acc.r), g = warp_sum(acc.g), b = warp_sum(acc.b);
+        cnt = warp_sum_u64(cnt);
+        h = warp_sum_u64(h);
+        tested = warp_sum_u64(tested);
+        if (lane == 0) {
+            O.rgb[3 * q + 0] = r;
+            O.rgb[3 * q + 1] = g;
+            O.rgb[3 * q + 2] = b;
+            if (O.count) O.count[q] = (uint32_t)cnt;
+            if (O.hash) O.hash[q] = h;
+            const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+            splat(O.image, Q.pixel[q], thr * K.P.norm_pb2d * Rgb{r, g, b});
+            if (O.tested) atomicAdd(O.tested, tested);
+        }
+    }
+}
+
 // All camera segments of an iteration in one persistent work-queue kernel: a warp takes the next
 // query (Morton order) and evaluates both segment estimators for it, PB2D over the photon LBVH
 // and BB1D over the beam-piece LBVH, with one camera context and one splat per query.
@@ -1024,6 +1077,23 @@ static int blocks_for(int variant)
     if (variant == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 6>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 5>, 128, 0);
     return nb > 0 ? nb : 1;
+}
+
+int pb2d_warp_blocks_per_sm(bool mixed)
+{
+    int nb = 0;
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pb2d_warp<true, 4, 6>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pb2d_warp<false, 4, 6>, 128, 0);
+    return nb > 0 ? nb : 1;
+}
+
+void launch_pb2d_warp(const GatherConsts& K, const LightSoA& L, const PhotonBVH& P, const SegQueriesDev& Q,
+                      const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid, bool mixed,
+                      unsigned int* work, int* status, const int32_t* order, cudaStream_t stream)
+{
+    if (Q.n <= 0) return;
+    if (mixed) k_pb2d_warp<true, 4, 6><<<grid, 128, 0, stream>>>(K, L, P, Q, cam, cs, O, work, status, order);
+    else k_pb2d_warp<false, 4, 6><<<grid, 128, 0, stream>>>(K, L, P, Q, cam, cs, O, work, status, order);
 }
 
 int bb1d_warp_blocks_per_sm(bool mixed, int variant)

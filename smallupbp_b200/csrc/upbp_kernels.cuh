@@ -202,6 +202,10 @@ void launch_piece_payload(const float4* pc, int n, const float4* bm_thr, const f
                           const struct LightSum* sums, PiecePayload* out, cudaStream_t stream);
 void launch_query_keys(const SegQueriesDev& Q, const float* bbox, uint32_t* keys, int32_t* iota, cudaStream_t stream);
 int bb1d_warp_blocks_per_sm(bool mixed, int variant);
+int pb2d_warp_blocks_per_sm(bool mixed);
+void launch_pb2d_warp(const GatherConsts& K, const LightSoA& L, const PhotonBVH& P, const SegQueriesDev& Q,
+                      const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid, bool mixed,
+                      unsigned int* work, int* status, const int32_t* order, cudaStream_t stream);
 int segments_warp_blocks_per_sm(bool mixed, int variant);
 void launch_segments_warp(const GatherConsts& K, const LightSoA& L, const PhotonBVH& P, const BeamBVH& B,
                           const BeamSoA& S, const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs,

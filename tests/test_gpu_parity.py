@@ -108,6 +108,23 @@ def test_bb1d_kernel_variants_same_candidates(stage, kernel, leaf):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("pb2d_kernel", [0, 1], ids=["thread", "warp"])
+@pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
+def test_pb2d_kernel_variants_same_candidates(stage, pb2d_kernel, path):
+    # the thread-per-query and the warp-cooperative persistent PB2D gathers find the reference's
+    # candidate set, in plain FP32 with the reference's contributions
+    w, r = G.load(path)
+    stage.set_tuning(pb2d_kernel=pb2d_kernel, bb1d_kernel=2)
+    try:
+        g = run(stage, w)
+        np.testing.assert_array_equal(g["count_pb2d"], r["count_pb2d"])
+        np.testing.assert_array_equal(g["hash_pb2d"], r["hash_pb2d"])
+        G.assert_close(g["pb2d"], r["pb2d"], "PB2D")
+    finally:
+        stage.set_tuning(pb2d_kernel=1)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("mode", [engine.MODE_PLAIN, engine.MODE_MIXED], ids=["plain", "mixed"])
 def test_knn_radii_bit_exact_with_exact_knn_oracle(stage, mode):
     # KNN radii at a size where photons and beam origins span many LBVH leaves: the CUDA KNN
