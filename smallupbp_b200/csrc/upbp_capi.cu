@@ -689,6 +689,7 @@ gen::GenLaunch generic_launch(upbp_ctx* c, const CamSum* cs_seg, const CamSum* c
     A.work = c->work.as<unsigned int>();
     A.status = c->status.as<int>();
     A.bb1d_grid = c->num_sms * gen::generic_bb1d_blocks_per_sm(grad_medium >= 0);
+    A.pb2d_grid = c->num_sms * gen::generic_pb2d_blocks_per_sm(grad_medium >= 0);
     return A;
 }
 

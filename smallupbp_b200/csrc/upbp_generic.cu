@@ -323,50 +323,113 @@ __device__ __forceinline__ void finish_lanes(const GenOut& O, bool valid, int64_
     }
 }
 
+// End of a warp's query (the warp kernels): the adjoint adds the lanes' gradient terms of this
+// query's pixel weight; otherwise the lanes' partial results, counts and hashes are reduced and
+// lane 0 writes the query's outputs.
+template <class T>
+__device__ __forceinline__ void finish_warp(const GenOut& O, int64_t q, const RgbT<T>& acc, int px, const float* thr,
+                                            double norm, unsigned long long cnt, unsigned long long h, int lane)
+{
+    if constexpr (std::is_same<T, Dual>::value) {
+        double w[3], g[kNT];
+        pixel_weights(O, px, thr, norm, w);
+        for (int i = 0; i < kNT; ++i) g[i] = 0.0;
+        lane_grad(acc, w, g);
+        for (int i = 0; i < kNT; ++i) g[i] = wsum(g[i]);
+        if (lane == 0)
+            for (int i = 0; i < kNT; ++i)
+                if (g[i] != 0.0) atomicAdd(&O.grad[i], g[i]);
+    } else {
+        RgbT<T> v{wsum(acc.r), wsum(acc.g), wsum(acc.b)};
+        for (int o = 16; o > 0; o >>= 1) {
+            cnt += __shfl_xor_sync(kFull, cnt, o);
+            h += __shfl_xor_sync(kFull, h, o);
+        }
+        if (lane == 0) finish_thread<T>(O, q, v, px, thr, norm, (uint32_t)cnt, h);
+    }
+}
+
 // ------------------------------------------------------------------ kernels
+constexpr int kGenQueue = 64;
+
+// PB2D, warp per query with a candidate queue (the scheme of the BB1D kernel below, over the
+// photon LBVH): the lanes test 32 photons at a time and evaluate the accepted ones 32 at a time.
 template <class T>
 __global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ GatherConsts K,
                                                   const __grid_constant__ GenConsts G, const LightSoA Lv,
                                                   const PhotonBVH B, const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
-                                                  const GenOut O)
+                                                  const GenOut O, unsigned int* __restrict__ work,
+                                                  int* __restrict__ status)
 {
+    constexpr int kWarps = 4;
     __shared__ MedT<T> media[UPBP_MAX_MEDIA];
+    __shared__ int s_stack[kWarps][kWarpStack];
+    __shared__ int s_leaves[kWarps][kWarpLeaves];
+    __shared__ int s_photon[kWarps][kGenQueue];
     stage_media_t<T>(G, media);
-    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool valid = q < Q.n;
-    uint32_t cnt = 0;
-    unsigned long long h = 0;
-    RgbT<T> res = rgb_zero<T>();
-    if (valid && (Q.flags[q] & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && B.n > 0) {
-        SegCtx<T> s;
-        init_ctx(s, K, Q, cam, cs, q);
-        const V3 inv = v3(safe_inv(s.df.x), safe_inv(s.df.y), safe_inv(s.df.z));
-        const float r2 = K.P.radius_pb2d * K.P.radius_pb2d;
-        res = seg_loop<T>(K, media, Q, q, s, [&](const MedT<T>& m, int, float dminf, float dmaxf) {
-            RgbT<T> acc = rgb_zero<T>();
-            traverse(B.nodes, B.n_leaves, s.of, inv, dminf - K.eps, dmaxf + K.eps, [&](int leaf) {
-                const int e = min(B.n, (leaf + 1) * B.leaf);
-                for (int i = leaf * B.leaf; i < e; ++i) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int* stack = s_stack[warp];
+    int* leaves = s_leaves[warp];
+    int* cq = s_photon[warp];
+    const int leaf_shift = __ffs(B.leaf) - 1;
+    const float r2 = K.P.radius_pb2d * K.P.radius_pb2d;
+    for (;;) {
+        unsigned qq = 0;
+        if (lane == 0) qq = atomicAdd(work, 1u);
+        const int64_t q = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (q >= Q.n) break;
+        RgbT<T> acc = rgb_zero<T>();
+        unsigned long long cnt = 0, h = 0;
+        if ((Q.flags[q] & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && B.n > 0) {
+            SegCtx<T> s;
+            init_ctx(s, K, Q, cam, cs, q);
+            const V3 inv = v3(safe_inv(s.df.x), safe_inv(s.df.y), safe_inv(s.df.z));
+            acc = seg_loop<T>(K, media, Q, q, s, [&](const MedT<T>& m, int, float dminf, float dmaxf) {
+                RgbT<T> part = rgb_zero<T>();
+                int qn = 0;
+                auto eval = [&](int e) {
+                    const int i = cq[e];
                     const float4 p = __ldg(&B.pos[i]);
-                    float t, d2;
                     const float r2i = B.r2 ? __ldg(&B.r2[i]) : r2;
-                    if (test_bre(s.of, s.df, dminf, dmaxf, v3(p.x, p.y, p.z), r2i, &t, &d2)) {
-                        const int lv = __float_as_int(p.w);
-                        ++cnt;
-                        h += mix64((unsigned long long)lv);
-                        acc = acc + pb2d_contrib<T>(K, m, Lv, s, lv, r2i);
+                    part = part + pb2d_contrib<T>(K, m, Lv, s, __float_as_int(p.w), r2i);
+                };
+                const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.of, inv, dminf - K.eps,
+                                              dmaxf + K.eps, stack, leaves, lane, [&](int i) {
+                    bool hit = false;
+                    if (i >= 0) {
+                        const float4 p = __ldg(&B.pos[i]);
+                        const float r2i = B.r2 ? __ldg(&B.r2[i]) : r2;
+                        float t, d2;
+                        if (test_bre(s.of, s.df, dminf, dmaxf, v3(p.x, p.y, p.z), r2i, &t, &d2)) {
+                            hit = true;
+                            ++cnt;
+                            h += mix64((unsigned long long)__float_as_int(p.w));
+                        }
                     }
-                }
+                    const unsigned vote = __ballot_sync(kFull, hit);
+                    if (vote == 0u) return;
+                    if (hit) cq[qn + __popc(vote & lt)] = i;
+                    qn += __popc(vote);
+                    __syncwarp();
+                    if (qn >= 32) {
+                        eval(qn - 32 + lane);
+                        qn -= 32;
+                        __syncwarp();
+                    }
+                });
+                if (lane < qn) eval(lane);
+                __syncwarp();
+                if (!ok && lane == 0) atomicOr(status, 1);
+                return part;
             });
-            return acc;
-        });
+        }
+        finish_warp<T>(O, q, acc, Q.pixel[q], Q.throughput + 3 * q, K.P.norm_pb2d, cnt, h, lane);
     }
-    finish_lanes<T>(O, valid, q, res, valid ? Q.pixel[q] : -1, valid ? Q.throughput + 3 * q : nullptr, K.P.norm_pb2d,
-                    cnt, h);
 }
 
-constexpr int kGenQueue = 64;
+
 
 // BB1D, warp per query with the candidate queue of the FP32 warp kernel.
 template <class T>
@@ -448,25 +511,7 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                 return part;
             });
         }
-        const int px = Q.pixel[q];
-        const double norm = K.P.norm_bb1d;
-        if constexpr (std::is_same<T, Dual>::value) {
-            double w[3], g[kNT];
-            pixel_weights(O, px, Q.throughput + 3 * q, norm, w);
-            for (int i = 0; i < kNT; ++i) g[i] = 0.0;
-            lane_grad(acc, w, g);
-            for (int i = 0; i < kNT; ++i) g[i] = wsum(g[i]);
-            if (lane == 0)
-                for (int i = 0; i < kNT; ++i)
-                    if (g[i] != 0.0) atomicAdd(&O.grad[i], g[i]);
-        } else {
-            RgbT<T> v{wsum(acc.r), wsum(acc.g), wsum(acc.b)};
-            for (int o = 16; o > 0; o >>= 1) {
-                cnt += __shfl_xor_sync(kFull, cnt, o);
-                h += __shfl_xor_sync(kFull, h, o);
-            }
-            if (lane == 0) finish_thread<T>(O, q, v, px, Q.throughput + 3 * q, norm, (uint32_t)cnt, h);
-        }
+        finish_warp<T>(O, q, acc, Q.pixel[q], Q.throughput + 3 * q, K.P.norm_bb1d, cnt, h, lane);
     }
 }
 
@@ -626,8 +671,8 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
     if (A.pq.n > 0 && A.beams.n > 0 && (A.K.P.techniques & UPBP_BP2D))
         k_gen_bp2d<T><<<(unsigned)((A.pq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.pq, A.out_bp2d);
     if (A.sq.n > 0 && A.photons.n > 0)
-        k_gen_pb2d<T><<<(unsigned)((A.sq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam,
-                                                                        A.cs_seg, A.out_pb2d);
+        k_gen_pb2d<T><<<A.pb2d_grid, 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam, A.cs_seg, A.out_pb2d,
+                                                  A.work + 1, A.status);
     if (A.sq.n > 0 && A.beams.n > 0)
         k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.sq, A.cam, A.cs_seg, A.out_bb1d, A.work,
                                                   A.status);
@@ -637,6 +682,14 @@ void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream)
 {
     if (adjoint) launch_all<Dual>(A, stream);
     else launch_all<double>(A, stream);
+}
+
+int generic_pb2d_blocks_per_sm(bool adjoint)
+{
+    int nb = 0;
+    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<Dual>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<double>, 128, 0);
+    return nb > 0 ? nb : 1;
 }
 
 int generic_bb1d_blocks_per_sm(bool adjoint)

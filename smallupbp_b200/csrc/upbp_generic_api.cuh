@@ -39,13 +39,15 @@ struct GenLaunch {
     const CamSum* cs_seg;
     const CamSum* cs_pt;
     GenOut out_pb2d, out_bb1d, out_pp3d, out_bp2d;
-    unsigned int* work;  // BB1D work counter (zeroed by the caller)
-    int* status;         // BB1D traversal status (zeroed by the caller)
+    unsigned int* work;  // work counters, [0] BB1D and [1] PB2D (zeroed by the caller)
+    int* status;         // traversal status (zeroed by the caller)
     int bb1d_grid;
+    int pb2d_grid;
 };
 
 void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream);
 int generic_bb1d_blocks_per_sm(bool adjoint);
+int generic_pb2d_blocks_per_sm(bool adjoint);
 
 }  // namespace gen
 }  // namespace upbp

@@ -112,8 +112,8 @@ def test_bb1d_kernel_variants_same_candidates(stage, kernel, leaf):
 @pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
 def test_pb2d_kernel_variants_same_candidates(stage, pb2d_kernel, path):
     # the thread-per-query and the warp-cooperative persistent PB2D gathers find the reference's
-    # candidate set, in plain FP32 with the reference's contributions
-    w, r = G.load(path)
+    # candidate set (the oracle's for KNN radii), in plain FP32 with the reference's contributions
+    w, r = G.expected(path)
     stage.set_tuning(pb2d_kernel=pb2d_kernel, bb1d_kernel=2)
     try:
         g = run(stage, w)
