@@ -664,6 +664,30 @@ void prepare_cam_sums(upbp_ctx* c, cudaStream_t s, const CamSum** cs_seg, const 
 }
 
 // The generic-precision gathers (FP64 evaluation, adjoint) over the context's structures.
+// Order the segment queries along a Morton curve of their midpoints, so that the warps in flight
+// traverse neighbouring parts of the LBVHs (L2 reuse).  nullptr: keep the given order.
+const int32_t* query_order(upbp_ctx* c, const SegQueriesDev& Q, cudaStream_t s)
+{
+    const int64_t nq = Q.n;
+    const bool have_bbox = c->n_pieces > 0 || c->n_ph > 0;
+    if (!c->order_queries || nq <= 1 || !have_bbox) return nullptr;
+    ensure(c, c->q_keys, sizeof(uint32_t) * nq);
+    ensure(c, c->q_keys_sorted, sizeof(uint32_t) * nq);
+    ensure(c, c->q_iota, sizeof(int32_t) * nq);
+    ensure(c, c->q_order, sizeof(int32_t) * nq);
+    launch_query_keys(Q, c->n_pieces > 0 ? c->bbox_pc.as<float>() : c->bbox_ph.as<float>(), c->q_keys.as<uint32_t>(),
+                      c->q_iota.as<int32_t>(), s);
+    size_t b = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b, c->q_keys.as<uint32_t>(), c->q_keys_sorted.as<uint32_t>(),
+                                    c->q_iota.as<int32_t>(), c->q_order.as<int32_t>(), (int)nq, 0, 30, s);
+    ensure(c, c->cub_tmp, b);
+    ck(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, b, c->q_keys.as<uint32_t>(), c->q_keys_sorted.as<uint32_t>(),
+                                          c->q_iota.as<int32_t>(), c->q_order.as<int32_t>(), (int)nq, 0, 30, s),
+       "SortPairs");
+    c->eval_launches += 5;
+    return c->q_order.as<int32_t>();
+}
+
 gen::GenLaunch generic_launch(upbp_ctx* c, const CamSum* cs_seg, const CamSum* cs_pt, int grad_medium)
 {
     gen::GenLaunch A{};
@@ -690,6 +714,7 @@ gen::GenLaunch generic_launch(upbp_ctx* c, const CamSum* cs_seg, const CamSum* c
     A.status = c->status.as<int>();
     A.bb1d_grid = c->num_sms * gen::generic_bb1d_blocks_per_sm(grad_medium >= 0);
     A.pb2d_grid = c->num_sms * gen::generic_pb2d_blocks_per_sm(grad_medium >= 0);
+    A.order = query_order(c, A.sq, c->stream);
     return A;
 }
 
@@ -775,27 +800,7 @@ void do_evaluate(upbp_ctx* c)
     }
     mark(c, 3, s);
     const SegQueriesDev Q = seg_dev(c);
-    // Order the segment queries along a Morton curve of their midpoints, so that the warps in
-    // flight traverse neighbouring parts of the LBVHs (L2 reuse).
-    const int32_t* order = nullptr;
-    const bool have_bbox = c->n_pieces > 0 || c->n_ph > 0;
-    if (c->order_queries && nq > 1 && have_bbox) {
-        ensure(c, c->q_keys, sizeof(uint32_t) * nq);
-        ensure(c, c->q_keys_sorted, sizeof(uint32_t) * nq);
-        ensure(c, c->q_iota, sizeof(int32_t) * nq);
-        ensure(c, c->q_order, sizeof(int32_t) * nq);
-        launch_query_keys(Q, c->n_pieces > 0 ? c->bbox_pc.as<float>() : c->bbox_ph.as<float>(),
-                          c->q_keys.as<uint32_t>(), c->q_iota.as<int32_t>(), s);
-        size_t b = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, b, c->q_keys.as<uint32_t>(), c->q_keys_sorted.as<uint32_t>(),
-                                        c->q_iota.as<int32_t>(), c->q_order.as<int32_t>(), (int)nq, 0, 30, s);
-        ensure(c, c->cub_tmp, b);
-        ck(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, b, c->q_keys.as<uint32_t>(), c->q_keys_sorted.as<uint32_t>(),
-                                              c->q_iota.as<int32_t>(), c->q_order.as<int32_t>(), (int)nq, 0, 30, s),
-           "SortPairs");
-        order = c->q_order.as<int32_t>();
-        c->eval_launches += 5;
-    }
+    const int32_t* order = query_order(c, Q, s);
     const bool fused = c->bb1d_kernel >= 3;  // PB2D and BB1D in the one persistent segment kernel
     if (nq > 0 && c->bb1d_kernel >= 1) {
         // persistent warp kernels: work counters (BB1D or the fused kernel: [0], PB2D: [1]) and the

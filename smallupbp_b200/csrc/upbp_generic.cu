@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ Gather
                                                   const PhotonBVH B, const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
                                                   const GenOut O, unsigned int* __restrict__ work,
-                                                  int* __restrict__ status)
+                                                  int* __restrict__ status, const int32_t* __restrict__ order)
 {
     constexpr int kWarps = 4;
     __shared__ MedT<T> media[UPBP_MAX_MEDIA];
@@ -378,8 +378,9 @@ __global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ Gather
     for (;;) {
         unsigned qq = 0;
         if (lane == 0) qq = atomicAdd(work, 1u);
-        const int64_t q = (int64_t)__shfl_sync(kFull, qq, 0);
-        if (q >= Q.n) break;
+        const int64_t item = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (item >= Q.n) break;
+        const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
         RgbT<T> acc = rgb_zero<T>();
         unsigned long long cnt = 0, h = 0;
         if ((Q.flags[q] & UPBP_Q_PB2D) && (K.P.techniques & UPBP_PB2D) && B.n > 0) {
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                                                   const BeamSoA Bs, const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
                                                   const GenOut O, unsigned int* __restrict__ work,
-                                                  int* __restrict__ status)
+                                                  int* __restrict__ status, const int32_t* __restrict__ order)
 {
     constexpr int kWarps = 4;
     __shared__ MedT<T> media[UPBP_MAX_MEDIA];
@@ -455,8 +456,9 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
     for (;;) {
         unsigned qq = 0;
         if (lane == 0) qq = atomicAdd(work, 1u);
-        const int64_t q = (int64_t)__shfl_sync(kFull, qq, 0);
-        if (q >= Q.n) break;
+        const int64_t item = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (item >= Q.n) break;
+        const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
         RgbT<T> acc = rgb_zero<T>();
         unsigned long long cnt = 0, h = 0;
         if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D) && B.n > 0) {
@@ -672,10 +674,10 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
         k_gen_bp2d<T><<<(unsigned)((A.pq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.pq, A.out_bp2d);
     if (A.sq.n > 0 && A.photons.n > 0)
         k_gen_pb2d<T><<<A.pb2d_grid, 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam, A.cs_seg, A.out_pb2d,
-                                                  A.work + 1, A.status);
+                                                  A.work + 1, A.status, A.order);
     if (A.sq.n > 0 && A.beams.n > 0)
         k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.sq, A.cam, A.cs_seg, A.out_bb1d, A.work,
-                                                  A.status);
+                                                  A.status, A.order);
 }
 
 void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream)

@@ -43,6 +43,7 @@ struct GenLaunch {
     int* status;         // traversal status (zeroed by the caller)
     int bb1d_grid;
     int pb2d_grid;
+    const int32_t* order;  // segment queries in Morton order of their midpoints, or nullptr
 };
 
 void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream);
