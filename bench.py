@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the image rel-L2 check against the FP64 mode")
     ap.add_argument("--no-device-passes", action="store_true",
                     help="skip the iteration traced on the device (light + camera passes, build, evaluate)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
@@ -328,6 +329,12 @@ def run_b200(args, cfg, rank, world, local_rank):
                "ms_per_step": e_ms / args.steps}
         st.close()
 
+    # accuracy of the measured mode on the benchmark workload: image rel-L2 against the FP64 mode
+    # (the same candidates, all geometry, contributions and MIS weights in FP64)
+    accuracy = None
+    if not args.no_accuracy:
+        accuracy = image_accuracy(works[0], dev, mode, tuning, stream)
+
     # whole iteration on the device: light and camera passes, build, evaluate, image read back
     device_passes = None
     if not args.no_device_passes and cfg.name != "beamstress":
@@ -379,8 +386,27 @@ def run_b200(args, cfg, rank, world, local_rank):
         "clocks": clock,
         "generate_s": gen_s,
         "device_passes": device_passes,
+        "accuracy": accuracy,
     }
     return line
+
+
+def image_accuracy(w, dev, mode, tuning, stream):
+    """Image rel-L2 of `mode` against the GPU FP64 mode on workload `w` (one iteration)."""
+    import torch
+    from smallupbp_b200 import engine
+    imgs, counts = {}, {}
+    for m in (mode, engine.MODE_FP64):
+        with torch.cuda.stream(stream), engine.EstimatorStage(dev, m) as st:
+            st.set_stream(stream.cuda_stream)
+            st.set_tuning(**tuning["best"])
+            st.run(w)
+            imgs[m] = st.image().astype(np.float64)
+            counts[m] = int(st.query_stats()["count_bb1d"].astype(np.int64).sum())
+    a, b = imgs[mode], imgs[engine.MODE_FP64]
+    l2 = float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+    return {"image_rel_l2_vs_fp64": l2, "bound": 1e-3, "within_bound": l2 <= 1e-3,
+            "same_bb1d_candidates": counts[mode] == counts[engine.MODE_FP64]}
 
 
 def run_device_passes(args, cfg, dev, mode, stream, tuning, npix, rank, world):
