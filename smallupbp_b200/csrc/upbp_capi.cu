@@ -90,6 +90,8 @@ struct upbp_ctx {
     int bo_n_leaves = 0;
     // query order (Morton code of the query span's midpoint)
     DBuf q_keys, q_keys_sorted, q_iota, q_order;
+    // BB1D work order: the heavy queries (by PB2D candidate count) first
+    DBuf bb_keys, bb_keys_sorted, bb_iota, bb_order, bb_sum;
     bool order_queries = true;
     int bm_n_leaves = 0;
     // mixed mode: FP64 partial sums of the MIS walks
@@ -825,6 +827,32 @@ void do_evaluate(upbp_ctx* c)
         c->eval_launches += 1;
     }
     mark(c, 4, s);
+    // The per-query BB1D cost varies by an order of magnitude, and a heavy query drawn late from
+    // the work queue keeps a few warps busy after the others have finished.  Its PB2D candidate
+    // count predicts it (both grow with the beam and photon density along the ray), so the
+    // queries above kHeavyFactor x the mean PB2D count go first.
+    const int32_t* bb_order = order;
+    if (order && nq > 1 && !fused && c->bb1d_kernel >= 1 && (c->P.techniques & UPBP_PB2D) && c->n_ph > 0) {
+        constexpr unsigned kHeavyFactor = 4;
+        ensure(c, c->bb_keys, sizeof(uint32_t) * nq);
+        ensure(c, c->bb_keys_sorted, sizeof(uint32_t) * nq);
+        ensure(c, c->bb_iota, sizeof(int32_t) * nq);
+        ensure(c, c->bb_order, sizeof(int32_t) * nq);
+        ensure(c, c->bb_sum, sizeof(unsigned long long));
+        ck(c, cudaMemsetAsync(c->bb_sum.p, 0, sizeof(unsigned long long), s), "memset");
+        launch_heavy_keys(c->cnt_pb2d.as<uint32_t>(), nq, c->bb_sum.as<unsigned long long>(), kHeavyFactor,
+                          c->q_keys.as<uint32_t>(), c->bb_keys.as<uint32_t>(), c->bb_iota.as<int32_t>(), s);
+        size_t b = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, b, c->bb_keys.as<uint32_t>(), c->bb_keys_sorted.as<uint32_t>(),
+                                        c->bb_iota.as<int32_t>(), c->bb_order.as<int32_t>(), (int)nq, 0, 31, s);
+        ensure(c, c->cub_tmp, b);
+        ck(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, b, c->bb_keys.as<uint32_t>(),
+                                              c->bb_keys_sorted.as<uint32_t>(), c->bb_iota.as<int32_t>(),
+                                              c->bb_order.as<int32_t>(), (int)nq, 0, 31, s),
+           "SortPairs");
+        bb_order = c->bb_order.as<int32_t>();
+        c->eval_launches += 4;
+    }
     if (nq > 0) {
         const BeamBVH B = beam_bvh(c);
         const BeamSoA S = beam_soa(c);
@@ -840,7 +868,7 @@ void do_evaluate(upbp_ctx* c)
         } else if (c->bb1d_kernel >= 1) {
             const int grid = c->num_sms * bb1d_warp_blocks_per_sm(mixed, c->bb1d_kernel);
             launch_bb1d_warp(K, L, B, S, Q, cam, cs_seg, O, grid, mixed, c->work.as<unsigned int>(),
-                             c->status.as<int>(), order, s, c->bb1d_kernel);
+                             c->status.as<int>(), bb_order, s, c->bb1d_kernel);
             record_status(c, s);
         } else {
             launch_gather_bb1d(K, L, B, S, Q, cam, cs_seg, O, c->block, mixed, s);
@@ -922,7 +950,8 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->pb_r2, &c->bm_rchange, &c->bm_r2max, &c->knn_status, &c->bo_pos, &c->bo_pts, &c->bo_codes,
                    &c->bo_codes_sorted, &c->bo_idx, &c->bo_idx_sorted, &c->bo_bbox, &c->bo_leaf_codes, &c->bo_nodes,
                    &c->bo_parent_int, &c->bo_parent_leaf, &c->bo_leaf_boxes, &c->bo_node_boxes, &c->bo_flags,
-                   &c->tr_cnt, &c->tr_off, &c->tr_status};
+                   &c->tr_cnt, &c->tr_off, &c->tr_status, &c->bb_keys, &c->bb_keys_sorted, &c->bb_iota,
+                   &c->bb_order, &c->bb_sum};
     for (DBuf* b : all) free_buf(*b);
     if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)

@@ -1162,7 +1162,36 @@ __global__ void k_query_keys(const SegQueriesDev Q, const float* __restrict__ bb
     keys[q] = code;
     iota[q] = (int32_t)q;
 }
+// Sum of the per-query PB2D candidate counts (integer, so the order of the atomics does not matter).
+__global__ void k_sum_counts(const uint32_t* __restrict__ cnt, int64_t n, unsigned long long* sum)
+{
+    unsigned long long v = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v += cnt[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(sum, v);
+}
+
+// BB1D work order: the queries whose PB2D candidate count exceeds `factor` times the mean come
+// first (they are the heaviest BB1D queries too), each group in Morton order of the midpoints.
+__global__ void k_heavy_keys(const uint32_t* __restrict__ cnt, int64_t n, const unsigned long long* __restrict__ sum,
+                             unsigned factor, const uint32_t* __restrict__ morton, uint32_t* keys, int32_t* iota)
+{
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const bool heavy = (unsigned long long)cnt[q] * (unsigned long long)n > (unsigned long long)factor * *sum;
+    keys[q] = (heavy ? 0u : (1u << 30)) | morton[q];
+    iota[q] = (int32_t)q;
+}
 }  // namespace
+
+void launch_heavy_keys(const uint32_t* cnt, int64_t n, unsigned long long* sum, unsigned factor,
+                       const uint32_t* morton, uint32_t* keys, int32_t* iota, cudaStream_t stream)
+{
+    if (n <= 0) return;
+    k_sum_counts<<<148 * 4, 256, 0, stream>>>(cnt, n, sum);
+    k_heavy_keys<<<(int)((n + 255) / 256), 256, 0, stream>>>(cnt, n, sum, factor, morton, keys, iota);
+}
 
 void launch_piece_payload(const float4* pc, int n, const float4* bm_thr, const float4* bm_pdf, const int2* bm_link,
                           const float* bm_radius, const int4* lv_info, const upbp_mis* lv_mis, const LightSum* sums,

@@ -201,6 +201,10 @@ void launch_piece_payload(const float4* pc, int n, const float4* bm_thr, const f
                           const float* bm_radius, const int4* lv_info, const upbp_mis* lv_mis,
                           const struct LightSum* sums, PiecePayload* out, cudaStream_t stream);
 void launch_query_keys(const SegQueriesDev& Q, const float* bbox, uint32_t* keys, int32_t* iota, cudaStream_t stream);
+// keys that put the queries with more than `factor` x the mean PB2D candidate count first, each
+// group in the given Morton order; *sum must be zero on entry
+void launch_heavy_keys(const uint32_t* cnt, int64_t n, unsigned long long* sum, unsigned factor,
+                       const uint32_t* morton, uint32_t* keys, int32_t* iota, cudaStream_t stream);
 int bb1d_warp_blocks_per_sm(bool mixed, int variant);
 int pb2d_warp_blocks_per_sm(bool mixed);
 void launch_pb2d_warp(const GatherConsts& K, const LightSoA& L, const PhotonBVH& P, const SegQueriesDev& Q,
