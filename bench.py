@@ -298,36 +298,54 @@ def run_b200(args, cfg, rank, world, local_rank):
         except Exception:
             traffic = None
 
-    # end to end through the public API from page-locked host buffers
+    # end to end through the public API from page-locked host buffers.  Two contexts on two
+    # streams take the steps in turn, so that a step's uploads (on its context's stream) overlap
+    # the previous step's evaluation; every step still uploads all its inputs and reads its image
+    # back inside the timed region.
     e2e = None
     if not args.no_e2e:
         pw = pinned_copy(works[0])
-        st = engine.EstimatorStage(dev, mode)
-        st.set_stream(stream.cuda_stream)
-        st.set_tuning(**tuning["best"])
+        streams = [stream, torch.cuda.Stream(device=dev)]
+        ctxs = []
+        for k in range(2):
+            st = engine.EstimatorStage(dev, mode)
+            st.set_stream(streams[k].cuda_stream)
+            st.set_tuning(**tuning["best"])
+            ctxs.append(st)
         host_img = torch.empty(npix * 3, dtype=torch.float32).pin_memory()
         s = abi.make_structs(pw)
         e_units = units[0]
-        with torch.cuda.stream(stream):
-            for _ in range(max(1, args.warmup)):
-                st.load(pw, s); st.set_queries(pw, s); st.build(); st.clear_image(); st.evaluate()
-                st.read_image_into(host_img.data_ptr())
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(args.steps):
-                st.load(pw, s); st.set_queries(pw, s); st.build(); st.clear_image(); st.evaluate()
-                st.read_image_into(host_img.data_ptr())
-            e1.record(stream)
+
+        def e2e_steps(n):
+            prev = None
+            for k in range(n):
+                st = ctxs[k % 2]
+                with torch.cuda.stream(streams[k % 2]):
+                    st.load(pw, s); st.set_queries(pw, s); st.build(); st.clear_image(); st.evaluate()
+                if prev is not None:
+                    prev.read_image_into(host_img.data_ptr())
+                prev = st
+            prev.read_image_into(host_img.data_ptr())
+
+        e2e_steps(max(2, args.warmup))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(streams[0])
+        streams[1].wait_event(e0)
+        e2e_steps(args.steps)
+        streams[0].wait_stream(streams[1])
+        e1.record(streams[0])
         torch.cuda.synchronize()
         e_ms = e0.elapsed_time(e1)
         if world > 1:
             e_ms = multi.max_over_ranks(e_ms, "cuda")
         e2e = {"value": e_units * args.steps * world / (e_ms / 1000.0), "unit": "queries/s",
                "h2d_bytes_per_step": input_bytes(works[0]), "d2h_bytes_per_step": npix * 3 * 4,
-               "ms_per_step": e_ms / args.steps}
-        st.close()
+               "ms_per_step": e_ms / args.steps,
+               "pipeline": "two contexts alternate; a step's uploads overlap the previous step's evaluation"}
+        for st in ctxs:
+            st.close()
 
     # accuracy of the measured mode on the benchmark workload: image rel-L2 against the FP64 mode
     # (the same candidates, all geometry, contributions and MIS weights in FP64)
