@@ -256,8 +256,9 @@ int upbp_set_mode(upbp_ctx* ctx, int mode);
  * 4 warps per SM, 2: the same kernel compiled for 6 blocks per SM, 3 and 4: one persistent
  * work-queue kernel for all camera segments that evaluates PB2D and BB1D per query, at 5 or 6
  * blocks per SM; the PB2D phase of upbp_last_timings is then 0 and the BB1D phase covers both).
- * pb2d_kernel picks the PB2D gather when it runs on its own (bb1d_kernel 0-2): 0 one thread per
- * query, 1 one warp per query from a persistent work queue with the candidate queue.
+ * pb2d_kernel picks the PB2D gather when it runs on its own (bb1d_kernel 0-2), and the B-P2D
+ * gather (bb1d_kernel 1-4): 0 one thread per query, 1 one warp per query from a persistent work
+ * queue with the candidate queue.
  * Defaults: leaves of 4, 128 threads, pieces of 4 radii, variant 2, PB2D variant 1. */
 typedef struct upbp_tuning {
     int32_t pb2d_leaf;

@@ -106,8 +106,8 @@ struct upbp_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     bool replay = false;     // capturing: reuse the last build's counts, allocate nothing, no host syncs
     bool evaluated = false;  // an evaluate ran after the last build (every buffer is sized)
-    bool graph_status = false;  // the graph copies the BB1D traversal status back
-    bool status_pending = false;  // status_host holds the last BB1D launch's flag
+    bool graph_status = false;  // the graph copies the warp gathers' traversal status back
+    bool status_pending = false;  // status_host holds the last evaluate's warp-gather status flag
     int num_sms = 0;
     int bb1d_kernel = 2;  // 0: thread per query, 1-2: warp-cooperative BB1D, 3-4: fused segment kernel
     int pb2d_kernel = 1;  // PB2D on its own: 0 thread per query, 1 warp-cooperative persistent
@@ -144,13 +144,14 @@ void ck(upbp_ctx* c, cudaError_t e, const char* what)
     }
 }
 
-// After a synchronisation of the context's stream: the BB1D warp gather sets status[0] when a
-// query's traversal stack would overflow; its candidate set is then incomplete, which is an error.
+// After a synchronisation of the context's stream: the warp gathers (PB2D, BB1D, B-P2D) set
+// status[0] when a query's traversal stack would overflow; its candidate set is then incomplete,
+// which is an error.
 void check_status(upbp_ctx* c)
 {
     if (c->status_pending && c->status_host && *c->status_host != 0)
-        fail(c, UPBP_ERR_CAPACITY, "BB1D traversal stack overflow in the last evaluate: a candidate set is "
-                                   "incomplete (use a larger bb1d_leaf or beam_piece_radii)");
+        fail(c, UPBP_ERR_CAPACITY, "traversal stack overflow in the last evaluate: a candidate set is "
+                                   "incomplete (use a larger leaf size or beam_piece_radii)");
 }
 
 // Timing event; inside a graph capture it must be an external event record node, or the
@@ -716,6 +717,7 @@ gen::GenLaunch generic_launch(upbp_ctx* c, const CamSum* cs_seg, const CamSum* c
     A.status = c->status.as<int>();
     A.bb1d_grid = c->num_sms * gen::generic_bb1d_blocks_per_sm(grad_medium >= 0);
     A.pb2d_grid = c->num_sms * gen::generic_pb2d_blocks_per_sm(grad_medium >= 0);
+    A.bp2d_grid = c->num_sms * gen::generic_bp2d_blocks_per_sm(grad_medium >= 0);
     A.order = query_order(c, A.sq, c->stream);
     return A;
 }
@@ -785,6 +787,18 @@ void do_evaluate(upbp_ctx* c)
         c->evaluated = true;
         return;
     }
+    const bool fused = c->bb1d_kernel >= 3;  // PB2D and BB1D in the one persistent segment kernel
+    // B-P2D and PB2D are both 2-D kernel gathers; pb2d_kernel selects thread or warp per query for both
+    const bool bp2d_warp = bp2d && c->pb2d_kernel == 1 && c->bb1d_kernel >= 1;
+    if ((nq > 0 && c->bb1d_kernel >= 1) || bp2d_warp) {
+        // persistent warp kernels: work counters (BB1D or the fused kernel: [0], PB2D: [1],
+        // B-P2D: [2]) and the traversal status word they share
+        if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
+        ensure(c, c->work, sizeof(unsigned int) * 4);
+        ensure(c, c->status, sizeof(int) * 4);
+        ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
+        ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
+    }
     mark(c, 2, s);
     if (np > 0) {
         const HashGridDev G = hash_dev(c);
@@ -796,23 +810,17 @@ void do_evaluate(upbp_ctx* c)
         if (bp2d) {
             const Outputs Ob{c->out_bp2d.as<float>(), img, c->cnt_bp2d.as<uint32_t>(),
                              c->hash_bp2d.as<unsigned long long>(), tested + 3};
-            launch_gather_bp2d(K, beam_bvh(c), beam_soa(c), Q, Ob, c->block, s);
+            if (bp2d_warp)
+                launch_bp2d_warp(K, beam_bvh(c), beam_soa(c), Q, Ob, c->num_sms * bp2d_warp_blocks_per_sm(),
+                                 c->work.as<unsigned int>() + 2, c->status.as<int>(), s);
+            else
+                launch_gather_bp2d(K, beam_bvh(c), beam_soa(c), Q, Ob, c->block, s);
             c->eval_launches += 1;
         }
     }
     mark(c, 3, s);
     const SegQueriesDev Q = seg_dev(c);
     const int32_t* order = query_order(c, Q, s);
-    const bool fused = c->bb1d_kernel >= 3;  // PB2D and BB1D in the one persistent segment kernel
-    if (nq > 0 && c->bb1d_kernel >= 1) {
-        // persistent warp kernels: work counters (BB1D or the fused kernel: [0], PB2D: [1]) and the
-        // traversal status word they share
-        if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
-        ensure(c, c->work, sizeof(unsigned int) * 4);
-        ensure(c, c->status, sizeof(int) * 4);
-        ck(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned int) * 4, s), "memset");
-        ck(c, cudaMemsetAsync(c->status.p, 0, sizeof(int) * 4, s), "memset");
-    }
     if (nq > 0 && !fused) {
         const PhotonBVH B = photon_bvh(c);
         Outputs O{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
@@ -875,6 +883,7 @@ void do_evaluate(upbp_ctx* c)
         }
         c->eval_launches += 1;
     }
+    if (bp2d_warp && !c->status_pending) record_status(c, s);
     mark(c, 5, s);
     ck(c, cudaGetLastError(), "gather launch");
     c->evaluated = true;

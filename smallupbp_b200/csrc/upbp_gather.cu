@@ -945,6 +945,126 @@ __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ Gat
 // the beam as the ray and the query point as the photon; the piece containing the foot point
 // takes it.  Value: beam throughput x transmittance to the foot point (divided by the free-flight
 // pdf for SHORT beams) x sigma_s x HG phase x (1 - d^2/r^2) / (pi r^2 / 2).
+// B-P2D contribution of one accepted (point, beam) pair: beam throughput x transmittance to the
+// foot point t (divided by the free-flight pdf for SHORT beams) x sigma_s x HG x the 2-D kernel.
+__device__ __forceinline__ Rgb bp2d_contrib(const DMedium& m, const BeamSoA& Bs, int beam, V3 cfix, V3 bdir, float t,
+                                            float d2, float r2)
+{
+    const float4 bthr = __ldg(&Bs.thr[beam]);
+    Rgb att = eval_att(m, t);
+    const float pfd = comp(att, m.min_idx);
+    if ((uint32_t)__float_as_int(bthr.w) & UPBP_SHORT_BEAM) att = att / pfd;
+    if (!rgb_positive(att)) return rgb(0.f);
+    float sinT;
+    const float phase = hg_pdf(cfix, neg3(bdir), m.g, &sinT);
+    if (phase <= 0.f) return rgb(0.f);
+    const float kernel = (1.f - d2 / r2) / (r2 * UPBP_PI_F * 0.5f);
+    if (!is_pos(kernel)) return rgb(0.f);
+    const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
+    return Rgb{bthr.x, bthr.y, bthr.z} * att * ss * (phase * kernel);
+}
+
+// B-P2D, warp per point query, persistent: the lanes test 32 beam pieces at a time (the zero-length
+// ray at the point makes the slab test a point-in-box test); accepted pairs go to the candidate
+// queue and are evaluated 32 at a time.
+template <int kWarps, int kMinBlocks>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bp2d_warp(const __grid_constant__ GatherConsts K,
+                                                                     const BeamBVH B, const BeamSoA Bs,
+                                                                     const PointQueriesDev Q, const Outputs O,
+                                                                     unsigned int* __restrict__ work,
+                                                                     int* __restrict__ status)
+{
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    __shared__ int s_stack[kWarps][kWarpStack];
+    __shared__ int s_leaves[kWarps][kWarpLeaves];
+    __shared__ CandQueue s_queue[kWarps];
+    stage_media(K, media);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int* stack = s_stack[warp];
+    int* leaves = s_leaves[warp];
+    CandQueue& cq = s_queue[warp];
+    const int leaf_shift = __ffs(B.leaf) - 1;
+    for (;;) {
+        unsigned qq = 0;
+        if (lane == 0) qq = atomicAdd(work, 1u);
+        const int64_t q = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (q >= Q.n) break;
+        Rgb part = rgb(0.f);
+        unsigned long long cnt = 0, h = 0, tested = 0;
+        const int mid = Q.medium_id[q];
+        const DMedium& m = media[mid];
+        if ((K.P.techniques & UPBP_BP2D) && m.has_scat && B.n > 0) {
+            const V3 x = v3(Q.position[3 * q], Q.position[3 * q + 1], Q.position[3 * q + 2]);
+            const V3 cfix = v3(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
+            int qn = 0;
+            auto eval = [&](int e) {
+                const int i = cq.piece[e];
+                const float4 g = cq.geo[e];  // t, d^2, r^2, -
+                const float4 pb = __ldg(&B.pb[i]);
+                const float4 pc = __ldg(&B.pc[i]);
+                part = part + bp2d_contrib(m, Bs, __float_as_int(pc.z), cfix, v3(pb.x, pb.y, pb.z), g.x, g.y, g.z);
+            };
+            const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, stack,
+                                          leaves, lane, [&](int i) {
+                bool hit = false;
+                float t = 0.f, d2 = 0.f, r2 = 0.f;
+                if (i >= 0) {
+                    const float4 pc = __ldg(&B.pc[i]);
+                    if (__float_as_int(pc.w) == mid) {
+                        const float4 pa = __ldg(&B.pa[i]);
+                        const float4 pb = __ldg(&B.pb[i]);
+                        ++tested;
+                        // bound: the beam's largest radius^2; then the radius at the foot point
+                        if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &t, &d2) &&
+                            t >= pc.x && t < pc.y) {  // the piece containing the foot point
+                            const int beam = __float_as_int(pc.z);
+                            const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t);
+                            r2 = rt * rt;
+                            if (!(Bs.rchange && d2 > r2)) {
+                                hit = true;
+                                ++cnt;
+                                h += mix64((unsigned long long)beam);
+                            }
+                        }
+                    }
+                }
+                const unsigned vote = __ballot_sync(kFull, hit);
+                if (vote == 0u) return;
+                if (hit) {
+                    const int pos = qn + __popc(vote & lt);
+                    cq.piece[pos] = i;
+                    cq.geo[pos] = make_float4(t, d2, r2, 0.f);
+                }
+                qn += __popc(vote);
+                __syncwarp();
+                if (qn >= 32) {
+                    eval(qn - 32 + lane);
+                    qn -= 32;
+                    __syncwarp();
+                }
+            });
+            if (lane < qn) eval(lane);
+            __syncwarp();
+            if (!ok && lane == 0) atomicOr(status, 1);
+        }
+        const float r = warp_sum(part.r), g = warp_sum(part.g), b = warp_sum(part.b);
+        cnt = warp_sum_u64(cnt);
+        h = warp_sum_u64(h);
+        tested = warp_sum_u64(tested);
+        if (lane == 0) {
+            O.rgb[3 * q + 0] = r;
+            O.rgb[3 * q + 1] = g;
+            O.rgb[3 * q + 2] = b;
+            if (O.count) O.count[q] = (uint32_t)cnt;
+            if (O.hash) O.hash[q] = h;
+            const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+            splat(O.image, Q.pixel[q], thr * K.P.norm_bb1d * Rgb{r, g, b});
+            if (O.tested) atomicAdd(O.tested, tested);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ GatherConsts K, const BeamBVH B,
                                                      const BeamSoA Bs, const PointQueriesDev Q, const Outputs O)
 {
@@ -960,7 +1080,6 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
     const DMedium& m = media[mid];
     if ((K.P.techniques & UPBP_BP2D) && m.has_scat && B.n > 0) {
         const V3 cfix = v3(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
-        const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
         // a zero-length ray at x: the slab test becomes point-in-box
         traverse(B.nodes, B.n_leaves, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, [&](int leaf) {
             const int e = min(B.n, (leaf + 1) * B.leaf);
@@ -979,17 +1098,7 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
                 if (Bs.rchange && d2 > r2) continue;
                 ++cnt;
                 h += mix64((unsigned long long)beam);
-                const float4 bthr = __ldg(&Bs.thr[beam]);
-                Rgb att = eval_att(m, t);
-                const float pfd = comp(att, m.min_idx);
-                if ((uint32_t)__float_as_int(bthr.w) & UPBP_SHORT_BEAM) att = att / pfd;
-                if (!rgb_positive(att)) continue;
-                float sinT;
-                const float phase = hg_pdf(cfix, neg3(v3(pb.x, pb.y, pb.z)), m.g, &sinT);
-                if (phase <= 0.f) continue;
-                const float kernel = (1.f - d2 / r2) / (r2 * UPBP_PI_F * 0.5f);
-                if (!is_pos(kernel)) continue;
-                res = res + Rgb{bthr.x, bthr.y, bthr.z} * att * ss * (phase * kernel);
+                res = res + bp2d_contrib(m, Bs, beam, cfix, v3(pb.x, pb.y, pb.z), t, d2, r2);
             }
         });
     }
@@ -1011,6 +1120,19 @@ void launch_gather_bp2d(const GatherConsts& K, const BeamBVH& B, const BeamSoA& 
     if (Q.n <= 0) return;
     const int grid = (int)((Q.n + block - 1) / block);
     k_gather_bp2d<<<grid, block, 0, stream>>>(K, B, S, Q, O);
+}
+
+int bp2d_warp_blocks_per_sm()
+{
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bp2d_warp<4, 6>, 128, 0);
+    return nb > 0 ? nb : 1;
+}
+
+void launch_bp2d_warp(const GatherConsts& K, const BeamBVH& B, const BeamSoA& S, const PointQueriesDev& Q,
+                      const Outputs& O, int grid, unsigned int* work, int* status, cudaStream_t stream)
+{
+    if (Q.n > 0) k_bp2d_warp<4, 6><<<grid, 128, 0, stream>>>(K, B, S, Q, O, work, status);
 }
 
 void launch_gather_pb2d(const GatherConsts& K, const LightSoA& L, const PhotonBVH& B, const SegQueriesDev& Q,

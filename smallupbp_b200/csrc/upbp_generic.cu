@@ -603,63 +603,116 @@ __global__ void __launch_bounds__(128) k_gen_pp3d(const __grid_constant__ Gather
                     cnt, h);
 }
 
-// B-P2D (extension, standalone, MIS weight 1) in T: the foot point re-solved in FP64.
+// B-P2D contribution (extension, standalone, MIS weight 1) in T of an accepted (point x, piece)
+// pair: the foot point re-solved in FP64.  r2d is the radius^2 the FP32 predicate accepted with.
+template <class T>
+__device__ __forceinline__ RgbT<T> bp2d_contrib_t(const MedT<T>& m, const BeamSoA& Bs, float4 pa, float4 pb, int beam,
+                                                  V3 x, const V3d& cfix, double r2d)
+{
+    const V3d o = v3d(pa.x, pa.y, pa.z), d = v3d(pb.x, pb.y, pb.z), p = v3d(x);
+    const double t = dot(sub(p, o), d);
+    const V3d qv = V3d{o.x + d.x * t - p.x, o.y + d.y * t - p.y, o.z + d.z * t - p.z};
+    const double d2 = dot(qv, qv);
+    const float4 bthr = __ldg(&Bs.thr[beam]);
+    RgbT<T> att = eval_att(m, t);
+    const T pfd = comp(att, m.min_idx);
+    if ((uint32_t)__float_as_int(bthr.w) & UPBP_SHORT_BEAM) att = att / pfd;
+    if (!positive(att)) return rgb_zero<T>();
+    double sinT;
+    const T phase = hg_pdf(cfix, neg(d), m.g, &sinT);
+    if (!(val(phase) > 0.0)) return rgb_zero<T>();
+    const double kernel = (1.0 - d2 / r2d) / (r2d * 3.14159265358979323846 * 0.5);
+    if (!(kernel > 1e-20)) return rgb_zero<T>();
+    return RgbT<T>{att.r * (double)bthr.x, att.g * (double)bthr.y, att.b * (double)bthr.z} *
+           RgbT<T>{m.ss[0], m.ss[1], m.ss[2]} * (phase * kernel);
+}
+
+// B-P2D in T, warp per point query from the persistent work queue: the lanes test 32 beam pieces
+// at a time with the FP32 predicate (a zero-length ray at the point: the slab test is
+// point-in-box) and evaluate the accepted ones 32 at a time from the candidate queue.
 template <class T>
 __global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ GatherConsts K,
                                                   const __grid_constant__ GenConsts G, const BeamBVH B,
-                                                  const BeamSoA Bs, const PointQueriesDev Q, const GenOut O)
+                                                  const BeamSoA Bs, const PointQueriesDev Q, const GenOut O,
+                                                  unsigned int* __restrict__ work, int* __restrict__ status)
 {
+    constexpr int kWarps = 4;
     __shared__ MedT<T> media[UPBP_MAX_MEDIA];
+    __shared__ int s_stack[kWarps][kWarpStack];
+    __shared__ int s_leaves[kWarps][kWarpLeaves];
+    __shared__ int s_piece[kWarps][kGenQueue];
+    __shared__ float s_r2[kWarps][kGenQueue];
     stage_media_t<T>(G, media);
-    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool valid = q < Q.n;
-    uint32_t cnt = 0;
-    unsigned long long h = 0;
-    RgbT<T> res = rgb_zero<T>();
-    if (valid) {
-        const V3 x = v3(Q.position[3 * q], Q.position[3 * q + 1], Q.position[3 * q + 2]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int* stack = s_stack[warp];
+    int* leaves = s_leaves[warp];
+    int* cq = s_piece[warp];
+    float* cr2 = s_r2[warp];
+    const int leaf_shift = __ffs(B.leaf) - 1;
+    for (;;) {
+        unsigned qq = 0;
+        if (lane == 0) qq = atomicAdd(work, 1u);
+        const int64_t q = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (q >= Q.n) break;
+        RgbT<T> acc = rgb_zero<T>();
+        unsigned long long cnt = 0, h = 0;
         const int mid = Q.medium_id[q];
         const MedT<T>& m = media[mid];
         if ((K.P.techniques & UPBP_BP2D) && m.has_scat && B.n > 0) {
+            const V3 x = v3(Q.position[3 * q], Q.position[3 * q + 1], Q.position[3 * q + 2]);
             const V3d cfix = v3d(Q.dir_fix[3 * q], Q.dir_fix[3 * q + 1], Q.dir_fix[3 * q + 2]);
-            traverse(B.nodes, B.n_leaves, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, [&](int leaf) {
-                const int e = min(B.n, (leaf + 1) * B.leaf);
-                for (int i = leaf * B.leaf; i < e; ++i) {
+            int qn = 0;
+            auto eval = [&](int e) {
+                const int i = cq[e];
+                const float4 pc = __ldg(&B.pc[i]);
+                acc = acc + bp2d_contrib_t<T>(m, Bs, __ldg(&B.pa[i]), __ldg(&B.pb[i]), __float_as_int(pc.z), x, cfix,
+                                              (double)cr2[e]);
+            };
+            const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, x, v3(1.f, 1.f, 1.f), 0.f, 0.f, stack,
+                                          leaves, lane, [&](int i) {
+                bool hit = false;
+                float r2 = 0.f;
+                if (i >= 0) {
                     const float4 pc = __ldg(&B.pc[i]);
-                    if (__float_as_int(pc.w) != mid) continue;
-                    const float4 pa = __ldg(&B.pa[i]);
-                    const float4 pb = __ldg(&B.pb[i]);
-                    float tf, d2f;
-                    if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &tf, &d2f)) continue;
-                    if (!(tf >= pc.x && tf < pc.y)) continue;
-                    const int beam = __float_as_int(pc.z);
-                    const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), tf), r2 = rt * rt;
-                    if (Bs.rchange && d2f > r2) continue;
-                    const double r2d = r2;
-                    ++cnt;
-                    h += mix64((unsigned long long)beam);
-                    const V3d o = v3d(pa.x, pa.y, pa.z), d = v3d(pb.x, pb.y, pb.z), p = v3d(x);
-                    const double t = dot(sub(p, o), d);
-                    const V3d qv = V3d{o.x + d.x * t - p.x, o.y + d.y * t - p.y, o.z + d.z * t - p.z};
-                    const double d2 = dot(qv, qv);
-                    const float4 bthr = __ldg(&Bs.thr[beam]);
-                    RgbT<T> att = eval_att(m, t);
-                    const T pfd = comp(att, m.min_idx);
-                    if ((uint32_t)__float_as_int(bthr.w) & UPBP_SHORT_BEAM) att = att / pfd;
-                    if (!positive(att)) continue;
-                    double sinT;
-                    const T phase = hg_pdf(cfix, neg(d), m.g, &sinT);
-                    if (!(val(phase) > 0.0)) continue;
-                    const double kernel = (1.0 - d2 / r2d) / (r2d * 3.14159265358979323846 * 0.5);
-                    if (!(kernel > 1e-20)) continue;
-                    res = res + RgbT<T>{att.r * (double)bthr.x, att.g * (double)bthr.y, att.b * (double)bthr.z} *
-                                    RgbT<T>{m.ss[0], m.ss[1], m.ss[2]} * (phase * kernel);
+                    if (__float_as_int(pc.w) == mid) {
+                        const float4 pa = __ldg(&B.pa[i]);
+                        const float4 pb = __ldg(&B.pb[i]);
+                        float tf, d2f;
+                        if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &tf, &d2f) &&
+                            tf >= pc.x && tf < pc.y) {
+                            const int beam = __float_as_int(pc.z);
+                            const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), tf);
+                            r2 = rt * rt;
+                            if (!(Bs.rchange && d2f > r2)) {
+                                hit = true;
+                                ++cnt;
+                                h += mix64((unsigned long long)beam);
+                            }
+                        }
+                    }
+                }
+                const unsigned vote = __ballot_sync(kFull, hit);
+                if (vote == 0u) return;
+                if (hit) {
+                    const int pos = qn + __popc(vote & lt);
+                    cq[pos] = i;
+                    cr2[pos] = r2;
+                }
+                qn += __popc(vote);
+                __syncwarp();
+                if (qn >= 32) {
+                    eval(qn - 32 + lane);
+                    qn -= 32;
+                    __syncwarp();
                 }
             });
+            if (lane < qn) eval(lane);
+            __syncwarp();
+            if (!ok && lane == 0) atomicOr(status, 1);
         }
+        finish_warp<T>(O, q, acc, Q.pixel[q], Q.throughput + 3 * q, K.P.norm_bb1d, cnt, h, lane);
     }
-    finish_lanes<T>(O, valid, q, res, valid ? Q.pixel[q] : -1, valid ? Q.throughput + 3 * q : nullptr, K.P.norm_bb1d,
-                    cnt, h);
 }
 
 }  // namespace
@@ -671,7 +724,7 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
         k_gen_pp3d<T><<<(unsigned)((A.pq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.L, A.hash, A.pq, A.cam, A.cs_pt,
                                                                         A.out_pp3d);
     if (A.pq.n > 0 && A.beams.n > 0 && (A.K.P.techniques & UPBP_BP2D))
-        k_gen_bp2d<T><<<(unsigned)((A.pq.n + 127) / 128), 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.pq, A.out_bp2d);
+        k_gen_bp2d<T><<<A.bp2d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.pq, A.out_bp2d, A.work + 2, A.status);
     if (A.sq.n > 0 && A.photons.n > 0)
         k_gen_pb2d<T><<<A.pb2d_grid, 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam, A.cs_seg, A.out_pb2d,
                                                   A.work + 1, A.status, A.order);
@@ -691,6 +744,14 @@ int generic_pb2d_blocks_per_sm(bool adjoint)
     int nb = 0;
     if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<Dual>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<double>, 128, 0);
+    return nb > 0 ? nb : 1;
+}
+
+int generic_bp2d_blocks_per_sm(bool adjoint)
+{
+    int nb = 0;
+    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bp2d<Dual>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bp2d<double>, 128, 0);
     return nb > 0 ? nb : 1;
 }
 

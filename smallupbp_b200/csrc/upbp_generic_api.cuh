@@ -39,16 +39,18 @@ struct GenLaunch {
     const CamSum* cs_seg;
     const CamSum* cs_pt;
     GenOut out_pb2d, out_bb1d, out_pp3d, out_bp2d;
-    unsigned int* work;  // work counters, [0] BB1D and [1] PB2D (zeroed by the caller)
+    unsigned int* work;  // work counters, [0] BB1D, [1] PB2D and [2] B-P2D (zeroed by the caller)
     int* status;         // traversal status (zeroed by the caller)
     int bb1d_grid;
     int pb2d_grid;
+    int bp2d_grid;
     const int32_t* order;  // segment queries in Morton order of their midpoints, or nullptr
 };
 
 void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream);
 int generic_bb1d_blocks_per_sm(bool adjoint);
 int generic_pb2d_blocks_per_sm(bool adjoint);
+int generic_bp2d_blocks_per_sm(bool adjoint);
 
 }  // namespace gen
 }  // namespace upbp

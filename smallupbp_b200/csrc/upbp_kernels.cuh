@@ -221,6 +221,9 @@ void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B
                       int variant);
 void launch_gather_bp2d(const GatherConsts& K, const BeamBVH& B, const BeamSoA& S, const PointQueriesDev& Q,
                         const Outputs& O, int block, cudaStream_t stream);
+int bp2d_warp_blocks_per_sm();
+void launch_bp2d_warp(const GatherConsts& K, const BeamBVH& B, const BeamSoA& S, const PointQueriesDev& Q,
+                      const Outputs& O, int grid, unsigned int* work, int* status, cudaStream_t stream);
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,
                         const upbp_mis* cam, const CamSum* cs, const Outputs& O, int block, bool mixed,
                         cudaStream_t stream);

@@ -42,13 +42,17 @@ def test_off_by_default_and_not_a_reference_bit():
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode", [engine.MODE_PLAIN, engine.MODE_MIXED], ids=["plain", "mixed"])
 @pytest.mark.parametrize("name", ["cube32x2048", "cube64x4096"])
-def test_gpu_bp2d_matches_oracle(mode, name):
+@pytest.mark.parametrize("pb2d_kernel", [0, 1], ids=["thread", "warp"])
+def test_gpu_bp2d_matches_oracle(mode, name, pb2d_kernel):
+    # pb2d_kernel selects the thread-per-query or the warp-cooperative persistent gather (B-P2D
+    # follows the PB2D choice)
     from oracle import port
 
     w = _workload(name)
     o = port.bp2d(w)
     rest = port.run(w)
     with engine.EstimatorStage(0, mode) as st:
+        st.set_tuning(pb2d_kernel=pb2d_kernel)
         st.run(w)
         rgb, cnt, h = st.bp2d_results()
         img = st.image()
