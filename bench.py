@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-device-passes", action="store_true",
                     help="skip the iteration traced on the device (light + camera passes, build, evaluate)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
+    ap.add_argument("--tuning", default=None,
+                    help='fixed tuning instead of the autotuner, JSON (e.g. \'{"bb1d_leaf": 8, "beam_piece_radii": 6}\')')
     ap.add_argument("--no-graph", action="store_true", help="direct calls instead of the captured CUDA graph")
     ap.add_argument("--adjoint", action="store_true",
                     help="time forward + adjoint (dL/d sigma_a, sigma_s, g) of an L2 image loss instead")
@@ -196,10 +198,12 @@ def run_b200(args, cfg, rank, world, local_rank):
         st.set_queries(w, s)
         if args.dropin:
             st.set_tuning(bb1d_kernel=0)
+        if args.tuning:
+            st.set_tuning(**json.loads(args.tuning))
         stages.append(st)
         all_structs.append(s)
     tuning = {"best": {k: getattr(stages[0].get_tuning(), k) for k, _ in abi.Tuning._fields_}, "autotuned": False}
-    if not args.no_autotune:
+    if not args.no_autotune and not args.tuning:
         from smallupbp_b200 import autotune
         t_at = time.time()
         with torch.cuda.stream(stream):

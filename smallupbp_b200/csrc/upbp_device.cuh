@@ -131,6 +131,15 @@ __device__ __forceinline__ bool test_bre(V3 o, V3 d, float tmin, float tmax, V3 
     return false;
 }
 
+// The first check of test_beam_beam: false where it rejects by the distance of the lines alone.
+__device__ __forceinline__ bool beam_beam_near(V3 O1, V3 d1, V3 O2, V3 d2, float maxDistSqr)
+{
+    const V3 c = xcross3(d1, d2);
+    const float sinThetaSqr = xdot3(c, c);
+    const float ad = xdot3(xsub3(O2, O1), c);
+    return !(xmul(ad, ad) >= xmul(maxDistSqr, sinThetaSqr));
+}
+
 // PhotonBeam::testIntersectionBeamBeam (Beams/PhotonBeam.hxx:238-296)
 __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float maxT1, V3 O2, V3 d2, float minT2,
                                                float maxT2, float maxDistSqr, float* oDist, float* oSin, float* oT1,

@@ -508,6 +508,7 @@ constexpr int kCandQueue = 64;
 struct CandQueue {
     int piece[kCandQueue];
     float4 geo[kCandQueue];  // dist, sin(theta), t1 (query), t2 (beam)
+    int near[kCandQueue];    // BB1D: pieces past the predicate's first check, waiting for the rest
 };
 
 // Per-warp scratch of the warp-cooperative gathers (shared memory).
@@ -564,8 +565,9 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                                                   g.z, g.w);
             }
         };
-        const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps, s.dmax + K.eps,
-                                      ws.stack, ws.leaves, lane, [&](int i) {
+        // the rest of the predicate for one piece per lane (i < 0: none) that passed its first
+        // check; accepted candidates go to the candidate queue
+        auto full = [&](int i) {
             bool hit = false;
             int entry = 0;
             float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f;
@@ -574,7 +576,6 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                 // the pieces that pass it
                 const float4 pa = __ldg(&B.pa[i]);
                 const float4 pb = __ldg(&B.pb[i]);
-                ++tested;
                 if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
                                    pb.w, &dist, &sinT, &t1, &t2)) {
                     const float4 pc = __ldg(&B.pc[i]);
@@ -605,7 +606,34 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                 qn -= 32;
                 __syncwarp();
             }
+        };
+        // about half of the tested pieces fail the predicate's first check (the distance of the
+        // lines); the others are queued and the rest of the predicate runs 32 at a time
+        int pn = 0;  // entries in the near queue (warp-uniform)
+        const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps, s.dmax + K.eps,
+                                      ws.stack, ws.leaves, lane, [&](int i) {
+            bool near = false;
+            if (i >= 0) {
+                const float4 pa = __ldg(&B.pa[i]);
+                const float4 pb = __ldg(&B.pb[i]);
+                ++tested;
+                near = beam_beam_near(s.o, s.d, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pb.w);
+            }
+            const unsigned vote = __ballot_sync(kFull, near);
+            if (vote == 0u) return;
+            if (near) cq.near[pn + __popc(vote & lt)] = i;
+            pn += __popc(vote);
+            __syncwarp();
+            if (pn >= 32) {
+                full(cq.near[pn - 32 + lane]);
+                pn -= 32;
+                __syncwarp();
+            }
         });
+        if (pn > 0) {
+            full(lane < pn ? cq.near[lane] : -1);
+            __syncwarp();
+        }
         if (lane < qn) eval(lane);
         __syncwarp();
         if (!ok && lane == 0) atomicOr(status, 1);
