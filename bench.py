@@ -64,10 +64,15 @@ def parse():
     ap.add_argument("--adjoint", action="store_true",
                     help="time forward + adjoint (dL/d sigma_a, sigma_s, g) of an L2 image loss instead")
     ap.add_argument("--dropin", action="store_true",
-                    help="the plain FP32 drop-in: thread-per-query BB1D gather, plain mode, default tuning")
+                    help="the plain FP32 drop-in: thread-per-query BB1D gather, plain mode, leaves of 2 and 3 r "
+                         "pieces (the best of a leaf / piece sweep for that gather on cube512)")
     a = ap.parse_args()
     if a.dropin:
         a.mode, a.no_autotune = "plain", True
+        t = {"bb1d_leaf": 2, "beam_piece_radii": 3.0}
+        t.update(json.loads(a.tuning) if a.tuning else {})
+        t["bb1d_kernel"] = 0
+        a.tuning = json.dumps(t)
     return a
 
 
@@ -196,8 +201,6 @@ def run_b200(args, cfg, rank, world, local_rank):
         s = abi.make_structs(w)
         st.load(w, s)
         st.set_queries(w, s)
-        if args.dropin:
-            st.set_tuning(bb1d_kernel=0)
         if args.tuning:
             st.set_tuning(**json.loads(args.tuning))
         stages.append(st)

@@ -259,7 +259,8 @@ int upbp_set_mode(upbp_ctx* ctx, int mode);
  * pb2d_kernel picks the PB2D gather when it runs on its own (bb1d_kernel 0-2), and the B-P2D
  * gather (bb1d_kernel 1-4): 0 one thread per query, 1 one warp per query from a persistent work
  * queue with the candidate queue.
- * Defaults: leaves of 4, 128 threads, pieces of 4 radii, variant 2, PB2D variant 1. */
+ * Defaults: photon leaves of 4, beam-piece leaves of 8, 128 threads, pieces of 6 radii, variant 2,
+ * PB2D variant 1. */
 typedef struct upbp_tuning {
     int32_t pb2d_leaf;
     int32_t bb1d_leaf;

@@ -30,7 +30,7 @@ from typing import Dict, Iterable, List, Optional, Tuple
 # searched one stage at a time (coordinate descent), each stage a grid over its knobs
 STAGES = (
     {"bb1d_kernel": (1, 2, 3, 4)},
-    {"bb1d_leaf": (2, 4, 8), "beam_piece_radii": (3.0, 4.0, 6.0)},
+    {"bb1d_leaf": (4, 8, 16), "beam_piece_radii": (4.0, 6.0, 8.0)},
     {"pb2d_kernel": (0, 1), "pb2d_leaf": (4, 8, 16), "block_threads": (128, 256)},
 )
 

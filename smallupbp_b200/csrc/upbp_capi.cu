@@ -39,9 +39,9 @@ struct upbp_ctx {
     cudaStream_t stream = nullptr;
     int mode = UPBP_MODE_PLAIN;
     int pb2d_leaf = 4;
-    int bb1d_leaf = 4;
+    int bb1d_leaf = 8;
     int block = 128;
-    float piece_len_r = 4.f;  // beam piece length in units of the beam radius
+    float piece_len_r = 6.f;  // beam piece length in units of the beam radius
     std::string err;
     upbp_params P{};
     bool have_params = false;

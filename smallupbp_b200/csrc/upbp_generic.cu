@@ -432,7 +432,8 @@ __global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ Gather
 
 
 
-// BB1D, warp per query with the candidate queue of the FP32 warp kernel.
+// BB1D, warp per query with the two queues of the FP32 warp kernel: pieces past the predicate's
+// first check, then accepted candidates.
 template <class T>
 __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ GatherConsts K,
                                                   const __grid_constant__ GenConsts G, const BeamBVH B,
@@ -446,12 +447,14 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
     __shared__ int s_stack[kWarps][kWarpStack];
     __shared__ int s_leaves[kWarps][kWarpLeaves];
     __shared__ int s_piece[kWarps][kGenQueue];
+    __shared__ int s_near[kWarps][kGenQueue];
     stage_media_t<T>(G, media);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     int* stack = s_stack[warp];
     int* leaves = s_leaves[warp];
     int* cq = s_piece[warp];
+    int* nq = s_near[warp];
     const int leaf_shift = __ffs(B.leaf) - 1;
     for (;;) {
         unsigned qq = 0;
@@ -476,8 +479,8 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                     const double rchg = Bs.rchange ? (double)__ldg(&Bs.rchange[__float_as_int(__ldg(&B.pc[i]).z)]) : 0.0;
                     part = part + bb1d_contrib<T>(K, m, s, py, v3d(pa.x, pa.y, pa.z), v3d(pb.x, pb.y, pb.z), rchg);
                 };
-                const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.of, inv, dminf - K.eps,
-                                              dmaxf + K.eps, stack, leaves, lane, [&](int i) {
+                // the rest of the predicate for one piece per lane (i < 0: none)
+                auto full = [&](int i) {
                     bool hit = false;
                     if (i >= 0) {
                         const float4 pc = __ldg(&B.pc[i]);
@@ -506,7 +509,31 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                         qn -= 32;
                         __syncwarp();
                     }
+                };
+                int pn = 0;  // entries in the near queue
+                const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.of, inv, dminf - K.eps,
+                                              dmaxf + K.eps, stack, leaves, lane, [&](int i) {
+                    bool near = false;
+                    if (i >= 0) {
+                        const float4 pa = __ldg(&B.pa[i]);
+                        const float4 pb = __ldg(&B.pb[i]);
+                        near = beam_beam_near(s.of, s.df, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pb.w);
+                    }
+                    const unsigned vote = __ballot_sync(kFull, near);
+                    if (vote == 0u) return;
+                    if (near) nq[pn + __popc(vote & lt)] = i;
+                    pn += __popc(vote);
+                    __syncwarp();
+                    if (pn >= 32) {
+                        full(nq[pn - 32 + lane]);
+                        pn -= 32;
+                        __syncwarp();
+                    }
                 });
+                if (pn > 0) {
+                    full(lane < pn ? nq[lane] : -1);
+                    __syncwarp();
+                }
                 if (lane < qn) eval(lane);
                 __syncwarp();
                 if (!ok && lane == 0) atomicOr(status, 1);

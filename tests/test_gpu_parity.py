@@ -104,7 +104,7 @@ def test_bb1d_kernel_variants_same_candidates(stage, kernel, leaf):
         G.assert_close(g["bb1d"], r["bb1d_brute"], "BB1D")
         G.assert_close(g["pb2d"], r["pb2d"], "PB2D")
     finally:
-        stage.set_tuning(bb1d_kernel=2, bb1d_leaf=4, beam_piece_radii=4.0)
+        stage.set_tuning(bb1d_kernel=2, bb1d_leaf=8, beam_piece_radii=6.0)
 
 
 @pytest.mark.gpu
