@@ -507,12 +507,25 @@ def cpu_baseline(w, seconds: float) -> dict:
     t = sess.eval(0, stride)
     sess.close()
     full_ms = sess.build_ms + t * stride
-    return {"value": total / (full_ms / 1000.0), "unit": "queries/s", "cores": threads, "kind": "reference",
-            "sample": "reference SmallUPBP estimators (EmbreeBre + PhotonBeamsEvaluator USE_GRID -gridres 64 + "
-                      "HashGrid/RangeQuery), one structure set per thread; every %d-th query timed (%.1f s) and "
-                      "extrapolated linearly, plus the per-thread build (%.1f s)" % (stride, t / 1000.0,
-                                                                                     sess.build_ms / 1000.0),
-            "ms_per_iteration": full_ms}
+    out = {"value": total / (full_ms / 1000.0), "unit": "queries/s", "cores": threads, "kind": "reference",
+           "sample": "reference SmallUPBP estimators (EmbreeBre + PhotonBeamsEvaluator USE_GRID -gridres 64 + "
+                     "HashGrid/RangeQuery), one structure set per thread; every %d-th query timed (%.1f s) and "
+                     "extrapolated linearly, plus the per-thread build (%.1f s)" % (stride, t / 1000.0,
+                                                                                    sess.build_ms / 1000.0),
+           "ms_per_iteration": full_ms}
+    # the same code on one core: its own build plus a sample about a quarter as long
+    one = ref.Session(w, ref.PB2D | ref.BB1D_GRID | ref.PP3D, 1)
+    n_max = max(n_seg, n_pt)
+    pstride = max(1, n_max // 64)
+    per_query1 = one.eval(1, pstride) / max(1, len(range(1, n_max, pstride)))
+    stride1 = max(1, int(math.ceil(per_query1 * n_max / (seconds * 250.0))))
+    t1 = one.eval(0, stride1)
+    one.close()
+    ms1 = one.build_ms + t1 * stride1
+    out["one_core"] = {"value": total / (ms1 / 1000.0), "unit": "queries/s", "ms_per_iteration": ms1,
+                       "sample": "every %d-th query timed on one thread (%.1f s), plus its build (%.1f s)" % (
+                           stride1, t1 / 1000.0, one.build_ms / 1000.0)}
+    return out
 
 
 def run_reference(args, cfg, rank, world):

@@ -645,6 +645,7 @@ BeamSoA beam_soa(upbp_ctx* c)
     S.radius = c->bm_radius.as<float>();
     S.rchange = (c->P.bb1d_knn > 0 && c->n_beams > 0 && (c->P.techniques & UPBP_BB1D)) ? c->bm_rchange.as<float>()
                                                                                           : nullptr;
+    S.radius_const = c->P.radius_bb1d;  // what k_pack_beams stores for every beam without KNN radii
     S.n = c->n_beams;
     return S;
 }

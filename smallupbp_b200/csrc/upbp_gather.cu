@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                                     pc.y, t1, t2))
                         continue;
                     const int beam = __float_as_int(pc.z);
-                    const float radius = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t2);
+                    const float radius = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), t2);
                     if (radius < dist) continue;  // PhotonBeam.hxx:411-413
                     ++cnt;
                     h += mix64((unsigned long long)beam);
@@ -561,7 +561,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                                                   g.z, g.w, beam_radius_at(Bs, beam, py.lv.z, g.w));
             } else {
                 part = part + bb1d_contrib<false>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                                  beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), g.w), g.x, g.y,
+                                                  beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), g.w), g.x, g.y,
                                                   g.z, g.w);
             }
         };
@@ -586,7 +586,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                     if (own != 0) {  // this piece may take it: the radius test (PhotonBeam.hxx:411-413)
                         const int beam = __float_as_int(pc.z);
                         const float radius = beam_radius_at(
-                            Bs, beam, kMixed ? __ldg(&B.pay[i].lv.z) : __ldg(&Bs.radius[beam]), t2);
+                            Bs, beam, beam_start_radius(Bs, kMixed ? &B.pay[i].lv.z : &Bs.radius[beam]), t2);
                         hit = !(radius < dist);
                         entry = own > 0 ? i : ~i;
                     }
@@ -1047,7 +1047,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bp2d_warp(const __g
                         if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &t, &d2) &&
                             t >= pc.x && t < pc.y) {  // the piece containing the foot point
                             const int beam = __float_as_int(pc.z);
-                            const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t);
+                            const float rt = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), t);
                             r2 = rt * rt;
                             if (!(Bs.rchange && d2 > r2)) {
                                 hit = true;
@@ -1122,7 +1122,7 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
                 if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &t, &d2)) continue;
                 if (!(t >= pc.x && t < pc.y)) continue;  // the piece containing the foot point
                 const int beam = __float_as_int(pc.z);
-                const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), t), r2 = rt * rt;
+                const float rt = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), t), r2 = rt * rt;
                 if (Bs.rchange && d2 > r2) continue;
                 ++cnt;
                 h += mix64((unsigned long long)beam);

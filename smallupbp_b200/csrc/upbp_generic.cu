@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                                                0.f, pa.w, pb.w, &dist, &sinT, &t1, &t2) &&
                                 piece_owns(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w,
                                            pc.x, pc.y, t1, t2) &&
-                                !(beam_radius_at(Bs, __float_as_int(pc.z), __ldg(&B.pay[i].lv.z), t2) < dist)) {
+                                !(beam_radius_at(Bs, __float_as_int(pc.z), beam_start_radius(Bs, &B.pay[i].lv.z), t2) < dist)) {
                                 hit = true;
                                 ++cnt;
                                 h += mix64((unsigned long long)__float_as_int(pc.z));
@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ Gather
                         if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &tf, &d2f) &&
                             tf >= pc.x && tf < pc.y) {
                             const int beam = __float_as_int(pc.z);
-                            const float rt = beam_radius_at(Bs, beam, __ldg(&Bs.radius[beam]), tf);
+                            const float rt = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), tf);
                             r2 = rt * rt;
                             if (!(Bs.rchange && d2f > r2)) {
                                 hit = true;

@@ -71,8 +71,16 @@ struct BeamSoA {
     const int2* link;    // light vertex, medium
     const float* radius; // start radius (the constant radius, or the KNN start radius)
     const float* rchange; // KNN radii: radius change per unit length (NULL: constant radius)
+    float radius_const;   // every beam's radius when rchange is NULL
     int64_t n;
 };
+
+// Start radius of a beam: the constant radius, or with KNN radii the beam's own, loaded from
+// `start` only then.
+__device__ __forceinline__ float beam_start_radius(const BeamSoA& S, const float* start)
+{
+    return S.rchange ? __ldg(start) : S.radius_const;
+}
 
 // Radius of a beam at t (PhotonBeam.hxx:411: mStartRadius + t * mRadiusChange).
 __device__ __forceinline__ float beam_radius_at(const BeamSoA& S, int beam, float start, float t)
