@@ -28,7 +28,11 @@ def nvcc() -> str:
 
 # Per-file flags: the device-side light and camera passes reproduce the host generator's FP64
 # operation order, so no multiply-add may be contracted there.
-FILE_FLAGS = {"upbp_trace.cu": ["-fmad=false"]}
+# upbp_trace.cu: the light and camera passes reproduce the host generator's FP64 arithmetic bit for
+# bit, so no FMA contraction.  upbp_gather.cu: the contributions use the fast approximate FP32
+# division (at most 2 ulp); the candidate predicates and the traversal use explicit IEEE
+# intrinsics (__fdiv_rn, __frcp_rn, __fmul_rn, ...), which the flag does not change.
+FILE_FLAGS = {"upbp_trace.cu": ["-fmad=false"], "upbp_gather.cu": ["-prec-div=false"]}
 
 
 def sources():

@@ -22,7 +22,8 @@ __device__ __forceinline__ bool slab(float lx, float ly, float lz, float hx, flo
     return tn <= tf;
 }
 
-__device__ __forceinline__ float safe_inv(float d) { return 1.f / (d == 0.f ? copysignf(1e-30f, d) : d); }
+// IEEE reciprocal whatever the file's division flags: the slab tests of the traversal use it
+__device__ __forceinline__ float safe_inv(float d) { return __frcp_rn(d == 0.f ? copysignf(1e-30f, d) : d); }
 
 // Stack traversal of a BVH2 with child boxes; calls leaf(k) for every leaf whose box the
 // segment [tmin, tmax] overlaps.  Returns false on stack overflow (reported through the
