@@ -535,7 +535,8 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
     const unsigned lt = ws.lt;
     CandQueue& cq = *ws.cq;
     const int leaf_shift = __ffs(B.leaf) - 1;
-    return segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
+    unsigned cnt32 = 0, tested32 = 0;  // per query: below 2^32
+    const Rgb res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
         Rgb part = rgb(0.f);
         const int mid = (int)(&m - media);
         int qn = 0;  // entries in the candidate queue (warp-uniform)
@@ -552,7 +553,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
             if (undecided &&
                 !piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y))
                 return;
-            ++cnt;
+            ++cnt32;
             h += mix64((unsigned long long)__float_as_int(pc.z));
             const int beam = __float_as_int(pc.z);
             if (kMixed) {
@@ -616,7 +617,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
             if (i >= 0) {
                 const float4 pa = __ldg(&B.pa[i]);
                 const float4 pb = __ldg(&B.pb[i]);
-                ++tested;
+                ++tested32;
                 near = beam_beam_near(s.o, s.d, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pb.w);
             }
             const unsigned vote = __ballot_sync(kFull, near);
@@ -639,6 +640,9 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
         if (!ok && lane == 0) atomicOr(status, 1);
         return part;
     });
+    cnt += cnt32;
+    tested += tested32;
+    return res;
 }
 
 // PB2D of one query by one warp over the photon LBVH, with the same candidate queue.
