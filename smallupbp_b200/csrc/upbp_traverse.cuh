@@ -27,7 +27,8 @@ __device__ __forceinline__ float safe_inv(float d) { return __frcp_rn(d == 0.f ?
 
 // Stack traversal of a BVH2 with child boxes; calls leaf(k) for every leaf whose box the
 // segment [tmin, tmax] overlaps.  Returns false on stack overflow (reported through the
-// status word; the 30-bit Morton build never gets that deep).
+// status word).  The stack holds at most one entry per tree level, and the LBVH has at most 63
+// (see kMaxTreeDepth below), so the 96 entries do not overflow.
 template <class LeafFn>
 __device__ __forceinline__ bool traverse(const BNode* __restrict__ nodes, int n_leaves, V3 o, V3 inv, float tmin,
                                          float tmax, LeafFn&& leaf)
@@ -77,7 +78,14 @@ __device__ __forceinline__ void splat(float* image, int px, Rgb v)
 // appends leaf hits to the warp's leaf list; once 32 leaves are gathered (or the traversal is
 // done) the warp tests the leaves' primitives 32 at a time, consecutive primitives to
 // consecutive lanes.  Returns false if the stack overflowed (the status word records it).
+//
+// The stack cannot overflow.  A step pops `take` nodes and pushes at most 2 x take children, so it
+// grows by at most `take`.  Up to kWarpStack - kMaxTreeDepth entries the warp pops as many as keep
+// it there (32 at most); above that it pops one node per step, a depth-first walk that adds at
+// most one entry per tree level below the popped node.  An LBVH over keys of 62 bits (30-bit
+// Morton code, 32-bit index tie-break) is at most 63 levels deep.
 constexpr int kWarpStack = 1024;
+constexpr int kMaxTreeDepth = 64;
 constexpr int kWarpLeaves = 96;
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -100,7 +108,7 @@ __device__ __forceinline__ bool warp_traverse(const BNode* __restrict__ nodes, i
     __syncwarp();
     while (sp > 0 || nleaf > 0) {
         if (sp > 0 && nleaf < 32) {
-            const int take = min(sp, 32);
+            const int take = min(min(sp, 32), max(1, kWarpStack - kMaxTreeDepth - sp));
             const int node = lane < take ? stack[sp - 1 - lane] : -1;
             sp -= take;
             __syncwarp();
@@ -121,7 +129,7 @@ __device__ __forceinline__ bool warp_traverse(const BNode* __restrict__ nodes, i
             const unsigned bll = __ballot_sync(kFull, ll), blr = __ballot_sync(kFull, lr);
             const int npush = __popc(bpl) + __popc(bpr);
             if (sp + npush > kWarpStack) {
-                ok = false;  // cannot happen for the tree depths of a 30-bit Morton build
+                ok = false;  // cannot happen (see above); kept as a guard
                 break;
             }
             const int ppos = sp + __popc(bpl & lt) + __popc(bpr & lt);
