@@ -271,10 +271,7 @@ __device__ Rgb bb1d_contrib_packed(const GatherConsts& K, const DMedium& m, cons
     const int pl = lvbits & 0x3fffffff;
     const bool finite = (lvbits >> 30) & 1;
     if ((uint32_t)(pl + 1 + s.L) > P.max_path_length || (uint32_t)(pl + 1 + s.L) < P.min_path_length) return rgb(0.f);
-    {
-        const float c = s.d.x * bdir.x + s.d.y * bdir.y + s.d.z * bdir.z;
-        if (1.f - c * c < 1e-2f) closest_approach_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
-    }
+
     if (s.L == 1 && t1 < P.min_dist_to_med) return rgb(0.f);
     const uint32_t bflags = (uint32_t)__float_as_int(py.thr.w);
     const uint32_t brsf = (uint32_t)__float_as_int(py.pdf.w);
@@ -590,6 +587,15 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                             Bs, beam, beam_start_radius(Bs, kMixed ? &B.pay[i].lv.z : &Bs.radius[beam]), t2);
                         hit = !(radius < dist);
                         entry = own > 0 ? i : ~i;
+                        if (kMixed && hit) {
+                            // near-parallel lines, 1 - (d1.d2)^2 small: the FP32 solve of
+                            // PhotonBeam.hxx:253-293 cancels, so the contribution gets the FP64
+                            // closest approach (the candidate decision above stays FP32)
+                            const float c = s.d.x * pb.x + s.d.y * pb.y + s.d.z * pb.z;
+                            if (1.f - c * c < 1e-2f)
+                                closest_approach_f64(s.o, s.d, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), dist,
+                                                     sinT, t1, t2);
+                        }
                     }
                 }
             }
