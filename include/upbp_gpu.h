@@ -252,8 +252,8 @@ const char* upbp_last_error(const upbp_ctx* ctx);
 int upbp_set_mode(upbp_ctx* ctx, int mode);
 /* Tunables (picked by smallupbp_b200.autotune): LBVH leaf sizes (powers of two), the block size
  * of the thread-per-query gathers, the BB1D beam-piece length in beam radii, and the BB1D
- * gather variant (0: thread per query, 1: warp-cooperative persistent work queue at 5 blocks of
- * 4 warps per SM, 2: the same kernel compiled for 6 blocks per SM, 3 and 4: one persistent
+ * gather variant (0: thread per query, 1: warp-cooperative persistent work queue at 6 blocks of
+ * 4 warps per SM, 2: the same kernel compiled for 7 blocks per SM, 3 and 4: one persistent
  * work-queue kernel for all camera segments that evaluates PB2D and BB1D per query, at 5 or 6
  * blocks per SM; the PB2D phase of upbp_last_timings is then 0 and the BB1D phase covers both).
  * pb2d_kernel picks the PB2D gather when it runs on its own (bb1d_kernel 0-2), and the B-P2D

@@ -5,7 +5,7 @@ The knobs (``upbp_tuning`` in ``include/upbp_gpu.h``):
 * ``bb1d_leaf`` and ``beam_piece_radii`` shape the BB1D beam-piece LBVH: shorter pieces and
   smaller leaves give tighter boxes (fewer tested pieces per query) at the price of more nodes;
 * ``bb1d_kernel`` picks the segment gathers: 1 or 2 the warp-cooperative BB1D kernel compiled for
-  5 or 6 blocks of 4 warps per SM (PB2D in its own kernel), 3 or 4 one persistent kernel for all
+  6 or 7 blocks of 4 warps per SM (PB2D in its own kernel), 3 or 4 one persistent kernel for all
   camera segments doing PB2D and BB1D per query;
 * ``pb2d_kernel`` picks the PB2D gather when it runs on its own: 0 one thread per query, 1 one
   warp per query from a persistent work queue;

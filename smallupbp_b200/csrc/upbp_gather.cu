@@ -537,19 +537,13 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
         Rgb part = rgb(0.f);
         const int mid = (int)(&m - media);
         int qn = 0;  // entries in the candidate queue (warp-uniform)
-        // evaluates queue entry e (one lane, one accepted candidate); an entry stored as ~piece
-        // still needs the FP64 ownership decision, taken here with all lanes busy
+        // evaluates queue entry e (one lane, one accepted candidate)
         auto eval = [&](int e) {
-            int i = cq.piece[e];
-            const bool undecided = i < 0;
-            if (undecided) i = ~i;
+            const int i = cq.piece[e];
             const float4 g = cq.geo[e];
             const float4 pa = __ldg(&B.pa[i]);
             const float4 pb = __ldg(&B.pb[i]);
             const float4 pc = __ldg(&B.pc[i]);
-            if (undecided &&
-                !piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y))
-                return;
             ++cnt32;
             h += mix64((unsigned long long)__float_as_int(pc.z));
             const int beam = __float_as_int(pc.z);
@@ -586,7 +580,11 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                         const float radius = beam_radius_at(
                             Bs, beam, beam_start_radius(Bs, kMixed ? &B.pay[i].lv.z : &Bs.radius[beam]), t2);
                         hit = !(radius < dist);
-                        entry = own > 0 ? i : ~i;
+                        // the FP32 values cannot decide: the FP64 closest point of the segments
+                        if (hit && own < 0)
+                            hit = piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
+                                                 pa.w, pc.x, pc.y);
+                        entry = i;
                         if (kMixed && hit) {
                             // near-parallel lines, 1 - (d1.d2)^2 small: the FP32 solve of
                             // PhotonBeam.hxx:253-293 cancels, so the contribution gets the FP64
@@ -1234,8 +1232,8 @@ template <bool kMixed>
 static int blocks_for(int variant)
 {
     int nb = 0;
-    if (variant == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 6>, 128, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 5>, 128, 0);
+    if (variant == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 7>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_warp<kMixed, 4, 6>, 128, 0);
     return nb > 0 ? nb : 1;
 }
 
@@ -1268,11 +1266,11 @@ void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B
 {
     if (Q.n <= 0) return;
     if (variant == 2) {
+        if (mixed) k_bb1d_warp<true, 4, 7><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+        else k_bb1d_warp<false, 4, 7><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
+    } else {
         if (mixed) k_bb1d_warp<true, 4, 6><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
         else k_bb1d_warp<false, 4, 6><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
-    } else {
-        if (mixed) k_bb1d_warp<true, 4, 5><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
-        else k_bb1d_warp<false, 4, 5><<<grid, 128, 0, stream>>>(K, L, B, S, Q, cam, cs, O, work, status, order);
     }
 }
 
