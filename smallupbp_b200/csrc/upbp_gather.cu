@@ -558,10 +558,12 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
             }
         };
         // the rest of the predicate for one piece per lane (i < 0: none) that passed its first
-        // check; accepted candidates go to the candidate queue
+        // check, with the ownership decision (in FP64 where the FP32 values cannot take it) and, in
+        // mixed mode, the FP64 closest approach of near-parallel pairs; both run here rather than
+        // in the evaluation, where the payload and the MIS inputs keep many more registers live.
+        // Accepted candidates go to the candidate queue.
         auto full = [&](int i) {
             bool hit = false;
-            int entry = 0;
             float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f;
             if (i >= 0) {
                 // the predicate reads only pa and pb; pc (piece interval, beam, medium) is loaded for
@@ -584,7 +586,6 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                         if (hit && own < 0)
                             hit = piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
                                                  pa.w, pc.x, pc.y);
-                        entry = i;
                         if (kMixed && hit) {
                             // near-parallel lines, 1 - (d1.d2)^2 small: the FP32 solve of
                             // PhotonBeam.hxx:253-293 cancels, so the contribution gets the FP64
@@ -601,7 +602,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
             if (vote == 0u) return;
             if (hit) {
                 const int pos = qn + __popc(vote & lt);
-                cq.piece[pos] = entry;
+                cq.piece[pos] = i;
                 cq.geo[pos] = make_float4(dist, sinT, t1, t2);
             }
             qn += __popc(vote);
