@@ -346,15 +346,17 @@ int upbp_last_timings(const upbp_ctx* ctx, float* build_ms, float* pp3d_ms, floa
 /* Allocation-free PP3D evaluation.  No counterpart in the reference: its HashGrid::Build and
  * HashGrid::Process with UPBP::RangeQuery (plain FP32 mode) for callers that cannot allocate
  * device memory -- a renderer plug-in inside a host application that owns the device memory
- * budget, code running during CUDA graph capture, or an embedded caller that reserves all
- * memory up front.  All pointers inside lv / pq and cam_mis / out_rgb ([pq->n][3]) are device
- * pointers the caller owns; nothing is allocated.  The scratch memory is one fixed array of
- * about 18 MiB inside the library, held on every GPU that loads it until the process exits;
- * it limits lv->n to UPBP_NOALLOC_MAX_LIGHT_VERTICES and params->hash_cells to
- * UPBP_NOALLOC_MAX_HASH_CELLS (larger sizes return UPBP_ERR_CAPACITY).  The first call on a
- * device looks up that device's scratch address, so make the first call before any stream
- * capture.  Every call shares the scratch array: calls that overlap on the GPU (other
- * streams, other host threads) race, so serialise them.  stream = cudaStream_t or NULL. */
+ * budget and forbids plug-ins to allocate, or an embedded caller that reserves all memory up
+ * front.  All pointers inside lv / pq and cam_mis / out_rgb ([pq->n][3]) are device pointers the
+ * caller owns; a null array for a non-empty count returns UPBP_ERR_INVALID_ARG; nothing is
+ * allocated.  The scratch memory is one fixed array of about 18 MiB inside the library, held on
+ * every GPU that loads it until the process exits; it limits lv->n to
+ * UPBP_NOALLOC_MAX_LIGHT_VERTICES and params->hash_cells to UPBP_NOALLOC_MAX_HASH_CELLS (larger
+ * sizes return UPBP_ERR_CAPACITY).  The first call on a device looks up that device's scratch
+ * address, so make the first call before any stream capture.  The call reads the photon count and
+ * the hash grid's bounds back to the host, so it waits for `stream`.  Every call shares the
+ * scratch array: calls that overlap on the GPU (other streams, other host threads) race, so
+ * serialise them.  stream = cudaStream_t or NULL. */
 #define UPBP_NOALLOC_MAX_LIGHT_VERTICES (1 << 17)
 #define UPBP_NOALLOC_MAX_HASH_CELLS (1 << 17)
 int upbp_pp3d_evaluate_noalloc(const upbp_params* params, const upbp_medium* media, int32_t n_media,

@@ -34,13 +34,19 @@ def lib(fp64: bool = False):
     return _libs[path]
 
 
-def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False, radii=None) -> Dict[str, np.ndarray]:
+def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False, radii=None,
+        reach: bool = True) -> Dict[str, np.ndarray]:
     """Evaluate workload ``w`` with the C restatement (``fp64``: the FP64 oracle build).
 
     ``radii`` = (photon radius^2 per light vertex, beam start radius, beam end radius) replaces the
-    KNN search (used to inject the radii the reference's own builds produced)."""
+    KNN search (used to inject the radii the reference's own builds produced).  ``reach``: apply the
+    BB1D reach rule that defines the CUDA path's candidate set (off: the reference's brute-force
+    candidate set, which also holds pairs the FP32 predicate accepts only through rounding)."""
     s, keep = abi.make_structs(w)
     l = lib(fp64)
+    l.upbp_oracle_set_reach.restype = None
+    l.upbp_oracle_set_reach.argtypes = [C.c_int]
+    l.upbp_oracle_set_reach(1 if reach else 0)
     l.upbp_oracle_set_radii.restype = None
     l.upbp_oracle_set_radii.argtypes = [abi.f32p] * 3
     if radii is not None:
@@ -63,6 +69,7 @@ def run(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False, radii=Non
                                P(out["count_bb1d"]), P(out["hash_bb1d"]), P(out["count_pp3d"]), P(out["hash_pp3d"]),
                                P(out["image"]))
     l.upbp_oracle_set_radii(None, None, None)
+    l.upbp_oracle_set_reach(1)
     if rc != 0:
         raise RuntimeError("upbp_oracle_run failed (%d)" % rc)
     del keep, radii

@@ -409,6 +409,48 @@ void upbp_oracle_set_radii(const float* ph_r2, const float* bm_start, const floa
     g_bm_end = bm_end;
 }
 
+/* The BB1D reach rule (not in the reference; the CUDA path defines its candidate set by it).  The
+ * reference predicate's FP32 t2 = (t1 + d1.O1 - d1.O2) / (d1.d2) (PhotonBeam.hxx:290) is
+ * ill-conditioned for nearly perpendicular pairs, so it accepts a few pairs whose segments do not
+ * come within the radius at all: the true closest point lies beyond the beam's end.  No spatial
+ * structure finds those reliably (the reference's own grid, Grid.hxx, misses them too).  With the
+ * rule on, a pair that the predicate and the radius test accept is kept only if the FP64 distance
+ * D of the query segment [dmin, dmax] and the beam segment [0, len] is at most r(u) + e, u being
+ * the beam parameter of the closest points, r(u) the radius there and e = 2e-5 + 1e-3 r.  With
+ * the rule off this is the reference's brute-force evaluator (Beams/PhBrute.hxx:77-85). */
+static int g_reach = 1;
+void upbp_oracle_set_reach(int on) { g_reach = on; }
+
+static int reach_ok(v3f O1, v3f d1, float dminf, float dmaxf, v3f O2, v3f d2, float lenf, float rs, float rc,
+                    float r)
+{
+    const double wx = (double)O1.x - O2.x, wy = (double)O1.y - O2.y, wz = (double)O1.z - O2.z;
+    const double ax = d1.x, ay = d1.y, az = d1.z, bx = d2.x, by = d2.y, bz = d2.z;
+    const double aa = ax * ax + ay * ay + az * az, cc = bx * bx + by * by + bz * bz, b = ax * bx + ay * by + az * bz;
+    const double dd = ax * wx + ay * wy + az * wz, ee = bx * wx + by * wy + bz * wz;
+    const double den = aa * cc - b * b, dmin = dminf, dmax = dmaxf, len = lenf;
+    const float extra = 2e-5f + 1e-3f * r;
+    double t = dmin, u = 0.0, rx, ry, rz, rho;
+    int inside = 0;
+    if (den > 1e-300) {
+        const double inv = 1.0 / den;
+        t = (b * ee - cc * dd) * inv;
+        u = (aa * ee - b * dd) * inv;
+        inside = t >= dmin && t <= dmax && u >= 0.0 && u <= len;
+    }
+    if (!inside) { /* clamp to the segments (the closest points of two segments) */
+        t = fmin(fmax(t, dmin), dmax);
+        u = fmin(fmax((b * t + ee) / cc, 0.0), len);
+        t = fmin(fmax((b * u - dd) / aa, dmin), dmax);
+        u = fmin(fmax((b * t + ee) / cc, 0.0), len);
+    }
+    rx = wx + t * ax - u * bx;
+    ry = wy + t * ay - u * by;
+    rz = wz + t * az - u * bz;
+    rho = (double)rs + u * (double)rc + (double)extra;
+    return rx * rx + ry * ry + rz * rz <= rho * rho;
+}
+
 /* EmbreeBre::build with KNN_RADIUS (Bre.cxx:685-725): radius = r * (2 * sqrt(d2_k)) over the
  * photons (light vertices in media); EmbreePhoton::set keeps radius * radius. */
 static float* knn_photon_r2(const upbp_light_vertices* lv, float r, int k)
@@ -674,6 +716,9 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
                         continue;
                     radius = rs + t2 * rd; /* mStartRadius + t2 * mRadiusChange (PhotonBeam.hxx:411) */
                     if (radius < dist) continue;
+                    if (g_reach && !reach_ok(s.of, s.df, dminf, dmaxf, Vf(B->origin + 3 * b), Vf(B->direction + 3 * b),
+                                             B->length[b], rs, rd, P->radius_bb1d))
+                        continue;
                     ++*cnt;
                     *hash += mix64((uint64_t)b);
                     seg = cadd(seg, bb1d_contrib(O, m, &s, b, dist, sinT, t1, t2, rs, rd));

@@ -381,6 +381,22 @@ __global__ void k_emit_sorted(const float* __restrict__ origin, const float* __r
     bx_.lo[0] = fminf(ax, bx) - mx; bx_.hi[0] = fmaxf(ax, bx) + mx;
     bx_.lo[1] = fminf(ay, by) - my; bx_.hi[1] = fmaxf(ay, by) + my;
     bx_.lo[2] = fminf(az, bz) - mz; bx_.hi[2] = fmaxf(az, bz) + mz;
+    // The first and the last piece own the pairs whose closest point is clamped to the beam's
+    // start or end; the query then passes within the reach of the end point in any direction, so
+    // those pieces' boxes hold the ball of radius r(end) + eps about it (the reach rule of
+    // piece_takes_f64).
+    if (k == 0) {
+        const float re = (rchange ? rs * 1.000001f : radius) + eps;
+        bx_.lo[0] = fminf(bx_.lo[0], ax - re); bx_.hi[0] = fmaxf(bx_.hi[0], ax + re);
+        bx_.lo[1] = fminf(bx_.lo[1], ay - re); bx_.hi[1] = fmaxf(bx_.hi[1], ay + re);
+        bx_.lo[2] = fminf(bx_.lo[2], az - re); bx_.hi[2] = fmaxf(bx_.hi[2], az + re);
+    }
+    if (k == cnt - 1) {
+        const float re = (rchange ? fmaxf(rs + len * rc, 0.f) * 1.000001f : radius) + eps;
+        bx_.lo[0] = fminf(bx_.lo[0], bx - re); bx_.hi[0] = fmaxf(bx_.hi[0], bx + re);
+        bx_.lo[1] = fminf(bx_.lo[1], by - re); bx_.hi[1] = fmaxf(bx_.hi[1], by + re);
+        bx_.lo[2] = fminf(bx_.lo[2], bz - re); bx_.hi[2] = fmaxf(bx_.hi[2], bz + re);
+    }
     pa[i] = make_float4(ox, oy, oz, len);
     pb[i] = make_float4(dx, dy, dz, r2);
     pc[i] = make_float4(t0, t1, __int_as_float(b), __int_as_float(medium[b]));

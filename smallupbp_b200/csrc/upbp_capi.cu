@@ -498,7 +498,7 @@ void do_build(upbp_ctx* c)
                            c->pc_perm.as<int32_t>(), s);
         sort_pairs(c, c->pc_codes.as<uint32_t>(), c->pc_codes_sorted.as<uint32_t>(), c->pc_perm.as<int32_t>(),
                    c->pc_perm_sorted.as<int32_t>(), np, 30);
-        const float eps = 1e-5f + 1e-3f * r;
+        const float eps = bb1d_box_eps(r);
         launch_emit_sorted(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(),
                            c->b_med_in.as<int32_t>(), nb, c->bm_offsets.as<int32_t>(), c->pc_perm_sorted.as<int32_t>(),
                            np, r, eps, rchange ? c->bm_radius.as<float>() : nullptr, rchange, r2max,
@@ -539,6 +539,7 @@ GatherConsts make_consts(upbp_ctx* c)
     for (int i = 0; i < K.n_media; ++i) K.media[i] = c->media[i];
     K.has_bb1d_beams = (c->P.techniques & UPBP_BB1D) && c->n_beams > 0;
     K.eps = 1e-4f;
+    K.bb1d_extra = bb1d_reach_extra(c->P.radius_bb1d);
     return K;
 }
 

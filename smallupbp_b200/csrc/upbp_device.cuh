@@ -167,18 +167,38 @@ __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float 
     return true;
 }
 
-// Which piece of a beam takes a candidate that test_beam_beam accepted.  The predicate does not
-// depend on the piece (it tests the whole beam), but its t2 = (t1 + d1.O1 - d1.O2) / (d1.d2) is
-// ill-conditioned for nearly perpendicular pairs, and t1, t2 for nearly parallel ones, so the
-// FP32 t2 can lie far from the true closest point -- in a piece whose box the query never
-// crosses.  The owner is the piece containing the point of the beam segment [0, len] closest to
-// the query segment [dmin, dmax], computed in FP64; every piece computes the same point, and the
-// query crosses the owner's box whenever the pair is geometrically within the radius (plus the
-// box slack).  Where the FP32 t1 and t2 are provably within m = 1e-4 * scale of the exact line
-// solution -- |c| (1 - c^2) > 0.04 with c = d1.d2 bounds their rounding error by about
-// 2.5e-5 * scale (measured over 2M random pairs in the unit cube) -- and away from the ends of
-// their ranges, the FP32 t2 decides without the FP64 solve.
-__device__ __forceinline__ double owner_param_f64(V3 O1, V3 d1, float dminf, float dmaxf, V3 O2, V3 d2, float lenf)
+// Which BB1D candidates are taken, and by which piece of the beam.
+//
+// The reference predicate (PhotonBeam.hxx:238-296) tests the whole beam; the beam is split into
+// pieces here only for culling, so exactly one piece must take each candidate, and whether a
+// candidate is found must not depend on the tree, the leaf size or the piece length.  The FP32 t2
+// = (t1 + d1.O1 - d1.O2) / (d1.d2) of the predicate is ill-conditioned for nearly perpendicular
+// pairs (and t1, t2 for nearly parallel ones): it can accept a pair whose true closest point lies
+// outside the beam segment, far from any box the query crosses, so no spatial search (nor the
+// reference's own grid, Grid.hxx) finds every such pair.  The candidate set is therefore defined
+// by a reach rule that every implementation here applies (the CUDA kernels and the C oracle):
+//
+//   taken  <=>  the FP32 predicate and the radius test accept the pair (reference order), and
+//               the FP64 distance D of the query segment [dmin, dmax] and the beam segment
+//               [0, len] satisfies D <= r(u) + e, where u is the beam parameter of their closest
+//               point, r(u) the beam radius there and e = bb1d_reach_extra(r).
+//
+// The rule keeps every pair whose segments really pass within the radius; it drops only pairs
+// that the FP32 predicate accepts through rounding.  The owner is the piece containing u.  Its box
+// contains every point within r(u) + e of the owned part of the segment -- for a u inside (0, len)
+// that point lies in the disc perpendicular to the beam, for u = 0 or len in the ball about the
+// end point, which the end pieces' boxes include -- so the traversal reaches the owner of every
+// taken pair, whatever the tree.
+__host__ __device__ __forceinline__ float bb1d_reach_extra(float r) { return 2e-5f + 1e-3f * r; }
+// slack of the piece boxes: the reach margin plus the rounding of the slab test
+__host__ __device__ __forceinline__ float bb1d_box_eps(float r) { return bb1d_reach_extra(r) + 1e-5f; }
+
+// FP64 closest points of the query segment [dmin, dmax] and the beam segment [0, len]: the beam
+// parameter u and the squared distance.
+struct SegClosest {
+    double u, d2;
+};
+__device__ __forceinline__ SegClosest seg_closest_f64(V3 O1, V3 d1, float dminf, float dmaxf, V3 O2, V3 d2, float lenf)
 {
     const double wx = (double)O1.x - O2.x, wy = (double)O1.y - O2.y, wz = (double)O1.z - O2.z;
     const double ax = d1.x, ay = d1.y, az = d1.z, bx = d2.x, by = d2.y, bz = d2.z;
@@ -186,23 +206,35 @@ __device__ __forceinline__ double owner_param_f64(V3 O1, V3 d1, float dminf, flo
     const double dd = ax * wx + ay * wy + az * wz, ee = bx * wx + by * wy + bz * wz;
     const double den = aa * cc - b * b;
     const double dmin = dminf, dmax = dmaxf, len = lenf;
-    double t = dmin;
+    double t = dmin, u = 0.0;
+    bool inside = false;
     if (den > 1e-300) {
         const double inv = 1.0 / den;
         t = (b * ee - cc * dd) * inv;
-        const double u = (aa * ee - b * dd) * inv;
-        if (t >= dmin && t <= dmax && u >= 0.0 && u <= len) return u;  // closest points inside both
+        u = (aa * ee - b * dd) * inv;
+        inside = t >= dmin && t <= dmax && u >= 0.0 && u <= len;  // closest points inside both
     }
-    t = fmin(fmax(t, dmin), dmax);
-    double u = fmin(fmax((b * t + ee) / cc, 0.0), len);
-    t = fmin(fmax((b * u - dd) / aa, dmin), dmax);
-    u = fmin(fmax((b * t + ee) / cc, 0.0), len);
-    return u;
+    if (!inside) {
+        t = fmin(fmax(t, dmin), dmax);
+        u = fmin(fmax((b * t + ee) / cc, 0.0), len);
+        t = fmin(fmax((b * u - dd) / aa, dmin), dmax);
+        u = fmin(fmax((b * t + ee) / cc, 0.0), len);
+    }
+    const double rx = wx + t * ax - u * bx, ry = wy + t * ay - u * by, rz = wz + t * az - u * bz;
+    return SegClosest{u, rx * rx + ry * ry + rz * rz};
 }
 
-// 1: this piece owns the candidate, 0: it does not, -1: undecided in FP32 (use piece_owns_f64).
-__device__ __forceinline__ int piece_owns_fast(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
-                                               float t_lo, float t_hi, float t1, float t2)
+// 1: this piece takes the candidate, 0: it does not (another piece owns it), -1: undecided in
+// FP32 (use piece_takes_f64).  Called after the predicate and the radius test accepted the pair
+// (dist <= radius = r(t2)); rc_abs = |dr/dt| of the beam radius (0 for a constant radius).
+// Where |c| (1 - c^2) > 0.04 with c = d1.d2, the rounding error of the FP32 t1 and t2 stays below
+// m = 1e-4 * scale, so t1, t2 more than m inside their ranges put the exact closest points inside
+// both segments: u is the exact t2, and D is the distance of the lines, which the FP32 dist
+// approximates within errb (|ad| carries at most 6 ulp of |O2 - O1|_1 and sin(theta) > 0.2 there;
+// errb is twice that bound).
+__device__ __forceinline__ int piece_takes_fast(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
+                                                float t_lo, float t_hi, float t1, float t2, float dist, float radius,
+                                                float rc_abs, float extra)
 {
     const float c = fabsf(d1.x * d2.x + d1.y * d2.y + d1.z * d2.z);
     if (c * (1.f - c * c) > 0.04f) {
@@ -210,25 +242,33 @@ __device__ __forceinline__ int piece_owns_fast(V3 O1, V3 d1, float dmin, float d
                                   fmaxf(fmaxf(fabsf(O2.y), fabsf(O2.z)), fmaxf(fmaxf(len, fabsf(dmax)), 1.f)));
         const float m = 1e-4f * scale;
         if (t1 > dmin + m && t1 < dmax - m && t2 > m && t2 < len - m) {
-            if (t2 >= t_lo + m && t2 < t_hi - m) return 1;
             if (t2 < t_lo - m || t2 >= t_hi + m) return 0;
+            if (t2 >= t_lo + m && t2 < t_hi - m) {
+                const float w1 = fabsf(O2.x - O1.x) + fabsf(O2.y - O1.y) + fabsf(O2.z - O1.z);
+                const float errb = 4e-6f * w1 + 3e-6f * dist + 1e-8f;
+                if (dist + errb + rc_abs * m <= radius + extra) return 1;
+            }
         }
     }
     return -1;
 }
 
-__device__ __forceinline__ bool piece_owns_f64(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
-                                               float t_lo, float t_hi)
+// The reach rule and the owner in FP64: rs, rc = the beam radius at 0 and its change per unit t.
+__device__ __forceinline__ bool piece_takes_f64(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
+                                                float t_lo, float t_hi, float rs, float rc, float extra)
 {
-    const double u = owner_param_f64(O1, d1, dmin, dmax, O2, d2, len);
-    return u >= (double)t_lo && (u < (double)t_hi || t_hi >= len);
+    const SegClosest sc = seg_closest_f64(O1, d1, dmin, dmax, O2, d2, len);
+    if (!(sc.u >= (double)t_lo && (sc.u < (double)t_hi || t_hi >= len))) return false;
+    const double rho = (double)rs + sc.u * (double)rc + (double)extra;
+    return sc.d2 <= rho * rho;
 }
 
-__device__ __forceinline__ bool piece_owns(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len, float t_lo,
-                                           float t_hi, float t1, float t2)
+__device__ __forceinline__ bool piece_takes(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
+                                            float t_lo, float t_hi, float t1, float t2, float dist, float radius,
+                                            float rs, float rc, float extra)
 {
-    const int f = piece_owns_fast(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi, t1, t2);
-    return f >= 0 ? f == 1 : piece_owns_f64(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi);
+    const int f = piece_takes_fast(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi, t1, t2, dist, radius, fabsf(rc), extra);
+    return f >= 0 ? f == 1 : piece_takes_f64(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi, rs, rc, extra);
 }
 
 // ------------------------------------------------------------------ MIS walks

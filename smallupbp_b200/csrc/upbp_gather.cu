@@ -481,12 +481,14 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                     if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
                                         pb.w, &dist, &sinT, &t1, &t2))
                         continue;
-                    if (!piece_owns(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pc.x,
-                                    pc.y, t1, t2))
-                        continue;
                     const int beam = __float_as_int(pc.z);
-                    const float radius = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), t2);
+                    const float rs = beam_start_radius(Bs, &Bs.radius[beam]);
+                    const float radius = beam_radius_at(Bs, beam, rs, t2);
                     if (radius < dist) continue;  // PhotonBeam.hxx:411-413
+                    if (!piece_takes(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pc.x,
+                                     pc.y, t1, t2, dist, radius, rs, Bs.rchange ? __ldg(&Bs.rchange[beam]) : 0.f,
+                                     K.bb1d_extra))
+                        continue;
                     ++cnt;
                     h += mix64((unsigned long long)beam);
                     acc = acc + bb1d_contrib<kMixed>(K, m, Lv, Bs, s, beam, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), radius,
@@ -573,19 +575,23 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                 if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
                                    pb.w, &dist, &sinT, &t1, &t2)) {
                     const float4 pc = __ldg(&B.pc[i]);
-                    const int own = __float_as_int(pc.w) == mid  // mMedium == medium (PhotonBeam.hxx:390)
-                                        ? piece_owns_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
-                                                          v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y, t1, t2)
-                                        : 0;
-                    if (own != 0) {  // this piece may take it: the radius test (PhotonBeam.hxx:411-413)
+                    if (__float_as_int(pc.w) == mid) {  // mMedium == medium (PhotonBeam.hxx:390)
+                        // the radius test (PhotonBeam.hxx:411-413), then the reach rule and the owner
                         const int beam = __float_as_int(pc.z);
-                        const float radius = beam_radius_at(
-                            Bs, beam, beam_start_radius(Bs, kMixed ? &B.pay[i].lv.z : &Bs.radius[beam]), t2);
+                        const float rs = beam_start_radius(Bs, kMixed ? &B.pay[i].lv.z : &Bs.radius[beam]);
+                        const float rc = Bs.rchange ? __ldg(&Bs.rchange[beam]) : 0.f;
+                        const float radius = beam_radius_at(Bs, beam, rs, t2);
                         hit = !(radius < dist);
-                        // the FP32 values cannot decide: the FP64 closest point of the segments
-                        if (hit && own < 0)
-                            hit = piece_owns_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                                 pa.w, pc.x, pc.y);
+                        if (hit) {
+                            const int own = piece_takes_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
+                                                             v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y, t1, t2, dist,
+                                                             radius, fabsf(rc), K.bb1d_extra);
+                            // the FP32 values cannot decide: the FP64 closest points of the segments
+                            hit = own >= 0 ? own == 1
+                                           : piece_takes_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
+                                                             v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y, rs, rc,
+                                                             K.bb1d_extra);
+                        }
                         if (kMixed && hit) {
                             // near-parallel lines, 1 - (d1.d2)^2 small: the FP32 solve of
                             // PhotonBeam.hxx:253-293 cancels, so the contribution gets the FP64

@@ -489,13 +489,19 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                             const float4 pb = __ldg(&B.pb[i]);
                             float dist, sinT, t1, t2;
                             if (test_beam_beam(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                               0.f, pa.w, pb.w, &dist, &sinT, &t1, &t2) &&
-                                piece_owns(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w,
-                                           pc.x, pc.y, t1, t2) &&
-                                !(beam_radius_at(Bs, __float_as_int(pc.z), beam_start_radius(Bs, &B.pay[i].lv.z), t2) < dist)) {
-                                hit = true;
-                                ++cnt;
-                                h += mix64((unsigned long long)__float_as_int(pc.z));
+                                               0.f, pa.w, pb.w, &dist, &sinT, &t1, &t2)) {
+                                const int beam = __float_as_int(pc.z);
+                                const float rs = beam_start_radius(Bs, &B.pay[i].lv.z);
+                                const float radius = beam_radius_at(Bs, beam, rs, t2);
+                                // the radius test (PhotonBeam.hxx:411-413), the reach rule and the owner
+                                if (!(radius < dist) &&
+                                    piece_takes(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
+                                                pa.w, pc.x, pc.y, t1, t2, dist, radius, rs,
+                                                Bs.rchange ? __ldg(&Bs.rchange[beam]) : 0.f, K.bb1d_extra)) {
+                                    hit = true;
+                                    ++cnt;
+                                    h += mix64((unsigned long long)beam);
+                                }
                             }
                         }
                     }

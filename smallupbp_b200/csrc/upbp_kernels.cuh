@@ -145,6 +145,7 @@ struct GatherConsts {
     int n_media;
     int has_bb1d_beams;  // PB2D: mBB1DPhotonBeams != NULL
     float eps;           // conservative box slack for traversal
+    float bb1d_extra;    // reach margin of the BB1D candidate rule (bb1d_reach_extra)
 };
 
 constexpr int kMaxKnn = 64;  // largest k of the KNN radii

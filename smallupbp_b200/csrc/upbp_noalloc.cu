@@ -1,16 +1,17 @@
 // Allocation-free PP3D evaluation: upbp_pp3d_evaluate_noalloc (include/upbp_gpu.h).
 //
 // Some callers cannot call cudaMalloc: a renderer plug-in running inside a host application
-// that owns the device memory budget (and forbids allocations from plug-ins), code running
-// while a CUDA graph is being captured, or an embedded caller that reserves all device
-// memory up front.  This entry point builds the PP3D hash grid and evaluates the point
-// queries without allocating anything: its scratch memory is the file-scope device array
-// below, a fixed size held by every GPU that loads the library until the process exits.
+// that owns the device memory budget (and forbids allocations from plug-ins), or an embedded
+// caller that reserves all device memory up front.  This entry point builds the PP3D hash grid
+// and evaluates the point queries without allocating anything: its scratch memory is the
+// file-scope device array below, a fixed size held by every GPU that loads the library until
+// the process exits.
 //
-// The caller passes device pointers for every input and output.  The scratch array is
-// shared by all calls: it keeps the last call's contents, everything that must start at
-// zero is cleared by each call, and calls that overlap on the GPU (different streams or
-// host threads) race on it.
+// The caller passes device pointers for every input and output.  The call reads two small
+// values back to the host (the photon count and the hash grid's bounding box), so it waits for
+// its stream.  The scratch array is shared by all calls: it keeps the last call's contents,
+// everything that must start at zero is cleared by each call, and calls that overlap on the
+// GPU (different streams or host threads) race on it.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -75,12 +76,27 @@ constexpr size_t kScratchBytes = kOffCub + kCubBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of g_noalloc_scratch per device, set up once per device (the host-side name
-// of the array is only a stand-in and must never be passed to a kernel).
+// Device address of g_noalloc_scratch per device, looked up on the first call on that device
+// with the device current (the host-side name of the array is only a stand-in and must never be
+// passed to a kernel).  Only a successful lookup is kept: after a failure the next call tries
+// again.
 constexpr int kMaxDevices = 64;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
-std::once_flag g_scratch_once[kMaxDevices];
-cudaError_t g_scratch_err[kMaxDevices] = {};
+std::mutex g_scratch_mutex;
+
+unsigned char* scratch_address(int dev)
+{
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_scratch_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_scratch_addr[dev];
+}
 
 __global__ void k_iota_noalloc(int32_t* v, int n)
 {
@@ -103,18 +119,21 @@ extern "C" int upbp_pp3d_evaluate_noalloc(const upbp_params* params, const upbp_
 {
     if (!params || !media || n_media <= 0 || n_media > UPBP_MAX_MEDIA || !lv || !pq || (pq->n > 0 && !out_rgb))
         return UPBP_ERR_INVALID_ARG;
+    // every array the call reads must be given for a non-empty count (a null pointer would fault
+    // on the device instead of returning an error)
+    if (lv->n > 0 && (!lv->position || !lv->throughput || !lv->dir_fix || !lv->cont_prob || !lv->path_idx ||
+                      !lv->path_length || !lv->medium_id || !lv->flags || !lv->mis || !lv->path_ends))
+        return UPBP_ERR_INVALID_ARG;
+    if (pq->n > 0 && (!cam_mis || !pq->position || !pq->dir_fix || !pq->medium_id || !pq->path_length ||
+                      !pq->throughput || !pq->pixel || !pq->cam_mis_begin))
+        return UPBP_ERR_INVALID_ARG;
     if (lv->n < 0 || lv->n > kMaxLv || params->hash_cells < 1 || params->hash_cells > kMaxCells || pq->n < 0)
         return UPBP_ERR_CAPACITY;
     if (!(params->radius_pp3d > 0.f)) return UPBP_ERR_INVALID_ARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return UPBP_ERR_CUDA;
-    std::call_once(g_scratch_once[dev], [dev] {
-        void* p = nullptr;
-        g_scratch_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (g_scratch_err[dev] == cudaSuccess) g_scratch_addr[dev] = static_cast<unsigned char*>(p);
-    });
-    if (g_scratch_err[dev] != cudaSuccess || !g_scratch_addr[dev]) return UPBP_ERR_CUDA;
-    unsigned char* base = g_scratch_addr[dev];
+    unsigned char* base = scratch_address(dev);
+    if (!base) return UPBP_ERR_CUDA;
     cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
     const upbp_params& P = *params;
     const int n = (int)lv->n;

@@ -6,10 +6,16 @@ the reference harness (oracle/_ref/libupbp_ref.so, built from the reference sour
 oracle/build_ref.py):  per-query PB2D / BB1D (grid and brute force) / PP3D contributions,
 per-query candidate counts and hashes, and the splatted image.
 
+The configuration-0 fixture (``config0_cube128``: the 128x128 cube, 16,384 light sub-paths,
+r = 0.01, seed 1234) is larger; it stores the reference's outputs and a SHA-256 digest of every
+input array instead of the inputs, which the seeded generator recreates (golden_io.load checks the
+digests).
+
 Run from the repository root:  python tests/golden/gen_golden.py [fixture names]
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import sys
 
@@ -34,6 +40,12 @@ CASES = [
     ("cube_wide_radius", "cube24x1536", dict(radius=0.08, seed=21)),
     ("cube_knn_radius", "cube24x1536", dict(radius=0.25, pb2d_knn=8, bb1d_knn=6, seed=31)),
 ]
+# fixtures that keep input digests instead of inputs (regenerated from the config at load time)
+DIGEST_CASES = [("config0_cube128", "cube128", dict())]
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
 
@@ -48,13 +60,17 @@ def scene(name: str, overrides: dict) -> W.SceneConfig:
 
 
 def main(names=None):
-    for fname, cname, over in CASES:
+    for fname, cname, over in CASES + DIGEST_CASES:
         if names and fname not in names:
             continue
         cfg = scene(cname, over)
         w = W.generate(cfg)
         o = ref.run(w, threads=8)
-        out = {"in_" + k: v for k, v in w.items()}
+        if (fname, cname, over) in DIGEST_CASES:
+            out = {"cfg_name": np.array(cname), "cfg_iteration": np.array(0)}
+            out.update({"digest_" + k: np.array(digest(v)) for k, v in w.items()})
+        else:
+            out = {"in_" + k: v for k, v in w.items()}
         for k in ("pb2d", "bb1d", "bb1d_brute", "pp3d", "count_pb2d", "hash_pb2d", "count_bb1d", "hash_bb1d",
                   "count_pp3d", "hash_pp3d", "image"):
             out["ref_" + k] = o[k]

@@ -16,11 +16,32 @@ RTOL = 1e-4
 ATOL_FRAC = 1e-6
 
 
+_regenerated: Dict[str, Dict[str, np.ndarray]] = {}
+
+
 def load(path: str) -> Tuple[Dict[str, np.ndarray], Dict[str, np.ndarray]]:
+    """Inputs and reference outputs of a fixture.  A fixture that stores input digests instead of
+    inputs (``cfg_name``) is regenerated from its configuration by the seeded generator, and every
+    array must match its digest."""
+    import hashlib
+
     from smallupbp_b200.workload import PARAMS_DTYPE
 
     z = np.load(path)
-    w = {k[3:]: z[k] for k in z.files if k.startswith("in_")}
+    if "cfg_name" in z.files:
+        if path not in _regenerated:
+            from smallupbp_b200 import workload as W
+
+            w = W.generate(W.config(str(z["cfg_name"])), int(z["cfg_iteration"]))
+            digests = {k[7:]: str(z[k]) for k in z.files if k.startswith("digest_")}
+            assert set(digests) == set(w), "fixture inputs changed: " + str(set(digests) ^ set(w))
+            for k, v in w.items():
+                got = hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()
+                assert got == digests[k], "the generator no longer reproduces %s of %s" % (k, name(path))
+            _regenerated[path] = w
+        w = dict(_regenerated[path])
+    else:
+        w = {k[3:]: z[k] for k in z.files if k.startswith("in_")}
     r = {k[4:]: z[k] for k in z.files if k.startswith("ref_")}
     if w["params"].dtype != PARAMS_DTYPE:  # fixtures written before fields were added: new fields 0
         p = np.zeros(1, PARAMS_DTYPE)

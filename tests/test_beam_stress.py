@@ -5,11 +5,12 @@ r = 0.002 (``workload.beam_stress``).
 The reference rejects a pair as parallel when |d1.d2|^2 - 1 is within 1e-5 (PhotonBeam.hxx:267-273),
 so all near-parallel/near-parallel pairs are rejected by every implementation; the pairs that stay
 are isotropic/isotropic and isotropic/near-parallel, some of them close enough to parallel for the
-FP32 closest-approach solve to lose digits.  Candidate sets must be bit-exact (all implementations
-use the reference's FP32 predicate), except for degenerate pairs that the FP32 predicate accepts
-only through rounding and that no spatial search can reach (explain_mismatches checks each such
-difference); contributions are compared against the FP64 oracle with per-query relative-error
-histograms.
+FP32 closest-approach solve to lose digits.  Candidate sets must be bit-exact against the oracle,
+which applies the same BB1D reach rule as the CUDA path: a pair the reference's FP32 predicate
+accepts is kept when the FP64 distance of the two segments is within the radius at the closest
+point plus 2e-5 + 1e-3 r.  The pairs the rule removes from the reference's brute-force set are
+checked one by one on the CPU (``rule_removed``).  Contributions are compared against the FP64
+oracle with per-query relative-error histograms.
 
 Run as a script on a GPU machine to print the histograms as JSON:
     python tests/test_beam_stress.py [n_beams n_queries]
@@ -121,56 +122,77 @@ def fp32_accepted(w, q):
     return np.nonzero(ok)[0]
 
 
-def exact_rejects(w, q, b, slack) -> bool:
-    """True when the pair fails testIntersectionBeamBeam evaluated exactly (FP64 line solution) by
-    more than ``slack``: line distance > r + slack, t1 outside (dmin - slack, dmax + slack), or t2
-    outside (-slack, len + slack)."""
+def rule_rejects(w, q, b) -> bool:
+    """The BB1D reach rule, restated in FP64 numpy: True when the segments of query q and beam b are
+    farther apart than r(u) + 2e-5 + 1e-3 r, u being the beam parameter of their closest points."""
     O1, d1 = w["sq_origin"][q].astype(float), w["sq_direction"][q].astype(float)
     a1, b1 = float(w["seg_dist_min"][q]), float(w["seg_dist_max"][q])
     O2, d2, ln = w["beam_origin"][b].astype(float), w["beam_direction"][b].astype(float), float(w["beam_length"][b])
-    r = float(w["params"]["radius_bb1d"][0])
+    r = float(np.float32(w["params"]["radius_bb1d"][0]))
     wv = O1 - O2
     bb, dd, ee, aa, cc = d1 @ d2, d1 @ wv, d2 @ wv, d1 @ d1, d2 @ d2
     den = aa * cc - bb * bb
-    if not den > 1e-300:
-        return True
-    t1 = (bb * ee - cc * dd) / den
-    t2 = (aa * ee - bb * dd) / den
-    dist = float(np.linalg.norm(wv + t1 * d1 - t2 * d2))
-    return dist > r + slack or not (a1 - slack < t1 < b1 + slack) or not (-slack < t2 < ln + slack)
+    t, u, inside = a1, 0.0, False
+    if den > 1e-300:
+        t, u = (bb * ee - cc * dd) / den, (aa * ee - bb * dd) / den
+        inside = a1 <= t <= b1 and 0.0 <= u <= ln
+    if not inside:
+        t = min(max(t, a1), b1)
+        u = min(max((bb * t + ee) / cc, 0.0), ln)
+        t = min(max((bb * u - dd) / aa, a1), b1)
+        u = min(max((bb * t + ee) / cc, 0.0), ln)
+    dist = float(np.linalg.norm(wv + t * d1 - u * d2))
+    extra = float(np.float32(2e-5) + np.float32(1e-3) * np.float32(r))
+    return dist > r + extra
 
 
-def explain_mismatches(w, gpu_count, gpu_hash, ref_count, ref_hash) -> dict:
-    """For every query whose GPU candidate set differs from the brute-force reference set, check
-    that the difference is exactly a set of degenerate pairs: pairs the FP32 predicate accepts only
-    through rounding -- evaluated exactly it rejects them by more than the traversal's box slack
-    (the FP32 t2 = (...)/(d1.d2) of a nearly perpendicular pair, or t1, t2 of a nearly parallel
-    one, lands far from the true closest point).  No spatial structure finds those; the
-    reference's own default grid does not either."""
-    r = float(w["params"]["radius_bb1d"][0])
-    slack = 1e-5 + 1e-3 * r
-    bad = np.nonzero((gpu_count != ref_count) | (gpu_hash != ref_hash))[0]
-    explained, degenerate_pairs = 0, 0
+def rule_removed(w, rule_count, rule_hash, ref_count, ref_hash) -> dict:
+    """For every query whose candidate set under the reach rule differs from the reference's
+    brute-force set, enumerate the FP32-accepted beams and check that the difference is exactly the
+    beams the rule rejects: the counts and the order-independent hashes must agree.  These are pairs
+    the FP32 predicate accepts only through rounding (a nearly perpendicular pair's FP32 t2 lands
+    inside the beam while the true closest point lies beyond its end)."""
+    bad = np.nonzero((rule_count != ref_count) | (rule_hash != ref_hash))[0]
+    removed = 0
     for q in bad:
         acc = fp32_accepted(w, q)
         assert len(acc) == ref_count[q], ("emulation", q, len(acc), ref_count[q])
         assert sum(mix64(int(b)) for b in acc) & M64 == int(ref_hash[q]), ("emulation hash", q)
-        degen = [int(b) for b in acc if exact_rejects(w, q, int(b), slack)]
-        missing = int(ref_count[q]) - int(gpu_count[q])
-        found = False
-        for k in range(len(degen) + 1):
-            from itertools import combinations
-            for sub in combinations(degen, k):
-                if len(sub) == missing and (int(ref_hash[q]) - sum(mix64(b) for b in sub)) & M64 == int(gpu_hash[q]):
-                    found = True
-                    degenerate_pairs += len(sub)
-                    break
-            if found:
-                break
-        assert found, ("unexplained candidate difference", int(q), int(gpu_count[q]), int(ref_count[q]), degen)
-        explained += 1
-    return {"queries_differing": int(len(bad)), "explained_by_degenerate_pairs": explained,
-            "degenerate_pairs": degenerate_pairs}
+        gone = [int(b) for b in acc if rule_rejects(w, q, int(b))]
+        kept_hash = (int(ref_hash[q]) - sum(mix64(b) for b in gone)) & M64
+        assert len(acc) - len(gone) == int(rule_count[q]) and kept_hash == int(rule_hash[q]), \
+            ("difference not explained by the reach rule", int(q), int(rule_count[q]), int(ref_count[q]), gone)
+        removed += len(gone)
+    return {"queries_differing": int(len(bad)), "pairs_removed": removed}
+
+
+def test_reach_rule_removes_only_rounding_pairs(stress):
+    """The oracle with the reach rule against the reference's brute-force definition (the oracle
+    with the rule off): every removed pair is one that the rule rejects, none is added."""
+    from oracle import port
+
+    a, b = port.run(stress), port.run(stress, reach=False)
+    assert (a["count_bb1d"] <= b["count_bb1d"]).all()
+    rep = rule_removed(stress, a["count_bb1d"], a["hash_bb1d"], b["count_bb1d"], b["hash_bb1d"])
+    assert rep["pairs_removed"] <= 1e-5 * b["count_bb1d"].astype(np.int64).sum() + 1, rep
+
+
+def test_rule_check_catches_a_planted_difference(stress):
+    """The checker itself: remove an ordinary pair from a copy of the oracle's counts and hashes (on
+    the CPU) and check that rule_removed rejects the difference."""
+    from oracle import port
+
+    w = stress
+    o = port.run(w, reach=False)
+    q = next(q for q in range(len(o["count_bb1d"])) if o["count_bb1d"][q] >= 1)
+    b = int(fp32_accepted(w, q)[0])
+    assert not rule_rejects(w, q, b)
+    cnt, h = o["count_bb1d"].copy(), o["hash_bb1d"].copy()
+    cnt[q] -= 1
+    h[q] = np.uint64((int(h[q]) - mix64(b)) & M64)
+    with pytest.raises(AssertionError, match="not explained"):
+        rule_removed(w, cnt, h, o["count_bb1d"], o["hash_bb1d"])
+    assert rule_removed(w, o["count_bb1d"], o["hash_bb1d"], o["count_bb1d"], o["hash_bb1d"])["queries_differing"] == 0
 
 
 def gpu_report(w) -> dict:
@@ -186,10 +208,10 @@ def gpu_report(w) -> dict:
             _, bb1d = st.segment_results()
             stats = st.query_stats()
             img = st.image()
-        out[name] = {"candidates_equal_fp64_oracle": bool(np.array_equal(stats["count_bb1d"], o64["count_bb1d"]) and
-                                                          np.array_equal(stats["hash_bb1d"], o64["hash_bb1d"])),
-                     "candidate_differences": explain_mismatches(w, stats["count_bb1d"], stats["hash_bb1d"],
-                                                                 o64["count_bb1d"], o64["hash_bb1d"]),
+        out[name] = {"candidates_equal_oracle": bool(np.array_equal(stats["count_bb1d"], o64["count_bb1d"]) and
+                                                     np.array_equal(stats["hash_bb1d"], o64["hash_bb1d"])),
+                     "queries_differing": int(((stats["count_bb1d"] != o64["count_bb1d"]) |
+                                               (stats["hash_bb1d"] != o64["hash_bb1d"])).sum()),
                      "vs_fp64": histogram(per_query_rel(bb1d, o64["bb1d"])),
                      "image_rel_l2_vs_fp64": G.image_rel_l2(img, o64["image"]),
                      "_bb1d": bb1d}
@@ -199,33 +221,12 @@ def gpu_report(w) -> dict:
     return out
 
 
-def test_mismatch_explanation_on_planted_differences(stress):
-    """The checker itself: plant a removed degenerate pair and a removed ordinary pair in a copy of
-    the oracle's counts/hashes (on the CPU) and check that only the first is accepted."""
-    from oracle import port
-
-    w = stress
-    o = port.run(w)
-    r = float(w["params"]["radius_bb1d"][0])
-    q = next(q for q in range(len(o["count_bb1d"])) if o["count_bb1d"][q] >= 1)
-    b = int(fp32_accepted(w, q)[0])
-    assert not exact_rejects(w, q, b, 1e-5 + 1e-3 * r)
-    cnt, h = o["count_bb1d"].copy(), o["hash_bb1d"].copy()
-    cnt[q] -= 1
-    h[q] = np.uint64((int(h[q]) - mix64(b)) & M64)
-    with pytest.raises(AssertionError, match="unexplained"):
-        explain_mismatches(w, cnt, h, o["count_bb1d"], o["hash_bb1d"])
-    rep = explain_mismatches(w, o["count_bb1d"], o["hash_bb1d"], o["count_bb1d"], o["hash_bb1d"])
-    assert rep["queries_differing"] == 0
-
-
 @pytest.mark.gpu
 def test_gpu_stress_against_fp64_oracle(stress):
     rep = gpu_report(stress)
     for name in ("plain", "mixed"):
-        # bit-exact up to degenerate FP32 accepts (explain_mismatches raises otherwise)
-        assert rep[name]["candidate_differences"]["queries_differing"] == \
-            rep[name]["candidate_differences"]["explained_by_degenerate_pairs"], name
+        # bit-exact: every query's count and candidate hash equal the oracle's (reach rule applied)
+        assert rep[name]["candidates_equal_oracle"], (name, rep[name]["queries_differing"])
         assert rep[name]["image_rel_l2_vs_fp64"] <= 1e-3, (name, rep[name]["image_rel_l2_vs_fp64"])
     # plain FP32 follows the FP32 reference arithmetic
     G.assert_close(rep["plain"]["_bb1d"], rep["_o32"], "plain BB1D vs FP32 oracle")
