@@ -8,9 +8,18 @@ into the framebuffer.  Units are queries (segment queries + point queries).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config cube1024]
 
-Multi-GPU (torchrun, one rank per GPU): every rank evaluates its own iterations (independent
-seeds, as the reference runs one renderer per thread over independent iterations) and the
-framebuffers are combined with one NCCL all-reduce per step: weak scaling.
+The headline arm is the batched mixed-precision stage.  On one GPU the same line also times, on the
+same workload, the plain FP32 stage with the same warp-cooperative kernels (autotuned on its own),
+the plain FP32 drop-in (one thread per query), and the mixed stage with B-P2D on, each with its
+image rel-L2 against the GPU FP64 mode; and it checks a sample of the queries against the
+reference's own estimators (``parity``).
+
+Multi-GPU: ``--gpus N`` without a launcher starts N ranks itself (torch.distributed.run, one rank
+per GPU, NCCL).  ``--shard queries`` (the default for N > 1): every rank builds the same structures
+over the whole iteration and evaluates its pixel tiles of the queries, and one framebuffer
+all-reduce per step combines them (strong scaling: one iteration gets faster).  ``--shard
+iterations``: every rank evaluates its own iterations (weak scaling, as the reference runs one
+renderer per thread over independent iterations).
 
 Prints ONE JSON line on rank 0.
 """
@@ -63,17 +72,35 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="direct calls instead of the captured CUDA graph")
     ap.add_argument("--adjoint", action="store_true",
                     help="time forward + adjoint (dL/d sigma_a, sigma_s, g) of an L2 image loss instead")
+    ap.add_argument("--shard", default=None, choices=["queries", "iterations"],
+                    help="multi-GPU work split (default: queries when N > 1)")
+    ap.add_argument("--no-arms", action="store_true",
+                    help="skip the plain FP32, drop-in and B-P2D comparison arms (one GPU only)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the check of sampled queries against the reference's estimators")
     ap.add_argument("--dropin", action="store_true",
                     help="the plain FP32 drop-in: thread-per-query BB1D gather, plain mode, leaves of 2 and 3 r "
                          "pieces (the best of a leaf / piece sweep for that gather on cube512)")
     a = ap.parse_args()
     if a.dropin:
         a.mode, a.no_autotune = "plain", True
-        t = {"bb1d_leaf": 2, "beam_piece_radii": 3.0}
+        t = dict(DROPIN_TUNING)
         t.update(json.loads(a.tuning) if a.tuning else {})
-        t["bb1d_kernel"] = 0
         a.tuning = json.dumps(t)
     return a
+
+
+# The plain FP32 drop-in: one thread per query for PB2D and BB1D, plain mode, leaves of 2 and 3 r
+# pieces (the best of a leaf / piece sweep for the thread-per-query BB1D gather on cube512).
+DROPIN_TUNING = {"bb1d_kernel": 0, "pb2d_kernel": 0, "bb1d_leaf": 2, "beam_piece_radii": 3.0}
+UPBP_BP2D = 65536
+
+# The reference CPU timings (the CPU baseline of the GPU arm and the --impl reference arm) use the
+# same deterministic stratified sample: every S-th query (segment and point queries alike) with S
+# chosen from the workload size so that one sample holds about REF_SAMPLE_QUERIES queries, and
+# sample k of n starting at offset k*S//n.  Each sample's time x S + the per-thread build time
+# extrapolates one whole iteration; the median over the samples is reported with its spread.
+REF_SAMPLE_QUERIES = 12000
 
 
 def dist_env():
@@ -174,54 +201,59 @@ def input_bytes(w) -> int:
     return int(sum(v.nbytes for k, v in w.items() if k not in ("params", "media")))
 
 
-def run_b200(args, cfg, rank, world, local_rank):
-    import torch
-    from smallupbp_b200 import abi, engine, multi, workload as W
+def kernel_source_hash() -> str:
+    """Digest of the kernel sources that the committed ncu traffic figure belongs to."""
+    import hashlib
+    h = hashlib.sha256()
+    csrc = os.path.join(ROOT, "smallupbp_b200", "csrc")
+    for f in ("upbp_gather.cu", "upbp_device.cuh", "upbp_traverse.cuh", "upbp_kernels.cuh", "upbp_build.cu",
+              "upbp_capi.cu"):
+        with open(os.path.join(csrc, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
 
-    torch.cuda.set_device(local_rank)
-    dev = local_rank
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    mode = engine.MODE_MIXED if args.mode == "mixed" else engine.MODE_PLAIN
-    n_iter = max(1, min(args.iterations, args.steps))
-    t0 = time.time()
-    works = []
-    for it in multi.rank_iterations(rank, world, n_iter):
-        works.append(W.make(cfg, iteration=it))
-    gen_s = time.time() - t0
-    stream = torch.cuda.Stream(device=dev)
-    npix = cfg.width * cfg.height
-    img_t = torch.zeros(npix * 3, dtype=torch.float32, device="cuda")
-    stages, all_structs = [], []
+
+def make_stages(works, dev, mode, stream, tuning=None):
+    from smallupbp_b200 import abi, engine
+    stages, structs = [], []
     for w in works:
         st = engine.EstimatorStage(dev, mode)
         st.set_stream(stream.cuda_stream)
         s = abi.make_structs(w)
         st.load(w, s)
         st.set_queries(w, s)
-        if args.tuning:
-            st.set_tuning(**json.loads(args.tuning))
+        if tuning:
+            st.set_tuning(**tuning)
         stages.append(st)
-        all_structs.append(s)
-    tuning = {"best": {k: getattr(stages[0].get_tuning(), k) for k, _ in abi.Tuning._fields_}, "autotuned": False}
-    if not args.no_autotune and not args.tuning:
-        from smallupbp_b200 import autotune
-        t_at = time.time()
-        with torch.cuda.stream(stream):
-            best, rep = autotune.autotune(stages[0], all_structs[0][0])
-        for st in stages[1:]:
-            st.set_tuning(**best)
-        tuning = {"best": best, "autotuned": True, "trials": rep["trials"], "seconds": time.time() - t_at}
-    units = [len(w["sq_path_length"]) + len(w["pq_path_length"]) for w in works]
+        structs.append(s)
+    return stages, structs
 
+
+def tune_stages(stages, structs, stream):
+    import torch
+    from smallupbp_b200 import autotune
+    t0 = time.time()
+    with torch.cuda.stream(stream):
+        best, rep = autotune.autotune(stages[0], structs[0][0])
+    for st in stages[1:]:
+        st.set_tuning(**best)
+    return {"best": best, "autotuned": True, "trials": rep["trials"], "seconds": time.time() - t0}
+
+
+def time_stages(stages, units, steps, warmup, stream, graph, world, img_t, dev, clocks=False):
+    """Warm-up, then `steps` timed steps (CUDA events on the library's stream; barrier and
+    synchronize on both sides; max over ranks).  A step is clear + build + evaluate of the next
+    iteration's stage, replayed as its CUDA graph after the warm-up, plus the framebuffer
+    all-reduce when world > 1."""
+    import torch
+    from smallupbp_b200 import engine, multi
+    n_iter = len(stages)
     graphs = set()
 
     def step(i):
         st = stages[i % n_iter]
         if id(st) in graphs:
-            st.launch_graph()  # clear + build + evaluate, captured after the warm-up
+            st.launch_graph()
         else:
             st.build()
             st.clear_image()
@@ -233,9 +265,9 @@ def run_b200(args, cfg, rank, world, local_rank):
                 dist.all_reduce(img_t)
 
     with torch.cuda.stream(stream):
-        for i in range(args.warmup):
+        for i in range(warmup):
             step(i)
-        if not args.no_graph:
+        if graph:
             for st in stages:
                 try:
                     st.capture_graph()
@@ -248,47 +280,107 @@ def run_b200(args, cfg, rank, world, local_rank):
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev)
-    clocks.start()
+    sampler = ClockSampler(dev) if clocks else None
+    if sampler:
+        sampler.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     kern = {"build_ms": [], "pp3d_ms": [], "pb2d_ms": [], "bb1d_ms": []}
-    launches = []
-    done_units = 0
+    launches, done = [], 0
     with torch.cuda.stream(stream):
         ev0.record(stream)
-        for i in range(args.steps):
+        for i in range(steps):
             step(i)
             st = stages[i % n_iter]
-            for k2, v in st.timings().items():
-                kern[k2].append(v)
+            for k, v in st.timings().items():
+                kern[k].append(v)
             b, e = st.launch_counts()
             launches.append(b + e)
-            done_units += units[i % n_iter]
+            done += units[i % n_iter]
         ev1.record(stream)
     torch.cuda.synchronize()
-    clock = clocks.stop()
+    clock = sampler.stop() if sampler else None
     ms = ev0.elapsed_time(ev1)
-    # max over ranks, total units over ranks
-    ms_max, units_total = ms, done_units
     if world > 1:
-        ms_max = multi.max_over_ranks(ms, "cuda")
-        units_total = int(multi.sum_over_ranks(done_units, "cuda"))
-    value = units_total / (ms_max / 1000.0)
+        import torch.distributed as dist
+        dist.barrier()
+        ms = multi.max_over_ranks(ms, "cuda")
+        done = int(multi.sum_over_ranks(done, "cuda"))
+    return {"ms": ms, "units": done, "value": done / (ms / 1000.0), "ms_per_step": ms / steps,
+            "kernels_ms": {k: statistics.mean(v) for k, v in kern.items()}, "launches": int(sum(launches)),
+            "clocks": clock}
 
-    # candidate statistics (outside the timed region) for the roofline
-    st0 = stages[0]
-    st0.build()
-    st0.clear_image()
-    st0.evaluate()
-    stats = st0.query_stats()
+
+def evaluate_once(st):
+    """Per-query results and the image of one evaluation (outside any timed region)."""
+    st.build()
+    st.clear_image()
+    st.evaluate()
+    pb2d, bb1d = st.segment_results()
+    return {"stats": st.query_stats(), "pb2d": pb2d, "bb1d": bb1d, "pp3d": st.point_results(),
+            "image": st.image().astype(np.float64)}
+
+
+def rel_l2(a, b) -> float:
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def fp64_image(w, dev, stream, tuning):
+    import torch
+    from smallupbp_b200 import engine
+    with torch.cuda.stream(stream), engine.EstimatorStage(dev, engine.MODE_FP64) as st:
+        st.set_stream(stream.cuda_stream)
+        st.set_tuning(**tuning)
+        st.run(w)
+        return st.image().astype(np.float64), st.query_stats()
+
+
+def run_b200(args, cfg, rank, world, local_rank):
+    import torch
+    from smallupbp_b200 import abi, engine, multi, workload as W
+
+    torch.cuda.set_device(local_rank)
+    dev = local_rank
+    shard = args.shard or ("queries" if world > 1 else "iterations")
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    mode = engine.MODE_MIXED if args.mode == "mixed" else engine.MODE_PLAIN
+    n_iter = max(1, min(args.iterations, args.steps))
+    t0 = time.time()
+    works = []
+    if shard == "queries":
+        # every rank: the same iterations, its pixel tiles of their queries
+        for it in range(n_iter):
+            works.append(multi.shard_workload(W.make(cfg, iteration=it), cfg.width, rank, world))
+    else:
+        for it in multi.rank_iterations(rank, world, n_iter):
+            works.append(W.make(cfg, iteration=it))
+    gen_s = time.time() - t0
+    stream = torch.cuda.Stream(device=dev)
+    npix = cfg.width * cfg.height
+    img_t = torch.zeros(npix * 3, dtype=torch.float32, device="cuda")
+    stages, all_structs = make_stages(works, dev, mode, stream, json.loads(args.tuning) if args.tuning else None)
+    tuning = {"best": {k: getattr(stages[0].get_tuning(), k) for k, _ in abi.Tuning._fields_}, "autotuned": False}
+    if not args.no_autotune and not args.tuning:
+        tuning = tune_stages(stages, all_structs, stream)
+    units = [len(w["sq_path_length"]) + len(w["pq_path_length"]) for w in works]
+    head = time_stages(stages, units, args.steps, args.warmup, stream, not args.no_graph, world, img_t, dev,
+                       clocks=True)
+    head["tuning"] = tuning["best"]
+    ms_max, value = head["ms"], head["value"]
+
+    # candidate statistics and per-query results (outside the timed region)
+    res0 = evaluate_once(stages[0])
+    stats = res0["stats"]
     nq, npq = len(works[0]["sq_path_length"]), len(works[0]["pq_path_length"])
     acc = {k: int(stats["count_" + k].astype(np.int64).sum()) for k in ("pb2d", "bb1d", "pp3d")}
-    tested = st0.tested_counts()
+    tested = stages[0].tested_counts()
     alg = {"pp3d": BYTES_PER_QUERY * npq + BYTES_PER_POINT_CAND * acc["pp3d"],
            "pb2d": BYTES_PER_QUERY * nq + BYTES_PER_POINT_CAND * acc["pb2d"],
            "bb1d": BYTES_PER_QUERY * nq + BYTES_PER_BB1D * acc["bb1d"]}
-    avg = {k: statistics.mean(v) for k, v in kern.items()}
+    avg = head["kernels_ms"]
     if tuning["best"].get("bb1d_kernel", 1) >= 3:
         # one persistent kernel evaluates PB2D and BB1D: its phase (bb1d_ms) carries both
         alg["bb1d"] += alg.pop("pb2d")
@@ -296,12 +388,18 @@ def run_b200(args, cfg, rank, world, local_rank):
     dom = max(("pp3d", "pb2d", "bb1d"), key=lambda k: avg[k + "_ms"])
     peak, peak_kind = measured_peak()
     achieved = alg[dom] / (avg[dom + "_ms"] / 1000.0) / 1e9 if avg[dom + "_ms"] > 0 else None
-    traffic = None
+    traffic, traffic_note = None, "no ncu capture committed for this kernel and workload"
     tfile = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (dom, cfg.name))
     if os.path.exists(tfile):
         try:
             with open(tfile) as fh:
-                traffic = json.load(fh).get("dram_bytes_per_launch")
+                tj = json.load(fh)
+            same_tuning = all(tuning["best"].get(k) == v for k, v in (tj.get("tuning") or {}).items())
+            if tj.get("kernel_source_hash") == kernel_source_hash() and same_tuning:
+                traffic = tj.get("dram_bytes_per_launch")
+                traffic_note = tj.get("how", "")
+            else:
+                traffic_note = "the committed ncu capture is of other kernel sources or another tuning: not used"
         except Exception:
             traffic = None
 
@@ -345,25 +443,46 @@ def run_b200(args, cfg, rank, world, local_rank):
         e1.record(streams[0])
         torch.cuda.synchronize()
         e_ms = e0.elapsed_time(e1)
+        e_units_total = e_units * args.steps
         if world > 1:
             e_ms = multi.max_over_ranks(e_ms, "cuda")
-        e2e = {"value": e_units * args.steps * world / (e_ms / 1000.0), "unit": "queries/s",
+            e_units_total = int(multi.sum_over_ranks(e_units_total, "cuda"))
+        e2e = {"value": e_units_total / (e_ms / 1000.0), "unit": "queries/s",
                "h2d_bytes_per_step": input_bytes(works[0]), "d2h_bytes_per_step": npix * 3 * 4,
                "ms_per_step": e_ms / args.steps,
                "pipeline": "two contexts alternate; a step's uploads overlap the previous step's evaluation"}
         for st in ctxs:
             st.close()
 
-    # accuracy of the measured mode on the benchmark workload: image rel-L2 against the FP64 mode
-    # (the same candidates, all geometry, contributions and MIS weights in FP64)
+    # accuracy of every arm on the benchmark workload: image rel-L2 against the GPU FP64 mode (the
+    # same candidates, all geometry, contributions and MIS weights in FP64)
+    img64 = None
     accuracy = None
     if not args.no_accuracy:
-        accuracy = image_accuracy(works[0], dev, mode, tuning, stream)
+        img64, stats64 = fp64_image(works[0], dev, stream, tuning["best"])
+        l2 = rel_l2(res0["image"], img64)
+        accuracy = {"image_rel_l2_vs_fp64": l2, "bound": 1e-3, "within_bound": l2 <= 1e-3,
+                    "same_bb1d_candidates": bool(np.array_equal(stats["count_bb1d"], stats64["count_bb1d"]) and
+                                                 np.array_equal(stats["hash_bb1d"], stats64["hash_bb1d"]))}
 
     # whole iteration on the device: light and camera passes, build, evaluate, image read back
     device_passes = None
-    if not args.no_device_passes and cfg.name != "beamstress":
+    if not args.no_device_passes and cfg.name != "beamstress" and shard == "iterations":
         device_passes = run_device_passes(args, cfg, dev, mode, stream, tuning, npix, rank, world)
+    for st in stages:
+        st.close()
+
+    # the comparison arms of the metric, on the same workload (one GPU)
+    arms = plain_res = None
+    if world == 1 and not args.no_arms and args.mode == "mixed" and not args.tuning:
+        arms, plain_res = run_arms(args, works, units, dev, stream, img_t, head, res0, img64)
+
+    parity = None
+    if rank == 0 and world == 1 and not args.no_parity:
+        checked = {args.mode: res0}
+        if plain_res is not None:
+            checked["plain"] = plain_res
+        parity = reference_parity(works[0], checked)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -372,10 +491,6 @@ def run_b200(args, cfg, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    for st in stages:
-        st.close()
-    if world > 1:
-        import torch.distributed as dist
         dist.destroy_process_group()
     if rank != 0:
         return None
@@ -388,7 +503,7 @@ def run_b200(args, cfg, rank, world, local_rank):
         "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if shard == "queries" and world > 1 else "weak",
         "vs_baseline": None,
         "dtype": "f32" if args.mode == "plain" else "f32+f64",
         "data": "synthetic: seeded UPBP light/camera passes (Philox) in the %s scene; no dataset" % cfg.name,
@@ -396,7 +511,12 @@ def run_b200(args, cfg, rank, world, local_rank):
                        iterations_cycled=n_iter,
                        queries_per_iteration={"segment": nq, "point": npq},
                        photons=int((works[0]["lv_flags"] & 1).sum()), beams=len(works[0]["beam_length"]),
-                       parallelism="dp%d (one iteration per rank, framebuffer all-reduce)" % world,
+                       parallelism=("dp%d: each rank builds the iteration's structures and evaluates its 32x32 pixel "
+                                    "tiles of the queries; framebuffer all-reduce" % world) if shard == "queries" else
+                                   ("dp%d: one iteration per rank, framebuffer all-reduce" % world),
+                       candidate_sets="the reference's brute-force BB1D estimator (PhBrute.hxx) under the reach rule "
+                                      "(FP64 segment distance <= r(u) + 2e-5 + 1e-3 r); the reference's default grid "
+                                      "(USE_GRID) differs where a closest approach falls on a DDA cell boundary",
                        tuning=tuning, cuda_graph=not args.no_graph),
         "ms_per_iteration": ms_max / args.steps,
         "kernels_ms": avg,
@@ -404,34 +524,144 @@ def run_b200(args, cfg, rank, world, local_rank):
         "tested_candidates": tested,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": achieved / peak if achieved is not None else None, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg[dom]},
+                     "traffic_note": traffic_note, "algorithmic_bytes_per_launch": alg[dom]},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": int(sum(launches)),
-        "clocks": clock,
+        "gpu_launches": head["launches"],
+        "clocks": head["clocks"],
         "generate_s": gen_s,
         "device_passes": device_passes,
         "accuracy": accuracy,
+        "arms": arms,
+        "parity": parity,
     }
     return line
 
 
-def image_accuracy(w, dev, mode, tuning, stream):
-    """Image rel-L2 of `mode` against the GPU FP64 mode on workload `w` (one iteration)."""
-    import torch
+def run_arms(args, works, units, dev, stream, img_t, head, res0, img64):
+    """The metric's comparison on the same workload and in the same run: plain FP32 with the same
+    warp-cooperative kernels (autotuned on its own), the plain FP32 drop-in (one thread per query),
+    and the mixed stage with B-P2D on; each with its image rel-L2 against the FP64 mode."""
     from smallupbp_b200 import engine
-    imgs, counts = {}, {}
-    for m in (mode, engine.MODE_FP64):
-        with torch.cuda.stream(stream), engine.EstimatorStage(dev, m) as st:
-            st.set_stream(stream.cuda_stream)
-            st.set_tuning(**tuning["best"])
-            st.run(w)
-            imgs[m] = st.image().astype(np.float64)
-            counts[m] = int(st.query_stats()["count_bb1d"].astype(np.int64).sum())
-    a, b = imgs[mode], imgs[engine.MODE_FP64]
-    l2 = float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
-    return {"image_rel_l2_vs_fp64": l2, "bound": 1e-3, "within_bound": l2 <= 1e-3,
-            "same_bb1d_candidates": counts[mode] == counts[engine.MODE_FP64]}
+    arms = {"mixed": {"ms_per_iteration": head["ms_per_step"], "value": head["value"],
+                      "bb1d_ms": head["kernels_ms"]["bb1d_ms"],
+                      "image_rel_l2_vs_fp64": rel_l2(res0["image"], img64) if img64 is not None else None}}
+    plain_res = None
+    for name, mode, tun, steps, warmup in (
+            ("plain_fp32", engine.MODE_PLAIN, None, args.steps, args.warmup),
+            ("dropin_fp32", engine.MODE_PLAIN, DROPIN_TUNING, min(args.steps, 2), 1)):
+        stages, structs = make_stages(works, dev, mode, stream, tun)
+        if tun:
+            tuning = {"best": dict(tun), "autotuned": False}
+        elif not args.no_autotune:
+            tuning = tune_stages(stages, structs, stream)
+        else:
+            tuning = {"best": None, "autotuned": False}
+        r = time_stages(stages, units, steps, warmup, stream, not args.no_graph, 1, img_t, dev)
+        res = evaluate_once(stages[0])
+        same = bool(np.array_equal(res["stats"]["count_bb1d"], res0["stats"]["count_bb1d"]) and
+                    np.array_equal(res["stats"]["hash_bb1d"], res0["stats"]["hash_bb1d"]))
+        arms[name] = {"ms_per_iteration": r["ms_per_step"], "value": r["value"], "steps": steps, "warmup": warmup,
+                      "bb1d_ms": r["kernels_ms"]["bb1d_ms"], "tuning": tuning["best"],
+                      "image_rel_l2_vs_fp64": rel_l2(res["image"], img64) if img64 is not None else None,
+                      "same_candidates_as_mixed": same}
+        if name == "plain_fp32":
+            plain_res = res
+        for st in stages:
+            st.close()
+    # B-P2D on (the fourth estimator; the reference has none, so the headline runs without it)
+    wb = []
+    for w in works:
+        w2 = dict(w)
+        w2["params"] = w["params"].copy()
+        w2["params"]["techniques"] = int(w["params"]["techniques"][0]) | UPBP_BP2D
+        wb.append(w2)
+    stages, _ = make_stages(wb, dev, engine.MODE_MIXED, stream, head["tuning"])
+    r = time_stages(stages, units, min(args.steps, 5), args.warmup, stream, not args.no_graph, 1, img_t, dev)
+    for st in stages:
+        st.close()
+    arms["mixed_with_bp2d"] = {"ms_per_iteration": r["ms_per_step"], "value": r["value"],
+                               "estimators": "PP3D+PB2D+BB1D+B-P2D (B-P2D standalone, MIS weight 1)"}
+    m = arms["mixed"]["ms_per_iteration"]
+    arms["speedup_mixed_vs_plain_fp32"] = arms["plain_fp32"]["ms_per_iteration"] / m
+    arms["speedup_mixed_vs_dropin_fp32"] = arms["dropin_fp32"]["ms_per_iteration"] / m
+    arms["target"] = "mixed >= 3x the plain FP32 GPU drop-in at image rel-L2 <= 1e-3 against FP64"
+    return arms, plain_res
+
+
+def reference_parity(w, results: dict) -> dict:
+    """Sampled queries of the benchmark workload evaluated by the reference's own estimator code
+    (EmbreeBre, the brute-force PhotonBeamsEvaluator, HashGrid + RangeQuery; oracle/_ref) and
+    compared with the GPU's per-query candidate counts, candidate hashes and contributions: every
+    S-th segment and point query, S chosen for about 2,000 segment queries."""
+    from oracle import ref
+    if not ref.available():
+        return {"unavailable": "oracle/_ref not built on this machine"}
+    t0 = time.time()
+    nq, npq = len(w["sq_path_length"]), len(w["pq_path_length"])
+    stride = max(1, nq // 2000)
+    sess = ref.Session(w, ref.PB2D | ref.BB1D_BRUTE | ref.PP3D | ref.CANDIDATES, ref_threads())
+    o = sess.eval_outputs(0, stride)
+    sess.close()
+    si, pi = np.arange(0, nq, stride), np.arange(0, npq, stride)
+    out = {"queries_checked": {"segment": int(len(si)), "point": int(len(pi))}, "stride": stride,
+           "reference": "PhotonBeamsEvaluator brute force (PhBrute.hxx), EmbreeBre, HashGrid/RangeQuery",
+           "accepted_checked": {k: int(o["count_" + k][idx].astype(np.int64).sum())
+                                for k, idx in (("pb2d", si), ("bb1d", si), ("pp3d", pi))}}
+    want = {"pb2d": o["pb2d"], "bb1d": o["bb1d_brute"], "pp3d": o["pp3d"]}
+    for name, res in results.items():
+        if res is None:
+            continue
+        mism, rel = {}, {}
+        for est, idx in (("pb2d", si), ("bb1d", si), ("pp3d", pi)):
+            st = res["stats"]
+            mism[est] = int(((st["count_" + est][idx] != o["count_" + est][idx]) |
+                             (st["hash_" + est][idx] != o["hash_" + est][idx])).sum())
+            g, r = res[est][idx].astype(np.float64), want[est][idx].astype(np.float64)
+            floor = 1e-6 * max(float(np.abs(r).max()) if len(r) else 0.0, 1e-30)
+            e = (np.abs(g - r) / (np.abs(r) + floor)).max(axis=1) if len(idx) else np.zeros(0)
+            rel[est] = {"max_rel": float(e.max()) if len(e) else 0.0,
+                        "within_1e-4": float((e <= 1e-4).mean()) if len(e) else 1.0}
+        out[name] = {"candidate_mismatches": mism, "contributions": rel}
+    out["seconds"] = time.time() - t0
+    return out
+
+
+def ref_threads() -> int:
+    """Host threads for the reference: all cores, fewer when host memory cannot hold a copy of the
+    structures per thread (about 5 GB each at cube1024)."""
+    cores = os.cpu_count() or 1
+    threads = cores
+    try:
+        with open("/proc/meminfo") as fh:
+            avail_gb = int([l for l in fh if l.startswith("MemAvailable")][0].split()[1]) / 1e6
+        threads = max(1, min(cores, int((avail_gb - 8) / 5.0)))
+    except Exception:
+        pass
+    return threads
+
+
+def reference_timing(w, samples: int, warmup: int, threads: int, stride_scale: int = 1) -> dict:
+    """The reference's estimators (grid BB1D at -gridres 64) timed on the shared stratified sample:
+    stride S (times stride_scale), sample k of `samples` at offset k*S//samples; each sample's
+    time x S plus the per-thread build extrapolates one iteration, and the median is reported."""
+    from oracle import ref
+    ref.set_grid_options(64)
+    sess = ref.Session(w, ref.PB2D | ref.BB1D_GRID | ref.PP3D, threads)
+    total = sess.n_segment + sess.n_point
+    S = max(1, int(round(total / REF_SAMPLE_QUERIES))) * stride_scale
+    offs = [(k * S) // samples for k in range(samples)]
+    for i in range(warmup):
+        sess.eval(offs[i % samples], S)
+    times = [sess.eval(o, S) for o in offs]
+    sess.close()
+    full = sorted(sess.build_ms + t * S for t in times)
+    med = statistics.median(full)
+    vals = [total / (f / 1000.0) for f in full]
+    return {"value": total / (med / 1000.0), "ms_per_iteration": med, "build_ms": sess.build_ms,
+            "sample_ms": [round(t, 1) for t in times], "median_sample_ms": statistics.median(times),
+            "stride": S, "sampled_fraction": 1.0 / S, "samples": samples,
+            "spread": {"min": min(vals), "max": max(vals)}}
 
 
 def run_device_passes(args, cfg, dev, mode, stream, tuning, npix, rank, world):
@@ -483,53 +713,35 @@ def run_device_passes(args, cfg, dev, mode, stream, tuning, npix, rank, world):
 
 def cpu_baseline(w, seconds: float) -> dict:
     """The reference estimator code (oracle/_ref, built from the reference sources) timed on this
-    host's cores on a 1-in-S sample of the queries, extrapolated to the full iteration."""
+    host's cores on the shared stratified sample (the same samples as --impl reference), median of
+    five, plus the same code on one core."""
     from oracle import ref
     if not ref.available():
         return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
                 "sample": "unavailable: oracle/_ref not built on this machine"}
-    cores = os.cpu_count() or 1
-    threads = cores
-    try:
-        with open("/proc/meminfo") as fh:
-            avail_gb = int([l for l in fh if l.startswith("MemAvailable")][0].split()[1]) / 1e6
-        threads = max(1, min(cores, int((avail_gb - 8) / 5.0)))
-    except Exception:
-        pass
-    ref.set_grid_options(64)
-    sess = ref.Session(w, ref.PB2D | ref.BB1D_GRID | ref.PP3D, threads)
-    n_seg, n_pt = sess.n_segment, sess.n_point
-    total = n_seg + n_pt
-    probe_stride = max(1, total // (threads * 8))
-    t_probe = sess.eval(1, probe_stride)
-    per_query_ms = t_probe / max(1, len(range(1, max(n_seg, n_pt), probe_stride)))
-    stride = max(1, int(math.ceil(per_query_ms * max(n_seg, n_pt) / (seconds * 1000.0))))
-    t = sess.eval(0, stride)
-    sess.close()
-    full_ms = sess.build_ms + t * stride
-    out = {"value": total / (full_ms / 1000.0), "unit": "queries/s", "cores": threads, "kind": "reference",
+    threads = ref_threads()
+    r = reference_timing(w, 5, 1, threads)
+    out = {"value": r["value"], "unit": "queries/s", "cores": threads, "kind": "reference",
            "sample": "reference SmallUPBP estimators (EmbreeBre + PhotonBeamsEvaluator USE_GRID -gridres 64 + "
-                     "HashGrid/RangeQuery), one structure set per thread; every %d-th query timed (%.1f s) and "
-                     "extrapolated linearly, plus the per-thread build (%.1f s)" % (stride, t / 1000.0,
-                                                                                    sess.build_ms / 1000.0),
-           "ms_per_iteration": full_ms}
-    # the same code on one core: its own build plus a sample about a quarter as long
-    one = ref.Session(w, ref.PB2D | ref.BB1D_GRID | ref.PP3D, 1)
-    n_max = max(n_seg, n_pt)
-    pstride = max(1, n_max // 64)
-    per_query1 = one.eval(1, pstride) / max(1, len(range(1, n_max, pstride)))
-    stride1 = max(1, int(math.ceil(per_query1 * n_max / (seconds * 250.0))))
-    t1 = one.eval(0, stride1)
-    one.close()
-    ms1 = one.build_ms + t1 * stride1
-    out["one_core"] = {"value": total / (ms1 / 1000.0), "unit": "queries/s", "ms_per_iteration": ms1,
-                       "sample": "every %d-th query timed on one thread (%.1f s), plus its build (%.1f s)" % (
-                           stride1, t1 / 1000.0, one.build_ms / 1000.0)}
+                     "HashGrid/RangeQuery), one structure set per thread; 5 samples of every %d-th query (strata "
+                     "k*%d/5), each %.1f s median, extrapolated linearly to the iteration plus the per-thread build "
+                     "(%.1f s); median of the 5" % (r["stride"], r["stride"], r["median_sample_ms"] / 1000.0,
+                                                   r["build_ms"] / 1000.0),
+           "ms_per_iteration": r["ms_per_iteration"], "sampled_fraction": r["sampled_fraction"],
+           "spread": r["spread"]}
+    one = reference_timing(w, 3, 0, 1, stride_scale=16)
+    out["one_core"] = {"value": one["value"], "unit": "queries/s", "ms_per_iteration": one["ms_per_iteration"],
+                       "sample": "3 samples of every %d-th query on one thread (%.1f s each), plus its build (%.1f s); "
+                                 "median" % (one["stride"], one["median_sample_ms"] / 1000.0, one["build_ms"] / 1000.0),
+                       "spread": one["spread"]}
     return out
 
 
 def run_reference(args, cfg, rank, world):
-    """--impl reference: the reference's own CPU estimator code on this host's cores."""
+    """--impl reference: the reference's own CPU estimator code on this host's cores.  A step is one
+    sample of the shared stratified sample (every S-th query; the samples take the strata
+    k*S/steps), timed; the value extrapolates the median sample to the whole iteration, with the
+    per-thread build.  Under torchrun only rank 0 works."""
     if rank != 0:
         return None
     from oracle import ref
@@ -537,38 +749,24 @@ def run_reference(args, cfg, rank, world):
     if not ref.available():
         return {"impl": "reference", "unavailable": "oracle/_ref (reference built from its sources) is not present"}
     w = W.make(cfg, iteration=0)
-    cores = os.cpu_count() or 1
-    threads = cores
-    try:
-        with open("/proc/meminfo") as fh:
-            avail_gb = int([l for l in fh if l.startswith("MemAvailable")][0].split()[1]) / 1e6
-        threads = max(1, min(cores, int((avail_gb - 8) / 5.0)))
-    except Exception:
-        pass
-    ref.set_grid_options(64)
-    sess = ref.Session(w, ref.PB2D | ref.BB1D_GRID | ref.PP3D, threads)
-    n = max(sess.n_segment, sess.n_point)
-    total = sess.n_segment + sess.n_point
-    probe = sess.eval(1, max(1, n // (threads * 8)))
-    per_q = probe / max(1, len(range(1, n, max(1, n // (threads * 8)))))
-    stride = max(1, int(math.ceil(per_q * n / (max(1.0, args.cpu_seconds / 2) * 1000.0))))
-    for i in range(args.warmup):
-        sess.eval(2 + i, stride * 4)
-    times = []
-    for i in range(args.steps):
-        times.append(sess.eval(i % stride, stride))
-    sess.close()
-    step_ms = sess.build_ms + statistics.mean(times) * stride
-    value = total / (step_ms / 1000.0)
+    threads = ref_threads()
+    r = reference_timing(w, max(1, args.steps), args.warmup, threads)
+    value = r["value"]
     return {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": r["median_sample_ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "impl": "reference",
         "data": "synthetic: seeded UPBP light/camera passes (Philox) in the %s scene; no dataset" % cfg.name,
         "config": dict(workload_desc(cfg), grid_resolution=64),
+        "ms_per_iteration": r["ms_per_iteration"],
+        "steps_are": "samples: each step evaluates every %d-th query (%.4f of the iteration); ms_per_step is the "
+                     "median sample's wall time, ms_per_iteration its extrapolation plus the per-thread build "
+                     "(%.1f s)" % (r["stride"], r["sampled_fraction"], r["build_ms"] / 1000.0),
+        "spread": r["spread"],
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "reference",
-                         "sample": "every %d-th query per step, extrapolated with the per-thread build (%.1f s)" % (
-                             stride, sess.build_ms / 1000.0)},
+                         "sample": "%d samples of every %d-th query (strata k*%d/%d), median extrapolated with the "
+                                   "per-thread build (%.1f s)" % (args.steps, r["stride"], r["stride"], args.steps,
+                                                                 r["build_ms"] / 1000.0)},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -642,9 +840,22 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     }
 
 
+def spawn_ranks(n: int) -> int:
+    """Start n ranks of this script (one per GPU) under torch.distributed.run on this node."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
     rank, world, local_rank = dist_env()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     from smallupbp_b200 import workload as W
     cfg = W.config(args.config)
     if args.impl == "reference":

@@ -118,6 +118,27 @@ class Session:
             raise RuntimeError("ref_eval failed")
         return o.gather_ms
 
+    def eval_outputs(self, offset: int, stride: int) -> Dict[str, np.ndarray]:
+        """Evaluate queries offset, offset+stride, ... and return their per-query outputs (rows of
+        the other queries stay zero) and ``gather_ms``.  Candidate counts and hashes are filled when
+        the session was prepared with CANDIDATES."""
+        nq, npq = self.n_segment, self.n_point
+        out = {"pb2d": np.zeros((nq, 3), np.float32), "bb1d": np.zeros((nq, 3), np.float32),
+               "bb1d_brute": np.zeros((nq, 3), np.float32), "pp3d": np.zeros((npq, 3), np.float32),
+               "count_pb2d": np.zeros(nq, np.uint32), "hash_pb2d": np.zeros(nq, np.uint64),
+               "count_bb1d": np.zeros(nq, np.uint32), "hash_bb1d": np.zeros(nq, np.uint64),
+               "count_pp3d": np.zeros(npq, np.uint32), "hash_pp3d": np.zeros(npq, np.uint64)}
+        o = RefOutputs(
+            pb2d_rgb=abi.ptr(out["pb2d"]), bb1d_rgb=abi.ptr(out["bb1d"]), bb1d_brute_rgb=abi.ptr(out["bb1d_brute"]),
+            pp3d_rgb=abi.ptr(out["pp3d"]), count_pb2d=abi.ptr(out["count_pb2d"]), hash_pb2d=abi.ptr(out["hash_pb2d"]),
+            count_bb1d=abi.ptr(out["count_bb1d"]), hash_bb1d=abi.ptr(out["hash_bb1d"]),
+            count_pp3d=abi.ptr(out["count_pp3d"]), hash_pp3d=abi.ptr(out["hash_pp3d"]))
+        rc = self._l.ref_eval(self._h, offset, stride, C.byref(o))
+        if rc != 0:
+            raise RuntimeError("ref_eval failed")
+        out["gather_ms"] = o.gather_ms
+        return out
+
     def close(self):
         if self._h:
             self._l.ref_release(self._h)

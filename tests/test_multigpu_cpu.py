@@ -1,9 +1,12 @@
 """The multi-rank host path on CPU: world size 2 over gloo, one process per rank.
 
-Each rank runs its round-robin share of the iterations (the oracle stands in for the device
-evaluation, which needs a GPU), and ``multi.combine_framebuffers`` must give the reference's final
-framebuffer: the mean over renderers of each renderer's mean over its iterations
-(``SmallUPBP.cxx:143-176``, ``Renderer.hxx:55-61``).
+Query shards: each rank evaluates its pixel tiles of one iteration's queries (the oracle stands in
+for the device evaluation, which needs a GPU) over the whole photon and beam records, and one
+all-reduce (sum) of the framebuffers must give the serial image of the iteration.
+
+Whole iterations: each rank runs its round-robin share of the iterations, and
+``multi.combine_framebuffers`` must give the reference's final framebuffer: the mean over renderers
+of each renderer's mean over its iterations (``SmallUPBP.cxx:143-176``, ``Renderer.hxx:55-61``).
 """
 import multiprocessing as mp
 import os
@@ -56,6 +59,76 @@ def _rank_main(rank, world, port, total, out_dir):
     np.save(os.path.join(out_dir, "rank%d.npy" % rank), t.numpy())
     np.save(os.path.join(out_dir, "rank%d_stats.npy" % rank), np.array([slow, units]))
     dist.destroy_process_group()
+
+
+def _shard_rank_main(rank, world, port, out_dir):
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from oracle import port as oport
+    from smallupbp_b200 import multi
+    from smallupbp_b200 import workload as W
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    cfg = W.config(CFG)
+    w = multi.shard_workload(W.generate(cfg, iteration=0), cfg.width, rank, world, tile=4)
+    t = torch.from_numpy(oport.run(w)["image"].astype(np.float64).reshape(-1))
+    dist.all_reduce(t)
+    units = multi.sum_over_ranks(len(w["sq_path_length"]) + len(w["pq_path_length"]), "cpu")
+    np.save(os.path.join(out_dir, "shard%d.npy" % rank), t.numpy())
+    np.save(os.path.join(out_dir, "shard%d_units.npy" % rank), np.array([units]))
+    dist.destroy_process_group()
+
+
+def test_query_shards_partition_the_queries():
+    from smallupbp_b200 import multi
+    from smallupbp_b200 import workload as W
+
+    cfg = W.config(CFG)
+    w = W.generate(cfg, iteration=0)
+    for world in (1, 2, 3, 8):
+        for key in ("sq_pixel", "pq_pixel"):
+            parts = [multi.query_shard(w[key], cfg.width, r, world, tile=4) for r in range(world)]
+            allq = np.sort(np.concatenate(parts))
+            np.testing.assert_array_equal(allq, np.arange(len(w[key])))
+            if world > 1 and key == "sq_pixel":
+                sizes = np.array([len(p) for p in parts])
+                assert sizes.min() > 0.5 * sizes.mean(), sizes
+    s = multi.shard_workload(w, cfg.width, 1, 2, tile=4)
+    assert len(s["sq_origin"]) == len(s["sq_pixel"]) < len(w["sq_pixel"])
+    assert s["seg_dist_min"] is w["seg_dist_min"] and s["beam_origin"] is w["beam_origin"]
+    with pytest.raises(ValueError):
+        multi.query_shard(w["sq_pixel"], cfg.width, 2, 2)
+
+
+def test_two_query_shards_sum_to_the_serial_image(tmp_path):
+    from oracle import port as oport
+    from smallupbp_b200 import workload as W
+
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_rank_main, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+            p.join()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    w = W.generate(W.config(CFG), iteration=0)
+    want = oport.run(w)["image"].astype(np.float64).reshape(-1)
+    assert np.abs(want).max() > 0
+    for r in range(2):
+        got = np.load(os.path.join(tmp_path, "shard%d.npy" % r))
+        np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-7 * np.abs(want).max())
+        units = np.load(os.path.join(tmp_path, "shard%d_units.npy" % r))[0]
+        assert units == len(w["sq_path_length"]) + len(w["pq_path_length"])
 
 
 def _image_shape():
