@@ -268,6 +268,10 @@ typedef struct upbp_tuning {
     float beam_piece_radii;
     int32_t bb1d_kernel;
     int32_t pb2d_kernel;
+    /* order in which the persistent gathers draw the segment queries: 0 along a Morton curve of
+     * their midpoints; 1 the camera rays (path length 1) along a Morton curve of their pixels,
+     * then the other segments by midpoint; 2 along a 5-D Morton curve of midpoint and direction */
+    int32_t query_order;
 } upbp_tuning;
 int upbp_set_tuning(upbp_ctx* ctx, const upbp_tuning* tuning);
 int upbp_get_tuning(const upbp_ctx* ctx, upbp_tuning* tuning);

@@ -61,7 +61,8 @@ class PointQueries(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("pb2d_leaf", C.c_int32), ("bb1d_leaf", C.c_int32), ("block_threads", C.c_int32),
-                ("beam_piece_radii", C.c_float), ("bb1d_kernel", C.c_int32), ("pb2d_kernel", C.c_int32)]
+                ("beam_piece_radii", C.c_float), ("bb1d_kernel", C.c_int32), ("pb2d_kernel", C.c_int32),
+                ("query_order", C.c_int32)]
 
 
 class QueryStats(C.Structure):

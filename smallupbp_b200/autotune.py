@@ -10,6 +10,9 @@ The knobs (``upbp_tuning`` in ``include/upbp_gpu.h``):
 * ``pb2d_kernel`` picks the PB2D gather when it runs on its own: 0 one thread per query, 1 one
   warp per query from a persistent work queue;
 * ``pb2d_leaf`` is the photon count per PB2D LBVH leaf;
+* ``query_order`` is the order in which the persistent gathers draw the segment queries: 0 along a
+  Morton curve of their midpoints, 1 the camera rays by pixel first (neighbouring pixels' rays
+  cross nearly the same beam pieces), then the other segments by midpoint;
 * ``block_threads`` is the block shape (queries per block) of the thread-per-query PB2D and PP3D
   gathers.
 
@@ -30,7 +33,7 @@ from typing import Dict, Iterable, List, Optional, Tuple
 # searched one stage at a time (coordinate descent), each stage a grid over its knobs
 STAGES = (
     {"bb1d_kernel": (1, 2, 3, 4)},
-    {"bb1d_leaf": (4, 8, 16), "beam_piece_radii": (4.0, 6.0, 8.0)},
+    {"bb1d_leaf": (4, 8, 16), "beam_piece_radii": (4.0, 6.0, 8.0), "query_order": (0, 1)},
     {"pb2d_kernel": (0, 1), "pb2d_leaf": (4, 8, 16), "block_threads": (128, 256)},
 )
 

@@ -111,6 +111,7 @@ struct upbp_ctx {
     int num_sms = 0;
     int bb1d_kernel = 2;  // 0: thread per query, 1-2: warp-cooperative BB1D, 3-4: fused segment kernel
     int pb2d_kernel = 1;  // PB2D on its own: 0 thread per query, 1 warp-cooperative persistent
+    int query_order = 1;  // segment query order of the persistent gathers (upbp_tuning.query_order)
     DBuf out_bp2d, cnt_bp2d, hash_bp2d;  // B-P2D (extension) per point query
     DBuf tr_cnt, tr_off, tr_status;  // device-side light / camera passes: per-path record counts and offsets
     DBuf out_pb2d, out_bb1d, out_pp3d, image, cnt_pb2d, cnt_bb1d, cnt_pp3d, hash_pb2d, hash_bb1d, hash_pp3d, tested;
@@ -680,8 +681,8 @@ const int32_t* query_order(upbp_ctx* c, const SegQueriesDev& Q, cudaStream_t s)
     ensure(c, c->q_keys_sorted, sizeof(uint32_t) * nq);
     ensure(c, c->q_iota, sizeof(int32_t) * nq);
     ensure(c, c->q_order, sizeof(int32_t) * nq);
-    launch_query_keys(Q, c->n_pieces > 0 ? c->bbox_pc.as<float>() : c->bbox_ph.as<float>(), c->q_keys.as<uint32_t>(),
-                      c->q_iota.as<int32_t>(), s);
+    launch_query_keys(Q, c->n_pieces > 0 ? c->bbox_pc.as<float>() : c->bbox_ph.as<float>(), c->query_order,
+                      c->P.image_width, c->q_keys.as<uint32_t>(), c->q_iota.as<int32_t>(), s);
     size_t b = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b, c->q_keys.as<uint32_t>(), c->q_keys_sorted.as<uint32_t>(),
                                     c->q_iota.as<int32_t>(), c->q_order.as<int32_t>(), (int)nq, 0, 30, s);
@@ -1000,12 +1001,14 @@ int upbp_set_tuning(upbp_ctx* c, const upbp_tuning* tu)
             fail(c, UPBP_ERR_INVALID_ARG, "beam_piece_radii must be in [1, 1024]");
         if (tu->bb1d_kernel < 0 || tu->bb1d_kernel > 4) fail(c, UPBP_ERR_INVALID_ARG, "bb1d_kernel must be in [0, 4]");
         if (tu->pb2d_kernel < 0 || tu->pb2d_kernel > 1) fail(c, UPBP_ERR_INVALID_ARG, "pb2d_kernel must be 0 or 1");
+        if (tu->query_order < 0 || tu->query_order > 2) fail(c, UPBP_ERR_INVALID_ARG, "query_order must be in [0, 2]");
         c->pb2d_leaf = tu->pb2d_leaf;
         c->bb1d_leaf = tu->bb1d_leaf;
         c->block = tu->block_threads;
         c->piece_len_r = tu->beam_piece_radii;
         c->bb1d_kernel = tu->bb1d_kernel;
         c->pb2d_kernel = tu->pb2d_kernel;
+        c->query_order = tu->query_order;
         c->built = false;
     });
 }
@@ -1019,6 +1022,7 @@ int upbp_get_tuning(const upbp_ctx* c, upbp_tuning* tu)
     tu->beam_piece_radii = c->piece_len_r;
     tu->bb1d_kernel = c->bb1d_kernel;
     tu->pb2d_kernel = c->pb2d_kernel;
+    tu->query_order = c->query_order;
     return UPBP_OK;
 }
 

@@ -140,10 +140,11 @@ __device__ __forceinline__ bool beam_beam_near(V3 O1, V3 d1, V3 O2, V3 d2, float
     return !(xmul(ad, ad) >= xmul(maxDistSqr, sinThetaSqr));
 }
 
-// PhotonBeam::testIntersectionBeamBeam (Beams/PhotonBeam.hxx:238-296)
+// PhotonBeam::testIntersectionBeamBeam (Beams/PhotonBeam.hxx:238-296).  On acceptance it can also
+// return b = d1.d2 and e = d2.O1 - d2.O2, the terms of the line solution that piece_takes_fast uses.
 __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float maxT1, V3 O2, V3 d2, float minT2,
                                                float maxT2, float maxDistSqr, float* oDist, float* oSin, float* oT1,
-                                               float* oT2)
+                                               float* oT2, float* oB = nullptr, float* oE = nullptr)
 {
     const V3 c = xcross3(d1, d2);
     const float sinThetaSqr = xdot3(c, c);
@@ -155,7 +156,8 @@ __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float 
     if (d1d2SqrMinus1 < 1e-5f && d1d2SqrMinus1 > -1e-5f) return false;
     const float d1O1 = xdot3(d1, O1);
     const float d1O2 = xdot3(d1, O2);
-    const float t1 = xdiv(xsub(xsub(d1O1, d1O2), xmul(d1d2, xsub(xdot3(d2, O1), xdot3(d2, O2)))), d1d2SqrMinus1);
+    const float e = xsub(xdot3(d2, O1), xdot3(d2, O2));
+    const float t1 = xdiv(xsub(xsub(d1O1, d1O2), xmul(d1d2, e)), d1d2SqrMinus1);
     if (t1 <= minT1 || t1 >= maxT1) return false;
     const float t2 = xdiv(xsub(xadd(t1, d1O1), d1O2), d1d2);
     if (t2 <= minT2 || t2 >= maxT2 || isnan(t2)) return false;
@@ -164,6 +166,8 @@ __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float 
     *oSin = s;
     *oT1 = t1;
     *oT2 = t2;
+    if (oB) *oB = d1d2;
+    if (oE) *oE = e;
     return true;
 }
 
@@ -225,28 +229,31 @@ __device__ __forceinline__ SegClosest seg_closest_f64(V3 O1, V3 d1, float dminf,
 }
 
 // 1: this piece takes the candidate, 0: it does not (another piece owns it), -1: undecided in
-// FP32 (use piece_takes_f64).  Called after the predicate and the radius test accepted the pair
-// (dist <= radius = r(t2)); rc_abs = |dr/dt| of the beam radius (0 for a constant radius).
-// Where |c| (1 - c^2) > 0.04 with c = d1.d2, the rounding error of the FP32 t1 and t2 stays below
-// m = 1e-4 * scale, so t1, t2 more than m inside their ranges put the exact closest points inside
-// both segments: u is the exact t2, and D is the distance of the lines, which the FP32 dist
-// approximates within errb (|ad| carries at most 6 ulp of |O2 - O1|_1 and sin(theta) > 0.2 there;
-// errb is twice that bound).
-__device__ __forceinline__ int piece_takes_fast(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
-                                                float t_lo, float t_hi, float t1, float t2, float dist, float radius,
-                                                float rc_abs, float extra)
+// FP32 (use piece_takes_f64).  Called after the predicate and the radius test accepted the pair,
+// with b = d1.d2, e = d2.O1 - d2.O2 and t1 from the predicate; rs, rc = the beam radius at 0 and
+// its change per unit t.  The reference's own t2 = (t1 + d1.O1 - d1.O2) / b is ill-conditioned for
+// nearly perpendicular pairs, so the beam parameter of the lines' closest points is taken as
+// u = e + b t1 instead, which is well-conditioned whenever the lines are not nearly parallel.
+// Where 1 - b^2 > 0.06, the rounding error of t1 and u stays below 39 ulp x scale / 0.06, well
+// under m = 1e-4 * scale, so t1 and u more than m inside their ranges put the exact closest points
+// inside both segments: u is the owner's parameter, and D is the distance of the lines, which the
+// FP32 dist approximates within errb (|ad| carries at most 6 ulp of |O2 - O1|_1 and sin(theta) >
+// 0.2 there; errb is twice that bound).
+__device__ __forceinline__ int piece_takes_fast(V3 O1, V3 d1, float dmin, float dmax, V3 O2, float len, float t_lo,
+                                                float t_hi, float t1, float b, float e, float dist, float rs,
+                                                float rc, float extra)
 {
-    const float c = fabsf(d1.x * d2.x + d1.y * d2.y + d1.z * d2.z);
-    if (c * (1.f - c * c) > 0.04f) {
+    if (1.f - b * b > 0.06f) {
         const float scale = fmaxf(fmaxf(fmaxf(fabsf(O1.x), fabsf(O1.y)), fmaxf(fabsf(O1.z), fabsf(O2.x))),
                                   fmaxf(fmaxf(fabsf(O2.y), fabsf(O2.z)), fmaxf(fmaxf(len, fabsf(dmax)), 1.f)));
         const float m = 1e-4f * scale;
-        if (t1 > dmin + m && t1 < dmax - m && t2 > m && t2 < len - m) {
-            if (t2 < t_lo - m || t2 >= t_hi + m) return 0;
-            if (t2 >= t_lo + m && t2 < t_hi - m) {
+        const float u = e + b * t1;
+        if (t1 > dmin + m && t1 < dmax - m && u > m && u < len - m) {
+            if (u < t_lo - m || u >= t_hi + m) return 0;
+            if (u >= t_lo + m && u < t_hi - m) {
                 const float w1 = fabsf(O2.x - O1.x) + fabsf(O2.y - O1.y) + fabsf(O2.z - O1.z);
                 const float errb = 4e-6f * w1 + 3e-6f * dist + 1e-8f;
-                if (dist + errb + rc_abs * m <= radius + extra) return 1;
+                if (dist + errb + fabsf(rc) * m <= rs + u * rc + extra) return 1;
             }
         }
     }
@@ -264,10 +271,10 @@ __device__ __forceinline__ bool piece_takes_f64(V3 O1, V3 d1, float dmin, float 
 }
 
 __device__ __forceinline__ bool piece_takes(V3 O1, V3 d1, float dmin, float dmax, V3 O2, V3 d2, float len,
-                                            float t_lo, float t_hi, float t1, float t2, float dist, float radius,
-                                            float rs, float rc, float extra)
+                                            float t_lo, float t_hi, float t1, float b, float e, float dist, float rs,
+                                            float rc, float extra)
 {
-    const int f = piece_takes_fast(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi, t1, t2, dist, radius, fabsf(rc), extra);
+    const int f = piece_takes_fast(O1, d1, dmin, dmax, O2, len, t_lo, t_hi, t1, b, e, dist, rs, rc, extra);
     return f >= 0 ? f == 1 : piece_takes_f64(O1, d1, dmin, dmax, O2, d2, len, t_lo, t_hi, rs, rc, extra);
 }
 

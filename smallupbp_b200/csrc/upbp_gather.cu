@@ -130,12 +130,12 @@ __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const Light
                                                        : rsp / cand.pb2d_factor;
     const upbp_mis lvm = load_mis(Lv.mis + lv);
     if (kMixed) {
-        const double wc = camera_weight_fast(s.L, cand, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
-                                             camRevPdfW * rsr / distSq, *s.e, 1.0f / rsr, *s.cs, s.ray_flags,
-                                             P.query_beam_type, P.photon_beam_type);
+        const float wc = camera_weight_fast(s.L, cand, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
+                                            camRevPdfW * rsr / distSq, *s.e, 1.0f / rsr, *s.cs, s.ray_flags,
+                                            P.query_beam_type, P.photon_beam_type);
         const LightSum ls = Lv.sums[lv];
-        const double wl = (double)last * (ls.a + (double)camDirPdfW * ls.c);
-        return (float)(1.0 / (wl + wc)) * unweighted;
+        const float wl = last * ((float)ls.a + camDirPdfW * (float)ls.c);
+        return (1.0f / (wl + wc)) * unweighted;
     }
     const CamView cam{s.cam, s.L, &cand, 1.0f / rsr};
     const float wCamera = camera_path_weight(s.L, last, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
@@ -244,13 +244,13 @@ __device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const Light
     const bool onDeltaLight = (lvm.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (lvm.flags & UPBP_MIS_IS_DELTA);
     const float ntl = onDeltaLight ? 0.f : bsdfDirPdfW * rsrB * fabsf(lvm.cos_theta_out) / distSqB;
     if (kMixed) {
-        const double wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ, *s.e,
-                                             1.0f / rsrQ, *s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
+        const float wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ, *s.e,
+                                            1.0f / rsrQ, *s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
         const LightSum ls = Lv.sums[lvi];
-        double inner = (double)ls.bptb;
-        if (!(s.ray_flags & UPBP_PREVIOUS)) inner += (double)ntl * (ls.d + ls.e * (double)(1.0f / rsrB));
-        const double wl = (double)last * (double)brec.pdf_a_inv * inner;
-        return (float)(1.0 / (wl + wc)) * unweighted;
+        float inner = ls.bptb;
+        if (!(s.ray_flags & UPBP_PREVIOUS)) inner += ntl * ((float)ls.d + (float)ls.e / rsrB);
+        const float wl = last * brec.pdf_a_inv * inner;
+        return (1.0f / (wl + wc)) * unweighted;
     }
     const CamView cam{s.cam, s.L, &cand, 1.0f / rsrQ};
     const float wCamera = camera_path_weight(s.L, last, sinT, rspInvB, ratioB, bsdfRevPdfW * rsrQ / distSqQ,
@@ -267,14 +267,14 @@ __device__ Rgb bb1d_contrib_packed(const GatherConsts& K, const DMedium& m, cons
                                    V3 bo, V3 bdir, float dist, float sinTheta, float t1, float t2, float radius)
 {
     const upbp_params& P = K.P;
-    const int lvbits = __float_as_int(py.lv.w);
-    const int pl = lvbits & 0x3fffffff;
-    const bool finite = (lvbits >> 30) & 1;
+    const unsigned lvbits = (unsigned)__float_as_int(py.lv.w);
+    const int pl = (int)(lvbits & kPayPathMask);
+    const bool finite = (lvbits & kPayFinite) != 0;
     if ((uint32_t)(pl + 1 + s.L) > P.max_path_length || (uint32_t)(pl + 1 + s.L) < P.min_path_length) return rgb(0.f);
 
     if (s.L == 1 && t1 < P.min_dist_to_med) return rgb(0.f);
-    const uint32_t bflags = (uint32_t)__float_as_int(py.thr.w);
-    const uint32_t brsf = (uint32_t)__float_as_int(py.pdf.w);
+    const uint32_t bflags = (lvbits & kPayShortBeam) ? UPBP_SHORT_BEAM : 0u;
+    const uint32_t brsf = (lvbits & kPayOriginInMedium) ? UPBP_ORIGIN_IN_MEDIUM : 0u;
     Rgb att = eval_att(m, t1 - s.dmin);
     const float pfdQ = comp(att, m.min_idx);
     if (s.ray_flags & UPBP_SHORT_BEAM) att = att / pfdQ;
@@ -316,13 +316,13 @@ __device__ Rgb bb1d_contrib_packed(const GatherConsts& K, const DMedium& m, cons
                                           : rspB / (ratioQ * f * sinT);
     else
         last = (bflags & UPBP_SHORT_BEAM) ? rspQ / (ratioB * f * sinT) : rspQ * rspB / (f * sinT);
-    const double wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfPdfW * rsrQ / distSqQ, *s.e,
-                                         1.0f / rsrQ, *s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
+    const float wc = camera_weight_fast(s.L, cand, last, sinT, rspInvB, ratioB, bsdfPdfW * rsrQ / distSqQ, *s.e,
+                                        1.0f / rsrQ, *s.cs, s.ray_flags, P.query_beam_type, P.photon_beam_type);
     const float ntl = bsdfPdfW * rsrB * py.lv.x / distSqB;
-    double inner = (double)py.lv.y;
-    if (!(s.ray_flags & UPBP_PREVIOUS)) inner += (double)ntl * (py.mis.x + py.mis.y * (double)(1.0f / rsrB));
-    const double wl = (double)last * (double)brecPdfAInv * inner;
-    return (float)(1.0 / (wl + wc)) * unweighted;
+    float inner = py.lv.y;
+    if (!(s.ray_flags & UPBP_PREVIOUS)) inner += ntl * (py.thr.w + py.pdf.w / rsrB);
+    const float wl = last * brecPdfAInv * inner;
+    return (1.0f / (wl + wc)) * unweighted;
 }
 
 // ----------------------------------------------------------------- segment loop
@@ -477,16 +477,16 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                     const float4 pa = __ldg(&B.pa[i]);
                     const float4 pb = __ldg(&B.pb[i]);
                     ++tested;
-                    float dist, sinT, t1, t2;
+                    float dist, sinT, t1, t2, bb, ee;
                     if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
-                                        pb.w, &dist, &sinT, &t1, &t2))
+                                        pb.w, &dist, &sinT, &t1, &t2, &bb, &ee))
                         continue;
                     const int beam = __float_as_int(pc.z);
                     const float rs = beam_start_radius(Bs, &Bs.radius[beam]);
                     const float radius = beam_radius_at(Bs, beam, rs, t2);
                     if (radius < dist) continue;  // PhotonBeam.hxx:411-413
                     if (!piece_takes(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pc.x,
-                                     pc.y, t1, t2, dist, radius, rs, Bs.rchange ? __ldg(&Bs.rchange[beam]) : 0.f,
+                                     pc.y, t1, bb, ee, dist, rs, Bs.rchange ? __ldg(&Bs.rchange[beam]) : 0.f,
                                      K.bb1d_extra))
                         continue;
                     ++cnt;
@@ -566,14 +566,14 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
         // Accepted candidates go to the candidate queue.
         auto full = [&](int i) {
             bool hit = false;
-            float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f;
+            float dist = 0.f, sinT = 0.f, t1 = 0.f, t2 = 0.f, bb = 0.f, ee = 0.f;
             if (i >= 0) {
                 // the predicate reads only pa and pb; pc (piece interval, beam, medium) is loaded for
                 // the pieces that pass it
                 const float4 pa = __ldg(&B.pa[i]);
                 const float4 pb = __ldg(&B.pb[i]);
                 if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
-                                   pb.w, &dist, &sinT, &t1, &t2)) {
+                                   pb.w, &dist, &sinT, &t1, &t2, &bb, &ee)) {
                     const float4 pc = __ldg(&B.pc[i]);
                     if (__float_as_int(pc.w) == mid) {  // mMedium == medium (PhotonBeam.hxx:390)
                         // the radius test (PhotonBeam.hxx:411-413), then the reach rule and the owner
@@ -583,9 +583,8 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                         const float radius = beam_radius_at(Bs, beam, rs, t2);
                         hit = !(radius < dist);
                         if (hit) {
-                            const int own = piece_takes_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
-                                                             v3(pb.x, pb.y, pb.z), pa.w, pc.x, pc.y, t1, t2, dist,
-                                                             radius, fabsf(rc), K.bb1d_extra);
+                            const int own = piece_takes_fast(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), pa.w,
+                                                             pc.x, pc.y, t1, bb, ee, dist, rs, rc, K.bb1d_extra);
                             // the FP32 values cannot decide: the FP64 closest points of the segments
                             hit = own >= 0 ? own == 1
                                            : piece_takes_f64(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z),
@@ -951,14 +950,11 @@ __global__ void __launch_bounds__(256) k_gather_pp3d(const __grid_constant__ Gat
                 const float mwfInv = 1.0f / lvm.pp3d_factor;
                 float wCamera, wLight;
                 if (kMixed) {
-                    const double wc = camera_weight_fast(L, eL, mwfInv, sinT, lvm.ray_sample_pdf_inv,
-                                                         lvm.ray_sample_pdfs_ratio, revPdf, eL1,
-                                                         eL1.ray_sample_rev_pdf_inv, csq, P.techniques,
-                                                         P.query_beam_type, P.photon_beam_type);
+                    wCamera = camera_weight_fast(L, eL, mwfInv, sinT, lvm.ray_sample_pdf_inv,
+                                                 lvm.ray_sample_pdfs_ratio, revPdf, eL1, eL1.ray_sample_rev_pdf_inv,
+                                                 csq, P.techniques, P.query_beam_type, P.photon_beam_type);
                     const LightSum ls = Lv.sums[lv];
-                    const double wl = (double)mwfInv * (ls.a + (double)dirPdf * ls.c);
-                    wCamera = (float)wc;
-                    wLight = (float)wl;
+                    wLight = mwfInv * ((float)ls.a + dirPdf * (float)ls.c);
                 } else {
                     wCamera = camera_path_weight(L, mwfInv, sinT, lvm.ray_sample_pdf_inv, lvm.ray_sample_pdfs_ratio,
                                                  revPdf, P.query_beam_type, P.photon_beam_type, P.techniques, camv);
@@ -1296,17 +1292,42 @@ __global__ void k_piece_payload(const float4* __restrict__ pc, int n, const floa
     const int4 info = lv_info[lv];
     const bool onDelta = (m.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (m.flags & UPBP_MIS_IS_DELTA);
     const LightSum ls = sums[lv];
+    const float4 thr = bm_thr[beam], pdf = bm_pdf[beam];
+    const uint32_t bflags = (uint32_t)__float_as_int(thr.w), brsf = (uint32_t)__float_as_int(pdf.w);
     PiecePayload p;
-    p.thr = bm_thr[beam];
-    p.pdf = bm_pdf[beam];
-    const int bits = (info.y & 0x3fffffff) | (((info.z & UPBP_LV_IS_FINITE) ? 1 : 0) << 30);
-    p.lv = make_float4(onDelta ? 0.f : fabsf(m.cos_theta_out), ls.bptb, bm_radius[beam], __int_as_float(bits));
-    p.mis = make_double2(ls.d, ls.e);
+    p.thr = make_float4(thr.x, thr.y, thr.z, (float)ls.d);
+    p.pdf = make_float4(pdf.x, pdf.y, pdf.z, (float)ls.e);
+    const unsigned bits = (unsigned)(info.y & kPayPathMask) | ((info.z & UPBP_LV_IS_FINITE) ? (unsigned)kPayFinite : 0u) |
+                          ((bflags & UPBP_SHORT_BEAM) ? (unsigned)kPayShortBeam : 0u) |
+                          ((brsf & UPBP_ORIGIN_IN_MEDIUM) ? kPayOriginInMedium : 0u);
+    p.lv = make_float4(onDelta ? 0.f : fabsf(m.cos_theta_out), ls.bptb, bm_radius[beam], __int_as_float((int)bits));
     out[i] = p;
 }
 
 // Morton code of the middle of a segment query's span (10 bits per axis in the given box).
-__global__ void k_query_keys(const SegQueriesDev Q, const float* __restrict__ bb, uint32_t* keys, int32_t* iota)
+// Spreads the low 10 bits of v to every third bit (3-D Morton interleave).
+__device__ __forceinline__ uint32_t spread3(uint32_t v)
+{
+    uint32_t r = 0;
+    for (int b = 0; b < 10; ++b) r |= ((v >> b) & 1u) << (3 * b);
+    return r;
+}
+// Spreads the low 14 bits of v to every second bit (2-D Morton interleave).
+__device__ __forceinline__ uint32_t spread2(uint32_t v)
+{
+    uint32_t r = 0;
+    for (int b = 0; b < 14; ++b) r |= ((v >> b) & 1u) << (2 * b);
+    return r;
+}
+
+// Sort key of a segment query (30 bits), by `mode` (upbp_tuning.query_order):
+//  0: 3-D Morton code of the midpoint of the query's span;
+//  1: camera rays (path length 1) first, along a 2-D Morton curve of their pixels (neighbouring
+//     pixels' rays cross nearly the same beam pieces), then the other segments by midpoint;
+//  2: 5-D Morton code of the midpoint (6 bits per axis) and the direction (octahedral map, 6 bits
+//     per axis).
+__global__ void k_query_keys(const SegQueriesDev Q, const float* __restrict__ bb, int mode, int width, uint32_t* keys,
+                             int32_t* iota)
 {
     const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (q >= Q.n) return;
@@ -1315,15 +1336,36 @@ __global__ void k_query_keys(const SegQueriesDev Q, const float* __restrict__ bb
     const float tm = isfinite(t) ? t : (sc > 0 ? Q.seg_dist_min[sb] : 0.f);
     float p[3];
     for (int c = 0; c < 3; ++c) p[c] = Q.origin[3 * q + c] + Q.direction[3 * q + c] * tm;
-    uint32_t code = 0;
     uint32_t ix[3];
     for (int c = 0; c < 3; ++c) {
         const float ext = bb[3 + c] - bb[c];
         const float u = ext > 0.f ? (p[c] - bb[c]) / ext : 0.f;
         ix[c] = (uint32_t)fminf(fmaxf(u * 1024.f, 0.f), 1023.f);
     }
-    for (int b = 9; b >= 0; --b)
-        code = (code << 3) | (((ix[0] >> b) & 1u) << 2) | (((ix[1] >> b) & 1u) << 1) | ((ix[2] >> b) & 1u);
+    uint32_t code = (spread3(ix[0]) << 2) | (spread3(ix[1]) << 1) | spread3(ix[2]);
+    if (mode == 1) {
+        const int px = Q.pixel[q];
+        if (Q.path_length[q] == 1 && px >= 0 && width > 0)
+            code = spread2((uint32_t)(px % width) & 0x3fffu) | (spread2((uint32_t)(px / width) & 0x3fffu) << 1);
+        else
+            code = (1u << 29) | (code >> 1);
+    } else if (mode == 2) {
+        // octahedral map of the direction to [0, 1)^2
+        const float dx = Q.direction[3 * q], dy = Q.direction[3 * q + 1], dz = Q.direction[3 * q + 2];
+        const float n = fabsf(dx) + fabsf(dy) + fabsf(dz);
+        float ox = n > 0.f ? dx / n : 0.f, oy = n > 0.f ? dy / n : 0.f;
+        if (dz < 0.f) {
+            const float tx = (1.f - fabsf(oy)) * (ox >= 0.f ? 1.f : -1.f);
+            oy = (1.f - fabsf(ox)) * (oy >= 0.f ? 1.f : -1.f);
+            ox = tx;
+        }
+        const uint32_t a[5] = {ix[0] >> 4, ix[1] >> 4, ix[2] >> 4,
+                               (uint32_t)fminf(fmaxf((ox * 0.5f + 0.5f) * 64.f, 0.f), 63.f),
+                               (uint32_t)fminf(fmaxf((oy * 0.5f + 0.5f) * 64.f, 0.f), 63.f)};
+        code = 0;
+        for (int b = 5; b >= 0; --b)
+            for (int k = 0; k < 5; ++k) code = (code << 1) | ((a[k] >> b) & 1u);
+    }
     keys[q] = code;
     iota[q] = (int32_t)q;
 }
@@ -1367,9 +1409,10 @@ void launch_piece_payload(const float4* pc, int n, const float4* bm_thr, const f
                                                              sums, out);
 }
 
-void launch_query_keys(const SegQueriesDev& Q, const float* bbox, uint32_t* keys, int32_t* iota, cudaStream_t stream)
+void launch_query_keys(const SegQueriesDev& Q, const float* bbox, int mode, int image_width, uint32_t* keys,
+                       int32_t* iota, cudaStream_t stream)
 {
-    if (Q.n > 0) k_query_keys<<<(int)((Q.n + 255) / 256), 256, 0, stream>>>(Q, bbox, keys, iota);
+    if (Q.n > 0) k_query_keys<<<(int)((Q.n + 255) / 256), 256, 0, stream>>>(Q, bbox, mode, image_width, keys, iota);
 }
 
 void launch_gather_pp3d(const GatherConsts& K, const LightSoA& L, const HashGridDev& G, const PointQueriesDev& Q,

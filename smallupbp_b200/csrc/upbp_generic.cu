@@ -183,20 +183,20 @@ __device__ __forceinline__ void closest_f64(V3d O1, V3d d1, V3d O2, V3d d2, doub
 
 template <class T>
 __device__ RgbT<T> bb1d_contrib(const GatherConsts& K, const MedT<T>& m, const SegCtx<T>& s, const PiecePayload& py,
-                                V3d bo, V3d bdir, double rchange)
+                                const LightSum& ls, V3d bo, V3d bdir, double rchange)
 {
     const upbp_params& P = K.P;
-    const int lvbits = __float_as_int(py.lv.w);
-    const int pl = lvbits & 0x3fffffff;
-    const bool finite = (lvbits >> 30) & 1;
+    const unsigned lvbits = (unsigned)__float_as_int(py.lv.w);
+    const int pl = (int)(lvbits & kPayPathMask);
+    const bool finite = (lvbits & kPayFinite) != 0;
     if ((uint32_t)(pl + 1 + s.L) > P.max_path_length || (uint32_t)(pl + 1 + s.L) < P.min_path_length)
         return rgb_zero<T>();
     double dist, sinTheta, t1, t2;
     closest_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
     if (s.L == 1 && t1 < P.min_dist_to_med) return rgb_zero<T>();
     const double radius = (double)py.lv.z + t2 * rchange;  // mStartRadius + t2 * mRadiusChange
-    const uint32_t bflags = (uint32_t)__float_as_int(py.thr.w);
-    const uint32_t brsf = (uint32_t)__float_as_int(py.pdf.w);
+    const uint32_t bflags = (lvbits & kPayShortBeam) ? UPBP_SHORT_BEAM : 0u;
+    const uint32_t brsf = (lvbits & kPayOriginInMedium) ? UPBP_ORIGIN_IN_MEDIUM : 0u;
     RgbT<T> att = eval_att(m, t1 - s.dmin);
     const T pfdQ = comp(att, m.min_idx);
     if (s.ray_flags & UPBP_SHORT_BEAM) att = att / pfdQ;
@@ -242,8 +242,8 @@ __device__ RgbT<T> bb1d_contrib(const GatherConsts& K, const MedT<T>& m, const S
     const T wc = camera_weight(P, s.L, cand, last, sinT, rspInvB, ratio, pdfW * rsrQ / distSqQ, *s.e, 1.0 / rsrQ,
                                *s.cs, s.ray_flags);
     const T ntl = pdfW * rsrB * ((double)py.lv.x / distSqB);
-    T inner = cst<T>((double)py.lv.y);
-    if (!(s.ray_flags & UPBP_PREVIOUS)) inner = inner + ntl * (py.mis.y / rsrB + py.mis.x);
+    T inner = cst<T>((double)ls.bptb);
+    if (!(s.ray_flags & UPBP_PREVIOUS)) inner = inner + ntl * (ls.e / rsrB + ls.d);
     const T wl = last * brecPdfAInv * inner;
     return unweighted / (wl + wc);
 }
@@ -437,7 +437,8 @@ __global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ Gather
 template <class T>
 __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ GatherConsts K,
                                                   const __grid_constant__ GenConsts G, const BeamBVH B,
-                                                  const BeamSoA Bs, const SegQueriesDev Q,
+                                                  const BeamSoA Bs, const LightSum* __restrict__ lsums,
+                                                  const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
                                                   const GenOut O, unsigned int* __restrict__ work,
                                                   int* __restrict__ status, const int32_t* __restrict__ order)
@@ -476,8 +477,10 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                     const float4 pa = __ldg(&B.pa[i]);
                     const float4 pb = __ldg(&B.pb[i]);
                     const PiecePayload py = B.pay[i];
-                    const double rchg = Bs.rchange ? (double)__ldg(&Bs.rchange[__float_as_int(__ldg(&B.pc[i]).z)]) : 0.0;
-                    part = part + bb1d_contrib<T>(K, m, s, py, v3d(pa.x, pa.y, pa.z), v3d(pb.x, pb.y, pb.z), rchg);
+                    const int beam = __float_as_int(__ldg(&B.pc[i]).z);
+                    const double rchg = Bs.rchange ? (double)__ldg(&Bs.rchange[beam]) : 0.0;
+                    const LightSum ls = lsums[__ldg(&Bs.link[beam]).x];
+                    part = part + bb1d_contrib<T>(K, m, s, py, ls, v3d(pa.x, pa.y, pa.z), v3d(pb.x, pb.y, pb.z), rchg);
                 };
                 // the rest of the predicate for one piece per lane (i < 0: none)
                 auto full = [&](int i) {
@@ -487,16 +490,16 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                         if (__float_as_int(pc.w) == mid) {
                             const float4 pa = __ldg(&B.pa[i]);
                             const float4 pb = __ldg(&B.pb[i]);
-                            float dist, sinT, t1, t2;
+                            float dist, sinT, t1, t2, bb, ee;
                             if (test_beam_beam(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                               0.f, pa.w, pb.w, &dist, &sinT, &t1, &t2)) {
+                                               0.f, pa.w, pb.w, &dist, &sinT, &t1, &t2, &bb, &ee)) {
                                 const int beam = __float_as_int(pc.z);
                                 const float rs = beam_start_radius(Bs, &B.pay[i].lv.z);
                                 const float radius = beam_radius_at(Bs, beam, rs, t2);
                                 // the radius test (PhotonBeam.hxx:411-413), the reach rule and the owner
                                 if (!(radius < dist) &&
                                     piece_takes(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                                pa.w, pc.x, pc.y, t1, t2, dist, radius, rs,
+                                                pa.w, pc.x, pc.y, t1, bb, ee, dist, rs,
                                                 Bs.rchange ? __ldg(&Bs.rchange[beam]) : 0.f, K.bb1d_extra)) {
                                     hit = true;
                                     ++cnt;
@@ -762,8 +765,8 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
         k_gen_pb2d<T><<<A.pb2d_grid, 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam, A.cs_seg, A.out_pb2d,
                                                   A.work + 1, A.status, A.order);
     if (A.sq.n > 0 && A.beams.n > 0)
-        k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.sq, A.cam, A.cs_seg, A.out_bb1d, A.work,
-                                                  A.status, A.order);
+        k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.L.sums, A.sq, A.cam, A.cs_seg,
+                                                  A.out_bb1d, A.work, A.status, A.order);
 }
 
 void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream)

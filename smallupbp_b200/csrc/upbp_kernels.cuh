@@ -45,12 +45,19 @@ struct PhotonBVH {
 
 // Payload of the beam a piece belongs to, packed per piece (mixed mode): everything an accepted
 // candidate reads besides the piece geometry, so it comes from the lines the warp just tested.
+// The light vertex's partial sums d, e are the FP64 LightSum values rounded to FP32 for the
+// per-candidate combination (the FP64 mode reads LightSum itself).
 struct __align__(16) PiecePayload {
-    float4 thr;   // beam throughput at origin rgb, beam flags (int bits)
-    float4 pdf;   // beam ray_sample_pdf, ray_sample_rev_pdf, last_pdf_w_inv, ray_sampling_flags (int bits)
-    float4 lv;    // light vertex |cos_theta_out| (0 on a delta light), bptb, radius, path_length | finite << 30
-    double2 mis;  // light vertex FP64 partial sums d, e (LightSum)
+    float4 thr;   // beam throughput at origin rgb, light vertex partial sum d
+    float4 pdf;   // beam ray_sample_pdf, ray_sample_rev_pdf, last_pdf_w_inv, light vertex partial sum e
+    float4 lv;    // light vertex |cos_theta_out| (0 on a delta light), bptb, radius, bits (payload_* below)
 };
+// bits of PiecePayload::lv.w: the light vertex's path length, whether it is finite, and the two beam
+// flags the contribution reads
+constexpr int kPayPathMask = 0x1fffffff;
+constexpr int kPayFinite = 1 << 29;
+constexpr int kPayShortBeam = 1 << 30;
+constexpr unsigned kPayOriginInMedium = 1u << 31;
 
 // Beam pieces (BB1D) in leaf order.  Piece = beam sub-interval [t_lo, t_hi).
 struct BeamBVH {
@@ -209,7 +216,8 @@ void launch_gather_bb1d(const GatherConsts& K, const LightSoA& L, const BeamBVH&
 void launch_piece_payload(const float4* pc, int n, const float4* bm_thr, const float4* bm_pdf, const int2* bm_link,
                           const float* bm_radius, const int4* lv_info, const upbp_mis* lv_mis,
                           const struct LightSum* sums, PiecePayload* out, cudaStream_t stream);
-void launch_query_keys(const SegQueriesDev& Q, const float* bbox, uint32_t* keys, int32_t* iota, cudaStream_t stream);
+void launch_query_keys(const SegQueriesDev& Q, const float* bbox, int mode, int image_width, uint32_t* keys,
+                       int32_t* iota, cudaStream_t stream);
 // keys that put the queries with more than `factor` x the mean PB2D candidate count first, each
 // group in the given Morton order; *sum must be zero on entry
 void launch_heavy_keys(const uint32_t* cnt, int64_t n, unsigned long long* sum, unsigned factor,

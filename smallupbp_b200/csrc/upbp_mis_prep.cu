@@ -73,7 +73,7 @@ __global__ void k_cam_sums(const upbp_mis* __restrict__ cam, const int64_t* __re
         }
         prod *= (double)m.rev_pdf_a;
         double o, b;
-        cam_merge_terms(m, !spec, m.sin_theta, m.ray_sample_rev_pdf_inv, m.ray_sample_rev_pdfs_ratio, tech, qbt, pbt, o,
+        cam_merge_terms<double>(m, !spec, m.sin_theta, m.ray_sample_rev_pdf_inv, m.ray_sample_rev_pdfs_ratio, tech, qbt, pbt, o,
                         b);
         s_other += prod * o;
         s_bb1d += prod * b;
@@ -84,6 +84,8 @@ __global__ void k_cam_sums(const upbp_mis* __restrict__ cam, const int64_t* __re
     CamSum c;
     c.s_other = s_other;
     c.s_bb1d = s_bb1d;
+    c.f_other = (float)s_other;
+    c.f_bb1d = (float)s_bb1d;
     c.flags = flags;
     c.pad = 0;
     out[q] = c;

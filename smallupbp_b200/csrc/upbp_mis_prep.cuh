@@ -38,6 +38,7 @@ struct __align__(8) LightSum {
 
 struct __align__(8) CamSum {
     double s_other, s_bb1d;
+    float f_other, f_bb1d;  // the same sums rounded to FP32, for the per-candidate combination
     uint32_t flags;  // bit0: reset inside the suffix, bit1: entry L-2 (or L-1 when L == 2) is specular
     uint32_t pad;
 };
@@ -65,51 +66,56 @@ __device__ __forceinline__ void light_merge_terms(const upbp_mis& m, uint32_t te
     }
 }
 
-// Camera-walk merging terms of one entry (PathWeight.hxx:88-126) with explicit ray reverse pdfs.
+// Camera-walk merging terms of one entry (PathWeight.hxx:88-126) with explicit ray reverse pdfs,
+// accumulated in R (double for the FP64 partial sums, float for the per-candidate combination).
+template <class R>
 __device__ __forceinline__ void cam_merge_terms(const upbp_mis& m, bool usable, float sinT, float rayRev,
                                                 float rayRevRatio, uint32_t tech, uint32_t qbt, uint32_t pbt,
-                                                double& other, double& bb1d)
+                                                R& other, R& bb1d)
 {
-    other = 0.0;
-    bb1d = 0.0;
-    if ((tech & UPBP_SURF) && usable) other += (double)m.surf_factor;
-    if (tech & UPBP_PP3D) other += (double)m.pp3d_factor;
+    other = 0;
+    bb1d = 0;
+    if ((tech & UPBP_SURF) && usable) other += (R)m.surf_factor;
+    if (tech & UPBP_PP3D) other += (R)m.pp3d_factor;
     if (tech & UPBP_PB2D)
-        other += (double)m.pb2d_factor * ((qbt & UPBP_LONG_BEAM) ? m.ray_sample_pdf_inv : m.ray_sample_pdfs_ratio);
+        other += (R)m.pb2d_factor * (R)((qbt & UPBP_LONG_BEAM) ? m.ray_sample_pdf_inv : m.ray_sample_pdfs_ratio);
     if ((tech & UPBP_BB1D) && (m.flags & UPBP_MIS_IN_MEDIUM_WITH_BEAMS)) {
-        const double s = (tech & UPBP_NO_SINE_IN_WEIGHTS) ? 1.0 : (double)sinT;
-        const double a = (qbt & UPBP_LONG_BEAM) ? (double)m.ray_sample_pdf_inv : (double)m.ray_sample_pdfs_ratio;
-        const double b = (pbt & UPBP_LONG_BEAM) ? (double)rayRev : (double)rayRevRatio;
-        bb1d += (double)m.bb1d_factor * m.bb1d_beam_selection_pdf * a * s * b;
+        const R s = (tech & UPBP_NO_SINE_IN_WEIGHTS) ? (R)1 : (R)sinT;
+        const R a = (qbt & UPBP_LONG_BEAM) ? (R)m.ray_sample_pdf_inv : (R)m.ray_sample_pdfs_ratio;
+        const R b = (pbt & UPBP_LONG_BEAM) ? (R)rayRev : (R)rayRevRatio;
+        bb1d += (R)m.bb1d_factor * (R)m.bb1d_beam_selection_pdf * a * s * b;
     }
 }
 
 // Camera weight from the candidate's index-0 record, entry L-1 (index 1, with the reverse
-// ray pdf the estimator writes) and the precomputed suffix.
-__device__ __forceinline__ double camera_weight_fast(int L, const upbp_mis& cand, float lastRev, float lastSin,
-                                                     float lastRayRev, float lastRayRevRatio, float ntl,
-                                                     const upbp_mis& e, float e_ray_rev, const CamSum& cs,
-                                                     uint32_t tech, uint32_t qbt, uint32_t pbt)
+// ray pdf the estimator writes) and the precomputed FP64 suffix.  The candidate's terms are
+// combined in FP32: every term is a non-negative product of pdfs, so the sum has no cancellation
+// and FP32 carries the weight to a few ulp; the recursive sums over the rest of the path are the
+// FP64 ones, rounded once (CamSum::f_other, f_bb1d).
+__device__ __forceinline__ float camera_weight_fast(int L, const upbp_mis& cand, float lastRev, float lastSin,
+                                                    float lastRayRev, float lastRayRevRatio, float ntl,
+                                                    const upbp_mis& e, float e_ray_rev, const CamSum& cs,
+                                                    uint32_t tech, uint32_t qbt, uint32_t pbt)
 {
-    double prod = (double)lastRev;
-    double o0, b0;
-    cam_merge_terms(cand, true, lastSin, lastRayRev, lastRayRevRatio, tech, qbt, pbt, o0, b0);
-    double w_o = prod * o0, w_b = prod * b0;
-    prod *= (double)cand.pdf_a_inv;
+    float prod = lastRev;
+    float o0, b0;
+    cam_merge_terms<float>(cand, true, lastSin, lastRayRev, lastRayRevRatio, tech, qbt, pbt, o0, b0);
+    float w_o = prod * o0, w_b = prod * b0;
+    prod *= cand.pdf_a_inv;
     const bool next0_spec = L >= 2 ? (e.flags & UPBP_MIS_IS_SPECULAR) != 0 : (cand.flags & UPBP_MIS_IS_SPECULAR) != 0;
     if ((tech & UPBP_BPT) && !next0_spec) w_o += prod;
     if (L >= 2) {
         const bool espec = (e.flags & UPBP_MIS_IS_SPECULAR) != 0;
-        if ((tech & UPBP_BB1D_PREVIOUS) && !espec) w_b = 0.0;
-        prod *= (double)(e.rev_pdf_a * ntl);
-        double o1, b1;
-        cam_merge_terms(e, !espec, e.sin_theta, e_ray_rev, e.ray_sample_rev_pdfs_ratio, tech, qbt, pbt, o1, b1);
+        if ((tech & UPBP_BB1D_PREVIOUS) && !espec) w_b = 0.f;
+        prod *= e.rev_pdf_a * ntl;
+        float o1, b1;
+        cam_merge_terms<float>(e, !espec, e.sin_theta, e_ray_rev, e.ray_sample_rev_pdfs_ratio, tech, qbt, pbt, o1, b1);
         w_o += prod * o1;
         w_b += prod * b1;
-        prod *= (double)e.pdf_a_inv;
+        prod *= e.pdf_a_inv;
         if ((tech & UPBP_BPT) && !espec && !(cs.flags & 2u)) w_o += prod;
-        w_o += prod * cs.s_other;
-        w_b = (cs.flags & 1u) ? prod * cs.s_bb1d : w_b + prod * cs.s_bb1d;
+        w_o += prod * cs.f_other;
+        w_b = (cs.flags & 1u) ? prod * cs.f_bb1d : w_b + prod * cs.f_bb1d;
     }
     return w_o + w_b;
 }

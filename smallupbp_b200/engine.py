@@ -158,7 +158,8 @@ class EstimatorStage:
         self._ck(self._l.upbp_set_mode(self._ctx, mode))
 
     def set_tuning(self, **kw):
-        """Update any of pb2d_leaf, bb1d_leaf, block_threads, beam_piece_radii, bb1d_kernel, pb2d_kernel."""
+        """Update any of pb2d_leaf, bb1d_leaf, block_threads, beam_piece_radii, bb1d_kernel, pb2d_kernel,
+        query_order."""
         t = self.get_tuning()
         for k, v in kw.items():
             if not hasattr(t, k):
