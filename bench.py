@@ -829,9 +829,9 @@ def run_adjoint(args, cfg, rank, world, local_rank):
     return {
         "metric": METRIC + " (forward + adjoint)", "value": units * args.steps / (total_ms / 1000.0), "unit": "queries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (adjoint f64 duals)",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (adjoint: f32 tangents, f64 accumulation)",
         "data": "synthetic: seeded UPBP light/camera passes (Philox) in the %s scene; no dataset" % cfg.name,
-        "config": dict(workload_desc(cfg), mode="mixed forward + dual-number adjoint",
+        "config": dict(workload_desc(cfg), mode="mixed forward + dual-number adjoint (FP32 tangents)",
                        loss="sum (I - I_target)^2, target sigma_s=0.7 sigma_a=0.05 g=0.5, at sigma_s=0.5 "
                             "sigma_a=0.1 g=0.3"),
         "adjoint": {"forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),

@@ -65,6 +65,20 @@ extern "C" {
 #define UPBP_BP2D 65536u /* extension, not a reference technique (above every reference flag; 2048 is
                          * SPECULAR_ONLY): B-P2D, photon beams x camera medium points with a 2-D
                          * kernel, as a standalone estimator with MIS weight 1 */
+/* Estimators without MIS, as VolLightTracer's pure algorithms run them (`-a pb2d`, `-a bb1d`,
+ * Renderers/VolLightTracer.hxx:296-412): EmbreeBre::build over VltLightVertex records
+ * (Bre.cxx:526-614) with evalBre and no AdditionalRayDataForMis, whose photons take the callback
+ * breIntersectFuncHomogeneous (Bre.cxx:239-291), and evalBeamBeamEstimate(..., BB1D, 0, NULL),
+ * which takes PhotonBeam::accumulate (Beams/PhotonBeam.hxx:315-367).  Every candidate then adds
+ * its unweighted contribution: no path-length or minimum-distance rejects and no MIS weight.  The
+ * caller sets norm_pb2d = 1 / mLightSubPathCount, norm_bb1d = 1 / mBB1DUsedLightSubPathCount and
+ * the query throughput to 1 (VolLightTracer.hxx:378, 384).  The MIS inputs may then be NULL:
+ * upbp_light_vertices.mis, path_idx, cont_prob and path_ends (n_paths 0); upbp_beams.ray_sample_pdf,
+ * ray_sample_rev_pdf, ray_sampling_flags, last_pdf_w_inv and light_vertex; upbp_segment_queries
+ * .last_pdf_w_inv and cam_mis_begin; and no camera MIS records.  The reference has no pure PP3D
+ * algorithm: UPBP_PP3D together with this bit is rejected.  (Not a reference flag: above every
+ * reference flag and UPBP_BP2D.) */
+#define UPBP_NO_MIS 131072u
 #define UPBP_ORIGIN_IN_MEDIUM 1u /* AbstractMedium::kOriginInMedium */
 #define UPBP_END_IN_MEDIUM 2u    /* AbstractMedium::kEndInMedium */
 

@@ -77,8 +77,10 @@ public:
     void build() { check(upbp_build(ctx_)); }
 
     /* One evalBre/evalBeamBeamEstimate call pair at camera path length L.  cam_mis points at
-     * mCameraVerticesMisData[0..L-1] as it is at the call.  `flags` = UPBP_Q_* (which estimators,
-     * origin in medium, lite segments).  Returns the ticket of the call. */
+     * mCameraVerticesMisData[0..L-1] as it is at the call, or is NULL for the calls without MIS
+     * data of VolLightTracer's pure PB2D / BB1D (UPBP_NO_MIS in the params' techniques, where
+     * last_pdf_w_inv is not read either).  `flags` = UPBP_Q_* (which estimators, origin in medium,
+     * lite segments).  Returns the ticket of the call. */
     int64_t record_segment(const float origin[3], const float direction[3], const std::vector<Segment>& segs,
                            uint32_t flags, int path_length, float last_pdf_w_inv, const float throughput[3],
                            int32_t pixel, const upbp_mis* cam_mis)
@@ -104,7 +106,7 @@ public:
         sq_lpw_.push_back(last_pdf_w_inv);
         sq_pixel_.push_back(pixel);
         sq_cam_begin_.push_back((int64_t)cam_.size());
-        cam_.insert(cam_.end(), cam_mis, cam_mis + path_length);
+        if (cam_mis) cam_.insert(cam_.end(), cam_mis, cam_mis + path_length);
         return t;
     }
 

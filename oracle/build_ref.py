@@ -15,15 +15,12 @@ fixes (backslash include paths, ``__declspec(align)``, missing ``typename``,
 MSVC-only casts).  They are applied to a COPY under ``oracle/_ref/src`` (which
 is git-ignored and never committed); the reference tree is only read.
 
-Embree 2.0's BVH is the one library piece that is NOT built: the harness
-provides the nine ``rtc*`` virtual-geometry entry points that ``Bre.cxx``
-calls (``rtcNewVirtualGeometry`` ... ``rtcDeleteIntersector1``) as an
-exhaustive AABB enumerator.  The BRE callback tests every photon exactly, and
-a photon that passes the BRE test always overlaps the ray in its AABB, so the
-candidate set and each candidate's contribution are unchanged; only the
-summation order differs from Embree's traversal order.
+Embree 2.0 is built too: its 40 core, BVH and ``sys`` sources (``EMBREE_SOURCES``)
+are compiled from the same patched copy and linked in, so ``EmbreeBre`` runs on
+Embree's own BVH and callback interface, exactly as the reference renderer does.
 
-Usage: python oracle/build_ref.py [--reference /root/reference]
+Usage: python oracle/build_ref.py [--reference DIR]
+(DIR defaults to $UPBP_REFERENCE_DIR, else /root/reference.)
 Exit status 0 and prints the built path; exits 2 (with a message) when the
 reference tree is absent (e.g. on a machine that only runs prebuilt files).
 """
@@ -51,6 +48,11 @@ CASE_FIXES = {
     "Debugimages.hxx": "DebugImages.hxx",
     "Beamdensity.hxx": "BeamDensity.hxx",
 }
+
+
+def reference_dir() -> str:
+    """Where the reference checkout lives: $UPBP_REFERENCE_DIR, else the default checkout path."""
+    return os.environ.get("UPBP_REFERENCE_DIR", "/root/reference")
 
 
 def copy_tree(ref: str) -> None:
@@ -204,7 +206,7 @@ def compile_lib() -> str:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=reference_dir())
     ap.add_argument("--no-copy", action="store_true", help="reuse the patched copy")
     args = ap.parse_args()
     if not os.path.isdir(os.path.join(args.reference, "SmallUPBP/src")):

@@ -43,3 +43,13 @@ void ref_bre_radii(const EmbreeBre& bre, const UPBPLightVertex* base, int64_t n,
         r2[ph.lightVertex - base] = ph.radiusSqr;
     }
 }
+
+/* Links the photons of a VltLightVertex build (Bre.cxx:526-614, which stores position, radius,
+ * direction and flux but no light vertex) to the light vertices they were made from: the build
+ * takes the in-medium vertices in order.  Only the candidate enumeration and the radii read it. */
+void ref_bre_link_photons(EmbreeBre& bre, const UPBPLightVertex* base, int64_t n)
+{
+    int k = 0;
+    for (int64_t i = 0; i < n && k < bre.numEmbreePhotons; ++i)
+        if (base[i].mInMedium) bre.embreePhotons[k++].lightVertex = base + i;
+}

@@ -12,6 +12,12 @@
  *   - the brute-force BB1D evaluator (PhBrute.hxx) is compiled in its own TU.
  * The camera MIS array mCameraVerticesMisData is loaded from the recorded
  * snapshot before every call, which is its state at the call in the renderer.
+ *
+ * With UPBP_NO_MIS in the techniques the harness runs the estimators as
+ * VolLightTracer's pure algorithms do (Renderers/VolLightTracer.hxx:296-412):
+ * EmbreeBre::build over VltLightVertex records (photons with the callback
+ * breIntersectFuncHomogeneous), evalBre and evalBeamBeamEstimate with no
+ * AdditionalRayDataForMis (PhotonBeam::accumulate), beams without light vertices.
  */
 #include <vector>
 #include <list>
@@ -41,6 +47,7 @@
 
 void* ref_brute_create(const Scene& scene, PhotonBeamsArray& beams, float radius, int knn);
 void ref_bre_radii(const EmbreeBre& bre, const UPBPLightVertex* base, int64_t n, float* r2);
+void ref_bre_link_photons(EmbreeBre& bre, const UPBPLightVertex* base, int64_t n);
 Rgb ref_brute_eval(void* h, BeamType bt, const Ray& ray, const VolumeSegments& segs, uint tech, uint rsf,
                    embree::AdditionalRayDataForMis* data);
 Rgb ref_brute_eval_lite(void* h, BeamType bt, const Ray& ray, const LiteVolumeSegments& segs, uint tech, uint rsf,
@@ -53,6 +60,7 @@ struct World {
     Scene scene;
     UPBP* upbp = nullptr;
     void* brute = nullptr;
+    std::vector<VltLightVertex> vlt;  // VolLightTracer's light vertices (UPBP_NO_MIS)
     ~World()
     {
         if (upbp) {
@@ -111,8 +119,9 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
                                                        m.continuation_prob, m.mean_cosine));
     }
     const float nl = (float)P.hash_cells;
+    const bool nomis = (P.techniques & UPBP_NO_MIS) != 0;
     w.scene.mCamera.mResolution = Vec2f(1.f, 1.f);
-    w.upbp = new UPBP(w.scene, UPBP::kCustom, P.techniques,
+    w.upbp = new UPBP(w.scene, UPBP::kCustom, P.techniques & ~UPBP_NO_MIS,
                       P.radius_pp3d, 1.f, P.radius_pp3d, 1.f, P.radius_pb2d, 1.f,
                       P.pb2d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.pb2d_knn,
                       (BeamType)P.query_beam_type, P.radius_bb1d, 1.f,
@@ -143,7 +152,7 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
         UPBPLightVertex& v = U.mLightVertices[(size_t)i];
         v.mHitpoint = P3(lv->position + 3 * i);
         v.mThroughput = C3(lv->throughput + 3 * i);
-        v.mPathIdx = lv->path_idx[i];
+        v.mPathIdx = lv->path_idx ? lv->path_idx[i] : 0;
         v.mPathLength = (uint)lv->path_length[i];
         v.mInMedium = (lv->flags[i] & UPBP_LV_IN_MEDIUM) != 0;
         v.mConnectable = (lv->flags[i] & UPBP_LV_CONNECTABLE) != 0;
@@ -155,11 +164,27 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
         } else {
             ++on_surface;
         }
-        v.mMisData = to_mis(lv->mis[i]);
+        if (lv->mis) v.mMisData = to_mis(lv->mis[i]);
     }
     U.mLightVerticesInMediumCount = in_medium;
     U.mLightVerticesOnSurfaceCount = on_surface;
-    U.mPathEnds.assign(lv->path_ends, lv->path_ends + lv->n_paths);
+    if (lv->path_ends) U.mPathEnds.assign(lv->path_ends, lv->path_ends + lv->n_paths);
+    if (nomis) {
+        // VolLightTracer's records (VolLightTracer.hxx:241-250): hitpoint, throughput, path
+        // length, in-medium flag and the BSDF, no MIS data
+        w.vlt.resize((size_t)lv->n);
+        for (int64_t i = 0; i < lv->n; ++i) {
+            VltLightVertex& v = w.vlt[(size_t)i];
+            const UPBPLightVertex& u = U.mLightVertices[(size_t)i];
+            v.mHitpoint = u.mHitpoint;
+            v.mThroughput = u.mThroughput;
+            v.mPrevThroughput = u.mThroughput;
+            v.mIncEdgeLength = 0.f;
+            v.mPathLength = u.mPathLength;
+            v.mIsInMedium = u.mInMedium ? 1 : 0;
+            v.mBSDF = u.mBSDF;
+        }
+    }
 
     // photon beams (UPBP::AddBeams record layout, UPBP.hxx:1783-1870)
     U.mPhotonBeamsArray.clear();
@@ -171,13 +196,14 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
             b.mRay = Ray(P3(bm->origin + 3 * i), D3(bm->direction + 3 * i));
             b.mLength = bm->length[i];
             b.mFlags = bm->flags[i];
-            b.mRaySamplePdf = bm->ray_sample_pdf[i];
-            b.mRaySampleRevPdf = bm->ray_sample_rev_pdf[i];
-            b.mRaySamplingFlags = bm->ray_sampling_flags[i];
-            b.mLastPdfWInv = bm->last_pdf_w_inv[i];
+            b.mRaySamplePdf = bm->ray_sample_pdf ? bm->ray_sample_pdf[i] : 0.f;
+            b.mRaySampleRevPdf = bm->ray_sample_rev_pdf ? bm->ray_sample_rev_pdf[i] : 0.f;
+            b.mRaySamplingFlags = bm->ray_sampling_flags ? bm->ray_sampling_flags[i] : 0u;
+            b.mLastPdfWInv = bm->last_pdf_w_inv ? bm->last_pdf_w_inv[i] : 0.f;
             b.mIsFirstSegment = false;
             b.mMedium = w.scene.mMedia[bm->medium_id[i]];
-            b.mLightVertex = &U.mLightVertices[(size_t)bm->light_vertex[i]];
+            // VolLightTracer::AddBeams stores no light vertex (VolLightTracer.hxx:586-640)
+            b.mLightVertex = (nomis || !bm->light_vertex) ? NULL : &U.mLightVertices[(size_t)bm->light_vertex[i]];
         }
     }
 
@@ -186,9 +212,19 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
         U.mPP3DHashGrid.Reserve(P.hash_cells);
         U.mPP3DHashGrid.Build(U.mLightVertices, P.radius_pp3d, PP3D);
     }
-    if ((what & (REF_PB2D | REF_CANDIDATES)) && U.mMergeWithLightVerticesPB2D && !U.mLightVertices.empty())
-        U.mPB2DEmbreeBre.build(&U.mLightVertices[0], (int)U.mLightVertices.size(),
-                               P.pb2d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.radius_pb2d, P.pb2d_knn, false);
+    if ((what & (REF_PB2D | REF_CANDIDATES)) && U.mMergeWithLightVerticesPB2D && !U.mLightVertices.empty()) {
+        if (nomis) {
+            // the VolLightTracer overload (Bre.cxx:526-614); the photons' light-vertex links, which
+            // that build leaves unset and its callback never reads, are filled for the candidate
+            // enumeration and the radii
+            U.mPB2DEmbreeBre.build(&w.vlt[0], (int)w.vlt.size(), P.pb2d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS,
+                                   P.radius_pb2d, P.pb2d_knn, false);
+            ref_bre_link_photons(U.mPB2DEmbreeBre, &U.mLightVertices[0], (int64_t)U.mLightVertices.size());
+        } else {
+            U.mPB2DEmbreeBre.build(&U.mLightVertices[0], (int)U.mLightVertices.size(),
+                                   P.pb2d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.radius_pb2d, P.pb2d_knn, false);
+        }
+    }
     if ((what & REF_BB1D_GRID) && U.mMergeWithLightVerticesBB1D && !U.mPhotonBeamsArray.empty())
         U.mBB1DPhotonBeams.build(U.mPhotonBeamsArray, P.bb1d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.radius_bb1d,
                                  P.bb1d_knn, false);
@@ -398,8 +434,19 @@ extern "C" int ref_eval(void* h, int64_t offset, int64_t stride, ref_outputs* ou
             const Rgb thr = C3(sq->throughput + 3 * q);
             const BeamType qbt = (BeamType)P.query_beam_type;
             // PB2D, UPBP.hxx:775-785 / 879-893
+            const bool nomis = (P.techniques & UPBP_NO_MIS) != 0;
             if ((qf & UPBP_Q_PB2D) && U.mMergeWithLightVerticesPB2D && !U.mLightVertices.empty()) {
-                if (what & REF_PB2D) {
+                if ((what & REF_PB2D) && nomis) {
+                    // VolLightTracer.hxx:378: evalBre(mPB2DBeamType, ray, mVolumeSegments)
+                    const Rgb c = lite ? U.mPB2DEmbreeBre.evalBre(qbt, ray, lsegs, PB2D, 0, NULL)
+                                       : U.mPB2DEmbreeBre.evalBre(qbt, ray, segs, PB2D, 0, NULL);
+                    if (out->pb2d_rgb) for (int k = 0; k < 3; ++k) out->pb2d_rgb[3 * q + k] = c[k];
+                    const int px = sq->pixel[q];
+                    if (img && px >= 0) {
+                        const Rgb add = thr * U.mPB2DNormalization * c;
+                        for (int k = 0; k < 3; ++k) img[3 * px + k] += add[k];
+                    }
+                } else if (what & REF_PB2D) {
                     load_camera(U, cam_mis, sq->cam_mis_begin[q], L);
                     embree::AdditionalRayDataForMis data(
                         &U.mLightVertices, &U.mPathEnds, &U.mCameraVerticesMisData, L, U.mMinPathLength,
@@ -439,20 +486,31 @@ extern "C" int ref_eval(void* h, int64_t offset, int64_t stride, ref_outputs* ou
                 for (int variant = 0; variant < 2; ++variant) {
                     if (variant == 0 && !(what & REF_BB1D_GRID)) continue;
                     if (variant == 1 && !(what & REF_BB1D_BRUTE)) continue;
-                    load_camera(U, cam_mis, sq->cam_mis_begin[q], L);
-                    embree::AdditionalRayDataForMis data(
-                        &U.mLightVertices, &U.mPathEnds, &U.mCameraVerticesMisData, L, U.mMinPathLength,
-                        U.mMaxPathLength, U.mQueryBeamType, U.mPhotonBeamType, sq->last_pdf_w_inv[q],
-                        U.mSurfMisWeightFactor, U.mPP3DMisWeightFactor, U.mPB2DMisWeightFactor, U.mBB1DMisWeightFactor,
-                        &U.mBB1DPhotonBeams, U.mBB1DMinMFP, U.mBB1DUsedLightSubPathCount, U.mMinDistToMed, 0.0f, 0.0f,
-                        0, &U.mDebugImages);
                     Rgb c;
-                    if (variant == 0)
-                        c = lite ? U.mBB1DPhotonBeams.evalBeamBeamEstimate(qbt, ray, lsegs, tech, rsf, &data)
-                                 : U.mBB1DPhotonBeams.evalBeamBeamEstimate(qbt, ray, segs, tech, rsf, &data);
-                    else
-                        c = lite ? ref_brute_eval_lite(w.brute, qbt, ray, lsegs, tech, rsf, &data)
-                                 : ref_brute_eval(w.brute, qbt, ray, segs, tech, rsf, &data);
+                    if (nomis) {
+                        // VolLightTracer.hxx:384: evalBeamBeamEstimate(..., BB1D, 0, NULL, &gridStats)
+                        GridStats gs;
+                        if (variant == 0)
+                            c = lite ? U.mBB1DPhotonBeams.evalBeamBeamEstimate(qbt, ray, lsegs, BB1D, 0, NULL, &gs)
+                                     : U.mBB1DPhotonBeams.evalBeamBeamEstimate(qbt, ray, segs, BB1D, 0, NULL, &gs);
+                        else
+                            c = lite ? ref_brute_eval_lite(w.brute, qbt, ray, lsegs, BB1D, 0, NULL)
+                                     : ref_brute_eval(w.brute, qbt, ray, segs, BB1D, 0, NULL);
+                    } else {
+                        load_camera(U, cam_mis, sq->cam_mis_begin[q], L);
+                        embree::AdditionalRayDataForMis data(
+                            &U.mLightVertices, &U.mPathEnds, &U.mCameraVerticesMisData, L, U.mMinPathLength,
+                            U.mMaxPathLength, U.mQueryBeamType, U.mPhotonBeamType, sq->last_pdf_w_inv[q],
+                            U.mSurfMisWeightFactor, U.mPP3DMisWeightFactor, U.mPB2DMisWeightFactor,
+                            U.mBB1DMisWeightFactor, &U.mBB1DPhotonBeams, U.mBB1DMinMFP, U.mBB1DUsedLightSubPathCount,
+                            U.mMinDistToMed, 0.0f, 0.0f, 0, &U.mDebugImages);
+                        if (variant == 0)
+                            c = lite ? U.mBB1DPhotonBeams.evalBeamBeamEstimate(qbt, ray, lsegs, tech, rsf, &data)
+                                     : U.mBB1DPhotonBeams.evalBeamBeamEstimate(qbt, ray, segs, tech, rsf, &data);
+                        else
+                            c = lite ? ref_brute_eval_lite(w.brute, qbt, ray, lsegs, tech, rsf, &data)
+                                     : ref_brute_eval(w.brute, qbt, ray, segs, tech, rsf, &data);
+                    }
                     float* dst = variant == 0 ? out->bb1d_rgb : out->bb1d_brute_rgb;
                     if (dst) for (int k = 0; k < 3; ++k) dst[3 * q + k] = c[k];
                     const int px = sq->pixel[q];

@@ -515,7 +515,7 @@ static rgb pb2d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int6
 {
     const upbp_params* P = O->P;
     const upbp_light_vertices* lv = O->lv;
-    const int pl = lv->path_length[j];
+    const int pl = (P->techniques & UPBP_NO_MIS) ? 0 : lv->path_length[j];
     rgb att, un;
     real pdf, rsp, rsr, ratio, sinT, phase, dirPdf, revPdf, r2, kernel, distSq, rspInv, last, wc, wl;
     rmis cand, lvm;
@@ -528,6 +528,16 @@ static rgb pb2d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int6
         t = dot(op, s->d);
         q.x = s->o.x + s->d.x * t - p.x; q.y = s->o.y + s->d.y * t - p.y; q.z = s->o.z + s->d.z * t - p.z;
         d2 = dot(q, q);
+    }
+    if (P->techniques & UPBP_NO_MIS) {
+        /* breIntersectFuncHomogeneous (Bre.cxx:239-291): VolLightTracer's pure PB2D, no rejects, no MIS:
+         * flux * attenuation * sigma_s * HG * (1 - d2/r2), divided by r2 pi / 2 */
+        att = eval_att(m, t - s->dmin);
+        if (s->ray_flags & UPBP_SHORT_BEAM) att = cdiv(att, comp(att, m->min_idx));
+        phase = hg_pdf(s->d, neg(V(lv->dir_fix + 3 * j)), m->g, &sinT);
+        r2 = O->ph_r2 ? (real)O->ph_r2[j] : (real)P->radius_pb2d * P->radius_pb2d;
+        un = cscale(cscale(cmul(cmul(C3(lv->throughput + 3 * j), att), Cr(m->ss)), phase), 1 - d2 / r2);
+        return cdiv(un, r2 * (IS_F64 ? (real)3.14159265358979323846 : (real)PI_F) * (real)0.5);
     }
     if ((uint32_t)(pl + s->L) > P->max_path_length || (uint32_t)(pl + s->L) < P->min_path_length) return cs(0);
     if (s->L == 1 && t < P->min_dist_to_med) return cs(0);
@@ -592,9 +602,10 @@ static rgb bb1d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int6
     const upbp_params* P = O->P;
     const upbp_beams* B = O->bm;
     const upbp_light_vertices* lv = O->lv;
-    const int lvi = B->light_vertex[b];
-    const int pl = lv->path_length[lvi];
-    const uint32_t bflags = B->flags[b], brsf = B->ray_sampling_flags[b];
+    const int nomis = (P->techniques & UPBP_NO_MIS) != 0;
+    const int lvi = nomis ? -1 : B->light_vertex[b];
+    const int pl = nomis ? 0 : lv->path_length[lvi];
+    const uint32_t bflags = B->flags[b], brsf = nomis ? 0u : B->ray_sampling_flags[b];
     rgb att, batt, un;
     real pfdQ, rspQ, rsrQ, ratioQ, pfdB, rspB, rsrB, ratioB, phase, sinDummy, dirPdf, revPdf, sel = 1;
     real distSqQ, rspInvQ, distSqB, rspInvB, sinT, f, last, wc, wl, ntl;
@@ -603,6 +614,20 @@ static rgb bb1d_contrib(const oracle* O, const medium* m, const seg_ctx* s, int6
     light_view lview;
     if (IS_F64) closest_f64(s->o, s->d, V(B->origin + 3 * b), V(B->direction + 3 * b), &dist, &sinTheta, &t1, &t2);
     radius = rstart + t2 * rchange;
+    if (nomis) {
+        /* PhotonBeam::accumulate without MIS data (PhotonBeam.hxx:315-367): VolLightTracer's pure BB1D */
+        att = eval_att(m, t1 - s->dmin);
+        batt = eval_att(m, t2);
+        if (s->ray_flags & UPBP_SHORT_BEAM) att = cdiv(att, comp(att, m->min_idx));
+        att = cmul(att, batt);
+        if (bflags & UPBP_SHORT_BEAM) att = cdiv(att, comp(batt, m->min_idx));
+        phase = hg_pdf(s->d, V(B->direction + 3 * b), m->g, &sinDummy);
+        return cdiv(cscale(cscale(cscale(cmul(cmul(cscale(C3(B->throughput + 3 * b), (real)1 / sel), Cr(m->ss)), att),
+                                         phase),
+                                  1 - dist * dist / (radius * radius)),
+                           3),
+                    4 * radius * sinTheta);
+    }
     if ((uint32_t)(pl + 1 + s->L) > P->max_path_length || (uint32_t)(pl + 1 + s->L) < P->min_path_length) return cs(0);
     if (s->L == 1 && t1 < P->min_dist_to_med) return cs(0);
     att = eval_att(m, t1 - s->dmin);
@@ -675,9 +700,9 @@ static rgb eval_segments(const oracle* O, const upbp_segment_queries* Q, int64_t
     s.o = V(Q->origin + 3 * q);
     s.d = V(Q->direction + 3 * q);
     s.L = Q->path_length[q];
-    s.lpw = Q->last_pdf_w_inv[q];
+    s.lpw = Q->last_pdf_w_inv ? Q->last_pdf_w_inv[q] : 0; /* NULL only without MIS (UPBP_NO_MIS) */
     s.ray_flags = bt | P->techniques;
-    s.snap = O->cam + Q->cam_mis_begin[q];
+    s.snap = (O->cam && Q->cam_mis_begin) ? O->cam + Q->cam_mis_begin[q] : NULL;
     for (i = 0; i < Q->seg_count[q]; ++i) {
         const int sg = Q->seg_begin[q] + i;
         const medium* m = &O->media[Q->seg_medium[sg]];

@@ -142,19 +142,26 @@ def make_structs(w: Dict[str, np.ndarray]) -> Tuple[dict, List[np.ndarray]]:
     keep: List[np.ndarray] = []
 
     def a(name, dtype=None):
+        """The array `name`, or None when the workload leaves it out (an MIS input of a workload
+        without MIS, which the C ABI then receives as NULL)."""
+        if name not in w:
+            return None
         x = np.ascontiguousarray(w[name]) if dtype is None else np.ascontiguousarray(w[name], dtype=dtype)
         keep.append(x)
         return x
 
+    def mis_ptr(x):
+        return None if x is None else x.ctypes.data_as(C.POINTER(Mis))
+
     params = Params.from_buffer_copy(a("params").tobytes())
     media_arr = a("media")
     media = (Medium * len(media_arr)).from_buffer_copy(media_arr.tobytes())
-    lvm = a("lv_mis")
+    lv_ends = a("lv_path_ends")
     lv = LightVertices(
-        n=len(w["lv_path_idx"]), position=ptr(a("lv_position")), throughput=ptr(a("lv_throughput")),
+        n=len(w["lv_path_length"]), position=ptr(a("lv_position")), throughput=ptr(a("lv_throughput")),
         dir_fix=ptr(a("lv_dir_fix")), cont_prob=ptr(a("lv_cont_prob")), path_idx=ptr(a("lv_path_idx")),
         path_length=ptr(a("lv_path_length")), medium_id=ptr(a("lv_medium_id")), flags=ptr(a("lv_flags")),
-        mis=lvm.ctypes.data_as(C.POINTER(Mis)), n_paths=len(w["lv_path_ends"]), path_ends=ptr(a("lv_path_ends")))
+        mis=mis_ptr(a("lv_mis")), n_paths=0 if lv_ends is None else len(lv_ends), path_ends=ptr(lv_ends))
     beams = Beams(
         n=len(w["beam_length"]), origin=ptr(a("beam_origin")), direction=ptr(a("beam_direction")),
         length=ptr(a("beam_length")), throughput=ptr(a("beam_throughput")), flags=ptr(a("beam_flags")),
@@ -174,7 +181,6 @@ def make_structs(w: Dict[str, np.ndarray]) -> Tuple[dict, List[np.ndarray]]:
         medium_id=ptr(a("pq_medium_id")), path_length=ptr(a("pq_path_length")), throughput=ptr(a("pq_throughput")),
         pixel=ptr(a("pq_pixel")), cam_mis_begin=ptr(a("pq_cam_mis_begin")))
     cm = a("cam_mis")
-    cam = cm.ctypes.data_as(C.POINTER(Mis))
     structs = dict(params=params, media=media, n_media=len(media_arr), lv=lv, beams=beams, sq=sq, pq=pq,
-                   cam_mis=cam, n_cam_mis=len(cm))
+                   cam_mis=mis_ptr(cm), n_cam_mis=0 if cm is None else len(cm))
     return structs, keep

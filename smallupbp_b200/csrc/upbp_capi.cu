@@ -63,6 +63,10 @@ struct upbp_ctx {
         seg_dmin, seg_dmax, seg_pdf, seg_rev, seg_att, seg_med;
     int64_t n_pq = 0;
     DBuf pq_pos, pq_dir, pq_med, pq_plen, pq_thr, pq_pixel, pq_cam_begin;
+    // the first MIS input given as NULL (allowed only with UPBP_NO_MIS), per upload; nullptr: none
+    const char* lv_mis_missing = nullptr;
+    const char* beam_mis_missing = nullptr;
+    const char* sq_mis_missing = nullptr;
 
     // packed light vertices
     DBuf lv_pos4, lv_dir4, lv_thr4, lv_info4, lv_inmed;
@@ -197,6 +201,22 @@ void upload(upbp_ctx* c, DBuf& b, const T* src, int64_t count, const char* name)
     ck(c, cudaMemcpyAsync(b.p, src, sizeof(T) * (size_t)count, cudaMemcpyDefault, c->stream), name);
 }
 
+// An MIS input, which the estimators without MIS (UPBP_NO_MIS) never read: a NULL array is
+// stored as `count` elements of the byte `fill` (zeros, or -1 for indices) and its name recorded
+// in *missing, so that a build or evaluate that needs it fails.
+template <class T>
+void upload_mis(upbp_ctx* c, DBuf& b, const T* src, int64_t count, const char* name, int fill, const char** missing)
+{
+    if (count <= 0) return;
+    if (src) {
+        upload(c, b, src, count, name);
+        return;
+    }
+    ensure(c, b, sizeof(T) * (size_t)count);
+    ck(c, cudaMemsetAsync(b.p, fill, sizeof(T) * (size_t)count, c->stream), name);
+    if (!*missing) *missing = name;
+}
+
 void free_buf(DBuf& b)
 {
     if (b.p) cudaFree(b.p);
@@ -289,6 +309,11 @@ void do_build(upbp_ctx* c)
     }
     const upbp_params& P = c->P;
     const int64_t n = c->n_lv;
+    const bool mis = !(P.techniques & UPBP_NO_MIS);
+    if (mis && n > 0 && c->lv_mis_missing)
+        fail(c, UPBP_ERR_INVALID_ARG, "light vertex %s is NULL (only UPBP_NO_MIS runs without it)", c->lv_mis_missing);
+    if (mis && c->n_beams > 0 && (P.techniques & UPBP_BB1D) && c->beam_mis_missing)
+        fail(c, UPBP_ERR_INVALID_ARG, "%s is NULL (only UPBP_NO_MIS runs without it)", c->beam_mis_missing);
     // ---- light vertices
     ensure(c, c->lv_pos4, sizeof(float4) * std::max<int64_t>(n, 1));
     ensure(c, c->lv_dir4, sizeof(float4) * std::max<int64_t>(n, 1));
@@ -302,7 +327,7 @@ void do_build(upbp_ctx* c)
                        c->lv_dir4.as<float4>(), c->lv_thr4.as<float4>(), c->lv_info4.as<int4>(),
                        c->lv_inmed.as<uint32_t>(), s);
     c->build_launches += 1;
-    if (c->mode != UPBP_MODE_PLAIN && n > 0) {
+    if (c->mode != UPBP_MODE_PLAIN && n > 0 && mis) {
         ensure(c, c->light_sums, sizeof(LightSum) * n);
         // the PB2D / BB1D walks see beamType | techniques, PP3D the techniques: same terms
         launch_light_sums(c->lv_mis.as<upbp_mis>(), c->path_ends.as<int32_t>(), c->n_paths, P.techniques,
@@ -514,9 +539,11 @@ void do_build(upbp_ctx* c)
         c->build_launches += 8;
         if (c->mode != UPBP_MODE_PLAIN) {
             ensure(c, c->pc_pay, sizeof(PiecePayload) * np);
+            // without MIS the payload holds the beam's throughput, flags and radius only
             launch_piece_payload(c->pc_c2.as<float4>(), np, c->bm_thr4.as<float4>(), c->bm_pdf4.as<float4>(),
-                                 c->bm_link.as<int2>(), c->bm_radius.as<float>(), c->lv_info4.as<int4>(),
-                                 c->lv_mis.as<upbp_mis>(), c->light_sums.as<LightSum>(), c->pc_pay.as<PiecePayload>(), s);
+                                 c->bm_link.as<int2>(), c->bm_radius.as<float>(),
+                                 mis ? c->lv_info4.as<int4>() : nullptr, mis ? c->lv_mis.as<upbp_mis>() : nullptr,
+                                 mis ? c->light_sums.as<LightSum>() : nullptr, c->pc_pay.as<PiecePayload>(), s);
             c->build_launches += 1;
         }
     }
@@ -766,9 +793,12 @@ void do_evaluate(upbp_ctx* c)
     unsigned long long* tested = c->tested.as<unsigned long long>();
 
     const bool mixed = c->mode == UPBP_MODE_MIXED;
+    const bool mis = !(c->P.techniques & UPBP_NO_MIS);
+    if (mis && nq > 0 && c->sq_mis_missing)
+        fail(c, UPBP_ERR_INVALID_ARG, "segment query %s is NULL (only UPBP_NO_MIS runs without it)", c->sq_mis_missing);
     const CamSum* cs_seg = nullptr;
     const CamSum* cs_pt = nullptr;
-    if (c->mode != UPBP_MODE_PLAIN) prepare_cam_sums(c, s, &cs_seg, &cs_pt);
+    if (c->mode != UPBP_MODE_PLAIN && mis) prepare_cam_sums(c, s, &cs_seg, &cs_pt);
     if (c->mode == UPBP_MODE_FP64) {
         // FP64 oracle on the GPU: the same candidates, FP64 geometry, contributions and MIS
         gen::GenLaunch A = generic_launch(c, cs_seg, cs_pt, -1);
@@ -1056,6 +1086,8 @@ int upbp_set_params(upbp_ctx* c, const upbp_params* p)
         if (p->image_width < 0 || p->image_height < 0) fail(c, UPBP_ERR_INVALID_ARG, "negative image size");
         if (p->pb2d_knn < 0 || p->pb2d_knn > kMaxKnn || p->bb1d_knn < 0 || p->bb1d_knn > kMaxKnn)
             fail(c, UPBP_ERR_INVALID_ARG, "KNN counts must be in [0, %d]", kMaxKnn);
+        if ((p->techniques & UPBP_NO_MIS) && (p->techniques & UPBP_PP3D))
+            fail(c, UPBP_ERR_INVALID_ARG, "UPBP_NO_MIS with UPBP_PP3D: the reference has no PP3D without MIS");
         c->P = *p;
         c->have_params = true;
         c->built = false;
@@ -1072,13 +1104,15 @@ int upbp_set_light_vertices(upbp_ctx* c, const upbp_light_vertices* lv)
         upload(c, c->lv_pos_in, lv->position, 3 * n, "position");
         upload(c, c->lv_thr_in, lv->throughput, 3 * n, "throughput");
         upload(c, c->lv_dir_in, lv->dir_fix, 3 * n, "dir_fix");
-        upload(c, c->lv_cont_in, lv->cont_prob, n, "cont_prob");
-        upload(c, c->lv_pidx_in, lv->path_idx, n, "path_idx");
+        c->lv_mis_missing = nullptr;
+        upload_mis(c, c->lv_cont_in, lv->cont_prob, n, "cont_prob", 0, &c->lv_mis_missing);
+        upload_mis(c, c->lv_pidx_in, lv->path_idx, n, "path_idx", 0, &c->lv_mis_missing);
         upload(c, c->lv_plen_in, lv->path_length, n, "path_length");
         upload(c, c->lv_med_in, lv->medium_id, n, "medium_id");
         upload(c, c->lv_flags_in, lv->flags, n, "flags");
-        upload(c, c->lv_mis, lv->mis, n, "mis");
-        upload(c, c->path_ends, lv->path_ends, lv->n_paths, "path_ends");
+        upload_mis(c, c->lv_mis, lv->mis, n, "mis", 0, &c->lv_mis_missing);
+        upload_mis(c, c->path_ends, lv->path_ends, lv->n_paths, "path_ends", 0, &c->lv_mis_missing);
+        if (n > 0 && lv->n_paths == 0 && !c->lv_mis_missing) c->lv_mis_missing = "path_ends";
         c->n_lv = n;
         c->n_paths = lv->n_paths;
         c->built = false;
@@ -1096,12 +1130,13 @@ int upbp_set_beams(upbp_ctx* c, const upbp_beams* b)
         upload(c, c->b_len, b->length, n, "beam length");
         upload(c, c->b_thr_in, b->throughput, 3 * n, "beam throughput");
         upload(c, c->b_flags_in, b->flags, n, "beam flags");
-        upload(c, c->b_rsp_in, b->ray_sample_pdf, n, "beam ray_sample_pdf");
-        upload(c, c->b_rsr_in, b->ray_sample_rev_pdf, n, "beam ray_sample_rev_pdf");
-        upload(c, c->b_rsf_in, b->ray_sampling_flags, n, "beam ray_sampling_flags");
-        upload(c, c->b_lpw_in, b->last_pdf_w_inv, n, "beam last_pdf_w_inv");
+        c->beam_mis_missing = nullptr;
+        upload_mis(c, c->b_rsp_in, b->ray_sample_pdf, n, "beam ray_sample_pdf", 0, &c->beam_mis_missing);
+        upload_mis(c, c->b_rsr_in, b->ray_sample_rev_pdf, n, "beam ray_sample_rev_pdf", 0, &c->beam_mis_missing);
+        upload_mis(c, c->b_rsf_in, b->ray_sampling_flags, n, "beam ray_sampling_flags", 0, &c->beam_mis_missing);
+        upload_mis(c, c->b_lpw_in, b->last_pdf_w_inv, n, "beam last_pdf_w_inv", 0, &c->beam_mis_missing);
         upload(c, c->b_med_in, b->medium_id, n, "beam medium_id");
-        upload(c, c->b_lv_in, b->light_vertex, n, "beam light_vertex");
+        upload_mis(c, c->b_lv_in, b->light_vertex, n, "beam light_vertex", 0xff, &c->beam_mis_missing);
         c->n_beams = n;
         c->built = false;
     });
@@ -1134,10 +1169,11 @@ int upbp_set_segment_queries(upbp_ctx* c, const upbp_segment_queries* q)
         upload(c, c->sq_seg_count, q->seg_count, n, "seg_count");
         upload(c, c->sq_flags, q->flags, n, "flags");
         upload(c, c->sq_plen, q->path_length, n, "path_length");
-        upload(c, c->sq_lpw, q->last_pdf_w_inv, n, "last_pdf_w_inv");
+        c->sq_mis_missing = nullptr;
+        upload_mis(c, c->sq_lpw, q->last_pdf_w_inv, n, "last_pdf_w_inv", 0, &c->sq_mis_missing);
         upload(c, c->sq_thr, q->throughput, 3 * n, "throughput");
         upload(c, c->sq_pixel, q->pixel, n, "pixel");
-        upload(c, c->sq_cam_begin, q->cam_mis_begin, n, "cam_mis_begin");
+        upload_mis(c, c->sq_cam_begin, q->cam_mis_begin, n, "cam_mis_begin", 0, &c->sq_mis_missing);
         upload(c, c->seg_dmin, q->seg_dist_min, s, "seg_dist_min");
         upload(c, c->seg_dmax, q->seg_dist_max, s, "seg_dist_max");
         upload(c, c->seg_pdf, q->seg_pdf, s, "seg_pdf");
@@ -1224,6 +1260,7 @@ int upbp_trace_light_paths(upbp_ctx* c, const upbp_scene* sc, uint32_t iteration
         cudaStream_t s = c->stream;
         ensure(c, c->tr_cnt, sizeof(int) * 2 * (n + 1));
         ensure(c, c->tr_off, sizeof(int) * 2 * (n + 1));
+        c->lv_mis_missing = c->beam_mis_missing = nullptr;  // the pass writes every record
         trace::LightOut O{};
         O.v_count = c->tr_cnt.as<int>();
         O.b_count = O.v_count + (n + 1);
@@ -1303,6 +1340,7 @@ int upbp_trace_camera_paths(upbp_ctx* c, const upbp_scene* sc, uint32_t iteratio
         cudaStream_t s = c->stream;
         ensure(c, c->tr_cnt, sizeof(int) * 4 * (n + 1));
         ensure(c, c->tr_off, sizeof(int) * 4 * (n + 1));
+        c->sq_mis_missing = nullptr;  // the pass writes every record
         trace::CameraOut O{};
         O.q_count = c->tr_cnt.as<int>();
         O.s_count = O.q_count + (n + 1);
@@ -1534,7 +1572,7 @@ int upbp_adjoint(upbp_ctx* c, const float* grad_image, int32_t medium, double* g
         ck(c, cudaMemsetAsync(c->grad_acc.p, 0, sizeof(double) * 8, s), "memset");
         const CamSum* cs_seg = nullptr;
         const CamSum* cs_pt = nullptr;
-        prepare_cam_sums(c, s, &cs_seg, &cs_pt);
+        if (!(c->P.techniques & UPBP_NO_MIS)) prepare_cam_sums(c, s, &cs_seg, &cs_pt);
         gen::GenLaunch A = generic_launch(c, cs_seg, cs_pt, medium);
         const gen::GenOut O{nullptr, nullptr, nullptr, nullptr, c->grad_img.as<float>(), c->grad_acc.as<double>()};
         A.out_pp3d = A.out_pb2d = A.out_bb1d = A.out_bp2d = O;

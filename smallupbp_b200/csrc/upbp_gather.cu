@@ -89,6 +89,44 @@ __device__ __forceinline__ void fill_cand(upbp_mis& c, const upbp_params& P, flo
     c.flags = flags;
 }
 
+// ----------------------------------------------------------------- estimators without MIS
+// breIntersectFuncHomogeneous (Bre.cxx:239-291), the callback of VolLightTracer's pure PB2D: the
+// photon's flux (its light vertex's throughput) x transmittance to the photon (over the
+// free-flight pdf for SHORT query beams) x sigma_s x HG x the 2-D Epanechnikov kernel, with no
+// rejects and no MIS weight.  The reference's expression divides the product by r^2 pi / 2.
+__device__ __forceinline__ Rgb pb2d_contrib_nomis(const DMedium& m, const LightSoA& Lv, const SegCtx& s, int lv,
+                                                  float t, float d2, float r2)
+{
+    Rgb att = eval_att(m, t - s.dmin);
+    if (s.ray_flags & UPBP_SHORT_BEAM) att = att / comp(att, m.min_idx);
+    const float4 ld = __ldg(&Lv.dir[lv]);
+    const float4 th = __ldg(&Lv.thr[lv]);
+    float sinT;
+    const float phase = hg_pdf(s.d, neg3(v3(ld.x, ld.y, ld.z)), m.g, &sinT);
+    const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
+    return (Rgb{th.x, th.y, th.z} * att * ss * phase * (1.f - d2 / r2)) / (r2 * UPBP_PI_F * 0.5f);
+}
+
+// PhotonBeam::accumulate without MIS data (PhotonBeam.hxx:315-367), VolLightTracer's pure BB1D:
+// (1 / beam selection pdf, 1 without beam reduction) x the beam's throughput x sigma_s x the query
+// and beam transmittances (each over its free-flight pdf for SHORT beams) x HG x the 1-D kernel.
+// The candidate test and the radius test are the caller's, as for accumulate2.
+__device__ __forceinline__ Rgb bb1d_contrib_nomis(const DMedium& m, const SegCtx& s, float4 bthr, bool beam_short,
+                                                  V3 bdir, float radius, float dist, float sinTheta, float t1,
+                                                  float t2)
+{
+    Rgb att = eval_att(m, t1 - s.dmin);
+    const Rgb batt = eval_att(m, t2);
+    if (s.ray_flags & UPBP_SHORT_BEAM) att = att / comp(att, m.min_idx);
+    att = att * batt;
+    if (beam_short) att = att / comp(batt, m.min_idx);
+    float sinDummy;
+    const float phase = hg_pdf(s.d, bdir, m.g, &sinDummy);
+    const Rgb ss{m.ss[0], m.ss[1], m.ss[2]};
+    return ((1.0f * Rgb{bthr.x, bthr.y, bthr.z} * ss * att * phase * (1.f - dist * dist / (radius * radius))) * 3.f) /
+           (4.f * radius * sinTheta);
+}
+
 // ----------------------------------------------------------------- PB2D contribution
 // breIntersectFuncHomogeneous2 after testIntersectionBre accepted photon `lv` at (t, d2).
 template <bool kMixed>
@@ -96,6 +134,7 @@ __device__ Rgb pb2d_contrib(const GatherConsts& K, const DMedium& m, const Light
                             float t, float d2, float r2)
 {
     const upbp_params& P = K.P;
+    if (P.techniques & UPBP_NO_MIS) return pb2d_contrib_nomis(m, Lv, s, lv, t, d2, r2);
     const int4 info = __ldg(&Lv.info[lv]);
     const int pl = info.y;
     if ((uint32_t)(pl + s.L) > P.max_path_length || (uint32_t)(pl + s.L) < P.min_path_length) return rgb(0.f);
@@ -182,6 +221,11 @@ __device__ Rgb bb1d_contrib(const GatherConsts& K, const DMedium& m, const Light
         if (1.f - c * c < 1e-2f) closest_approach_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
     }
     const upbp_params& P = K.P;
+    if (P.techniques & UPBP_NO_MIS) {
+        const float4 bthr = __ldg(&Bs.thr[beam]);
+        const bool bshort = ((uint32_t)__float_as_int(bthr.w) & UPBP_SHORT_BEAM) != 0;
+        return bb1d_contrib_nomis(m, s, bthr, bshort, bdir, radius, dist, sinTheta, t1, t2);
+    }
     const int2 link = __ldg(&Bs.link[beam]);
     const int lvi = link.x;
     const int4 info = __ldg(&Lv.info[lvi]);
@@ -268,6 +312,8 @@ __device__ Rgb bb1d_contrib_packed(const GatherConsts& K, const DMedium& m, cons
 {
     const upbp_params& P = K.P;
     const unsigned lvbits = (unsigned)__float_as_int(py.lv.w);
+    if (P.techniques & UPBP_NO_MIS)
+        return bb1d_contrib_nomis(m, s, py.thr, (lvbits & kPayShortBeam) != 0, bdir, radius, dist, sinTheta, t1, t2);
     const int pl = (int)(lvbits & kPayPathMask);
     const bool finite = (lvbits & kPayFinite) != 0;
     if ((uint32_t)(pl + 1 + s.L) > P.max_path_length || (uint32_t)(pl + 1 + s.L) < P.min_path_length) return rgb(0.f);
@@ -383,7 +429,7 @@ __device__ __forceinline__ void init_seg_ctx(SegCtx& s, const GatherConsts& K, c
     s.cam = cam + Q.cam_mis_begin[q];
     s.e = e_store;
     s.cs = cs_store;
-    if (kMixed && leader) {
+    if (kMixed && leader && !(K.P.techniques & UPBP_NO_MIS)) {
         if (s.L >= 2) *e_store = load_mis(s.cam + s.L - 1);
         *cs_store = cs[q];
     }
@@ -1288,10 +1334,16 @@ __global__ void k_piece_payload(const float4* __restrict__ pc, int n, const floa
     if (i >= n) return;
     const int beam = __float_as_int(pc[i].z);
     const int lv = bm_link[beam].x;
-    const upbp_mis m = load_mis(lv_mis + lv);
-    const int4 info = lv_info[lv];
+    // without MIS (lv_info == nullptr) the beams need not have light vertices
+    upbp_mis m{};
+    int4 info = make_int4(0, 0, 0, 0);
+    LightSum ls{};
+    if (lv_info) {
+        m = load_mis(lv_mis + lv);
+        info = lv_info[lv];
+        ls = sums[lv];
+    }
     const bool onDelta = (m.flags & UPBP_MIS_ON_LIGHT_SOURCE) && (m.flags & UPBP_MIS_IS_DELTA);
-    const LightSum ls = sums[lv];
     const float4 thr = bm_thr[beam], pdf = bm_pdf[beam];
     const uint32_t bflags = (uint32_t)__float_as_int(thr.w), brsf = (uint32_t)__float_as_int(pdf.w);
     PiecePayload p;

@@ -5,9 +5,10 @@
 // breIntersectFuncHomogeneous2 (Bre/Bre.cxx:293-464), PhotonBeam::accumulate2
 // (Beams/PhotonBeam.hxx:386-607) and UPBP::RangeQuery::Process (Renderers/UPBP.hxx:86-133) with
 // the O(1) MIS weights of the FP64 partial sums (upbp_mis_prep.cuh).  With T = double every
-// result is an FP64 oracle computed on the GPU; with T = Dual every candidate also carries the
-// derivatives of its contribution with respect to one medium's sigma_a, sigma_s and g, and the
-// kernels accumulate sum_pixels dL/dI . dI/dtheta -- the adjoint of the estimator sum.
+// result is an FP64 oracle computed on the GPU; with T = DualF every candidate also carries the
+// derivatives (FP32 tangents) of its contribution with respect to one medium's sigma_a, sigma_s
+// and g, and the kernels accumulate sum_pixels dL/dI . dI/dtheta in FP64 -- the adjoint of the
+// estimator sum.
 #include <cfloat>
 #include <cstdint>
 
@@ -105,11 +106,33 @@ __device__ __forceinline__ void init_ctx(SegCtx<T>& s, const GatherConsts& K, co
 }
 
 // ------------------------------------------------------------------ PB2D (Bre.cxx:293-464)
+// Without MIS (UPBP_NO_MIS): breIntersectFuncHomogeneous (Bre.cxx:239-291), every accepted photon's
+// unweighted contribution, the candidate geometry re-solved in FP64.
+template <class T>
+__device__ RgbT<T> pb2d_contrib_nomis(const MedT<T>& m, const LightSoA& Lv, const SegCtx<T>& s, int lv, double r2)
+{
+    const float4 lp = __ldg(&Lv.pos[lv]);
+    const V3d p = v3d(lp.x, lp.y, lp.z);
+    const double t = dot(sub(p, s.o), s.d);
+    const V3d qv = V3d{s.o.x + s.d.x * t - p.x, s.o.y + s.d.y * t - p.y, s.o.z + s.d.z * t - p.z};
+    const double d2 = dot(qv, qv);
+    RgbT<T> att = eval_att(m, t - s.dmin);
+    if (s.ray_flags & UPBP_SHORT_BEAM) att = att / comp(att, m.min_idx);
+    const float4 ld = __ldg(&Lv.dir[lv]);
+    const float4 th = __ldg(&Lv.thr[lv]);
+    double sinT;
+    const T phase = hg_pdf(s.d, neg(v3d(ld.x, ld.y, ld.z)), m.g, &sinT);
+    const double kernel = (1.0 - d2 / r2) / (r2 * 3.14159265358979323846 * 0.5);
+    return RgbT<T>{att.r * (double)th.x, att.g * (double)th.y, att.b * (double)th.z} *
+           RgbT<T>{m.ss[0], m.ss[1], m.ss[2]} * (phase * kernel);
+}
+
 template <class T>
 __device__ RgbT<T> pb2d_contrib(const GatherConsts& K, const MedT<T>& m, const LightSoA& Lv, const SegCtx<T>& s,
                                 int lv, float r2f)
 {
     const upbp_params& P = K.P;
+    if (P.techniques & UPBP_NO_MIS) return pb2d_contrib_nomis<T>(m, Lv, s, lv, (double)r2f);
     const int4 info = __ldg(&Lv.info[lv]);
     const int pl = info.y;
     if ((uint32_t)(pl + s.L) > P.max_path_length || (uint32_t)(pl + s.L) < P.min_path_length) return rgb_zero<T>();
@@ -181,11 +204,34 @@ __device__ __forceinline__ void closest_f64(V3d O1, V3d d1, V3d O2, V3d d2, doub
     sinT = s;
 }
 
+// Without MIS (UPBP_NO_MIS): PhotonBeam::accumulate (PhotonBeam.hxx:315-367), the unweighted
+// contribution in FP64.
+template <class T>
+__device__ RgbT<T> bb1d_contrib_nomis(const MedT<T>& m, const SegCtx<T>& s, const PiecePayload& py, V3d bo,
+                                      V3d bdir, double rchange)
+{
+    double dist, sinTheta, t1, t2;
+    closest_f64(s.o, s.d, bo, bdir, dist, sinTheta, t1, t2);
+    const double radius = (double)py.lv.z + t2 * rchange;
+    const unsigned lvbits = (unsigned)__float_as_int(py.lv.w);
+    RgbT<T> att = eval_att(m, t1 - s.dmin);
+    const RgbT<T> batt = eval_att(m, t2);
+    if (s.ray_flags & UPBP_SHORT_BEAM) att = att / comp(att, m.min_idx);
+    att = att * batt;
+    if (lvbits & kPayShortBeam) att = att / comp(batt, m.min_idx);
+    double sinDummy;
+    const T phase = hg_pdf(s.d, bdir, m.g, &sinDummy);
+    const double kern = (1.0 - dist * dist / (radius * radius)) * 3.0 / (4.0 * radius * sinTheta);
+    return RgbT<T>{att.r * (double)py.thr.x, att.g * (double)py.thr.y, att.b * (double)py.thr.z} *
+           RgbT<T>{m.ss[0], m.ss[1], m.ss[2]} * (phase * kern);
+}
+
 template <class T>
 __device__ RgbT<T> bb1d_contrib(const GatherConsts& K, const MedT<T>& m, const SegCtx<T>& s, const PiecePayload& py,
                                 const LightSum& ls, V3d bo, V3d bdir, double rchange)
 {
     const upbp_params& P = K.P;
+    if (P.techniques & UPBP_NO_MIS) return bb1d_contrib_nomis<T>(m, s, py, bo, bdir, rchange);
     const unsigned lvbits = (unsigned)__float_as_int(py.lv.w);
     const int pl = (int)(lvbits & kPayPathMask);
     const bool finite = (lvbits & kPayFinite) != 0;
@@ -254,7 +300,7 @@ __device__ RgbT<T> bb1d_contrib(const GatherConsts& K, const MedT<T>& m, const S
 template <class T>
 __device__ __forceinline__ void lane_grad(const RgbT<T>& v, const double w[3], double g[kNT])
 {
-    if constexpr (std::is_same<T, Dual>::value) {
+    if constexpr (is_dual<T>::value) {
 #pragma unroll
         for (int i = 0; i < kNT; ++i) g[i] += w[0] * v.r.d[i] + w[1] * v.g.d[i] + w[2] * v.b.d[i];
     }
@@ -278,7 +324,7 @@ template <class T>
 __device__ __forceinline__ void finish_thread(const GenOut& O, int64_t q, const RgbT<T>& v, int px, const float* thr,
                                               double norm, uint32_t cnt, unsigned long long h)
 {
-    if constexpr (std::is_same<T, Dual>::value) {
+    if constexpr (is_dual<T>::value) {
         double w[3], g[kNT];
         pixel_weights(O, px, thr, norm, w);
         for (int i = 0; i < kNT; ++i) g[i] = 0.0;
@@ -307,7 +353,7 @@ template <class T>
 __device__ __forceinline__ void finish_lanes(const GenOut& O, bool valid, int64_t q, const RgbT<T>& v, int px,
                                              const float* thr, double norm, uint32_t cnt, unsigned long long h)
 {
-    if constexpr (std::is_same<T, Dual>::value) {
+    if constexpr (is_dual<T>::value) {
         double w[3] = {0.0, 0.0, 0.0}, g[kNT];
         for (int i = 0; i < kNT; ++i) g[i] = 0.0;
         if (valid) {
@@ -330,7 +376,7 @@ template <class T>
 __device__ __forceinline__ void finish_warp(const GenOut& O, int64_t q, const RgbT<T>& acc, int px, const float* thr,
                                             double norm, unsigned long long cnt, unsigned long long h, int lane)
 {
-    if constexpr (std::is_same<T, Dual>::value) {
+    if constexpr (is_dual<T>::value) {
         double w[3], g[kNT];
         pixel_weights(O, px, thr, norm, w);
         for (int i = 0; i < kNT; ++i) g[i] = 0.0;
@@ -479,7 +525,8 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                     const PiecePayload py = B.pay[i];
                     const int beam = __float_as_int(__ldg(&B.pc[i]).z);
                     const double rchg = Bs.rchange ? (double)__ldg(&Bs.rchange[beam]) : 0.0;
-                    const LightSum ls = lsums[__ldg(&Bs.link[beam]).x];
+                    const LightSum ls =
+                        (K.P.techniques & UPBP_NO_MIS) ? LightSum{} : lsums[__ldg(&Bs.link[beam]).x];
                     part = part + bb1d_contrib<T>(K, m, s, py, ls, v3d(pa.x, pa.y, pa.z), v3d(pb.x, pb.y, pb.z), rchg);
                 };
                 // the rest of the predicate for one piece per lane (i < 0: none)
@@ -771,14 +818,14 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
 
 void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream)
 {
-    if (adjoint) launch_all<Dual>(A, stream);
+    if (adjoint) launch_all<DualF>(A, stream);
     else launch_all<double>(A, stream);
 }
 
 int generic_pb2d_blocks_per_sm(bool adjoint)
 {
     int nb = 0;
-    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<Dual>, 128, 0);
+    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<DualF>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<double>, 128, 0);
     return nb > 0 ? nb : 1;
 }
@@ -786,7 +833,7 @@ int generic_pb2d_blocks_per_sm(bool adjoint)
 int generic_bp2d_blocks_per_sm(bool adjoint)
 {
     int nb = 0;
-    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bp2d<Dual>, 128, 0);
+    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bp2d<DualF>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bp2d<double>, 128, 0);
     return nb > 0 ? nb : 1;
 }
@@ -794,7 +841,7 @@ int generic_bp2d_blocks_per_sm(bool adjoint)
 int generic_bb1d_blocks_per_sm(bool adjoint)
 {
     int nb = 0;
-    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bb1d<Dual>, 128, 0);
+    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bb1d<DualF>, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bb1d<double>, 128, 0);
     return nb > 0 ? nb : 1;
 }

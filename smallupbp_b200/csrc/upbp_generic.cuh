@@ -3,8 +3,9 @@
 //   * double -- the FP64 evaluation mode (an FP64 oracle on the GPU: the candidate sets come from
 //     the same FP32 predicates, the candidate geometry is re-solved in FP64 and all contribution
 //     and MIS arithmetic is FP64), and
-//   * Dual   -- forward-mode tangents with respect to one medium's sigma_a (rgb), sigma_s (rgb)
-//     and g, used by the adjoint kernels (the vector-Jacobian product of the estimator sum).
+//   * DualF  -- forward-mode tangents (FP32) with respect to one medium's sigma_a (rgb),
+//     sigma_s (rgb) and g, used by the adjoint kernels (the vector-Jacobian product of the
+//     estimator sum).
 // Transmittance is recomputed from the medium at every use, never stored.
 #pragma once
 
@@ -18,123 +19,154 @@ namespace gen {
 
 constexpr int kNT = 7;  // tangent slots: sigma_a r,g,b, sigma_s r,g,b, g
 
-struct Dual {
-    double v;
-    double d[kNT];
+// Forward-mode number: a value and its kNT tangents, in scalar S.  The adjoint runs in
+// DualF (FP32 value and tangents: half the registers of FP64, within the 1e-3 gradient bound);
+// DualD keeps FP64 for checks of the tangent arithmetic itself.
+template <class S>
+struct DualS {
+    S v;
+    S d[kNT];
 };
+using DualD = DualS<double>;
+using DualF = DualS<float>;
+template <class T> struct is_dual : std::false_type {};
+template <class S> struct is_dual<DualS<S>> : std::true_type {};
 
-__device__ __forceinline__ Dual dual(double v)
+template <class S>
+__device__ __forceinline__ DualS<S> dual(S v)
 {
-    Dual r;
+    DualS<S> r;
     r.v = v;
 #pragma unroll
-    for (int i = 0; i < kNT; ++i) r.d[i] = 0.0;
+    for (int i = 0; i < kNT; ++i) r.d[i] = S(0);
     return r;
 }
-__device__ __forceinline__ Dual operator+(const Dual& a, const Dual& b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator+(const DualS<S>& a, const DualS<S>& b)
 {
-    Dual r;
+    DualS<S> r;
     r.v = a.v + b.v;
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = a.d[i] + b.d[i];
     return r;
 }
-__device__ __forceinline__ Dual operator-(const Dual& a, const Dual& b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator-(const DualS<S>& a, const DualS<S>& b)
 {
-    Dual r;
+    DualS<S> r;
     r.v = a.v - b.v;
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = a.d[i] - b.d[i];
     return r;
 }
-__device__ __forceinline__ Dual operator-(const Dual& a)
+template <class S>
+__device__ __forceinline__ DualS<S> operator-(const DualS<S>& a)
 {
-    Dual r;
+    DualS<S> r;
     r.v = -a.v;
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = -a.d[i];
     return r;
 }
-__device__ __forceinline__ Dual operator*(const Dual& a, const Dual& b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator*(const DualS<S>& a, const DualS<S>& b)
 {
-    Dual r;
+    DualS<S> r;
     r.v = a.v * b.v;
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
     return r;
 }
-__device__ __forceinline__ Dual operator/(const Dual& a, const Dual& b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator/(const DualS<S>& a, const DualS<S>& b)
 {
-    Dual r;
-    const double ib = 1.0 / b.v;
+    DualS<S> r;
+    const S ib = S(1) / b.v;
     r.v = a.v * ib;
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
     return r;
 }
-__device__ __forceinline__ Dual operator+(const Dual& a, double b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator+(const DualS<S>& a, double b)
 {
-    Dual r = a;
-    r.v += b;
+    DualS<S> r = a;
+    r.v += (S)b;
     return r;
 }
-__device__ __forceinline__ Dual operator+(double a, const Dual& b) { return b + a; }
-__device__ __forceinline__ Dual operator-(const Dual& a, double b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator+(double a, const DualS<S>& b) { return b + a; }
+template <class S>
+__device__ __forceinline__ DualS<S> operator-(const DualS<S>& a, double b)
 {
-    Dual r = a;
-    r.v -= b;
+    DualS<S> r = a;
+    r.v -= (S)b;
     return r;
 }
-__device__ __forceinline__ Dual operator-(double a, const Dual& b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator-(double a, const DualS<S>& b)
 {
-    Dual r = -b;
-    r.v += a;
+    DualS<S> r = -b;
+    r.v += (S)a;
     return r;
 }
-__device__ __forceinline__ Dual operator*(const Dual& a, double b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator*(const DualS<S>& a, double b)
 {
-    Dual r;
-    r.v = a.v * b;
+    DualS<S> r;
+    const S sb = (S)b;
+    r.v = a.v * sb;
 #pragma unroll
-    for (int i = 0; i < kNT; ++i) r.d[i] = a.d[i] * b;
+    for (int i = 0; i < kNT; ++i) r.d[i] = a.d[i] * sb;
     return r;
 }
-__device__ __forceinline__ Dual operator*(double a, const Dual& b) { return b * a; }
-__device__ __forceinline__ Dual operator/(const Dual& a, double b) { return a * (1.0 / b); }
-__device__ __forceinline__ Dual operator/(double a, const Dual& b)
+template <class S>
+__device__ __forceinline__ DualS<S> operator*(double a, const DualS<S>& b) { return b * a; }
+template <class S>
+__device__ __forceinline__ DualS<S> operator/(const DualS<S>& a, double b) { return a * (1.0 / b); }
+template <class S>
+__device__ __forceinline__ DualS<S> operator/(double a, const DualS<S>& b)
 {
-    Dual r;
-    const double ib = 1.0 / b.v;
-    r.v = a * ib;
+    DualS<S> r;
+    const S ib = S(1) / b.v;
+    r.v = (S)a * ib;
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = -r.v * ib * b.d[i];
     return r;
 }
-__device__ __forceinline__ Dual& operator+=(Dual& a, const Dual& b) { return a = a + b; }
-__device__ __forceinline__ Dual& operator*=(Dual& a, const Dual& b) { return a = a * b; }
+template <class S>
+__device__ __forceinline__ DualS<S>& operator+=(DualS<S>& a, const DualS<S>& b) { return a = a + b; }
+template <class S>
+__device__ __forceinline__ DualS<S>& operator*=(DualS<S>& a, const DualS<S>& b) { return a = a * b; }
 
 __device__ __forceinline__ double val(double x) { return x; }
-__device__ __forceinline__ double val(const Dual& x) { return x.v; }
+template <class S>
+__device__ __forceinline__ double val(const DualS<S>& x) { return (double)x.v; }
 
 template <class T> __device__ __forceinline__ T cst(double v);
 template <> __device__ __forceinline__ double cst<double>(double v) { return v; }
-template <> __device__ __forceinline__ Dual cst<Dual>(double v) { return dual(v); }
+template <> __device__ __forceinline__ DualD cst<DualD>(double v) { return dual<double>(v); }
+template <> __device__ __forceinline__ DualF cst<DualF>(double v) { return dual<float>((float)v); }
 
 __device__ __forceinline__ double t_exp(double x) { return exp(x); }
-__device__ __forceinline__ Dual t_exp(const Dual& x)
+__device__ __forceinline__ float t_exp_s(float x) { return expf(x); }
+__device__ __forceinline__ double t_exp_s(double x) { return exp(x); }
+template <class S>
+__device__ __forceinline__ DualS<S> t_exp(const DualS<S>& x)
 {
-    Dual r;
-    r.v = exp(x.v);
+    DualS<S> r;
+    r.v = t_exp_s(x.v);
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = r.v * x.d[i];
     return r;
 }
 __device__ __forceinline__ double t_sqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ Dual t_sqrt(const Dual& x)
+template <class S>
+__device__ __forceinline__ DualS<S> t_sqrt(const DualS<S>& x)
 {
-    Dual r;
+    DualS<S> r;
     r.v = sqrt(x.v);
-    const double k = r.v > 0.0 ? 0.5 / r.v : 0.0;
+    const S k = r.v > S(0) ? S(0.5) / r.v : S(0);
 #pragma unroll
     for (int i = 0; i < kNT; ++i) r.d[i] = k * x.d[i];
     return r;
@@ -219,7 +251,7 @@ __device__ __forceinline__ MedT<T> make_med(const upbp_medium& raw, bool seed)
     m.mfp = (st[0] > 0 || st[1] > 0 || st[2] > 0) ? 1.0 / mx : INFINITY;
     m.g = cst<T>((double)raw.mean_cosine);
     m.cont = raw.continuation_prob;
-    if constexpr (std::is_same<T, Dual>::value) {
+    if constexpr (is_dual<T>::value) {
         if (seed) {
             for (int c = 0; c < 3; ++c) {
                 const double sa = raw.absorption[c] < 0.f ? -1.0 : 1.0, ss = raw.scattering[c] < 0.f ? -1.0 : 1.0;

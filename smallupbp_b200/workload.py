@@ -43,6 +43,13 @@ SHORT_BEAM, LONG_BEAM = 1, 2
 BPT, SURF, PP3D, PB2D, BB1D = 4, 8, 16, 32, 64
 BP2D = 65536  # extension: B-P2D (standalone, MIS weight 1); not a reference technique
 NO_SINE_IN_WEIGHTS, PREVIOUS, COMPATIBLE, BB1D_PREVIOUS = 128, 256, 512, 1024
+NO_MIS = 131072  # the estimators without MIS of VolLightTracer's pure -a pb2d / -a bb1d (upbp_gpu.h)
+
+# MIS inputs that the estimators without MIS never read: without_mis() leaves them out, and the C
+# ABI receives them as NULL
+MIS_ONLY_INPUTS = ("lv_mis", "lv_path_idx", "lv_cont_prob", "lv_path_ends", "beam_ray_sample_pdf",
+                   "beam_ray_sample_rev_pdf", "beam_ray_sampling_flags", "beam_last_pdf_w_inv", "beam_light_vertex",
+                   "sq_last_pdf_w_inv", "sq_cam_mis_begin", "cam_mis")
 ORIGIN_IN_MEDIUM, END_IN_MEDIUM = 1, 2
 MIS_IS_DELTA, MIS_ON_LIGHT_SOURCE, MIS_IS_SPECULAR, MIS_IN_MEDIUM_WITH_BEAMS = 1, 2, 4, 8
 LV_IN_MEDIUM, LV_CONNECTABLE, LV_IS_FINITE = 1, 2, 4
@@ -890,3 +897,21 @@ def make(cfg: SceneConfig, iteration: int = 0) -> Dict[str, np.ndarray]:
     if cfg.name == "beamstress":
         return beam_stress(2_000_000, 2_000_000, radius=cfg.radius, seed=cfg.seed + iteration)
     return generate(cfg, iteration)
+
+
+def without_mis(w: Dict[str, np.ndarray], techniques: int = PB2D | BB1D) -> Dict[str, np.ndarray]:
+    """The workload as VolLightTracer's pure algorithms query it (Renderers/VolLightTracer.hxx:296-412):
+    the same photons, beams and camera segments, the estimators without MIS (``NO_MIS`` with PB2D
+    and/or BB1D), no point queries (the reference has no pure PP3D), and the MIS-only arrays left
+    out."""
+    out = {k: v for k, v in w.items() if k not in MIS_ONLY_INPUTS and not k.startswith("pq_")}
+    p = w["params"].copy()
+    p["techniques"] = (int(techniques) & (PB2D | BB1D | BP2D)) | NO_MIS
+    out["params"] = p
+    out["pq_position"] = np.zeros((0, 3), np.float32)
+    out["pq_dir_fix"] = np.zeros((0, 3), np.float32)
+    for k in ("pq_medium_id", "pq_path_length", "pq_pixel"):
+        out[k] = np.zeros(0, np.int32)
+    out["pq_throughput"] = np.zeros((0, 3), np.float32)
+    out["pq_cam_mis_begin"] = np.zeros(0, np.int64)
+    return out

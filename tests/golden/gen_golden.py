@@ -42,6 +42,14 @@ CASES = [
 ]
 # fixtures that keep input digests instead of inputs (regenerated from the config at load time)
 DIGEST_CASES = [("config0_cube128", "cube128", dict())]
+# the estimators without MIS of VolLightTracer's pure -a pb2d / -a bb1d (W.without_mis: the MIS-only
+# inputs are left out, so the C ABI gets NULL for them)
+NOMIS_CASES = [
+    ("cube_nomis_long", "cube32x2048", dict(radius=0.02, seed=41)),
+    ("cube_nomis_short", "cube24x1536", dict(query_beam_type=W.SHORT_BEAM, photon_beam_type=W.SHORT_BEAM,
+                                             radius=0.03, seed=43)),
+    ("boxes_nomis", "boxes", dict(seed=47)),
+]
 
 
 def digest(a: np.ndarray) -> str:
@@ -60,11 +68,13 @@ def scene(name: str, overrides: dict) -> W.SceneConfig:
 
 
 def main(names=None):
-    for fname, cname, over in CASES + DIGEST_CASES:
+    for fname, cname, over in CASES + DIGEST_CASES + NOMIS_CASES:
         if names and fname not in names:
             continue
         cfg = scene(cname, over)
         w = W.generate(cfg)
+        if (fname, cname, over) in NOMIS_CASES:
+            w = W.without_mis(w)
         o = ref.run(w, threads=8)
         if (fname, cname, over) in DIGEST_CASES:
             out = {"cfg_name": np.array(cname), "cfg_iteration": np.array(0)}
@@ -80,7 +90,7 @@ def main(names=None):
         path = os.path.join(HERE, fname + ".npz")
         np.savez_compressed(path, **out)
         print("%-22s lv=%d beams=%d sq=%d pq=%d  cand pb2d=%d bb1d=%d pp3d=%d  %.0f KB" % (
-            fname, len(w["lv_path_idx"]), len(w["beam_length"]), len(w["sq_path_length"]), len(w["pq_path_length"]),
+            fname, len(w["lv_path_length"]), len(w["beam_length"]), len(w["sq_path_length"]), len(w["pq_path_length"]),
             o["count_pb2d"].sum(), o["count_bb1d"].sum(), o["count_pp3d"].sum(), os.path.getsize(path) / 1024))
 
 

@@ -57,7 +57,7 @@ def name(path: str) -> str:
 
 def rel_errors(got: np.ndarray, want: np.ndarray) -> np.ndarray:
     """Per-query max-channel relative error with the absolute floor."""
-    floor = ATOL_FRAC * max(float(np.abs(want).max()), 1e-30)
+    floor = ATOL_FRAC * max(float(np.abs(want).max()) if want.size else 0.0, 1e-30)
     return (np.abs(got - want) / (np.abs(want) + floor)).max(axis=1)
 
 

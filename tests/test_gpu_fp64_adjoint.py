@@ -196,3 +196,49 @@ def test_autograd_function_l2_loss():
                (L(0.1, 0.5, 0.3 + h) - L(0.1, 0.5, 0.3 - h)) / (2 * h))
     for a, f in zip(grads, fds):
         assert abs(a - f) <= 5e-3 * abs(f) + 1e-12, (grads, fds)
+
+
+@pytest.mark.gpu
+def test_adjoint_at_config4_size():
+    # Configuration 4 at full size: the cube at 512x512 with 262,144 light paths, loss = L2 against
+    # the image rendered with sigma_s = 0.7, sigma_a = 0.05, g = 0.5, evaluated at sigma_s = 0.5,
+    # sigma_a = 0.1, g = 0.3.  The adjoint (FP32 tangents, FP64 accumulation, mixed-mode structures)
+    # against central differences (step 1e-3) of the FP64 GPU forward of the same loss.  (The FP64
+    # CPU oracle's gradient is checked at the small size above: its brute-force candidate search
+    # over 512^2 queries would take hours.)
+    import torch
+
+    w = W.make(W.config("diff512"))
+    medium = 1
+    media = np.array(w["media"], copy=True)
+    tgt_media = _with_media(media, medium, np.full(3, 0.05), np.full(3, 0.7), 0.5)
+    with engine.EstimatorStage(0, engine.MODE_FP64) as fd:
+        fd.run(w)
+        fd.set_media(tgt_media)
+        fd.clear_image()
+        fd.evaluate()
+        target = fd.image().astype(np.float64)
+        fd.set_media(media)
+        fd.clear_image()
+        fd.evaluate()
+        img = fd.image().astype(np.float64)
+        grad_img = (2.0 * (img - target)).astype(np.float32)
+
+        def loss(m):
+            fd.set_media(m)
+            fd.clear_image()
+            fd.evaluate()
+            return float(((fd.image().astype(np.float64) - target) ** 2).sum())
+
+        fds = {}
+        for name, t0, mk, sl in _directions(media, medium):
+            h = 1e-3
+            fds[name] = (loss(mk(t0 + h)) - loss(mk(t0 - h))) / (2 * h)
+    with engine.EstimatorStage(0, engine.MODE_MIXED) as st:
+        st.run(w)
+        gi = torch.from_numpy(grad_img.reshape(-1)).cuda()
+        torch.cuda.synchronize()
+        adj = st.adjoint(gi.data_ptr(), medium)
+    for name, t0, mk, sl in _directions(media, medium):
+        assert abs(fds[name]) > 0, name
+        assert abs(adj[sl].sum() - fds[name]) <= RTOL_GRAD * abs(fds[name]), (name, adj[sl].sum(), fds[name])
