@@ -14,6 +14,12 @@ the plain FP32 drop-in (one thread per query), and the mixed stage with B-P2D on
 image rel-L2 against the GPU FP64 mode; and it checks a sample of the queries against the
 reference's own estimators (``parity``).
 
+On one GPU with the default workload the line also carries ``secondary_configs``: short runs of
+configuration 2 (``boxes3``: the fused persistent kernel replayed as a CUDA graph against
+per-estimator launches), configuration 3 (``beamstress``: mixed, plain FP32 and FP64, per-query
+error percentiles against FP64) and configuration 4 (``diff512``: forward and adjoint times, device
+memory, the adjoint against central differences of the FP64 forward).
+
 Multi-GPU: ``--gpus N`` without a launcher starts N ranks itself (torch.distributed.run, one rank
 per GPU, NCCL).  ``--shard queries`` (the default for N > 1): every rank builds the same structures
 over the whole iteration and evaluates its pixel tiles of the queries, and one framebuffer
@@ -76,6 +82,8 @@ def parse():
                     help="multi-GPU work split (default: queries when N > 1)")
     ap.add_argument("--no-arms", action="store_true",
                     help="skip the plain FP32, drop-in and B-P2D comparison arms (one GPU only)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the short runs of the other configurations (boxes3, beamstress, diff512)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of sampled queries against the reference's estimators")
     ap.add_argument("--dropin", action="store_true",
@@ -488,6 +496,10 @@ def run_b200(args, cfg, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(works[0], args.cpu_seconds)
 
+    secondary = None
+    if world == 1 and not args.no_secondary and cfg.name == "cube1024":
+        secondary = run_secondary(dev, stream)
+
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -534,8 +546,135 @@ def run_b200(args, cfg, rank, world, local_rank):
         "accuracy": accuracy,
         "arms": arms,
         "parity": parity,
+        "secondary_configs": secondary,
     }
     return line
+
+
+def run_secondary(dev, stream):
+    """The other benchmark configurations, timed briefly in the same run (3 timed evaluations after a
+    warm-up, CUDA events on the library's stream, the library's default tuning):
+
+    * configuration 2 (`boxes3`, traced on the device): the fused persistent kernel for all camera
+      segments replayed as a CUDA graph against per-estimator launches without a graph, mixed mode;
+    * configuration 3 (`beamstress`): mixed, plain FP32 and FP64 modes, with the per-query relative
+      error of mixed and plain against FP64 (percentiles) and the image rel-L2;
+    * configuration 4 (`diff512`): forward (mixed) and adjoint of the L2 loss against the target
+      medium, their times, the device memory, and the adjoint against central differences (step 1e-3)
+      of the FP64 forward."""
+    import torch
+    from smallupbp_b200 import engine, workload as W
+
+    def timed(st, fn, n=3):
+        with torch.cuda.stream(stream):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(n):
+                fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {}
+    # configuration 2
+    cfg = W.config("boxes3")
+    c2 = {}
+    for name, tun, graph in (("fused_persistent_graph", {"bb1d_kernel": 4}, True),
+                             ("per_estimator_launches", {"bb1d_kernel": 2}, False)):
+        with torch.cuda.stream(stream):
+            st = engine.EstimatorStage(dev, engine.MODE_MIXED)
+            st.set_stream(stream.cuda_stream)
+            st.set_tuning(**tun)
+            st.trace(cfg, 0)
+            st.build(); st.clear_image(); st.evaluate()
+            queries = st.input_bytes("sq_pixel") // 4 + st.input_bytes("pq_pixel") // 4
+            if graph:
+                st.capture_graph()
+                ms = timed(st, st.launch_graph)
+            else:
+                ms = timed(st, lambda: (st.build(), st.clear_image(), st.evaluate()))
+            c2[name] = {"ms_per_iteration": ms, "queries_per_s": queries / (ms / 1000.0), "tuning": tun}
+            st.close()
+    c2["queries_per_iteration"] = int(queries)
+    out["boxes3"] = c2
+    # configuration 3
+    w = W.make(W.config("beamstress"))
+    res = {}
+    for name, mode in (("mixed", engine.MODE_MIXED), ("plain_fp32", engine.MODE_PLAIN), ("fp64", engine.MODE_FP64)):
+        with torch.cuda.stream(stream):
+            st = engine.EstimatorStage(dev, mode)
+            st.set_stream(stream.cuda_stream)
+            st.run(w)
+            ms = timed(st, lambda: (st.clear_image(), st.evaluate()))
+            _, bb1d = st.segment_results()
+            res[name] = {"ms": ms, "bb1d": bb1d.astype(np.float64), "image": st.image().astype(np.float64),
+                         "count": st.query_stats()["count_bb1d"]}
+            st.close()
+    ref = res["fp64"]
+    c3 = {"queries": len(w["sq_path_length"]), "beams": len(w["beam_length"]),
+          "fp64_ms": ref["ms"], "accepted_pairs": int(ref["count"].astype(np.int64).sum())}
+    nz = np.abs(ref["bb1d"]).max(axis=1) > 0
+    for name in ("mixed", "plain_fp32"):
+        r = res[name]
+        err = (np.abs(r["bb1d"] - ref["bb1d"]) / np.maximum(np.abs(ref["bb1d"]), 1e-30)).max(axis=1)[nz]
+        c3[name] = {"ms": r["ms"], "same_candidates": bool(np.array_equal(r["count"], ref["count"])),
+                    "image_rel_l2_vs_fp64": rel_l2(r["image"], ref["image"]),
+                    "per_query_rel_err_vs_fp64": {q: float(np.percentile(err, p)) for q, p in
+                                                  (("p50", 50), ("p99", 99), ("p99.9", 99.9), ("max", 100))}
+                    if err.size else None}
+    out["beamstress"] = c3
+    # configuration 4
+    w = W.make(W.config("diff512"))
+    media = np.array(w["media"], copy=True)
+    medium = 1
+
+    def with_media(sa, ss, g):
+        m = np.array(media, copy=True)
+        m[medium]["absorption"], m[medium]["scattering"], m[medium]["mean_cosine"] = sa, ss, g
+        return m
+
+    with torch.cuda.stream(stream):
+        fd = engine.EstimatorStage(dev, engine.MODE_FP64)
+        fd.set_stream(stream.cuda_stream)
+        fd.run(w)
+
+        def image(m):
+            fd.set_media(m)
+            fd.clear_image()
+            fd.evaluate()
+            return fd.image().astype(np.float64)
+
+        target = image(with_media((0.05,) * 3, (0.7,) * 3, 0.5))
+        base = image(media)
+        grad_img = torch.from_numpy((2.0 * (base - target)).astype(np.float32).reshape(-1)).cuda(dev)
+        st = engine.EstimatorStage(dev, engine.MODE_MIXED)
+        st.set_stream(stream.cuda_stream)
+        st.run(w)
+        torch.cuda.synchronize()
+        fwd_ms = timed(st, lambda: (st.clear_image(), st.evaluate()))
+        adj = st.adjoint(grad_img.data_ptr(), medium)
+        adj_ms = timed(st, lambda: st.adjoint(grad_img.data_ptr(), medium))
+        dev_bytes = st.device_bytes()
+        st.close()
+        m0 = media[medium]
+        sa0, ss0, g0 = float(m0["absorption"][0]), float(m0["scattering"][0]), float(m0["mean_cosine"])
+        h = 1e-3
+        loss = lambda m: float(((image(m) - target) ** 2).sum())
+        fds = {"sigma_a": (loss(with_media((sa0 + h,) * 3, (ss0,) * 3, g0)) -
+                           loss(with_media((sa0 - h,) * 3, (ss0,) * 3, g0))) / (2 * h),
+               "sigma_s": (loss(with_media((sa0,) * 3, (ss0 + h,) * 3, g0)) -
+                           loss(with_media((sa0,) * 3, (ss0 - h,) * 3, g0))) / (2 * h),
+               "g": (loss(with_media((sa0,) * 3, (ss0,) * 3, g0 + h)) - loss(with_media((sa0,) * 3, (ss0,) * 3, g0 - h))) / (2 * h)}
+        fd.close()
+    got = {"sigma_a": float(adj[0:3].sum()), "sigma_s": float(adj[3:6].sum()), "g": float(adj[6])}
+    out["diff512"] = {"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "device_bytes": int(dev_bytes),
+                      "transmittance": "recomputed in the adjoint, not stored",
+                      "grad_adjoint": got, "grad_central_differences_fp64": fds,
+                      "max_rel_err": max(abs(got[k] - fds[k]) / max(abs(fds[k]), 1e-30) for k in got),
+                      "bound": 1e-3}
+    return out
 
 
 def run_arms(args, works, units, dev, stream, img_t, head, res0, img64):

@@ -165,6 +165,12 @@ typedef struct upbp_params {
      * varying linearly along the beam (PhotonBeamsEvaluator::build, PhBeams.cxx:72-123). */
     int32_t pb2d_knn;           /* mPB2DRadiusKNN when mPB2DRadiusCalculation == KNN_RADIUS, else 0 */
     int32_t bb1d_knn;           /* mBB1DRadiusKNN when mBB1DRadiusCalculation == KNN_RADIUS, else 0 */
+    /* How the KNN radii find "the k-th nearest": 0 (default) as the reference does, with its
+     * kd-tree search (KdTreeTmplPtr::KNNQuery, Misc/KdTmpl.hxx), so that the radii equal the
+     * reference's bit for bit; that search is approximate (its heap bound stays unset until k points
+     * are held, the (k+1)-th then replaces the farthest whatever its distance, and its descent treats
+     * the nodes from n/2 - 1 on as leaves).  1: the exact distance to the k-th nearest point. */
+    int32_t knn_exact;
 } upbp_params;
 
 /* Light vertices (mLightVertices): n entries, stored per light path in

@@ -96,3 +96,22 @@ def bp2d(w: Dict[str, np.ndarray], stride: int = 1, fp64: bool = False) -> Dict[
         raise RuntimeError("upbp_oracle_bp2d failed (%d)" % rc)
     del keep
     return out
+
+
+def knn_radii(w: Dict[str, np.ndarray], fp64: bool = False) -> Dict[str, np.ndarray]:
+    """The KNN radii of the oracle's builds for workload ``w`` (``params.knn_exact`` picks the
+    reference's kd-tree search or the exact k-th nearest distance): photon radius^2 per light
+    vertex, beam start and end radius."""
+    s, keep = abi.make_structs(w)
+    l = lib(fp64)
+    l.upbp_oracle_knn_radii.restype = C.c_int
+    l.upbp_oracle_knn_radii.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.LightVertices), C.POINTER(abi.Beams),
+                                        abi.f32p, abi.f32p, abi.f32p]
+    out = {"ph_r2": np.zeros(s["lv"].n, np.float32), "bm_start": np.zeros(s["beams"].n, np.float32),
+           "bm_end": np.zeros(s["beams"].n, np.float32)}
+    rc = l.upbp_oracle_knn_radii(C.byref(s["params"]), C.byref(s["lv"]), C.byref(s["beams"]), abi.ptr(out["ph_r2"]),
+                                 abi.ptr(out["bm_start"]), abi.ptr(out["bm_end"]))
+    if rc != 0:
+        raise RuntimeError("upbp_oracle_knn_radii failed (%d)" % rc)
+    del keep
+    return out

@@ -34,6 +34,7 @@
  * (distances along the rays, closest approach, sin theta) is re-solved in FP64
  * and all contribution and MIS arithmetic is FP64.
  */
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -396,6 +397,198 @@ static float knn_d2(const float* pts, const int64_t* idx, int64_t n, const float
     return nb > 0 ? best[nb - 1] : 0.f;
 }
 
+/* The reference's own search (KdTreeTmplPtr, Misc/KdTmpl.hxx), restated step for step: it is
+ * approximate, and its radii are what the reference renders with.  Jensen's left-balanced kd-tree
+ * in heap order (node i has children 2i and 2i+1), built by recursive median splits along the
+ * longest side of the current box (BuildUp and _balanceSegment, KdTmpl.hxx:321-468) with
+ * Sedgewick's in-place partition (_medianSplit, :354-383); the query walks it with an explicit
+ * stack (KNNQuery, :692-760) and keeps the candidates in a max-heap that is built only once k
+ * points are held (_checkAddNearest, :600-687).  Two properties make it approximate: the heap
+ * bound stays at the initial radius until the heap is built, and the (k+1)-th point then replaces
+ * the largest held one whatever its distance; and the descent treats nodes from n/2 - 1 on as
+ * leaves, so some points are never visited.  The radius the builds use is dist2[1] afterwards:
+ * the heap root, or with at most k points found the first one found. */
+typedef struct {
+    float p[3];
+    int plane;
+} kd_node;
+
+/* _medianSplit: partition a[start..end] along `axis` so that a[median] holds its sorted value */
+static void kd_split(kd_node* a, int start, int end, int median, int axis)
+{
+    int left = start, right = end;
+    while (right > left) {
+        const float v = a[right].p[axis];
+        int i = left - 1, j = right;
+        kd_node t;
+        for (;;) {
+            while (a[++i].p[axis] < v) {
+            }
+            while (a[--j].p[axis] > v && j > left) {
+            }
+            if (i >= j) break;
+            t = a[i]; a[i] = a[j]; a[j] = t;
+        }
+        t = a[i]; a[i] = a[right]; a[right] = t;
+        if (i >= median) right = i - 1;
+        if (i <= median) left = i + 1;
+    }
+}
+
+/* _balanceSegment: node `index` of the balanced tree from org[start..end] in the box lo..hi */
+static void kd_balance(kd_node* bal, kd_node* org, int index, int start, int end, float lo[3], float hi[3])
+{
+    const int n = end - start + 1;
+    int median = 1, axis = 2;
+    while (4 * median <= n) median += median;
+    if (3 * median <= n) median = median + median + start - 1;
+    else median = end - median + 1;
+    if (hi[0] - lo[0] > hi[1] - lo[1] && hi[0] - lo[0] > hi[2] - lo[2]) axis = 0;
+    else if (hi[1] - lo[1] > hi[2] - lo[2]) axis = 1;
+    kd_split(org, start, end, median, axis);
+    bal[index] = org[median];
+    bal[index].plane = axis;
+    if (median > start) {
+        if (start < median - 1) {
+            const float keep = hi[axis];
+            hi[axis] = bal[index].p[axis];
+            kd_balance(bal, org, 2 * index, start, median - 1, lo, hi);
+            hi[axis] = keep;
+        } else {
+            bal[2 * index] = org[start];
+        }
+    }
+    if (median < end) {
+        if (median + 1 < end) {
+            const float keep = lo[axis];
+            lo[axis] = bal[index].p[axis];
+            kd_balance(bal, org, 2 * index + 1, median + 1, end, lo, hi);
+            lo[axis] = keep;
+        } else {
+            bal[2 * index + 1] = org[end];
+        }
+    }
+}
+
+/* AddItem + BuildUp over pts[idx[i]] (idx NULL: pts[i]) in that order; returns the tree, node 1
+ * the root, or NULL on allocation failure */
+static kd_node* kd_build(const float* pts, const int64_t* idx, int64_t n)
+{
+    kd_node* org = (kd_node*)malloc(sizeof(kd_node) * (size_t)(n + 1));
+    kd_node* bal = (kd_node*)malloc(sizeof(kd_node) * (size_t)(n + 1));
+    float lo[3] = {1e18f, 1e18f, 1e18f}, hi[3] = {-1e18f, -1e18f, -1e18f};
+    int64_t i;
+    int a;
+    if (!org || !bal) { free(org); free(bal); return NULL; }
+    memset(org, 0, sizeof(kd_node) * (size_t)(n + 1));
+    for (i = 0; i < n; ++i) {
+        const float* p = pts + 3 * (idx ? idx[i] : i);
+        for (a = 0; a < 3; ++a) {
+            org[i + 1].p[a] = p[a];
+            if (p[a] < lo[a]) lo[a] = p[a];
+            if (p[a] > hi[a]) hi[a] = p[a];
+        }
+    }
+    if (n > 1) {
+        memset(bal, 0, sizeof(kd_node) * (size_t)(n + 1));
+        kd_balance(bal, org, 1, 1, (int)n, lo, hi);
+        free(org);
+        return bal;
+    }
+    free(bal);
+    return org;
+}
+
+/* _checkAddNearest for one node */
+static void kd_add(const kd_node* p, const float* q, float* heap, int k, int* found, int* got_heap, float* maxd)
+{
+    float d1 = p->p[0] - q[0];
+    float d2 = d1 * d1;
+    d1 = p->p[1] - q[1];
+    d2 += d1 * d1;
+    d1 = p->p[2] - q[2];
+    d2 += d1 * d1;
+    if (!(d2 < heap[0])) return;
+    if (*found < k) {
+        heap[++*found] = d2;
+        if (*maxd < d2) *maxd = d2;
+        return;
+    }
+    if (!*got_heap) { /* heapify heap[1..found] (largest at 1) */
+        const int half = *found >> 1;
+        int kk;
+        for (kk = half; kk >= 1; --kk) {
+            int parent = kk, j;
+            const float v = heap[kk];
+            while (parent <= half) {
+                j = parent + parent;
+                if (j < *found && heap[j] < heap[j + 1]) ++j;
+                if (v >= heap[j]) break;
+                heap[parent] = heap[j];
+                parent = j;
+            }
+            heap[parent] = v;
+        }
+        *got_heap = 1;
+    }
+    {   /* the root leaves, d2 sinks from the top */
+        int parent = 1, j = 2;
+        while (j <= *found) {
+            if (j < *found && heap[j] < heap[j + 1]) ++j;
+            if (d2 > heap[j]) break;
+            heap[parent] = heap[j];
+            parent = j;
+            j += j;
+        }
+        heap[parent] = d2;
+        heap[0] = *maxd = heap[1];
+    }
+}
+
+/* KNNQuery with the initial radius sqrt(FLT_MAX) of the builds (Bre.cxx:44, PhBeams.cxx:48); returns
+ * dist2[1] */
+static float kd_knn_d2(const kd_node* t, int64_t n, const float* q, int k)
+{
+    float heap[257];
+    struct { int index; float d2; } stack[64];
+    const int half = (int)(n / 2 - 1);
+    const float r0 = sqrtf(FLT_MAX);
+    int found = 0, got_heap = 0, level = 0, index = 1, camefrom;
+    float maxd = 0.0f;
+    if (k > 256) k = 256;
+    heap[0] = r0 * r0;
+    heap[1] = 0.0f;
+    if (n < 1) return 0.0f;
+    for (;;) {
+        while (index < half) {
+            const kd_node* p = &t[index];
+            const float d1 = q[p->plane] - p->p[p->plane];
+            index *= 2;
+            if (d1 > 0.0f) ++index;
+            stack[level].index = index;
+            stack[level].d2 = d1 * d1;
+            ++level;
+        }
+        kd_add(&t[index], q, heap, k, &found, &got_heap, &maxd);
+        do {
+            camefrom = index;
+            index /= 2;
+            --level;
+            if (index == 0) return heap[1];
+        } while (stack[level].d2 >= heap[0] || camefrom != stack[level].index);
+        kd_add(&t[index], q, heap, k, &found, &got_heap, &maxd);
+        index = stack[level].index ^ 1;
+        ++level;
+    }
+}
+
+/* The k-NN distance the radius builds use: the reference's search, or (exact) the k-th smallest */
+static float knn_dist2(const kd_node* tree, const float* pts, const int64_t* idx, int64_t n, const float* q, int k,
+                       int exact)
+{
+    return exact ? knn_d2(pts, idx, n, q, k) : kd_knn_d2(tree, n, q, k);
+}
+
 /* Radii given from outside instead of the KNN search (tests inject the radii the reference's own
  * builds produced, so that everything but the search is compared with the reference).  Per light
  * vertex photon radius^2; per beam start and end radius.  NULL pointers: compute by KNN. */
@@ -453,7 +646,7 @@ static int reach_ok(v3f O1, v3f d1, float dminf, float dmaxf, v3f O2, v3f d2, fl
 
 /* EmbreeBre::build with KNN_RADIUS (Bre.cxx:685-725): radius = r * (2 * sqrt(d2_k)) over the
  * photons (light vertices in media); EmbreePhoton::set keeps radius * radius. */
-static float* knn_photon_r2(const upbp_light_vertices* lv, float r, int k)
+static float* knn_photon_r2(const upbp_light_vertices* lv, float r, int k, int exact)
 {
     int64_t i, n = 0;
     int64_t* idx = (int64_t*)malloc(sizeof(int64_t) * (size_t)(lv->n > 0 ? lv->n : 1));
@@ -461,11 +654,17 @@ static float* knn_photon_r2(const upbp_light_vertices* lv, float r, int k)
     if (!idx || !r2) { free(idx); free(r2); return NULL; }
     for (i = 0; i < lv->n; ++i)
         if (lv->flags[i] & UPBP_LV_IN_MEDIUM) idx[n++] = i;
+    {
+        kd_node* tree = exact ? NULL : kd_build(lv->position, idx, n);
+        if (!exact && !tree && n > 0) { free(idx); free(r2); return NULL; }
 #pragma omp parallel for schedule(dynamic, 64)
-    for (i = 0; i < n; ++i) {
-        const int64_t j = idx[i];
-        const float radius = r * (2.0f * sqrtf(knn_d2(lv->position, idx, n, lv->position + 3 * j, k)));
-        r2[j] = radius * radius;
+        for (i = 0; i < n; ++i) {
+            const int64_t j = idx[i];
+            const float radius =
+                r * (2.0f * sqrtf(knn_dist2(tree, lv->position, idx, n, lv->position + 3 * j, k, exact)));
+            r2[j] = radius * radius;
+        }
+        free(tree);
     }
     free(idx);
     return r2;
@@ -473,21 +672,24 @@ static float* knn_photon_r2(const upbp_light_vertices* lv, float r, int k)
 
 /* PhotonBeamsEvaluator::build with KNN_RADIUS (PhBeams.cxx:77-123): start / end radius from the
  * k-th nearest beam origin to the beam's origin / end, max(2 * sqrt(d2_k) * r, 0.001). */
-static int knn_beam_radii(const upbp_beams* bm, float r, int k, float** start, float** change, float** r2)
+static int knn_beam_radii(const upbp_beams* bm, float r, int k, int exact, float** start, float** change, float** r2,
+                          float* end_out)
 {
     int64_t b;
+    kd_node* tree = NULL;
     *start = (float*)malloc(sizeof(float) * (size_t)(bm->n > 0 ? bm->n : 1));
     *change = (float*)malloc(sizeof(float) * (size_t)(bm->n > 0 ? bm->n : 1));
     *r2 = (float*)malloc(sizeof(float) * (size_t)(bm->n > 0 ? bm->n : 1));
     if (!*start || !*change || !*r2) return -1;
+    if (!exact && bm->n > 0 && !(tree = kd_build(bm->origin, NULL, bm->n))) return -1;
 #pragma omp parallel for schedule(dynamic, 64)
     for (b = 0; b < bm->n; ++b) {
         const float* o = bm->origin + 3 * b;
         const float* d = bm->direction + 3 * b;
         const float len = bm->length[b];
         const float end[3] = {o[0] + d[0] * len, o[1] + d[1] * len, o[2] + d[2] * len};
-        float rs = 2.0f * sqrtf(knn_d2(bm->origin, NULL, bm->n, o, k)) * r;
-        float re = 2.0f * sqrtf(knn_d2(bm->origin, NULL, bm->n, end, k)) * r;
+        float rs = 2.0f * sqrtf(knn_dist2(tree, bm->origin, NULL, bm->n, o, k, exact)) * r;
+        float re = 2.0f * sqrtf(knn_dist2(tree, bm->origin, NULL, bm->n, end, k, exact)) * r;
         float mx;
         rs = rs > 0.001f ? rs : 0.001f;
         re = re > 0.001f ? re : 0.001f;
@@ -495,7 +697,9 @@ static int knn_beam_radii(const upbp_beams* bm, float r, int k, float** start, f
         (*start)[b] = rs;
         (*r2)[b] = mx * mx;
         (*change)[b] = (re - rs) / len;
+        if (end_out) end_out[b] = re;
     }
+    free(tree);
     return 0;
 }
 
@@ -888,6 +1092,30 @@ static rgb pp3d_query(const oracle* O, const hashgrid* g, const upbp_point_queri
     return res;
 }
 
+/* The KNN radii the oracle's builds use (params.knn_exact picks the search): photon radius^2 per
+ * light vertex (0 off the media), beam start and end radius (mStartRadius, mEndRadius).  Any
+ * output may be NULL. */
+int upbp_oracle_knn_radii(const upbp_params* P, const upbp_light_vertices* lv, const upbp_beams* bm, float* ph_r2,
+                          float* bm_start, float* bm_end)
+{
+    if (!P) return -1;
+    if (ph_r2 && lv && P->pb2d_knn > 0) {
+        float* r2 = knn_photon_r2(lv, P->radius_pb2d, P->pb2d_knn, P->knn_exact);
+        if (!r2) return -1;
+        memcpy(ph_r2, r2, sizeof(float) * (size_t)lv->n);
+        free(r2);
+    }
+    if ((bm_start || bm_end) && bm && P->bb1d_knn > 0) {
+        float *rs = NULL, *rc = NULL, *r2 = NULL;
+        int64_t b;
+        if (knn_beam_radii(bm, P->radius_bb1d, P->bb1d_knn, P->knn_exact, &rs, &rc, &r2, bm_end) != 0) return -1;
+        for (b = 0; b < bm->n; ++b)
+            if (bm_start) bm_start[b] = rs[b];
+        free(rs); free(rc); free(r2);
+    }
+    return 0;
+}
+
 /* ---------------------------------------------------------------- entry point */
 /*
  * Evaluate queries with index % stride == 0.  Any output pointer may be NULL.
@@ -914,12 +1142,13 @@ int upbp_oracle_run(const upbp_params* P, const upbp_medium* media, int32_t n_me
     O.cam = cam;
     O.has_beams = (P->techniques & UPBP_BB1D) && bm && bm->n > 0;
     if (P->pb2d_knn > 0 && (P->techniques & UPBP_PB2D)) {
-        O.ph_r2 = knn_photon_r2(lv, P->radius_pb2d, P->pb2d_knn);
+        O.ph_r2 = knn_photon_r2(lv, P->radius_pb2d, P->pb2d_knn, P->knn_exact);
         if (!O.ph_r2) return -1;
         if (g_ph_r2) memcpy(O.ph_r2, g_ph_r2, sizeof(float) * (size_t)lv->n);
     }
     if (P->bb1d_knn > 0 && O.has_beams) {
-        if (knn_beam_radii(bm, P->radius_bb1d, P->bb1d_knn, &O.bm_start, &O.bm_change, &O.bm_r2) != 0) return -1;
+        if (knn_beam_radii(bm, P->radius_bb1d, P->bb1d_knn, P->knn_exact, &O.bm_start, &O.bm_change, &O.bm_r2, NULL) != 0)
+            return -1;
         if (g_bm_start && g_bm_end) {
             int64_t b;
             for (b = 0; b < bm->n; ++b) {  /* PhBeams.cxx:117-121 from the given start / end */
@@ -1029,7 +1258,8 @@ int upbp_oracle_bp2d(const upbp_params* P, const upbp_medium* media, int32_t n_m
     float *bs = NULL, *bc = NULL, *br2 = NULL; /* KNN beam radii */
     if (!P || !media || n_media <= 0 || n_media > ORACLE_MAX_MEDIA || !bm || !pq || stride < 1) return -1;
     for (i = 0; i < n_media; ++i) M[i] = make_medium(&media[i]);
-    if (P->bb1d_knn > 0 && (P->techniques & UPBP_BP2D) && knn_beam_radii(bm, P->radius_bb1d, P->bb1d_knn, &bs, &bc, &br2))
+    if (P->bb1d_knn > 0 && (P->techniques & UPBP_BP2D) &&
+        knn_beam_radii(bm, P->radius_bb1d, P->bb1d_knn, P->knn_exact, &bs, &bc, &br2, NULL))
         return -1;
 #pragma omp parallel for schedule(dynamic, 8)
     for (q = 0; q < pq->n; q += stride) {

@@ -11,6 +11,8 @@
 #include <vector>
 
 #include "upbp_generic_api.cuh"
+#include "upbp_kdtree.cuh"
+#include "upbp_kdtree.cuh"
 #include "upbp_kernels.cuh"
 #include "upbp_mis_prep.cuh"
 #include "upbp_trace.cuh"
@@ -89,6 +91,9 @@ struct upbp_ctx {
     // KNN radii: per-photon radius^2 (leaf order); per-beam radius change and max radius^2 (the
     // start radius goes to bm_radius); the LBVH over beam origins for the beam KNN search
     DBuf pb_r2, bm_rchange, bm_r2max, knn_status;
+    // the reference's kd-tree search for the KNN radii (knn_exact = 0): working array, tree, node
+    // boxes, partition scratch
+    DBuf kd_org, kd_tree, kd_boxes, kd_pa, kd_pb;
     DBuf bo_pos, bo_pts, bo_codes, bo_codes_sorted, bo_idx, bo_idx_sorted, bo_bbox, bo_leaf_codes, bo_nodes,
         bo_parent_int, bo_parent_leaf, bo_leaf_boxes, bo_node_boxes, bo_flags;
     int bo_n_leaves = 0;
@@ -294,6 +299,20 @@ void build_lbvh(upbp_ctx* c, const uint32_t* codes_sorted, int n, int leaf, DBuf
     c->build_launches += 3;
 }
 
+// The reference's kd-tree over n points pos[idx[i]] in that order (launch_kd_build) in the context's
+// kd buffers; bbox = the points' bounding box on the device.
+void build_kd_tree(upbp_ctx* c, const float4* pos, const int32_t* idx, int n, const float* bbox)
+{
+    ensure(c, c->kd_org, sizeof(float4) * (n + 1));
+    ensure(c, c->kd_tree, sizeof(float4) * (n + 1));
+    ensure(c, c->kd_boxes, sizeof(float) * 6 * (n + 1));
+    ensure(c, c->kd_pa, sizeof(int) * (n + 1));
+    ensure(c, c->kd_pb, sizeof(int) * (n + 1));
+    launch_kd_build(pos, idx, n, bbox, c->kd_org.as<float4>(), c->kd_tree.as<float4>(), c->kd_boxes.as<float>(),
+                    c->kd_pa.as<int>(), c->kd_pb.as<int>(), c->stream);
+    c->build_launches += kd_build_launches(n);
+}
+
 void do_build(upbp_ctx* c)
 {
     if (!c->have_params) fail(c, UPBP_ERR_INVALID_ARG, "upbp_set_params was not called");
@@ -413,8 +432,16 @@ void do_build(upbp_ctx* c)
             // KNN photon radii over the LBVH just built (its boxes hold the points), then refit
             // the boxes to the per-photon spheres
             ensure(c, c->pb_r2, sizeof(float) * nph);
-            launch_photon_knn_r2(c->pb_pos.as<float4>(), nph, c->pb_nodes.as<BNode>(), c->pb_n_leaves, leaf, P.pb2d_knn,
-                                 P.radius_pb2d, c->pb_r2.as<float>(), c->knn_status.as<int>(), s);
+            if (P.knn_exact) {
+                launch_photon_knn_r2(c->pb_pos.as<float4>(), nph, c->pb_nodes.as<BNode>(), c->pb_n_leaves, leaf,
+                                     P.pb2d_knn, P.radius_pb2d, c->pb_r2.as<float>(), c->knn_status.as<int>(), s);
+            } else {
+                // the reference's search over the photons in light-vertex order (EmbreeBre::build,
+                // Bre.cxx:685-699), queried at every photon of the LBVH
+                build_kd_tree(c, c->lv_pos4.as<float4>(), c->ph_lv.as<int32_t>(), nph, c->bbox_ph.as<float>());
+                launch_kd_photon_r2(c->kd_tree.as<float4>(), nph, c->pb_pos.as<float4>(), nph, P.pb2d_knn,
+                                    P.radius_pb2d, c->pb_r2.as<float>(), s);
+            }
             launch_photon_leaf_boxes_r2(c->pb_pos.as<float4>(), c->pb_r2.as<float>(), nph, leaf, 1e-5f,
                                         c->pb_leaf_boxes.as<Box>(), s);
             const int ni = std::max(1, c->pb_n_leaves - 1);
@@ -443,7 +470,7 @@ void do_build(upbp_ctx* c)
         const float* rchange = nullptr;
         const float* r2max = nullptr;
         if (P.bb1d_knn > 0) {
-            // KNN beam radii: an LBVH over the beam origins, two queries per beam
+            // KNN beam radii from the beam origins
             const int n = (int)nb;
             ensure(c, c->bo_pos, sizeof(float4) * n);
             ensure(c, c->bo_pts, sizeof(float4) * n);
@@ -460,26 +487,36 @@ void do_build(upbp_ctx* c)
             float* part = reinterpret_cast<float*>(c->bbox_partial.as<int32_t>() + 8);
             launch_bbox_partial(c->bo_pos.as<float4>(), nullptr, n, part, ob, s);
             launch_bbox_final(part, ob, c->bo_bbox.as<float>(), s);
-            k_iota<<<(n + 255) / 256, 256, 0, s>>>(c->bo_idx.as<int32_t>(), n);
-            launch_morton_points(c->bo_pos.as<float4>(), c->bo_idx.as<int32_t>(), n, c->bo_bbox.as<float>(),
-                                 c->bo_codes.as<uint32_t>(), s);
-            sort_pairs(c, c->bo_codes.as<uint32_t>(), c->bo_codes_sorted.as<uint32_t>(), c->bo_idx.as<int32_t>(),
-                       c->bo_idx_sorted.as<int32_t>(), n, 30);
-            launch_gather_photons(c->bo_idx_sorted.as<int32_t>(), c->bo_pos.as<float4>(), n, c->bo_pts.as<float4>(),
-                                  s);
-            constexpr int kOriginLeaf = 4;
-            ensure(c, c->bo_leaf_boxes, sizeof(Box) * ((n + kOriginLeaf - 1) / kOriginLeaf));
-            launch_photon_leaf_boxes(c->bo_pts.as<float4>(), n, kOriginLeaf, 0.f, 1e-6f, c->bo_leaf_boxes.as<Box>(), s);
-            build_lbvh(c, c->bo_codes_sorted.as<uint32_t>(), n, kOriginLeaf, c->bo_leaf_codes, c->bo_nodes,
-                       c->bo_parent_int, c->bo_parent_leaf, c->bo_leaf_boxes, c->bo_node_boxes, c->bo_flags,
-                       c->bo_n_leaves);
-            launch_beam_knn(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(), n,
-                            c->bo_nodes.as<BNode>(), c->bo_n_leaves, c->bo_pts.as<float4>(), kOriginLeaf, P.bb1d_knn,
-                            r, c->bm_radius.as<float>(), c->bm_rchange.as<float>(), c->bm_r2max.as<float>(),
-                            c->knn_status.as<int>(), s);
+            c->build_launches += 3;
+            if (!P.knn_exact) {
+                // the reference's search over the beam origins in beam order (PhBeams.cxx:80-91)
+                build_kd_tree(c, c->bo_pos.as<float4>(), nullptr, n, c->bo_bbox.as<float>());
+                launch_kd_beam_radii(c->kd_tree.as<float4>(), n, c->b_origin.as<float>(), c->b_dir.as<float>(),
+                                     c->b_len.as<float>(), n, P.bb1d_knn, r, c->bm_radius.as<float>(),
+                                     c->bm_rchange.as<float>(), c->bm_r2max.as<float>(), s);
+                c->build_launches += 1;
+            } else {  // the exact search: an LBVH over the beam origins, two queries per beam
+                k_iota<<<(n + 255) / 256, 256, 0, s>>>(c->bo_idx.as<int32_t>(), n);
+                launch_morton_points(c->bo_pos.as<float4>(), c->bo_idx.as<int32_t>(), n, c->bo_bbox.as<float>(),
+                                     c->bo_codes.as<uint32_t>(), s);
+                sort_pairs(c, c->bo_codes.as<uint32_t>(), c->bo_codes_sorted.as<uint32_t>(), c->bo_idx.as<int32_t>(),
+                           c->bo_idx_sorted.as<int32_t>(), n, 30);
+                launch_gather_photons(c->bo_idx_sorted.as<int32_t>(), c->bo_pos.as<float4>(), n, c->bo_pts.as<float4>(),
+                                      s);
+                constexpr int kOriginLeaf = 4;
+                ensure(c, c->bo_leaf_boxes, sizeof(Box) * ((n + kOriginLeaf - 1) / kOriginLeaf));
+                launch_photon_leaf_boxes(c->bo_pts.as<float4>(), n, kOriginLeaf, 0.f, 1e-6f, c->bo_leaf_boxes.as<Box>(), s);
+                build_lbvh(c, c->bo_codes_sorted.as<uint32_t>(), n, kOriginLeaf, c->bo_leaf_codes, c->bo_nodes,
+                           c->bo_parent_int, c->bo_parent_leaf, c->bo_leaf_boxes, c->bo_node_boxes, c->bo_flags,
+                           c->bo_n_leaves);
+                launch_beam_knn(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(), n,
+                                c->bo_nodes.as<BNode>(), c->bo_n_leaves, c->bo_pts.as<float4>(), kOriginLeaf, P.bb1d_knn,
+                                r, c->bm_radius.as<float>(), c->bm_rchange.as<float>(), c->bm_r2max.as<float>(),
+                                c->knn_status.as<int>(), s);
+                c->build_launches += 9;
+            }
             rchange = c->bm_rchange.as<float>();
             r2max = c->bm_r2max.as<float>();
-            c->build_launches += 12;
         }
         const float piece_len = std::max(1e-6f, c->piece_len_r * r);
         ensure(c, c->bm_counts, sizeof(int32_t) * (nb + 1));
@@ -662,6 +699,9 @@ BeamBVH beam_bvh(upbp_ctx* c)
     B.pay = c->mode != UPBP_MODE_PLAIN ? c->pc_pay.as<PiecePayload>() : nullptr;
     B.leaf = std::max(1, c->bb1d_leaf);
     B.n_leaves = c->bm_n_leaves;
+    // k_emit_sorted writes the piece window into pb.w when every beam has the radius radius_bb1d
+    B.window = c->P.bb1d_knn > 0 ? 0 : 1;
+    B.r2c = c->P.radius_bb1d * c->P.radius_bb1d;
     return B;
 }
 
@@ -989,7 +1029,8 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->hash_pb2d, &c->hash_bb1d, &c->hash_pp3d, &c->tested, &c->light_sums, &c->cam_sums_seg,
                    &c->cam_sums_pt, &c->work, &c->status, &c->pc_pay, &c->q_keys, &c->q_keys_sorted, &c->q_iota,
                    &c->q_order, &c->grad_img, &c->grad_acc, &c->out_bp2d, &c->cnt_bp2d, &c->hash_bp2d,
-                   &c->pb_r2, &c->bm_rchange, &c->bm_r2max, &c->knn_status, &c->bo_pos, &c->bo_pts, &c->bo_codes,
+                   &c->pb_r2, &c->bm_rchange, &c->bm_r2max, &c->knn_status, &c->kd_org, &c->kd_tree,
+                   &c->kd_boxes, &c->kd_pa, &c->kd_pb, &c->bo_pos, &c->bo_pts, &c->bo_codes,
                    &c->bo_codes_sorted, &c->bo_idx, &c->bo_idx_sorted, &c->bo_bbox, &c->bo_leaf_codes, &c->bo_nodes,
                    &c->bo_parent_int, &c->bo_parent_leaf, &c->bo_leaf_boxes, &c->bo_node_boxes, &c->bo_flags,
                    &c->tr_cnt, &c->tr_off, &c->tr_status, &c->bb_keys, &c->bb_keys_sorted, &c->bb_iota,

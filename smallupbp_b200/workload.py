@@ -75,7 +75,7 @@ PARAMS_FIELDS = (
     ("norm_pp3d", "<f4"), ("norm_pb2d", "<f4"), ("norm_bb1d", "<f4"),
     ("bb1d_min_mfp", "<f4"), ("min_dist_to_med", "<f4"),
     ("hash_cells", "<i4"), ("image_width", "<i4"), ("image_height", "<i4"),
-    ("pb2d_knn", "<i4"), ("bb1d_knn", "<i4"),
+    ("pb2d_knn", "<i4"), ("bb1d_knn", "<i4"), ("knn_exact", "<i4"),
 )
 PARAMS_DTYPE = np.dtype(list(PARAMS_FIELDS))
 

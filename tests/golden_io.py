@@ -78,26 +78,7 @@ def uses_knn(w: Dict[str, np.ndarray]) -> bool:
     return int(p["pb2d_knn"][0]) > 0 or int(p["bb1d_knn"][0]) > 0
 
 
-# The reference's KNN radius (KdTree::KNNQuery) starts filling its max-heap without updating the
-# heap bound, so the (k+1)-th point its kd-tree visits always replaces the heap maximum: the radius
-# is the k-th smallest distance with the largest of the first k visited points left out, which
-# depends on the kd-tree layout.  The CUDA path and the oracle use the exact k-th nearest
-# distance; on KNN fixtures they may differ from the reference on this fraction of queries.
-KNN_MISMATCH_FRACTION = 0.02
-
-
 def expected(path: str) -> Tuple[Dict[str, np.ndarray], Dict[str, np.ndarray]]:
-    """Workload and the outputs the CUDA path must reproduce: the reference's for constant radii,
-    the oracle's (exact k-th nearest distance) for KNN radii."""
-    w, r = load(path)
-    if not uses_knn(w):
-        return w, r
-    from oracle import port
-
-    o = port.run(w)
-    r = dict(r)
-    for k in ("pb2d", "pp3d", "count_pb2d", "hash_pb2d", "count_bb1d", "hash_bb1d", "count_pp3d", "hash_pp3d",
-              "image"):
-        r[k] = o[k]
-    r["bb1d"] = r["bb1d_brute"] = o["bb1d"]
-    return w, r
+    """Workload and the outputs the CUDA path must reproduce: the reference's own (with KNN radii
+    too: the default search is the reference's kd-tree search, knn_exact = 0)."""
+    return load(path)

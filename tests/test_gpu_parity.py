@@ -125,11 +125,14 @@ def test_pb2d_kernel_variants_same_candidates(stage, pb2d_kernel, path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("knn_exact", [0, 1], ids=["reference_search", "exact"])
 @pytest.mark.parametrize("mode", [engine.MODE_PLAIN, engine.MODE_MIXED], ids=["plain", "mixed"])
-def test_knn_radii_bit_exact_with_exact_knn_oracle(stage, mode):
-    # KNN radii at a size where photons and beam origins span many LBVH leaves: the CUDA KNN
-    # search must find the exact k-th nearest distance the oracle computes, so candidate sets
-    # match bit for bit (PB2D, BB1D and B-P2D).
+def test_knn_radii_bit_exact_with_the_oracle(stage, mode, knn_exact):
+    # KNN radii at a size where photons and beam origins span many tree levels: with knn_exact = 0
+    # the CUDA kd-tree search must return what the reference's search returns (the oracle's
+    # restatement of it is pinned to the reference's own radii), with knn_exact = 1 the exact k-th
+    # nearest distance; either way the candidate sets match the oracle's bit for bit (PB2D, BB1D and
+    # B-P2D).
     from oracle import port
     from smallupbp_b200 import workload as W
 
@@ -137,6 +140,7 @@ def test_knn_radii_bit_exact_with_exact_knn_oracle(stage, mode):
     cfg.radius, cfg.pb2d_knn, cfg.bb1d_knn = 0.3, 10, 7
     w = W.generate(cfg)
     w["params"]["techniques"] |= W.BP2D
+    w["params"]["knn_exact"] = knn_exact
     o = port.run(w)
     ob = port.bp2d(w)
     g = run(stage, w, mode)
@@ -150,3 +154,25 @@ def test_knn_radii_bit_exact_with_exact_knn_oracle(stage, mode):
     np.testing.assert_array_equal(cnt, ob["count_bp2d"])
     np.testing.assert_array_equal(h, ob["hash_bp2d"])
     assert G.image_rel_l2(g["image"], o["image"] + ob["image"]) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_knn_reference_search_at_cube512(stage):
+    # The reference's KNN search on 10^5-point sets: the top levels of the kd-tree are partitioned
+    # block-parallel (segments of more than 4096 points), the rest one thread per segment.  A sample of
+    # the queries (every 97th) must see the oracle's candidate sets, which follow the reference's radii.
+    from oracle import port
+    from smallupbp_b200 import workload as W
+
+    cfg = W.config("cube512")
+    cfg.pb2d_knn, cfg.bb1d_knn = 12, 8
+    w = W.generate(cfg)
+    assert int((w["lv_flags"] & 1).sum()) > 50_000 and len(w["beam_length"]) > 50_000
+    o = port.run(w, stride=97)
+    g = run(stage, w, engine.MODE_MIXED)
+    q = np.arange(0, len(g["count_bb1d"]), 97)
+    for est in ("pb2d", "bb1d"):
+        np.testing.assert_array_equal(g["count_" + est][q], o["count_" + est][q], err_msg=est)
+        np.testing.assert_array_equal(g["hash_" + est][q], o["hash_" + est][q], err_msg=est)
+    qp = np.arange(0, len(g["count_pp3d"]), 97)
+    np.testing.assert_array_equal(g["hash_pp3d"][qp], o["hash_pp3d"][qp])

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import golden_io as G
-from oracle import port
+from oracle import port, ref
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -15,16 +15,10 @@ def built():
         build_oracle.build()
 
 
-def _ref_radii(w, r):
-    """For KNN fixtures, the radii the reference's own KNN search produced (stored in the fixture):
-    with them injected, everything but the search itself is compared with the reference."""
-    return (r["ph_r2"], r["bm_start"], r["bm_end"]) if G.uses_knn(w) else None
-
-
 @pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
 def test_oracle_candidate_sets_match_reference(path):
     w, r = G.load(path)
-    o = port.run(w, radii=_ref_radii(w, r))
+    o = port.run(w)
     for est in ("pb2d", "bb1d", "pp3d"):
         np.testing.assert_array_equal(o["count_" + est], r["count_" + est], err_msg=est)
         np.testing.assert_array_equal(o["hash_" + est], r["hash_" + est], err_msg=est)
@@ -33,7 +27,7 @@ def test_oracle_candidate_sets_match_reference(path):
 @pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
 def test_oracle_contributions_match_reference(path):
     w, r = G.load(path)
-    o = port.run(w, radii=_ref_radii(w, r))
+    o = port.run(w)
     G.assert_close(o["pb2d"], r["pb2d"], "PB2D")
     G.assert_close(o["bb1d"], r["bb1d_brute"], "BB1D")
     G.assert_close(o["pp3d"], r["pp3d"], "PP3D")
@@ -46,35 +40,53 @@ def _knn_d2(pts, q, k):
 
 
 @pytest.mark.parametrize("path", [p for p in G.FIXTURES if "knn" in p], ids=G.name)
-def test_knn_radii_against_the_reference_search(path):
-    """The exact k-th nearest distance (the oracle's and the CUDA path's KNN radius) against the
-    radius the reference's kd-tree search produced.  The reference's search is approximate: its
-    heap starts without a bound (the (k+1)-th visited point always evicts the current maximum) and
-    its descent stops at index < N/2 - 1, so it can miss near points and return a larger radius,
-    never a smaller one."""
+def test_knn_radii_equal_the_reference_search(path):
+    """With knn_exact = 0 (the default) the oracle's KNN radii are the ones the reference's own
+    kd-tree search produced (stored in the fixture), bit for bit.  The exact k-th nearest distance
+    (knn_exact = 1) never gives a larger radius: the reference's search is approximate (its heap
+    bound starts unset, so the (k+1)-th visited point evicts the farthest held one, and its descent
+    stops at index < n/2 - 1), so it can miss near points."""
     w, r = G.load(path)
+    inm = np.nonzero(w["lv_flags"] & 1)[0]
+    o = port.knn_radii(w)
+    np.testing.assert_array_equal(o["ph_r2"][inm], r["ph_r2"][inm])
+    np.testing.assert_array_equal(o["bm_start"], r["bm_start"])
+    np.testing.assert_array_equal(o["bm_end"], r["bm_end"])
+    we = dict(w)
+    we["params"] = w["params"].copy()
+    we["params"]["knn_exact"] = 1
+    e = port.knn_radii(we)
     f = np.float32
     p = w["params"]
-    k1, k2 = int(p["pb2d_knn"][0]), int(p["bb1d_knn"][0])
-    inm = np.nonzero(w["lv_flags"] & 1)[0]
+    k1 = int(p["pb2d_knn"][0])
     pos = w["lv_position"]
     exact = np.zeros(len(pos), f)
     for j in inm:
         rad = f(p["radius_pb2d"][0]) * (f(2.0) * np.sqrt(_knn_d2(pos[inm], pos[j], k1)))
         exact[j] = rad * rad
-    assert (r["ph_r2"][inm] >= exact[inm]).all()
-    assert (r["ph_r2"][inm] == exact[inm]).mean() >= 0.95
-    o, d, ln = w["beam_origin"], w["beam_direction"], w["beam_length"]
-    rb = f(p["radius_bb1d"][0])
-    start = np.array([max(f(2.0) * np.sqrt(_knn_d2(o, o[b], k2)) * rb, f(0.001)) for b in range(len(o))], f)
-    end = np.array([max(f(2.0) * np.sqrt(_knn_d2(o, o[b] + d[b] * ln[b], k2)) * rb, f(0.001)) for b in range(len(o))], f)
-    assert (r["bm_start"] >= start).all() and (r["bm_end"] >= end).all()
-    assert (r["bm_start"] == start).mean() >= 0.95 and (r["bm_end"] == end).mean() >= 0.9
-    # and the oracle's own KNN search gives exactly these radii: candidate sets and results then
-    # differ from the reference only where a radius differs
-    o_exact = port.run(w)
-    o_ref = port.run(w, radii=_ref_radii(w, r))
-    assert (o_exact["count_pb2d"] != o_ref["count_pb2d"]).mean() <= 0.05
+    np.testing.assert_array_equal(e["ph_r2"][inm], exact[inm])
+    assert (r["ph_r2"][inm] >= e["ph_r2"][inm]).all()
+    assert (r["bm_start"] >= e["bm_start"]).all() and (r["bm_end"] >= e["bm_end"]).all()
+    assert (r["ph_r2"][inm] != e["ph_r2"][inm]).any() or (r["bm_start"] != e["bm_start"]).any()
+
+
+def test_knn_radii_equal_the_reference_search_at_a_larger_size():
+    """The reference's search on sets of some 10^5 points (deeper trees, more ties and heap paths):
+    the oracle's radii equal those of the reference's own builds, run here through the harness."""
+    from smallupbp_b200 import workload as W
+
+    if not ref.available():
+        pytest.skip("reference oracle not built")
+    cfg = W.config("cube512")
+    cfg.pb2d_knn, cfg.bb1d_knn = 12, 8
+    w = W.generate(cfg)
+    rr = ref.radii(w)
+    o = port.knn_radii(w)
+    inm = np.nonzero(w["lv_flags"] & 1)[0]
+    assert len(inm) > 50_000 and len(w["beam_length"]) > 50_000
+    np.testing.assert_array_equal(o["ph_r2"][inm], rr["ph_r2"][inm])
+    np.testing.assert_array_equal(o["bm_start"], rr["bm_start"])
+    np.testing.assert_array_equal(o["bm_end"], rr["bm_end"])
 
 
 def test_oracle_stride_subset_is_consistent():
