@@ -398,14 +398,7 @@ __global__ void k_emit_sorted(const float* __restrict__ origin, const float* __r
         bx_.lo[2] = fminf(bx_.lo[2], bz - re); bx_.hi[2] = fmaxf(bx_.hi[2], bz + re);
     }
     pa[i] = make_float4(ox, oy, oz, len);
-    float w = r2;
-    if (!r2max) {
-        // one radius for every beam: pb.w holds the piece window (BeamBVH::window), rounded outwards
-        const __half lo = k == 0 ? __float2half(-INFINITY) : __float2half_rd(t0);
-        const __half hi = k == cnt - 1 ? __float2half(INFINITY) : __float2half_ru(t1);
-        w = __uint_as_float((unsigned)__half_as_ushort(lo) | ((unsigned)__half_as_ushort(hi) << 16));
-    }
-    pb[i] = make_float4(dx, dy, dz, w);
+    pb[i] = make_float4(dx, dy, dz, r2);
     pc[i] = make_float4(t0, t1, __int_as_float(b), __int_as_float(medium[b]));
     boxes[i] = bx_;
 }

@@ -699,9 +699,6 @@ BeamBVH beam_bvh(upbp_ctx* c)
     B.pay = c->mode != UPBP_MODE_PLAIN ? c->pc_pay.as<PiecePayload>() : nullptr;
     B.leaf = std::max(1, c->bb1d_leaf);
     B.n_leaves = c->bm_n_leaves;
-    // k_emit_sorted writes the piece window into pb.w when every beam has the radius radius_bb1d
-    B.window = c->P.bb1d_knn > 0 ? 0 : 1;
-    B.r2c = c->P.radius_bb1d * c->P.radius_bb1d;
     return B;
 }
 

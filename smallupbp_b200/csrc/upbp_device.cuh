@@ -10,7 +10,6 @@
 #pragma once
 
 #include <cstdint>
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "../../include/upbp_gpu.h"
@@ -141,33 +140,6 @@ __device__ __forceinline__ bool beam_beam_near(V3 O1, V3 d1, V3 O2, V3 d2, float
     return !(xmul(ad, ad) >= xmul(maxDistSqr, sinThetaSqr));
 }
 
-// Stage-1 window filter of a beam piece: can this piece own a candidate of the query?  The owner of
-// a taken pair is the piece containing u, the beam parameter of the closest points of the query
-// and beam segments (the reach rule below).  For lines that are not nearly parallel
-// (|d1 x d2|^2 > 0.04) u is the beam parameter of the lines' closest points,
-// tb = ((O2 - O1) x d1).(d1 x d2) / |d1 x d2|^2, up to the rounding of tb (below 5e-5 x scale), the
-// shift of a closest point clamped to the query's ends (the FP32 t1 the predicate accepted is
-// within 6e-5 x scale of the exact one there), or a clamp to the beam's ends, which only the first
-// and the last piece own (their window is open on that side).  A piece whose window
-// [t_lo - M, t_hi + M], M = 1e-3 x (scale + |O2 - O1|_1 + len), does not contain tb owns nothing
-// for this query: the pieces of a crossing beam next to its owner are dropped before the rest of
-// the predicate.  (Checked on the CPU over 3.2 M taken pairs with crossings at the segment ends: no
-// owner dropped.)  scale_q = max(|O1|_inf, |dmax|, 1) of the query.
-__device__ __forceinline__ bool piece_window_ok(V3 O1, V3 d1, V3 O2, V3 d2, float len, float window, float scale_q)
-{
-    const float wx = O2.x - O1.x, wy = O2.y - O1.y, wz = O2.z - O1.z;
-    const float cx = d1.y * d2.z - d1.z * d2.y, cy = d1.z * d2.x - d1.x * d2.z, cz = d1.x * d2.y - d1.y * d2.x;
-    const float s2 = cx * cx + cy * cy + cz * cz;
-    if (!(s2 > 0.04f)) return true;
-    const float ux = wy * d1.z - wz * d1.y, uy = wz * d1.x - wx * d1.z, uz = wx * d1.y - wy * d1.x;
-    const float tb = __fdividef(ux * cx + uy * cy + uz * cz, s2);
-    const float m = 1e-3f * (scale_q + fabsf(wx) + fabsf(wy) + fabsf(wz) + len);
-    const unsigned bits = __float_as_uint(window);
-    const float lo = __half2float(__ushort_as_half((unsigned short)(bits & 0xffffu)));
-    const float hi = __half2float(__ushort_as_half((unsigned short)(bits >> 16)));
-    return tb >= lo - m && tb <= hi + m;
-}
-
 // PhotonBeam::testIntersectionBeamBeam (Beams/PhotonBeam.hxx:238-296).  On acceptance it can also
 // return b = d1.d2 and e = d2.O1 - d2.O2, the terms of the line solution that piece_takes_fast uses.
 __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float maxT1, V3 O2, V3 d2, float minT2,
@@ -262,25 +234,29 @@ __device__ __forceinline__ SegClosest seg_closest_f64(V3 O1, V3 d1, float dminf,
 // its change per unit t.  The reference's own t2 = (t1 + d1.O1 - d1.O2) / b is ill-conditioned for
 // nearly perpendicular pairs, so the beam parameter of the lines' closest points is taken as
 // u = e + b t1 instead, which is well-conditioned whenever the lines are not nearly parallel.
-// Where 1 - b^2 > 0.06, the rounding error of t1 and u stays below 39 ulp x scale / 0.06, well
-// under m = 1e-4 * scale, so t1 and u more than m inside their ranges put the exact closest points
-// inside both segments: u is the owner's parameter, and D is the distance of the lines, which the
-// FP32 dist approximates within errb (|ad| carries at most 6 ulp of |O2 - O1|_1 and sin(theta) >
-// 0.2 there; errb is twice that bound).
+// The rounding error of t1 and u grows as 1 / (1 - b^2) (t1 divides by b^2 - 1): it stays below
+// 39 ulp x scale / (1 - b^2), under m = 6e-6 x scale / (1 - b^2), so t1 and u more than m inside
+// their ranges put the exact closest points inside both segments: u is the owner's parameter, and
+// D is the distance of the lines, which the FP32 dist approximates within errb (|ad| carries at
+// most 6 ulp of |O2 - O1|_1 and is divided by sin(theta); errb is twice that bound).  Below
+// 1 - b^2 = 0.002 (the lines within 2.6 degrees of parallel) the FP64 solve decides.  (Checked on
+// the CPU against the FP64 rule over 64 M piece decisions of pairs concentrated at 1 - b^2 in
+// [0.0006, 0.12]: none differs.)
 __device__ __forceinline__ int piece_takes_fast(V3 O1, V3 d1, float dmin, float dmax, V3 O2, float len, float t_lo,
                                                 float t_hi, float t1, float b, float e, float dist, float rs,
                                                 float rc, float extra)
 {
-    if (1.f - b * b > 0.06f) {
+    const float om = 1.f - b * b;
+    if (om > 0.002f) {
         const float scale = fmaxf(fmaxf(fmaxf(fabsf(O1.x), fabsf(O1.y)), fmaxf(fabsf(O1.z), fabsf(O2.x))),
                                   fmaxf(fmaxf(fabsf(O2.y), fabsf(O2.z)), fmaxf(fmaxf(len, fabsf(dmax)), 1.f)));
-        const float m = 1e-4f * scale;
+        const float m = __fdividef(6e-6f * scale, om);
         const float u = e + b * t1;
         if (t1 > dmin + m && t1 < dmax - m && u > m && u < len - m) {
             if (u < t_lo - m || u >= t_hi + m) return 0;
             if (u >= t_lo + m && u < t_hi - m) {
                 const float w1 = fabsf(O2.x - O1.x) + fabsf(O2.y - O1.y) + fabsf(O2.z - O1.z);
-                const float errb = 4e-6f * w1 + 3e-6f * dist + 1e-8f;
+                const float errb = 8e-7f * w1 * rsqrtf(om) + 3e-6f * dist + 1e-8f;
                 if (dist + errb + fabsf(rc) * m <= rs + u * rc + extra) return 1;
             }
         }

@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(256) k_gather_bb1d(const __grid_constant__ Gat
                     ++tested;
                     float dist, sinT, t1, t2, bb, ee;
                     if (!test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
-                                        piece_r2(B, pb.w), &dist, &sinT, &t1, &t2, &bb, &ee))
+                                        pb.w, &dist, &sinT, &t1, &t2, &bb, &ee))
                         continue;
                     const int beam = __float_as_int(pc.z);
                     const float rs = beam_start_radius(Bs, &Bs.radius[beam]);
@@ -619,7 +619,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                 const float4 pa = __ldg(&B.pa[i]);
                 const float4 pb = __ldg(&B.pb[i]);
                 if (test_beam_beam(s.o, s.d, s.dmin, s.dmax, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w,
-                                   piece_r2(B, pb.w), &dist, &sinT, &t1, &t2, &bb, &ee)) {
+                                   pb.w, &dist, &sinT, &t1, &t2, &bb, &ee)) {
                     const float4 pc = __ldg(&B.pc[i]);
                     if (__float_as_int(pc.w) == mid) {  // mMedium == medium (PhotonBeam.hxx:390)
                         // the radius test (PhotonBeam.hxx:411-413), then the reach rule and the owner
@@ -664,11 +664,8 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                 __syncwarp();
             }
         };
-        // about half of the tested pieces fail the predicate's first check (the distance of the
-        // lines), and with one radius for every beam the pieces of a crossing beam next to the one
-        // that can own the pair fail the window filter (piece_window_ok); the others are queued and
-        // the rest of the predicate runs 32 at a time
-        const float scale_q = fmaxf(fmaxf(fabsf(s.o.x), fabsf(s.o.y)), fmaxf(fabsf(s.o.z), fmaxf(fabsf(s.dmax), 1.f)));
+        // about a third of the tested pieces pass the predicate's first check (the distance of the
+        // lines); they are queued and the rest of the predicate runs 32 at a time
         int pn = 0;  // entries in the near queue (warp-uniform)
         const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.o, inv, s.dmin - K.eps, s.dmax + K.eps,
                                       ws.stack, ws.leaves, lane, [&](int i) {
@@ -677,9 +674,7 @@ __device__ __forceinline__ Rgb bb1d_query_warp(const GatherConsts& K, const DMed
                 const float4 pa = __ldg(&B.pa[i]);
                 const float4 pb = __ldg(&B.pb[i]);
                 ++tested32;
-                near = beam_beam_near(s.o, s.d, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), piece_r2(B, pb.w)) &&
-                       (!B.window ||
-                        piece_window_ok(s.o, s.d, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pa.w, pb.w, scale_q));
+                near = beam_beam_near(s.o, s.d, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pb.w);
             }
             const unsigned vote = __ballot_sync(kFull, near);
             if (vote == 0u) return;
@@ -1106,7 +1101,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_bp2d_warp(const __g
                         const float4 pb = __ldg(&B.pb[i]);
                         ++tested;
                         // bound: the beam's largest radius^2; then the radius at the foot point
-                        if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, piece_r2(B, pb.w), &t, &d2) &&
+                        if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &t, &d2) &&
                             t >= pc.x && t < pc.y) {  // the piece containing the foot point
                             const int beam = __float_as_int(pc.z);
                             const float rt = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), t);
@@ -1181,7 +1176,7 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
                 ++tested;
                 float t, d2;
                 // bound: the beam's largest radius^2; then the radius at the foot point
-                if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, piece_r2(B, pb.w), &t, &d2)) continue;
+                if (!test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &t, &d2)) continue;
                 if (!(t >= pc.x && t < pc.y)) continue;  // the piece containing the foot point
                 const int beam = __float_as_int(pc.z);
                 const float rt = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), t), r2 = rt * rt;

@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                             const float4 pb = __ldg(&B.pb[i]);
                             float dist, sinT, t1, t2, bb, ee;
                             if (test_beam_beam(s.of, s.df, dminf, dmaxf, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                               0.f, pa.w, piece_r2(B, pb.w), &dist, &sinT, &t1, &t2, &bb, &ee)) {
+                                               0.f, pa.w, pb.w, &dist, &sinT, &t1, &t2, &bb, &ee)) {
                                 const int beam = __float_as_int(pc.z);
                                 const float rs = beam_start_radius(Bs, &B.pay[i].lv.z);
                                 const float radius = beam_radius_at(Bs, beam, rs, t2);
@@ -566,8 +566,6 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                         __syncwarp();
                     }
                 };
-                const float scale_q =
-                    fmaxf(fmaxf(fabsf(s.of.x), fabsf(s.of.y)), fmaxf(fabsf(s.of.z), fmaxf(fabsf(dmaxf), 1.f)));
                 int pn = 0;  // entries in the near queue
                 const bool ok = warp_traverse(B.nodes, B.n_leaves, B.n, leaf_shift, s.of, inv, dminf - K.eps,
                                               dmaxf + K.eps, stack, leaves, lane, [&](int i) {
@@ -575,10 +573,7 @@ __global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ Gather
                     if (i >= 0) {
                         const float4 pa = __ldg(&B.pa[i]);
                         const float4 pb = __ldg(&B.pb[i]);
-                        near = beam_beam_near(s.of, s.df, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                              piece_r2(B, pb.w)) &&
-                               (!B.window || piece_window_ok(s.of, s.df, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z),
-                                                             pa.w, pb.w, scale_q));
+                        near = beam_beam_near(s.of, s.df, v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), pb.w);
                     }
                     const unsigned vote = __ballot_sync(kFull, near);
                     if (vote == 0u) return;
@@ -767,7 +762,7 @@ __global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ Gather
                         const float4 pa = __ldg(&B.pa[i]);
                         const float4 pb = __ldg(&B.pb[i]);
                         float tf, d2f;
-                        if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, piece_r2(B, pb.w), &tf, &d2f) &&
+                        if (test_bre(v3(pa.x, pa.y, pa.z), v3(pb.x, pb.y, pb.z), 0.f, pa.w, x, pb.w, &tf, &d2f) &&
                             tf >= pc.x && tf < pc.y) {
                             const int beam = __float_as_int(pc.z);
                             const float rt = beam_radius_at(Bs, beam, beam_start_radius(Bs, &Bs.radius[beam]), tf);

@@ -62,22 +62,14 @@ constexpr unsigned kPayOriginInMedium = 1u << 31;
 // Beam pieces (BB1D) in leaf order.  Piece = beam sub-interval [t_lo, t_hi).
 struct BeamBVH {
     const float4* pa;    // beam origin xyz, beam length
-    const float4* pb;    // beam direction xyz, w: max radius^2 (KNN radii) or the piece window (below)
+    const float4* pb;    // beam direction xyz, max radius^2   (pa, pb: all the predicate reads)
     const float4* pc;    // t_lo, t_hi, beam id (int bits), medium (int bits)
     const BNode* nodes;
     const PiecePayload* pay;  // mixed mode, per piece
     int n;
     int leaf;
     int n_leaves;
-    // With one radius for every beam pb.w holds the piece's window instead of the radius^2 r2c:
-    // t_lo rounded down and t_hi rounded up to FP16 (low and high half), -inf / +inf at the beam's
-    // first / last piece (piece_window_ok).
-    int window;
-    float r2c;
 };
-
-// max radius^2 of the beam of a piece record (the predicate's maxDistSqr, PhotonBeam.hxx:250)
-__device__ __forceinline__ float piece_r2(const BeamBVH& B, float pbw) { return B.window ? B.r2c : pbw; }
 
 // Beam payload (index = beam id).
 struct BeamSoA {

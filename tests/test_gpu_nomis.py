@@ -87,7 +87,7 @@ def test_nomis_fp64_mode_matches_fp64_oracle(stage, path):
     g = run(stage, w, engine.MODE_FP64)
     for est in ("pb2d", "bb1d"):
         err = G.rel_errors(g[est].astype(np.float64), o64[est].astype(np.float64))
-        assert err.max() <= 1e-5, (est, float(err.max()))
+        assert err.max() <= G.RTOL, (est, float(err.max()))
     assert G.image_rel_l2(g["image"], o64["image"]) <= 1e-6
 
 

@@ -61,16 +61,21 @@ def test_deterministic_candidates_and_stable_image(stage):
 @pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
 def test_mixed_mode_candidates_and_contributions(stage, path):
     # Mixed mode: same FP32 candidate predicates (bit-exact sets), FP64 MIS partial sums and an FP64
-    # closest-approach solve for near-parallel beam pairs.  Against the FP32 reference the
-    # per-query contributions agree within 1e-4 except where the reference's own FP32 geometry
-    # cancels; the image agrees within 1e-4 rel L2.
+    # closest-approach solve for near-parallel beam pairs.  Every query's contribution is within
+    # 1e-4 of the FP32 reference or, where the reference's own FP32 geometry cancels, of the FP64
+    # oracle (the same candidates, FP64 arithmetic); the image agrees within 1e-4 rel L2.
+    from oracle import port
+
     w, r = G.expected(path)
     g = run(stage, w, engine.MODE_MIXED)
     for est in ("pb2d", "bb1d", "pp3d"):
         np.testing.assert_array_equal(g["hash_" + est], r["hash_" + est], err_msg=est)
+    o64 = port.run(w, fp64=True)
     for est, rk in (("pb2d", "pb2d"), ("bb1d", "bb1d_brute"), ("pp3d", "pp3d")):
-        err = G.rel_errors(g[est].astype(np.float64), r[rk].astype(np.float64))
-        assert (err <= G.RTOL).mean() >= 0.995, (est, float(err.max()))
+        got = g[est].astype(np.float64)
+        err = np.minimum(G.rel_errors(got, r[rk].astype(np.float64)), G.rel_errors(got, o64[est].astype(np.float64)))
+        worst = int(np.argmax(err)) if len(err) else -1
+        assert (err <= G.RTOL).all(), (est, int((err > G.RTOL).sum()), float(err[worst]) if worst >= 0 else None)
     assert G.image_rel_l2(g["image"], r["image"]) <= 1e-4
 
 
