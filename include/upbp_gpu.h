@@ -295,6 +295,29 @@ typedef struct upbp_tuning {
 } upbp_tuning;
 int upbp_set_tuning(upbp_ctx* ctx, const upbp_tuning* tuning);
 int upbp_get_tuning(const upbp_ctx* ctx, upbp_tuning* tuning);
+
+/* BB1D over the reference's uniform grid of beams (Beams/PhGrid.hxx, Beams/Grid.hxx: the
+ * evaluator of the reference's default USE_GRID build, PhBeams.hxx:30-34) instead of the LBVH over
+ * beam pieces.  The grid has the reference's resolution, cell lists and cell order, and its DDA
+ * walk tests the beams of each visited cell with the query restricted to the cell's t range
+ * (Grid.hxx:322-398), so a pair whose closest point lies on a cell boundary is found in both cells
+ * or in neither, as in the reference.  Optionally the reference's beam reduction (-gridmax,
+ * -gridred; Grid.hxx:558-631) tests at most max_beams_in_cell beams of each cell and divides the
+ * contribution by the cell's selection pdf: reduction 0 (PRESAMPLE, the reference's default) only,
+ * with the reference's own random stream (std::mt19937_64 seeded with `seed`, through
+ * std::uniform_real_distribution<float> as libstdc++ defines it), and, as in the reference
+ * (Config.hxx:1111-1112), only for the estimator without MIS (UPBP_NO_MIS).  The other reductions
+ * draw from that stream in the order the queries are made, which a parallel evaluation does not
+ * reproduce: they return UPBP_ERR_INVALID_ARG.  Plain and mixed modes; the grid build needs one
+ * host synchronisation (its cell-list size), so its iterations are not captured as CUDA graphs.
+ * grid_res 0 (the default) switches the grid off. */
+typedef struct upbp_bb1d_grid {
+    uint32_t grid_res;          /* -gridres: PhotonBeamsEvaluator::sGridSize (reference default 256) */
+    uint32_t max_beams_in_cell; /* -gridmax: sMaxBeamsInCell (0: no reduction) */
+    uint32_t reduction;         /* -gridred: sReductionType (0: PRESAMPLE) */
+    int32_t seed;               /* PhotonBeamsEvaluator::mSeed (UPBP.hxx:417: base seed + iteration) */
+} upbp_bb1d_grid;
+int upbp_set_bb1d_grid(upbp_ctx* ctx, const upbp_bb1d_grid* grid);
 /* CUDA stream (cudaStream_t as void*) used by all later calls; NULL = the context's own stream. */
 int upbp_set_stream(upbp_ctx* ctx, void* stream);
 

@@ -46,12 +46,17 @@ def lib():
                                  C.c_int32, C.POINTER(RefOutputs)]
         _lib.ref_set_grid_options.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
         _lib.ref_set_grid_options.restype = None
+        _lib.ref_set_grid_seed.argtypes = [C.c_int32]
+        _lib.ref_set_grid_seed.restype = None
     return _lib
 
 
-def set_grid_options(grid_size: int = 256, max_beams_in_cell: int = 0, reduction_type: int = 0) -> None:
-    """The reference's -gridres / -gridmax / -gridred options (defaults 256, 0, 0)."""
+def set_grid_options(grid_size: int = 256, max_beams_in_cell: int = 0, reduction_type: int = 0,
+                     seed: int = 1234) -> None:
+    """The reference's -gridres / -gridmax / -gridred options (defaults 256, 0, 0) and the grid
+    evaluator's reduction seed (PhotonBeamsEvaluator::mSeed, default 1234)."""
     lib().ref_set_grid_options(grid_size, max_beams_in_cell, reduction_type)
+    lib().ref_set_grid_seed(seed)
 
 
 def run(w: Dict[str, np.ndarray], what: int = PB2D | BB1D_GRID | BB1D_BRUTE | PP3D | CANDIDATES,

@@ -54,6 +54,10 @@ Rgb ref_brute_eval_lite(void* h, BeamType bt, const Ray& ray, const LiteVolumeSe
                         embree::AdditionalRayDataForMis* data);
 void ref_brute_destroy(void* h);
 
+/* the seed of the grid's beam reduction (PhotonBeamsEvaluator::mSeed; the evaluator's own default
+ * is 1234, PhBeams.hxx:56) */
+static int g_grid_seed = 1234;
+
 namespace {
 
 struct World {
@@ -225,9 +229,11 @@ void setup_world(World& w, const upbp_params& P, const upbp_medium* media, int n
                                    P.pb2d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.radius_pb2d, P.pb2d_knn, false);
         }
     }
-    if ((what & REF_BB1D_GRID) && U.mMergeWithLightVerticesBB1D && !U.mPhotonBeamsArray.empty())
+    if ((what & REF_BB1D_GRID) && U.mMergeWithLightVerticesBB1D && !U.mPhotonBeamsArray.empty()) {
+        U.mBB1DPhotonBeams.mSeed = g_grid_seed;
         U.mBB1DPhotonBeams.build(U.mPhotonBeamsArray, P.bb1d_knn > 0 ? KNN_RADIUS : CONSTANT_RADIUS, P.radius_bb1d,
                                  P.bb1d_knn, false);
+    }
     if ((what & (REF_BB1D_BRUTE | REF_CANDIDATES)) && U.mMergeWithLightVerticesBB1D && !U.mPhotonBeamsArray.empty())
         w.brute = ref_brute_create(w.scene, U.mPhotonBeamsArray, P.radius_bb1d, P.bb1d_knn);
 }
@@ -304,6 +310,8 @@ extern "C" void ref_set_grid_options(uint32_t grid_size, uint32_t max_beams_in_c
     PhotonBeamsEvaluator::sMaxBeamsInCell = max_beams_in_cell;
     PhotonBeamsEvaluator::sReductionType = reduction_type;
 }
+
+extern "C" void ref_set_grid_seed(int32_t seed) { g_grid_seed = seed; }
 
 struct RefSession {
     upbp_params P;

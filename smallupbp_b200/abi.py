@@ -65,6 +65,12 @@ class Tuning(C.Structure):
                 ("query_order", C.c_int32)]
 
 
+class Bb1dGrid(C.Structure):
+    """upbp_bb1d_grid: the reference's uniform beam grid (-gridres, -gridmax, -gridred, mSeed)."""
+    _fields_ = [("grid_res", C.c_uint32), ("max_beams_in_cell", C.c_uint32), ("reduction", C.c_uint32),
+                ("seed", C.c_int32)]
+
+
 class QueryStats(C.Structure):
     _fields_ = [("count_pb2d", u32p), ("hash_pb2d", u64p), ("count_bb1d", u32p), ("hash_bb1d", u64p),
                 ("count_pp3d", u32p), ("hash_pp3d", u64p)]

@@ -88,6 +88,13 @@ struct upbp_ctx {
     int n_pieces = 0;
     DBuf bm_leaf_codes, bm_nodes, bm_parent_int, bm_parent_leaf, bm_leaf_boxes, bm_node_boxes, bm_flagsbuf;
     DBuf pc_pay;  // mixed mode: beam payload packed per piece
+    // BB1D over the reference's uniform grid (upbp_set_bb1d_grid)
+    upbp_bb1d_grid bgrid{};
+    DBuf gr_hdr, gr_partial, gr_counts, gr_offsets, gr_keys, gr_keys_sorted, gr_keys_unique, gr_num, gr_cellcount,
+        gr_cells, gr_ptr, gr_pdf, gr_draws, gr_draw_off, gr_rnd;
+    GridHeader gr_host{};           // the last build's header
+    int64_t gr_raw = 0, gr_pairs = 0, gr_draws_total = 0;  // its sizes (a replay reuses them)
+    bool gr_valid = false;
     // KNN radii: per-photon radius^2 (leaf order); per-beam radius change and max radius^2 (the
     // start radius goes to bm_radius); the LBVH over beam origins for the beam KNN search
     DBuf pb_r2, bm_rchange, bm_r2max, knn_status;
@@ -266,6 +273,118 @@ void sort_pairs(upbp_ctx* c, const uint32_t* kin, uint32_t* kout, const int32_t*
     c->build_launches += 4;
 }
 
+int bits_for(uint32_t maxv);
+
+// The reference's uniform grid of beams (upbp_grid.cu).  Three host synchronisations read the
+// sizes that the next steps allocate (the raw and the unique (cell, beam) pairs, the random draws);
+// a replay under graph capture reuses the last build's.
+void build_grid(upbp_ctx* c, cudaStream_t s, float radius, const float* rstart, const float* rchange)
+{
+    const int64_t nb = c->n_beams;
+    const upbp_bb1d_grid& g = c->bgrid;
+    const float* org = c->b_origin.as<float>();
+    const float* dir = c->b_dir.as<float>();
+    const float* len = c->b_len.as<float>();
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(1024, (nb + 255) / 256));
+    ensure(c, c->gr_hdr, sizeof(GridHeader));
+    ensure(c, c->gr_partial, sizeof(float) * 6 * blocks);
+    GridHeader* hdr = c->gr_hdr.as<GridHeader>();
+    launch_grid_header(org, dir, len, rstart, rchange, radius, nb, g.grid_res, g.max_beams_in_cell,
+                       c->gr_partial.as<float>(), blocks, hdr, s);
+    ensure(c, c->gr_counts, sizeof(unsigned long long) * (nb + 1));
+    ensure(c, c->gr_offsets, sizeof(unsigned long long) * (nb + 1));
+    unsigned long long* cnt = c->gr_counts.as<unsigned long long>();
+    unsigned long long* off = c->gr_offsets.as<unsigned long long>();
+    launch_grid_count(org, dir, len, rstart, rchange, radius, nb, hdr, cnt, s);
+    ck(c, cudaMemsetAsync(cnt + nb, 0, sizeof(unsigned long long), s), "memset");
+    size_t b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b, cnt, off, (int)(nb + 1), s);
+    ensure(c, c->cub_tmp, b);
+    ck(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, b, cnt, off, (int)(nb + 1), s), "ExclusiveSum");
+    if (!c->replay) {
+        unsigned long long raw = 0;
+        ck(c, cudaMemcpyAsync(&raw, off + nb, sizeof(raw), cudaMemcpyDeviceToHost, s), "copy grid pairs");
+        ck(c, cudaMemcpyAsync(&c->gr_host, hdr, sizeof(GridHeader), cudaMemcpyDeviceToHost, s), "copy grid header");
+        ck(c, cudaStreamSynchronize(s), "sync");
+        if (c->gr_host.n_cells < 2)
+            fail(c, UPBP_ERR_INVALID_ARG, "the beams' box has no extent along an axis: no beam grid");
+        if (raw >= (1ull << 31))
+            fail(c, UPBP_ERR_CAPACITY, "the beam grid holds %llu cell entries (at most 2^31 - 1)", raw);
+        c->gr_raw = (int64_t)raw;
+    }
+    const int64_t raw = c->gr_raw;
+    const uint32_t nc = c->gr_host.n_cells;
+    ensure(c, c->gr_keys, sizeof(unsigned long long) * std::max<int64_t>(raw, 1));
+    ensure(c, c->gr_keys_sorted, sizeof(unsigned long long) * std::max<int64_t>(raw, 1));
+    ensure(c, c->gr_keys_unique, sizeof(unsigned long long) * std::max<int64_t>(raw, 1));
+    ensure(c, c->gr_num, sizeof(int64_t));
+    launch_grid_emit(org, dir, len, rstart, rchange, radius, nb, hdr, off, c->gr_keys.as<unsigned long long>(), s);
+    const int end_bit = 32 + bits_for(nc);
+    b = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, b, c->gr_keys.as<unsigned long long>(),
+                                   c->gr_keys_sorted.as<unsigned long long>(), (int)raw, 0, end_bit, s);
+    ensure(c, c->cub_tmp, b);
+    ck(c, cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, b, c->gr_keys.as<unsigned long long>(),
+                                         c->gr_keys_sorted.as<unsigned long long>(), (int)raw, 0, end_bit, s),
+       "SortKeys");
+    b = 0;
+    cub::DeviceSelect::Unique(nullptr, b, c->gr_keys_sorted.as<unsigned long long>(),
+                              c->gr_keys_unique.as<unsigned long long>(), c->gr_num.as<int64_t>(), (int64_t)raw, s);
+    ensure(c, c->cub_tmp, b);
+    ck(c, cub::DeviceSelect::Unique(c->cub_tmp.p, b, c->gr_keys_sorted.as<unsigned long long>(),
+                                    c->gr_keys_unique.as<unsigned long long>(), c->gr_num.as<int64_t>(), (int64_t)raw,
+                                    s),
+       "Unique");
+    if (!c->replay) {
+        int64_t n = 0;
+        ck(c, cudaMemcpyAsync(&n, c->gr_num.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "copy grid pairs");
+        ck(c, cudaStreamSynchronize(s), "sync");
+        c->gr_pairs = n;
+    }
+    const int64_t np = c->gr_pairs;
+    ensure(c, c->gr_cellcount, sizeof(uint32_t) * nc);
+    ensure(c, c->gr_cells, sizeof(uint32_t) * nc);
+    ensure(c, c->gr_ptr, sizeof(int32_t) * std::max<int64_t>(np, 1));
+    ck(c, cudaMemsetAsync(c->gr_cellcount.p, 0, sizeof(uint32_t) * nc, s), "memset");
+    launch_grid_lists(c->gr_keys_unique.as<unsigned long long>(), np, c->gr_cellcount.as<uint32_t>(),
+                      c->gr_ptr.as<int32_t>(), s);
+    b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b, c->gr_cellcount.as<uint32_t>(), c->gr_cells.as<uint32_t>(), (int)nc, s);
+    ensure(c, c->cub_tmp, b);
+    ck(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, b, c->gr_cellcount.as<uint32_t>(), c->gr_cells.as<uint32_t>(),
+                                        (int)nc, s),
+       "ExclusiveSum");
+    c->build_launches += 12;
+    if (g.max_beams_in_cell > 0) {
+        ensure(c, c->gr_draws, sizeof(uint32_t) * nc);
+        ensure(c, c->gr_draw_off, sizeof(uint32_t) * nc);
+        ensure(c, c->gr_pdf, sizeof(float) * nc);
+        launch_grid_draws(c->gr_cells.as<uint32_t>(), nc, g.max_beams_in_cell, c->gr_draws.as<uint32_t>(), s);
+        b = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, b, c->gr_draws.as<uint32_t>(), c->gr_draw_off.as<uint32_t>(), (int)nc,
+                                      s);
+        ensure(c, c->cub_tmp, b);
+        ck(c, cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, b, c->gr_draws.as<uint32_t>(), c->gr_draw_off.as<uint32_t>(),
+                                            (int)nc, s),
+           "ExclusiveSum");
+        if (!c->replay) {  // the last cell (the sentinel) draws nothing: the total is its offset
+            uint32_t t = 0;
+            ck(c, cudaMemcpyAsync(&t, c->gr_draw_off.as<uint32_t>() + nc - 1, sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, s),
+               "copy grid draws");
+            ck(c, cudaStreamSynchronize(s), "sync");
+            c->gr_draws_total = t;
+        }
+        ensure(c, c->gr_rnd, sizeof(float) * std::max<int64_t>(c->gr_draws_total, 1));
+        // std::mt19937_64 takes the int seed converted to its 64-bit result type
+        launch_mt64_floats((unsigned long long)(long long)g.seed, c->gr_draws_total, c->gr_rnd.as<float>(), s);
+        launch_grid_presample(c->gr_cells.as<uint32_t>(), nc, g.max_beams_in_cell, c->gr_draw_off.as<uint32_t>(),
+                              c->gr_rnd.as<float>(), c->gr_ptr.as<int32_t>(), c->gr_pdf.as<float>(), s);
+        c->build_launches += 5;
+    }
+    c->gr_valid = true;
+}
+
 int bits_for(uint32_t maxv)
 {
     int b = 1;
@@ -333,6 +452,14 @@ void do_build(upbp_ctx* c)
         fail(c, UPBP_ERR_INVALID_ARG, "light vertex %s is NULL (only UPBP_NO_MIS runs without it)", c->lv_mis_missing);
     if (mis && c->n_beams > 0 && (P.techniques & UPBP_BB1D) && c->beam_mis_missing)
         fail(c, UPBP_ERR_INVALID_ARG, "%s is NULL (only UPBP_NO_MIS runs without it)", c->beam_mis_missing);
+    if (c->bgrid.grid_res > 0) {
+        if (c->mode == UPBP_MODE_FP64)
+            fail(c, UPBP_ERR_INVALID_ARG, "the beam grid (upbp_set_bb1d_grid) runs in plain and mixed mode");
+        if (c->bgrid.max_beams_in_cell > 0 && mis)
+            fail(c, UPBP_ERR_INVALID_ARG,
+                 "beam reduction (max_beams_in_cell) works only for the estimator without MIS (UPBP_NO_MIS), "
+                 "as in the reference");
+    }
     // ---- light vertices
     ensure(c, c->lv_pos4, sizeof(float4) * std::max<int64_t>(n, 1));
     ensure(c, c->lv_dir4, sizeof(float4) * std::max<int64_t>(n, 1));
@@ -456,6 +583,7 @@ void do_build(upbp_ctx* c)
     const int replay_pieces = c->n_pieces;
     c->n_pieces = 0;
     c->bm_n_leaves = 0;
+    c->gr_valid = false;
     const int64_t nb = c->n_beams;
     if (nb > 0 && (P.techniques & UPBP_BB1D)) {
         const float r = P.radius_bb1d;
@@ -583,6 +711,7 @@ void do_build(upbp_ctx* c)
                                  mis ? c->light_sums.as<LightSum>() : nullptr, c->pc_pay.as<PiecePayload>(), s);
             c->build_launches += 1;
         }
+        if (c->bgrid.grid_res > 0) build_grid(c, s, r, rchange ? c->bm_radius.as<float>() : nullptr, rchange);
     }
     mark(c, 1, s);
     ck(c, cudaGetLastError(), "build launch");
@@ -700,6 +829,21 @@ BeamBVH beam_bvh(upbp_ctx* c)
     B.leaf = std::max(1, c->bb1d_leaf);
     B.n_leaves = c->bm_n_leaves;
     return B;
+}
+
+BeamGrid grid_dev(upbp_ctx* c)
+{
+    BeamGrid G{};
+    G.hdr = c->gr_hdr.as<GridHeader>();
+    G.cells = c->gr_cells.as<uint32_t>();
+    G.pdf = c->bgrid.max_beams_in_cell > 0 ? c->gr_pdf.as<float>() : nullptr;
+    G.ptr = c->gr_ptr.as<int32_t>();
+    G.origin = c->b_origin.as<float>();
+    G.dir = c->b_dir.as<float>();
+    G.length = c->b_len.as<float>();
+    G.medium = c->b_med_in.as<int32_t>();
+    G.r2max = (c->P.bb1d_knn > 0) ? c->bm_r2max.as<float>() : nullptr;
+    return G;
 }
 
 BeamSoA beam_soa(upbp_ctx* c)
@@ -857,10 +1001,12 @@ void do_evaluate(upbp_ctx* c)
         c->evaluated = true;
         return;
     }
-    const bool fused = c->bb1d_kernel >= 3;  // PB2D and BB1D in the one persistent segment kernel
+    const bool grid_mode = c->bgrid.grid_res > 0 && c->gr_valid;
+    // PB2D and BB1D in the one persistent segment kernel (not with the beam grid)
+    const bool fused = c->bb1d_kernel >= 3 && !grid_mode;
     // B-P2D and PB2D are both 2-D kernel gathers; pb2d_kernel selects thread or warp per query for both
     const bool bp2d_warp = bp2d && c->pb2d_kernel == 1 && c->bb1d_kernel >= 1;
-    if ((nq > 0 && c->bb1d_kernel >= 1) || bp2d_warp) {
+    if ((nq > 0 && (c->bb1d_kernel >= 1 || grid_mode)) || bp2d_warp) {
         // persistent warp kernels: work counters (BB1D or the fused kernel: [0], PB2D: [1],
         // B-P2D: [2]) and the traversal status word they share
         if (!c->num_sms) ck(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device), "attr");
@@ -936,7 +1082,11 @@ void do_evaluate(upbp_ctx* c)
         const BeamSoA S = beam_soa(c);
         Outputs O{c->out_bb1d.as<float>(), img, c->cnt_bb1d.as<uint32_t>(),
                   c->hash_bb1d.as<unsigned long long>(), tested + 1};
-        if (fused) {
+        if (grid_mode) {
+            const int grid = c->num_sms * bb1d_grid_blocks_per_sm(mixed);
+            launch_bb1d_grid(K, L, grid_dev(c), S, Q, cam, cs_seg, O, grid, mixed, c->work.as<unsigned int>(),
+                             bb_order, s);
+        } else if (fused) {
             const Outputs Opb{c->out_pb2d.as<float>(), img, c->cnt_pb2d.as<uint32_t>(),
                               c->hash_pb2d.as<unsigned long long>(), tested + 0};
             const int grid = c->num_sms * segments_warp_blocks_per_sm(mixed, c->bb1d_kernel);
@@ -1077,6 +1227,22 @@ int upbp_set_tuning(upbp_ctx* c, const upbp_tuning* tu)
         c->bb1d_kernel = tu->bb1d_kernel;
         c->pb2d_kernel = tu->pb2d_kernel;
         c->query_order = tu->query_order;
+        c->built = false;
+    });
+}
+
+int upbp_set_bb1d_grid(upbp_ctx* c, const upbp_bb1d_grid* g)
+{
+    return guarded(c, [&] {
+        drop_graph(c);
+        if (!g) fail(c, UPBP_ERR_INVALID_ARG, "grid is NULL");
+        if (g->grid_res > 1024) fail(c, UPBP_ERR_INVALID_ARG, "grid_res must be at most 1024");
+        if (g->grid_res > 0 && g->max_beams_in_cell > 0 && g->reduction != 0)
+            fail(c, UPBP_ERR_INVALID_ARG,
+                 "reduction %u draws from the reference's random stream in the order the queries are made; "
+                 "only the PRESAMPLE reduction (0) is reproduced",
+                 g->reduction);
+        c->bgrid = *g;
         c->built = false;
     });
 }
@@ -1598,6 +1764,8 @@ int upbp_adjoint(upbp_ctx* c, const float* grad_image, int32_t medium, double* g
         if (!c->built) fail(c, UPBP_ERR_NOT_BUILT, "upbp_build was not called");
         if (c->mode == UPBP_MODE_PLAIN)
             fail(c, UPBP_ERR_INVALID_ARG, "the adjoint needs UPBP_MODE_MIXED or UPBP_MODE_FP64 structures");
+        if (c->bgrid.grid_res > 0)
+            fail(c, UPBP_ERR_INVALID_ARG, "the adjoint evaluates BB1D over the beam pieces, not the beam grid");
         cudaStream_t s = c->stream;
         c->eval_launches = 0;
         c->status_pending = false;

@@ -1197,7 +1197,228 @@ __global__ void __launch_bounds__(256) k_gather_bp2d(const __grid_constant__ Gat
     if (O.tested) atomicAdd(O.tested, tested);
 }
 
+// ----------------------------------------------------------------- BB1D over the beam grid
+// SSE min_ps / max_ps: the second operand unless the first compares below / above it
+__device__ __forceinline__ float sse_min(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float sse_max(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float pick3(int k, float a, float b, float c) { return k == 0 ? a : (k == 1 ? b : c); }
+
+// Grid::intersect (Grid.hxx:322-398): the DDA walk of one segment [mint, maxt] of the query ray
+// through the reference's grid, with the reference's float operations (the box test of
+// BoundingBox3::intersect, Structs/BoundingBox.hxx:218-272, with its SSE operand order, which
+// turns the NaN of a zero direction component into an unbounded slab).  visit(cell, cell_mint,
+// cell_maxt) for every visited cell, in order; the walk leaves the grid after at most
+// res0 + res1 + res2 cells.
+template <class Visit>
+__device__ __forceinline__ void grid_walk(const GridHeader& h, V3 o, V3 d, float mint, float maxt, Visit&& visit)
+{
+    const float ix = __fdiv_rn(1.f, d.x), iy = __fdiv_rn(1.f, d.y), iz = __fdiv_rn(1.f, d.z);
+    float lmax = 0.f, lmin = 0.f;
+    for (int k = 0; k < 3; ++k) {
+        const float ok = pick3(k, o.x, o.y, o.z), ik = pick3(k, ix, iy, iz);
+        const float l1 = __fmul_rn(__fsub_rn(h.lo[k], ok), ik);
+        const float l2 = __fmul_rn(__fsub_rn(h.hi[k], ok), ik);
+        const float mx = sse_max(sse_min(l1, INFINITY), sse_min(l2, INFINITY));
+        const float mn = sse_min(sse_max(l1, -INFINITY), sse_max(l2, -INFINITY));
+        lmax = k == 0 ? mx : sse_min(lmax, mx);
+        lmin = k == 0 ? mn : sse_max(lmin, mn);
+    }
+    if (!(lmax >= lmin)) return;
+    const float tmn = lmin < mint ? mint : lmin;
+    const float tmx = lmax > maxt ? maxt : lmax;
+    if (!(tmx > tmn)) return;
+    float dx = __fmul_rn(h.cell[0], ix), dy = __fmul_rn(h.cell[1], iy), dz = __fmul_rn(h.cell[2], iz);
+    const float ex = __fmul_rn(__fsub_rn(__fadd_rn(o.x, __fmul_rn(d.x, tmn)), h.lo[0]), h.inv_cell[0]);
+    const float ey = __fmul_rn(__fsub_rn(__fadd_rn(o.y, __fmul_rn(d.y, tmn)), h.lo[1]), h.inv_cell[1]);
+    const float ez = __fmul_rn(__fsub_rn(__fadd_rn(o.z, __fmul_rn(d.z, tmn)), h.lo[2]), h.inv_cell[2]);
+    // Grid::posToVoxel: Utils::clamp((int)pos, 0, res - 1)
+    int px = max(0, min((int)ex, h.res[0] - 1));
+    int py = max(0, min((int)ey, h.res[1] - 1));
+    int pz = max(0, min((int)ez, h.res[2] - 1));
+    uint32_t cell = (uint32_t)px + (uint32_t)h.res[0] * ((uint32_t)py + (uint32_t)h.res[1] * (uint32_t)pz);
+    int sx = 1, sy = 1, sz = 1, cx = h.res[0], cy = h.res[1], cz = h.res[2];
+    if (!(d.x >= 0.f)) { sx = -1; cx = -1; dx = -dx; }
+    if (!(d.y >= 0.f)) { sy = -1; cy = -1; dy = -dy; }
+    if (!(d.z >= 0.f)) { sz = -1; cz = -1; dz = -dz; }
+    float lx = __fmul_rn(__fmul_rn(__fsub_rn((float)(px + (sx > 0 ? 1 : 0)), ex), ix), h.cell[0]);
+    float ly = __fmul_rn(__fmul_rn(__fsub_rn((float)(py + (sy > 0 ? 1 : 0)), ey), iy), h.cell[1]);
+    float lz = __fmul_rn(__fmul_rn(__fsub_rn((float)(pz + (sz > 0 ? 1 : 0)), ez), iz), h.cell[2]);
+    float t = tmn;
+    const int steps = h.res[0] + h.res[1] + h.res[2] + 3;
+    for (int it = 0; it < steps; ++it) {
+        // Vector3::argMin (Structs/Vector3.hxx:473-475)
+        const int ax = (lx < ly) ? ((lx < lz) ? 0 : 2) : ((ly < lz) ? 1 : 2);
+        const float la = pick3(ax, lx, ly, lz);
+        const float tn = __fadd_rn(t, la);
+        visit(cell, t, tmx < tn ? tmx : tn);  // std::min(t + l[minAxis], _maxt)
+        t = tn;
+        lx = __fsub_rn(lx, la);
+        ly = __fsub_rn(ly, la);
+        lz = __fsub_rn(lz, la);
+        if (ax == 0) {
+            lx = dx;
+            cell += h.shift[0] * (uint32_t)sx;
+            px += sx;
+            if (px == cx) return;
+        } else if (ax == 1) {
+            ly = dy;
+            cell += h.shift[1] * (uint32_t)sy;
+            py += sy;
+            if (py == cy) return;
+        } else {
+            lz = dz;
+            cell += h.shift[2] * (uint32_t)sz;
+            pz += sz;
+            if (pz == cz) return;
+        }
+        if (!(t < tmx)) return;
+    }
+}
+
+// The cells of one warp's walk waiting for their beams to be tested.
+constexpr int kGridQueue = 32;
+struct GridQueue {
+    float tmin[kGridQueue], tmax[kGridQueue], pdf[kGridQueue];
+    uint32_t begin[kGridQueue];
+    uint32_t first[kGridQueue + 1];  // the first item of every queued cell; first[n] = all items
+};
+
+// BB1D of one query by one warp over the beam grid.  The walk runs on every lane alike and queues
+// the visited cells that hold beams (the first max_beams_in_cell of an over-full cell of a reduced
+// grid, Grid.hxx:453-465); once 32 or more (cell, beam) items wait, the lanes test them 32 at a
+// time: PhotonBeam::accumulate / accumulate2 (PhotonBeam.hxx:315-367, 375-480) with the query
+// restricted to the cell's t range, the contribution divided by the cell's selection pdf.
+template <bool kMixed>
+__device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMedium* media, const LightSoA& Lv,
+                                               const BeamGrid& G, const GridHeader& hdr, const BeamSoA& Bs,
+                                               const SegQueriesDev& Q, int64_t q, SegCtx& s, GridQueue& gq,
+                                               int lane, unsigned long long& cnt, unsigned long long& h)
+{
+    const float r2c = __fmul_rn(Bs.radius_const, Bs.radius_const);  // mMaxRadiusSqr of a constant radius
+    unsigned cnt32 = 0;
+    const Rgb res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
+        Rgb part = rgb(0.f);
+        const int mid = (int)(&m - media);
+        int qc = 0;  // queued cells (warp-uniform)
+        auto flush = [&]() {
+            const uint32_t total = gq.first[qc];
+            for (uint32_t base = 0; base < total; base += 32) {
+                const uint32_t it = base + (uint32_t)lane;
+                if (it < total) {
+                    int e = 0;
+                    while (e + 1 < qc && gq.first[e + 1] <= it) ++e;
+                    const int b = __ldg(&G.ptr[gq.begin[e] + (it - gq.first[e])]);
+                    if (__ldg(&G.medium[b]) == mid) {  // mMedium == medium
+                        const V3 o2 = v3(__ldg(&G.origin[3 * b]), __ldg(&G.origin[3 * b + 1]), __ldg(&G.origin[3 * b + 2]));
+                        const V3 d2 = v3(__ldg(&G.dir[3 * b]), __ldg(&G.dir[3 * b + 1]), __ldg(&G.dir[3 * b + 2]));
+                        const float r2 = G.r2max ? __ldg(&G.r2max[b]) : r2c;
+                        float dist, sinT, t1, t2;
+                        if (test_beam_beam(s.o, s.d, gq.tmin[e], gq.tmax[e], o2, d2, 0.f, __ldg(&G.length[b]), r2, &dist,
+                                           &sinT, &t1, &t2)) {
+                            const float radius = beam_radius_at(Bs, b, beam_start_radius(Bs, &Bs.radius[b]), t2);
+                            if (!(radius < dist)) {  // PhotonBeam.hxx:334-336 / 411-413
+                                ++cnt32;
+                                h += mix64((unsigned long long)b);
+                                Rgb c = bb1d_contrib<kMixed>(K, m, Lv, Bs, s, b, o2, d2, radius, dist, sinT, t1, t2);
+                                const float pdf = gq.pdf[e];
+                                if (pdf != 1.f) c = c * __fdiv_rn(1.f, pdf);
+                                part = part + c;
+                            }
+                        }
+                    }
+                }
+            }
+            qc = 0;
+            __syncwarp();
+        };
+        grid_walk(hdr, s.o, s.d, s.dmin, s.dmax, [&](uint32_t cell, float cmin, float cmax) {
+            const uint32_t begin = __ldg(&G.cells[cell]);
+            uint32_t n = __ldg(&G.cells[cell + 1]) - begin;
+            const float pdf = G.pdf ? __ldg(&G.pdf[cell]) : 1.f;
+            if (pdf != 1.f) n = hdr.max_beams;  // intersectPresampled: the first max_beams of the cell
+            if (n == 0) return;
+            if (lane == 0) {
+                if (qc == 0) gq.first[0] = 0;
+                gq.tmin[qc] = cmin;
+                gq.tmax[qc] = cmax;
+                gq.pdf[qc] = pdf;
+                gq.begin[qc] = begin;
+                gq.first[qc + 1] = gq.first[qc] + n;
+            }
+            __syncwarp();
+            ++qc;
+            if (qc == kGridQueue || gq.first[qc] >= 32) flush();
+        });
+        if (qc > 0) flush();
+        return part;
+    });
+    cnt += cnt32;
+    return res;
+}
+
+template <bool kMixed>
+__global__ void __launch_bounds__(128) k_bb1d_grid(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+                                                  const BeamGrid G, const BeamSoA Bs, const SegQueriesDev Q,
+                                                  const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
+                                                  const Outputs O, unsigned int* __restrict__ work,
+                                                  const int32_t* __restrict__ order)
+{
+    constexpr int kWarps = 4;
+    __shared__ DMedium media[UPBP_MAX_MEDIA];
+    __shared__ GridHeader s_hdr;
+    __shared__ GridQueue s_q[kWarps];
+    __shared__ upbp_mis s_e[kWarps];
+    __shared__ CamSum s_cs[kWarps];
+    if (threadIdx.x == 0) s_hdr = *G.hdr;
+    stage_media(K, media);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned qq = 0;
+        if (lane == 0) qq = atomicAdd(work, 1u);
+        const int64_t item = (int64_t)__shfl_sync(kFull, qq, 0);
+        if (item >= Q.n) break;
+        const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
+        Rgb acc = rgb(0.f);
+        unsigned long long cnt = 0, h = 0;
+        if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D)) {
+            SegCtx s;
+            init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &s_e[warp], &s_cs[warp], lane == 0);
+            __syncwarp();
+            acc = bb1d_query_grid<kMixed>(K, media, Lv, G, s_hdr, Bs, Q, q, s, s_q[warp], lane, cnt, h);
+        }
+        const float r = warp_sum(acc.r), g = warp_sum(acc.g), b = warp_sum(acc.b);
+        cnt = warp_sum_u64(cnt);
+        h = warp_sum_u64(h);
+        if (lane == 0) {
+            O.rgb[3 * q + 0] = r;
+            O.rgb[3 * q + 1] = g;
+            O.rgb[3 * q + 2] = b;
+            if (O.count) O.count[q] = (uint32_t)cnt;
+            if (O.hash) O.hash[q] = h;
+            const Rgb thr{Q.throughput[3 * q], Q.throughput[3 * q + 1], Q.throughput[3 * q + 2]};
+            splat(O.image, Q.pixel[q], thr * K.P.norm_bb1d * Rgb{r, g, b});
+        }
+    }
+}
+
 }  // namespace
+
+int bb1d_grid_blocks_per_sm(bool mixed)
+{
+    int nb = 0;
+    if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_grid<true>, 128, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bb1d_grid<false>, 128, 0);
+    return nb > 0 ? nb : 1;
+}
+
+void launch_bb1d_grid(const GatherConsts& K, const LightSoA& L, const BeamGrid& G, const BeamSoA& S,
+                      const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
+                      bool mixed, unsigned int* work, const int32_t* order, cudaStream_t stream)
+{
+    if (Q.n <= 0) return;
+    if (mixed) k_bb1d_grid<true><<<grid, 128, 0, stream>>>(K, L, G, S, Q, cam, cs, O, work, order);
+    else k_bb1d_grid<false><<<grid, 128, 0, stream>>>(K, L, G, S, Q, cam, cs, O, work, order);
+}
 
 void launch_gather_bp2d(const GatherConsts& K, const BeamBVH& B, const BeamSoA& S, const PointQueriesDev& Q,
                         const Outputs& O, int block, cudaStream_t stream)

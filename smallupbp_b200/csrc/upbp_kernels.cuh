@@ -71,6 +71,28 @@ struct BeamBVH {
     int n_leaves;
 };
 
+// The reference's uniform grid of beams (Beams/Grid.hxx:222-279, built by upbp_grid.cu): its
+// box, cell size and resolution, and the cell lists in the reference's order.
+struct GridHeader {
+    float lo[3], hi[3];          // mAABB
+    float cell[3], inv_cell[3];  // mCellSize, mInvCellSize
+    int res[3];                  // mRes
+    uint32_t shift[3];           // mIndexShift
+    uint32_t n_cells;            // mCells.size(): (res0 + 1)(res1 + 1)(res2 + 1) + 1
+    uint32_t max_beams;          // mMaxBeamsInCell (0: no reduction)
+};
+struct BeamGrid {
+    const GridHeader* hdr;
+    const uint32_t* cells;  // mCells: the first entry of every cell's list (n_cells entries)
+    const float* pdf;       // mPdfs, NULL: 1 in every cell (no reduction)
+    const int32_t* ptr;     // mPointers: beam ids, each cell's beams in descending id order
+    const float* origin;    // the beams as uploaded: origin xyz, direction xyz, length, medium
+    const float* dir;
+    const float* length;
+    const int32_t* medium;
+    const float* r2max;     // KNN radii: mMaxRadiusSqr per beam; NULL: radius^2
+};
+
 // Beam payload (index = beam id).
 struct BeamSoA {
     const float4* thr;   // throughput at origin rgb, flags (int bits)
@@ -232,6 +254,30 @@ void launch_segments_warp(const GatherConsts& K, const LightSoA& L, const Photon
                           const BeamSoA& S, const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs,
                           const Outputs& Opb, const Outputs& Obb, int grid, bool mixed, unsigned int* work,
                           int* status, const int32_t* order, cudaStream_t stream, int variant);
+// BB1D over the reference's uniform grid (upbp_set_bb1d_grid): warp per query, persistent.
+int bb1d_grid_blocks_per_sm(bool mixed);
+void launch_bb1d_grid(const GatherConsts& K, const LightSoA& L, const BeamGrid& G, const BeamSoA& S,
+                      const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
+                      bool mixed, unsigned int* work, const int32_t* order, cudaStream_t stream);
+// Grid build steps (upbp_grid.cu): the beams' boxes and the grid header; the (cell, beam) pairs of
+// every beam's rasterisation, counted and then written as sort keys; the cell lists from the
+// sorted, unique keys; the PRESAMPLE reduction from the reference's random stream.
+void launch_grid_header(const float* origin, const float* dir, const float* length, const float* rstart,
+                        const float* rchange, float radius, int64_t nb, uint32_t grid_res, uint32_t max_beams,
+                        float* partial, int blocks, GridHeader* hdr, cudaStream_t s);
+void launch_grid_count(const float* origin, const float* dir, const float* length, const float* rstart,
+                       const float* rchange, float radius, int64_t nb, const GridHeader* hdr,
+                       unsigned long long* counts, cudaStream_t s);
+void launch_grid_emit(const float* origin, const float* dir, const float* length, const float* rstart,
+                      const float* rchange, float radius, int64_t nb, const GridHeader* hdr,
+                      const unsigned long long* offsets, unsigned long long* keys, cudaStream_t s);
+void launch_grid_lists(const unsigned long long* keys, int64_t n, uint32_t* counts, int32_t* ptr, cudaStream_t s);
+void launch_grid_draws(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t* draws,
+                       cudaStream_t s);
+void launch_mt64_floats(unsigned long long seed, int64_t n, float* out, cudaStream_t s);
+void launch_grid_presample(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, const uint32_t* draw_off,
+                           const float* rnd, int32_t* ptr, float* pdf, cudaStream_t s);
+
 void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
                       const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,
                       bool mixed, unsigned int* work, int* status, const int32_t* order, cudaStream_t stream,

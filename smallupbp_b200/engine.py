@@ -31,7 +31,7 @@ MODE_PLAIN, MODE_MIXED, MODE_FP64 = 0, 1, 2
 
 EXPORTS = (
     "upbp_ctx_create", "upbp_ctx_destroy", "upbp_last_error", "upbp_set_mode", "upbp_set_tuning", "upbp_get_tuning",
-    "upbp_set_stream", "upbp_set_media", "upbp_set_params", "upbp_set_light_vertices", "upbp_set_beams",
+    "upbp_set_bb1d_grid", "upbp_set_stream", "upbp_set_media", "upbp_set_params", "upbp_set_light_vertices", "upbp_set_beams",
     "upbp_build", "upbp_set_camera_mis", "upbp_set_segment_queries", "upbp_set_point_queries", "upbp_evaluate",
     "upbp_read_segment_results", "upbp_read_point_results", "upbp_read_query_stats", "upbp_clear_image",
     "upbp_read_image", "upbp_last_launch_count", "upbp_last_timings", "upbp_destroy_structures",
@@ -83,6 +83,7 @@ def lib():
         l.upbp_set_mode.argtypes = [vp, C.c_int]
         l.upbp_set_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
         l.upbp_get_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
+        l.upbp_set_bb1d_grid.argtypes = [vp, C.POINTER(abi.Bb1dGrid)]
         l.upbp_set_stream.argtypes = [vp, vp]
         l.upbp_set_media.argtypes = [vp, C.POINTER(abi.Medium), C.c_int32]
         l.upbp_set_params.argtypes = [vp, C.POINTER(abi.Params)]
@@ -166,6 +167,12 @@ class EstimatorStage:
                 raise KeyError(k)
             setattr(t, k, v)
         self._ck(self._l.upbp_set_tuning(self._ctx, C.byref(t)))
+
+    def set_bb1d_grid(self, grid_res: int, max_beams_in_cell: int = 0, reduction: int = 0, seed: int = 1234):
+        """BB1D over the reference's uniform beam grid of resolution ``grid_res`` (0: the LBVH over
+        beam pieces), optionally reduced to ``max_beams_in_cell`` beams per cell (PRESAMPLE)."""
+        g = abi.Bb1dGrid(grid_res=grid_res, max_beams_in_cell=max_beams_in_cell, reduction=reduction, seed=seed)
+        self._ck(self._l.upbp_set_bb1d_grid(self._ctx, C.byref(g)))
 
     def get_tuning(self) -> "abi.Tuning":
         t = abi.Tuning()

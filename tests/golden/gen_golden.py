@@ -51,6 +51,15 @@ NOMIS_CASES = [
     ("boxes_nomis", "boxes", dict(seed=47)),
 ]
 
+# the estimator without MIS over the reference's uniform beam grid with the PRESAMPLE beam reduction
+# (-gridres, -gridmax, -gridred 0, the evaluator's seed): ref_bb1d and the image follow the grid
+GRID_CASES = [
+    ("cube_nomis_grid_reduced", "cube32x2048", dict(radius=0.02, seed=41), (32, 2, 0, 1234)),
+    ("boxes_nomis_grid_reduced", "boxes", dict(seed=47), (16, 3, 0, 77)),
+    ("cube_nomis_grid_short", "cube24x1536", dict(query_beam_type=W.SHORT_BEAM, photon_beam_type=W.SHORT_BEAM,
+                                                  radius=0.03, seed=43), (64, 0, 0, 1234)),
+]
+
 
 def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
@@ -92,6 +101,26 @@ def main(names=None):
         print("%-22s lv=%d beams=%d sq=%d pq=%d  cand pb2d=%d bb1d=%d pp3d=%d  %.0f KB" % (
             fname, len(w["lv_path_length"]), len(w["beam_length"]), len(w["sq_path_length"]), len(w["pq_path_length"]),
             o["count_pb2d"].sum(), o["count_bb1d"].sum(), o["count_pp3d"].sum(), os.path.getsize(path) / 1024))
+
+    for fname, cname, over, grid in GRID_CASES:
+        if names and fname not in names:
+            continue
+        cfg = scene(cname, over)
+        w = W.without_mis(W.generate(cfg))
+        ref.set_grid_options(grid[0], grid[1], grid[2], grid[3])
+        try:
+            o = ref.run(w, what=ref.PB2D | ref.BB1D_GRID | ref.PP3D, threads=8)
+        finally:
+            ref.set_grid_options()
+        out = {"in_" + k: v for k, v in w.items()}
+        out["grid_options"] = np.array(grid, np.int64)
+        for k in ("pb2d", "bb1d", "pp3d", "image"):
+            out["ref_" + k] = o[k]
+        path = os.path.join(HERE, fname + ".npz")
+        np.savez_compressed(path, **out)
+        print("%-26s grid=%s beams=%d sq=%d  bb1d nonzero=%d  %.0f KB" % (
+            fname, grid, len(w["beam_length"]), len(w["sq_path_length"]), int((np.abs(o["bb1d"]).max(1) > 0).sum()),
+            os.path.getsize(path) / 1024))
 
 
 if __name__ == "__main__":

@@ -8,7 +8,10 @@ from typing import Dict, Tuple
 import numpy as np
 
 GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FIXTURES = sorted(glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+# fixtures of the reference's uniform beam grid (with its beam reduction): grid_options and the grid's
+# outputs only (tests/test_gpu_grid.py); the others hold every estimator's outputs and candidates
+GRID_FIXTURES = sorted(glob.glob(os.path.join(GOLDEN_DIR, "*_grid_*.npz")))
+FIXTURES = sorted(set(glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))) - set(GRID_FIXTURES))
 
 # Per-query contribution tolerance of the FP32 path against the reference (relative), with an
 # absolute floor of ATOL_FRAC times the largest contribution of that estimator in the fixture.

@@ -38,14 +38,15 @@ def test_library_exports_every_declared_entry_point(lib):
 
 def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sizes.c"
-    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\nint main(void){printf("%%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu\\n",'
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\nint main(void){printf("%%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu %%zu\\n",'
                    'sizeof(upbp_mis), sizeof(upbp_medium), sizeof(upbp_params), sizeof(upbp_light_vertices),'
-                   'sizeof(upbp_beams), sizeof(upbp_segment_queries), sizeof(upbp_point_queries), sizeof(upbp_query_stats), sizeof(upbp_tuning));return 0;}' % HEADER)
+                   'sizeof(upbp_beams), sizeof(upbp_segment_queries), sizeof(upbp_point_queries), sizeof(upbp_query_stats), sizeof(upbp_tuning),'
+                   'sizeof(upbp_bb1d_grid));return 0;}' % HEADER)
     exe = tmp_path / "sizes"
     subprocess.check_call(["gcc", str(src), "-o", str(exe)])
     got = [int(x) for x in subprocess.check_output([str(exe)]).split()]
     want = [C.sizeof(t) for t in (abi.Mis, abi.Medium, abi.Params, abi.LightVertices, abi.Beams,
-                                  abi.SegmentQueries, abi.PointQueries, abi.QueryStats, abi.Tuning)]
+                                  abi.SegmentQueries, abi.PointQueries, abi.QueryStats, abi.Tuning, abi.Bb1dGrid)]
     assert got == want
 
 

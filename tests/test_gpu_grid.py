@@ -1,0 +1,139 @@
+"""BB1D over the reference's uniform beam grid (upbp_set_bb1d_grid) against the reference's own grid
+evaluator (Beams/PhGrid.hxx, Beams/Grid.hxx, run by the reference harness): the grid's cells, cell
+lists and DDA walk reproduce the reference's, so every query's contribution agrees within 1e-4,
+including the pairs that the walk finds in two cells or in none where a closest point falls on a
+cell boundary.  With the PRESAMPLE beam reduction (-gridmax, -gridred 0) the same beams are kept
+in every over-full cell, which only the reference's own random stream and shuffle give.
+"""
+import numpy as np
+import pytest
+
+import golden_io as G
+from smallupbp_b200 import engine
+
+
+@pytest.fixture(scope="module")
+def stage():
+    s = engine.EstimatorStage(0, engine.MODE_PLAIN)
+    yield s
+    s.close()
+
+
+def run(stage, w, mode, grid):
+    stage.set_mode(mode)
+    stage.set_bb1d_grid(*grid)
+    try:
+        stage.run(w)
+        pb2d, bb1d = stage.segment_results()
+        return dict(bb1d=bb1d, pb2d=pb2d, image=stage.image(), **stage.query_stats())
+    finally:
+        stage.set_bb1d_grid(0)
+
+
+def grid_options(path):
+    return tuple(int(x) for x in np.load(path)["grid_options"])
+
+
+@pytest.mark.gpu
+def test_grid_fixtures_present():
+    assert len(G.GRID_FIXTURES) >= 3
+    assert any(grid_options(p)[1] > 0 for p in G.GRID_FIXTURES)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", G.GRID_FIXTURES, ids=G.name)
+def test_grid_without_mis_matches_reference(stage, path):
+    w, r = G.load(path)
+    g = run(stage, w, engine.MODE_PLAIN, grid_options(path))
+    G.assert_close(g["bb1d"], r["bb1d"], "BB1D over the reference grid")
+    assert G.image_rel_l2(g["image"], r["image"]) <= 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", G.GRID_FIXTURES, ids=G.name)
+def test_grid_mixed_mode_same_candidates(stage, path):
+    # mixed mode: the same (cell, beam) pairs as plain FP32; the FP64 closest approach of
+    # near-parallel pairs moves only their contributions
+    w, r = G.load(path)
+    grid = grid_options(path)
+    p = run(stage, w, engine.MODE_PLAIN, grid)
+    m = run(stage, w, engine.MODE_MIXED, grid)
+    np.testing.assert_array_equal(m["count_bb1d"], p["count_bb1d"])
+    np.testing.assert_array_equal(m["hash_bb1d"], p["hash_bb1d"])
+    err = G.rel_errors(m["bb1d"].astype(np.float64), r["bb1d"].astype(np.float64))
+    assert (err <= G.RTOL).mean() >= 0.99, float(err.max())
+    assert G.image_rel_l2(m["image"], r["image"]) <= 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", G.FIXTURES, ids=G.name)
+def test_grid_with_mis_matches_reference_grid(stage, path):
+    # every fixture holds the reference's grid estimate at its default resolution (-gridres 256) as
+    # well as the brute-force one; the two differ where a closest point falls on a cell boundary
+    w, r = G.load(path)
+    g = run(stage, w, engine.MODE_PLAIN, (256, 0, 0, 1234))
+    G.assert_close(g["bb1d"], r["bb1d"], "BB1D over the reference grid (256)")
+    G.assert_close(g["pb2d"], r["pb2d"], "PB2D (unchanged by the grid)")
+
+
+@pytest.mark.gpu
+def test_grid_reduction_depends_on_the_seed(stage):
+    path = [p for p in G.GRID_FIXTURES if grid_options(p)[1] > 0][0]
+    w, r = G.load(path)
+    res, mx, red, seed = grid_options(path)
+    a = run(stage, w, engine.MODE_PLAIN, (res, mx, red, seed))
+    b = run(stage, w, engine.MODE_PLAIN, (res, mx, red, seed + 1))
+    full = run(stage, w, engine.MODE_PLAIN, (res, 0, 0, seed))
+    G.assert_close(a["bb1d"], r["bb1d"], "reduced, the fixture's seed")
+    changed = np.abs(b["bb1d"] - a["bb1d"]).max(1) > 1e-6 * np.abs(a["bb1d"]).max()
+    assert changed.mean() > 0.2
+    # the reduction tests fewer pairs than the full grid
+    assert a["count_bb1d"].sum() < full["count_bb1d"].sum()
+
+
+@pytest.mark.gpu
+def test_grid_options_rejected(stage):
+    path = [p for p in G.GRID_FIXTURES if grid_options(p)[1] > 0][0]
+    w, _ = G.load(path)
+    # the order-dependent reductions
+    with pytest.raises(engine.UpbpError) as e:
+        stage.set_bb1d_grid(32, 2, 1, 1234)
+    assert e.value.code == -1
+    with pytest.raises(engine.UpbpError):
+        stage.set_bb1d_grid(4096)
+    # the reduction needs the estimator without MIS
+    wm, _ = G.load(G.FIXTURES[0])
+    stage.set_mode(engine.MODE_PLAIN)
+    stage.set_bb1d_grid(32, 2, 0, 1234)
+    try:
+        with pytest.raises(engine.UpbpError) as e:
+            stage.run(wm)
+        assert "without MIS" in str(e.value)
+        # the FP64 mode has no grid
+        stage.set_mode(engine.MODE_FP64)
+        with pytest.raises(engine.UpbpError):
+            stage.run(w)
+    finally:
+        stage.set_bb1d_grid(0)
+        stage.set_mode(engine.MODE_PLAIN)
+    # and the context still works afterwards
+    stage.run(w)
+
+
+@pytest.mark.gpu
+def test_grid_against_the_reference_at_a_larger_size(stage):
+    # a 128 x 128 cube iteration without MIS (16,384 light paths), reduced to 4 beams per cell of a
+    # 64-cell grid, against the reference harness run here on the same inputs
+    from oracle import ref
+    from smallupbp_b200 import workload as W
+
+    cfg = W.config("cube128")
+    w = W.without_mis(W.generate(cfg, 0))
+    grid = (64, 4, 0, 2024)
+    ref.set_grid_options(*grid)
+    try:
+        o = ref.run(w, what=ref.BB1D_GRID, threads=8)
+    finally:
+        ref.set_grid_options()
+    g = run(stage, w, engine.MODE_PLAIN, grid)
+    G.assert_close(g["bb1d"], o["bb1d"], "BB1D, reduced grid, cube128")
