@@ -561,7 +561,9 @@ def run_secondary(dev, stream):
       error of mixed and plain against FP64 (percentiles) and the image rel-L2;
     * configuration 4 (`diff512`): forward (mixed) and adjoint of the L2 loss against the target
       medium, their times, the device memory, and the adjoint against central differences (step 1e-3)
-      of the FP64 forward."""
+      of the FP64 forward;
+    * the reference's uniform beam grid at -gridres 64 on cube1024 (mixed), against the LBVH over
+      beam pieces: build and BB1D times, accepted pairs, image rel-L2 between the two."""
     import torch
     from smallupbp_b200 import engine, workload as W
 
@@ -629,6 +631,26 @@ def run_secondary(dev, stream):
                                                   (("p50", 50), ("p99", 99), ("p99.9", 99.9), ("max", 100))}
                     if err.size else None}
     out["beamstress"] = c3
+    # the reference's uniform beam grid (upbp_set_bb1d_grid) on the headline workload at -gridres
+    # 64, the resolution of the CPU baseline: build + evaluate against the LBVH over beam pieces
+    cfg = W.config("cube1024")
+    cg = {"grid_res": 64}
+    for name, grid in (("lbvh_pieces", None), ("reference_grid", 64)):
+        with torch.cuda.stream(stream):
+            st = engine.EstimatorStage(dev, engine.MODE_MIXED)
+            st.set_stream(stream.cuda_stream)
+            if grid:
+                st.set_bb1d_grid(grid)
+            st.trace(cfg, 0)
+            st.build(); st.clear_image(); st.evaluate()
+            ms = timed(st, lambda: (st.build(), st.clear_image(), st.evaluate()))
+            t = st.timings()
+            cg[name] = {"ms_per_iteration": ms, "build_ms": t["build_ms"], "bb1d_ms": t["bb1d_ms"],
+                        "accepted_pairs": int(st.query_stats()["count_bb1d"].astype(np.int64).sum()),
+                        "image": st.image().astype(np.float64)}
+            st.close()
+    cg["image_rel_l2_grid_vs_pieces"] = rel_l2(cg["reference_grid"].pop("image"), cg["lbvh_pieces"].pop("image"))
+    out["cube1024_reference_grid"] = cg
     # configuration 4
     w = W.make(W.config("diff512"))
     media = np.array(w["media"], copy=True)

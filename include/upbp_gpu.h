@@ -308,9 +308,10 @@ int upbp_get_tuning(const upbp_ctx* ctx, upbp_tuning* tuning);
  * std::uniform_real_distribution<float> as libstdc++ defines it), and, as in the reference
  * (Config.hxx:1111-1112), only for the estimator without MIS (UPBP_NO_MIS).  The other reductions
  * draw from that stream in the order the queries are made, which a parallel evaluation does not
- * reproduce: they return UPBP_ERR_INVALID_ARG.  Plain and mixed modes; the grid build needs one
- * host synchronisation (its cell-list size), so its iterations are not captured as CUDA graphs.
- * grid_res 0 (the default) switches the grid off. */
+ * reproduce: they return UPBP_ERR_INVALID_ARG.  Plain and mixed modes (not UPBP_MODE_FP64, not the
+ * adjoint).  The grid build reads its sizes on the host (three synchronisations: the cell entries,
+ * the unique ones, the random draws); a CUDA graph from upbp_capture_graph replays the build with
+ * the sizes of the build before it.  grid_res 0 (the default) switches the grid off. */
 typedef struct upbp_bb1d_grid {
     uint32_t grid_res;          /* -gridres: PhotonBeamsEvaluator::sGridSize (reference default 256) */
     uint32_t max_beams_in_cell; /* -gridmax: sMaxBeamsInCell (0: no reduction) */

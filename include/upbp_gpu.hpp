@@ -73,6 +73,14 @@ public:
     }
     void set_light_vertices(const upbp_light_vertices& lv) { check(upbp_set_light_vertices(ctx_, &lv)); }
     void set_beams(const upbp_beams& b) { check(upbp_set_beams(ctx_, &b)); }
+    /* PhotonBeamsEvaluator::sGridSize / sMaxBeamsInCell / sReductionType and mSeed (the -gridres,
+     * -gridmax and -gridred options): BB1D over the reference's uniform beam grid. */
+    void set_bb1d_grid(uint32_t grid_res, uint32_t max_beams_in_cell = 0, uint32_t reduction = 0,
+                       int32_t seed = 1234)
+    {
+        const upbp_bb1d_grid g{grid_res, max_beams_in_cell, reduction, seed};
+        check(upbp_set_bb1d_grid(ctx_, &g));
+    }
     /* HashGrid::Build + EmbreeBre::build + PhotonBeamsEvaluator::build for the uploaded records. */
     void build() { check(upbp_build(ctx_)); }
 
