@@ -302,20 +302,23 @@ int upbp_get_tuning(const upbp_ctx* ctx, upbp_tuning* tuning);
  * walk tests the beams of each visited cell with the query restricted to the cell's t range
  * (Grid.hxx:322-398), so a pair whose closest point lies on a cell boundary is found in both cells
  * or in neither, as in the reference.  Optionally the reference's beam reduction (-gridmax,
- * -gridred; Grid.hxx:558-631) tests at most max_beams_in_cell beams of each cell and divides the
- * contribution by the cell's selection pdf: reduction 0 (PRESAMPLE, the reference's default) only,
- * with the reference's own random stream (std::mt19937_64 seeded with `seed`, through
- * std::uniform_real_distribution<float> as libstdc++ defines it), and, as in the reference
- * (Config.hxx:1111-1112), only for the estimator without MIS (UPBP_NO_MIS).  The other reductions
- * draw from that stream in the order the queries are made, which a parallel evaluation does not
- * reproduce: they return UPBP_ERR_INVALID_ARG.  Plain and mixed modes (not UPBP_MODE_FP64, not the
- * adjoint).  The grid build reads its sizes on the host (three synchronisations: the cell entries,
- * the unique ones, the random draws); a CUDA graph from upbp_capture_graph replays the build with
- * the sizes of the build before it.  grid_res 0 (the default) switches the grid off. */
+ * -gridred; Grid.hxx:453-631) tests max_beams_in_cell beams of each over-full cell and divides the
+ * contribution by the cell's selection pdf max_beams / beams.  The build's draws are the
+ * reference's own (std::mt19937_64 seeded with `seed`, through std::uniform_real_distribution<float>
+ * as libstdc++ defines it): PRESAMPLE (0, the reference's default) is reproduced exactly, and
+ * OFFSET (1) shuffles each over-full cell as the reference does.  The per-query draws of OFFSET,
+ * RESAMPLE_FIXED (2) and SAMPLED (3) come in the reference from the same stream in the order the
+ * queries are made, which a parallel evaluation cannot follow; here they are a function of (seed,
+ * query, segment, cell, draw) with the same distributions.  As in the reference
+ * (Config.hxx:1111-1112), the reduction is for the estimator without MIS (UPBP_NO_MIS) only.
+ * Plain and mixed modes (not UPBP_MODE_FP64, not the adjoint).  The grid build reads its sizes
+ * on the host (three synchronisations: the cell entries, the unique ones, the random draws); a
+ * CUDA graph from upbp_capture_graph replays the build with the sizes of the build before it.
+ * grid_res 0 (the default) switches the grid off. */
 typedef struct upbp_bb1d_grid {
     uint32_t grid_res;          /* -gridres: PhotonBeamsEvaluator::sGridSize (reference default 256) */
     uint32_t max_beams_in_cell; /* -gridmax: sMaxBeamsInCell (0: no reduction) */
-    uint32_t reduction;         /* -gridred: sReductionType (0: PRESAMPLE) */
+    uint32_t reduction;         /* -gridred: sReductionType (0 PRESAMPLE, 1 OFFSET, 2 RESAMPLE_FIXED, 3 SAMPLED) */
     int32_t seed;               /* PhotonBeamsEvaluator::mSeed (UPBP.hxx:417: base seed + iteration) */
 } upbp_bb1d_grid;
 int upbp_set_bb1d_grid(upbp_ctx* ctx, const upbp_bb1d_grid* grid);

@@ -289,7 +289,7 @@ void build_grid(upbp_ctx* c, cudaStream_t s, float radius, const float* rstart, 
     ensure(c, c->gr_hdr, sizeof(GridHeader));
     ensure(c, c->gr_partial, sizeof(float) * 6 * blocks);
     GridHeader* hdr = c->gr_hdr.as<GridHeader>();
-    launch_grid_header(org, dir, len, rstart, rchange, radius, nb, g.grid_res, g.max_beams_in_cell,
+    launch_grid_header(org, dir, len, rstart, rchange, radius, nb, g.grid_res, g.max_beams_in_cell, g.reduction, g.seed,
                        c->gr_partial.as<float>(), blocks, hdr, s);
     ensure(c, c->gr_counts, sizeof(unsigned long long) * (nb + 1));
     ensure(c, c->gr_offsets, sizeof(unsigned long long) * (nb + 1));
@@ -359,7 +359,8 @@ void build_grid(upbp_ctx* c, cudaStream_t s, float radius, const float* rstart, 
         ensure(c, c->gr_draws, sizeof(uint32_t) * nc);
         ensure(c, c->gr_draw_off, sizeof(uint32_t) * nc);
         ensure(c, c->gr_pdf, sizeof(float) * nc);
-        launch_grid_draws(c->gr_cells.as<uint32_t>(), nc, g.max_beams_in_cell, c->gr_draws.as<uint32_t>(), s);
+        launch_grid_draws(c->gr_cells.as<uint32_t>(), nc, g.max_beams_in_cell, g.reduction, c->gr_draws.as<uint32_t>(),
+                          s);
         b = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, b, c->gr_draws.as<uint32_t>(), c->gr_draw_off.as<uint32_t>(), (int)nc,
                                       s);
@@ -378,8 +379,9 @@ void build_grid(upbp_ctx* c, cudaStream_t s, float radius, const float* rstart, 
         ensure(c, c->gr_rnd, sizeof(float) * std::max<int64_t>(c->gr_draws_total, 1));
         // std::mt19937_64 takes the int seed converted to its 64-bit result type
         launch_mt64_floats((unsigned long long)(long long)g.seed, c->gr_draws_total, c->gr_rnd.as<float>(), s);
-        launch_grid_presample(c->gr_cells.as<uint32_t>(), nc, g.max_beams_in_cell, c->gr_draw_off.as<uint32_t>(),
-                              c->gr_rnd.as<float>(), c->gr_ptr.as<int32_t>(), c->gr_pdf.as<float>(), s);
+        launch_grid_reduce(c->gr_cells.as<uint32_t>(), nc, g.max_beams_in_cell, g.reduction,
+                           c->gr_draw_off.as<uint32_t>(), c->gr_rnd.as<float>(), c->gr_ptr.as<int32_t>(),
+                           c->gr_pdf.as<float>(), s);
         c->build_launches += 5;
     }
     c->gr_valid = true;
@@ -1237,11 +1239,8 @@ int upbp_set_bb1d_grid(upbp_ctx* c, const upbp_bb1d_grid* g)
         drop_graph(c);
         if (!g) fail(c, UPBP_ERR_INVALID_ARG, "grid is NULL");
         if (g->grid_res > 1024) fail(c, UPBP_ERR_INVALID_ARG, "grid_res must be at most 1024");
-        if (g->grid_res > 0 && g->max_beams_in_cell > 0 && g->reduction != 0)
-            fail(c, UPBP_ERR_INVALID_ARG,
-                 "reduction %u draws from the reference's random stream in the order the queries are made; "
-                 "only the PRESAMPLE reduction (0) is reproduced",
-                 g->reduction);
+        if (g->reduction > 3)
+            fail(c, UPBP_ERR_INVALID_ARG, "reduction must be 0 (PRESAMPLE), 1 (OFFSET), 2 (RESAMPLE_FIXED) or 3 (SAMPLED)");
         c->bgrid = *g;
         c->built = false;
     });

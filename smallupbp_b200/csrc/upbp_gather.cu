@@ -1279,13 +1279,30 @@ __device__ __forceinline__ void grid_walk(const GridHeader& h, V3 o, V3 d, float
 constexpr int kGridQueue = 32;
 struct GridQueue {
     float tmin[kGridQueue], tmax[kGridQueue], pdf[kGridQueue];
-    uint32_t begin[kGridQueue];
-    uint32_t first[kGridQueue + 1];  // the first item of every queued cell; first[n] = all items
+    uint32_t begin[kGridQueue], beams[kGridQueue];
+    unsigned long long key[kGridQueue];  // the cell's draws (reductions 1-3)
+    uint32_t first[kGridQueue + 1];      // the first item of every queued cell; first[n] = all items
 };
 
+// The per-query draws of the OFFSET, RESAMPLE_FIXED and SAMPLED reductions (Grid.hxx:466-548).  The
+// reference takes them from the grid's one sequential stream in the order the queries are made;
+// here each is a function of (seed, query, segment, cell, draw), the same uniform distribution
+// whatever the order of evaluation: a SplitMix64 finaliser, 24 bits to [0, 1).
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ float grid_draw(unsigned long long key, uint32_t j)
+{
+    return (float)(splitmix64(key + (unsigned long long)j * 0xD1B54A32D192ED03ull) >> 40) * 0x1p-24f;
+}
+
 // BB1D of one query by one warp over the beam grid.  The walk runs on every lane alike and queues
-// the visited cells that hold beams (the first max_beams_in_cell of an over-full cell of a reduced
-// grid, Grid.hxx:453-465); once 32 or more (cell, beam) items wait, the lanes test them 32 at a
+// the visited cells that hold beams (max_beams_in_cell items of an over-full cell of a reduced
+// grid, Grid.hxx:453-548); once 32 or more (cell, beam) items wait, the lanes test them 32 at a
 // time: PhotonBeam::accumulate / accumulate2 (PhotonBeam.hxx:315-367, 375-480) with the query
 // restricted to the cell's t range, the contribution divided by the cell's selection pdf.
 template <bool kMixed>
@@ -1307,8 +1324,24 @@ __device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMed
                 if (it < total) {
                     int e = 0;
                     while (e + 1 < qc && gq.first[e + 1] <= it) ++e;
-                    const int b = __ldg(&G.ptr[gq.begin[e] + (it - gq.first[e])]);
-                    if (__ldg(&G.medium[b]) == mid) {  // mMedium == medium
+                    const uint32_t j = it - gq.first[e], begin = gq.begin[e], beams = gq.beams[e];
+                    // the beam of item j: intersectPresampled / intersectOffsetted / intersectFixedSampled /
+                    // intersectSampled (Grid.hxx:453-548); unreduced cells and PRESAMPLE: the j-th of the list
+                    uint32_t at = begin + j;
+                    bool take = true;
+                    if (gq.pdf[e] != 1.f && hdr.reduction != 0) {
+                        if (hdr.reduction == 1) {
+                            const uint32_t off = (uint32_t)__fmul_rn(grid_draw(gq.key[e], 0), (float)beams);
+                            const uint32_t k = min(hdr.max_beams, beams - min(off, beams));
+                            at = j < k ? begin + off + j : begin + (j - k);
+                        } else if (hdr.reduction == 2) {
+                            at = begin + min((uint32_t)__fmul_rn(grid_draw(gq.key[e], j), (float)beams), beams - 1);
+                        } else {
+                            take = grid_draw(gq.key[e], j) < gq.pdf[e];
+                        }
+                    }
+                    const int b = __ldg(&G.ptr[at]);
+                    if (take && __ldg(&G.medium[b]) == mid) {  // mMedium == medium
                         const V3 o2 = v3(__ldg(&G.origin[3 * b]), __ldg(&G.origin[3 * b + 1]), __ldg(&G.origin[3 * b + 2]));
                         const V3 d2 = v3(__ldg(&G.dir[3 * b]), __ldg(&G.dir[3 * b + 1]), __ldg(&G.dir[3 * b + 2]));
                         const float r2 = G.r2max ? __ldg(&G.r2max[b]) : r2c;
@@ -1331,11 +1364,16 @@ __device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMed
             qc = 0;
             __syncwarp();
         };
+        // the reductions' draws of this query and segment
+        const unsigned long long qkey =
+            splitmix64(((unsigned long long)(uint32_t)hdr.seed << 32) ^ (unsigned long long)q) ^
+            ((unsigned long long)__float_as_uint(s.dmin) * 0x94D049BB133111EBull);
         grid_walk(hdr, s.o, s.d, s.dmin, s.dmax, [&](uint32_t cell, float cmin, float cmax) {
             const uint32_t begin = __ldg(&G.cells[cell]);
-            uint32_t n = __ldg(&G.cells[cell + 1]) - begin;
+            const uint32_t beams = __ldg(&G.cells[cell + 1]) - begin;
             const float pdf = G.pdf ? __ldg(&G.pdf[cell]) : 1.f;
-            if (pdf != 1.f) n = hdr.max_beams;  // intersectPresampled: the first max_beams of the cell
+            // a reduced cell tests max_beams beams, SAMPLED draws for each of them
+            const uint32_t n = (pdf != 1.f && hdr.reduction != 3) ? hdr.max_beams : beams;
             if (n == 0) return;
             if (lane == 0) {
                 if (qc == 0) gq.first[0] = 0;
@@ -1343,6 +1381,8 @@ __device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMed
                 gq.tmax[qc] = cmax;
                 gq.pdf[qc] = pdf;
                 gq.begin[qc] = begin;
+                gq.beams[qc] = beams;
+                gq.key[qc] = splitmix64(qkey + (unsigned long long)cell * 0x9E3779B97F4A7C15ull);
                 gq.first[qc + 1] = gq.first[qc] + n;
             }
             __syncwarp();

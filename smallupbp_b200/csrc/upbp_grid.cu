@@ -7,10 +7,11 @@
 //    Grid.hxx:177-219), a cell entered once per beam: each (cell, beam) pair becomes a 64-bit key
 //    cell << 32 | ~beam, and sorted unique keys give the cell lists with every cell's beams in
 //    descending id order, the order in which Grid's Store pass fills them;
-//  * the PRESAMPLE reduction (Grid::reduceBeams, Grid.hxx:558-598): the over-full cells, in cell
-//    order, each shuffle their first max_beams entries with max_beams draws from the reference's
-//    stream: std::mt19937_64 (Rng.hxx:51-62) through std::uniform_real_distribution<float>, which
-//    libstdc++ computes as float(x) / 2^64 from one 64-bit output, clamped below 1.
+//  * the reductions' build (Grid::reduceBeams, Grid.hxx:558-631): the over-full cells, in cell
+//    order, take their draws from the reference's stream, std::mt19937_64 (Rng.hxx:51-62) through
+//    std::uniform_real_distribution<float>, which libstdc++ computes as float(x) / 2^64 from one
+//    64-bit output, clamped below 1: PRESAMPLE shuffles the first max_beams entries of a cell
+//    (max_beams draws), OFFSET all of them (beams - 1 draws).
 // The float operations are the reference's (SSE, no fused multiply-add), written with the _rn
 // intrinsics so that the compiler does not contract them.
 #include <cfloat>
@@ -105,7 +106,7 @@ __global__ void k_grid_boxes_partial(const float* __restrict__ origin, const flo
 // Grid::build (Grid.hxx:222-241): the resolution from the box's largest extent, the cell size and
 // its inverse, the index shifts.
 __global__ void k_grid_header(const float* __restrict__ partial, int blocks, uint32_t grid_res, uint32_t max_beams,
-                              GridHeader* hdr)
+                              uint32_t reduction, int32_t seed, GridHeader* hdr)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     GridHeader h;
@@ -131,6 +132,8 @@ __global__ void k_grid_header(const float* __restrict__ partial, int blocks, uin
     h.shift[2] = (uint32_t)h.res[0] * (uint32_t)h.res[1];
     h.n_cells = ((uint32_t)h.res[0] + 1u) * ((uint32_t)h.res[1] + 1u) * ((uint32_t)h.res[2] + 1u) + 1u;
     h.max_beams = max_beams;
+    h.reduction = reduction;
+    h.seed = seed;
     // a box without extent along an axis (or not finite) has no cells: n_cells 0 stops the
     // rasterisation kernels and the host rejects the build
     bool ok = true;
@@ -241,14 +244,17 @@ __global__ void k_grid_lists(const unsigned long long* __restrict__ keys, int64_
     }
 }
 
-// draws of every cell: max_beams for an over-full cell, else none (Grid.hxx:576-596)
+// the build's draws of every cell (Grid.hxx:571-631): PRESAMPLE max_beams and OFFSET beams - 1 for
+// an over-full cell, the resampling reductions none
 __global__ void k_grid_draws(const uint32_t* __restrict__ cells, uint32_t n_cells, uint32_t max_beams,
-                             uint32_t* draws)
+                             uint32_t reduction, uint32_t* draws)
 {
     // mPdfs covers the cells 0 .. n_cells - 2 (reduceBeams: cells = mCells.size() - 1)
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)n_cells;
-         i += (int64_t)gridDim.x * blockDim.x)
-        draws[i] = (i + 1 < (int64_t)n_cells && cells[i + 1] - cells[i] > max_beams) ? max_beams : 0u;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t beams = i + 1 < (int64_t)n_cells ? cells[i + 1] - cells[i] : 0u;
+        draws[i] = beams <= max_beams ? 0u : (reduction == 0 ? max_beams : (reduction == 1 ? beams - 1 : 0u));
+    }
 }
 
 // std::mt19937_64 (the 64-bit Mersenne Twister: n = 312, m = 156, r = 31, a = 0xb5026f5aa96619e9,
@@ -302,11 +308,12 @@ __global__ void __launch_bounds__(kMtN) k_mt64_floats(unsigned long long seed, i
     }
 }
 
-// Grid::reduceBeams, PRESAMPLE (Grid.hxx:571-598): per over-full cell, a partial Fisher-Yates
-// shuffle of its first max_beams entries, and the cell's selection pdf max_beams / beams.
-__global__ void k_grid_presample(const uint32_t* __restrict__ cells, uint32_t n_cells, uint32_t max_beams,
-                                 const uint32_t* __restrict__ draw_off, const float* __restrict__ rnd, int32_t* ptr,
-                                 float* pdf)
+// Grid::reduceBeams (Grid.hxx:558-631): every cell's selection pdf, max_beams / beams for an
+// over-full cell; PRESAMPLE shuffles the first max_beams entries of such a cell (a partial
+// Fisher-Yates from the front), OFFSET shuffles all of them (from the back).
+__global__ void k_grid_reduce(const uint32_t* __restrict__ cells, uint32_t n_cells, uint32_t max_beams,
+                              uint32_t reduction, const uint32_t* __restrict__ draw_off, const float* __restrict__ rnd,
+                              int32_t* ptr, float* pdf)
 {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c + 1 < (int64_t)n_cells;
          c += (int64_t)gridDim.x * blockDim.x) {
@@ -317,12 +324,23 @@ __global__ void k_grid_presample(const uint32_t* __restrict__ cells, uint32_t n_
         }
         pdf[c] = __fdiv_rn((float)max_beams, (float)beams);
         const float* r = rnd + draw_off[c];
-        for (uint32_t i = 0; i < max_beams; ++i) {
-            const uint32_t j = i + (uint32_t)__fmul_rn(r[i], (float)(beams - i));
-            if (j < beams) {  // r < 1: always
-                const int32_t t = ptr[begin + i];
-                ptr[begin + i] = ptr[begin + j];
-                ptr[begin + j] = t;
+        if (reduction == 0) {
+            for (uint32_t i = 0; i < max_beams; ++i) {
+                const uint32_t j = i + (uint32_t)__fmul_rn(r[i], (float)(beams - i));
+                if (j < beams) {  // r < 1: always
+                    const int32_t t = ptr[begin + i];
+                    ptr[begin + i] = ptr[begin + j];
+                    ptr[begin + j] = t;
+                }
+            }
+        } else if (reduction == 1) {
+            for (uint32_t i = beams - 1, k = 0; i > 0; --i, ++k) {
+                const uint32_t j = (uint32_t)__fmul_rn(r[k], (float)(i + 1));
+                if (j <= i) {  // r < 1: always
+                    const int32_t t = ptr[begin + i];
+                    ptr[begin + i] = ptr[begin + j];
+                    ptr[begin + j] = t;
+                }
             }
         }
     }
@@ -332,10 +350,11 @@ __global__ void k_grid_presample(const uint32_t* __restrict__ cells, uint32_t n_
 
 void launch_grid_header(const float* origin, const float* dir, const float* length, const float* rstart,
                         const float* rchange, float radius, int64_t nb, uint32_t grid_res, uint32_t max_beams,
-                        float* partial, int blocks, GridHeader* hdr, cudaStream_t s)
+                        uint32_t reduction, int32_t seed, float* partial, int blocks, GridHeader* hdr,
+                        cudaStream_t s)
 {
     k_grid_boxes_partial<<<blocks, kThreads, 0, s>>>(origin, dir, length, rstart, rchange, radius, nb, partial);
-    k_grid_header<<<1, 32, 0, s>>>(partial, blocks, grid_res, max_beams, hdr);
+    k_grid_header<<<1, 32, 0, s>>>(partial, blocks, grid_res, max_beams, reduction, seed, hdr);
 }
 void launch_grid_count(const float* origin, const float* dir, const float* length, const float* rstart,
                        const float* rchange, float radius, int64_t nb, const GridHeader* hdr,
@@ -357,19 +376,22 @@ void launch_grid_lists(const unsigned long long* keys, int64_t n, uint32_t* coun
 {
     if (n > 0) k_grid_lists<<<blocks_for(n), kThreads, 0, s>>>(keys, n, counts, ptr);
 }
-void launch_grid_draws(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t* draws, cudaStream_t s)
+void launch_grid_draws(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t reduction,
+                       uint32_t* draws, cudaStream_t s)
 {
-    if (n_cells > 0) k_grid_draws<<<blocks_for(n_cells), kThreads, 0, s>>>(cells, n_cells, max_beams, draws);
+    if (n_cells > 0)
+        k_grid_draws<<<blocks_for(n_cells), kThreads, 0, s>>>(cells, n_cells, max_beams, reduction, draws);
 }
 void launch_mt64_floats(unsigned long long seed, int64_t n, float* out, cudaStream_t s)
 {
     if (n > 0) k_mt64_floats<<<1, kMtN, 0, s>>>(seed, n, out);
 }
-void launch_grid_presample(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, const uint32_t* draw_off,
-                           const float* rnd, int32_t* ptr, float* pdf, cudaStream_t s)
+void launch_grid_reduce(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t reduction,
+                        const uint32_t* draw_off, const float* rnd, int32_t* ptr, float* pdf, cudaStream_t s)
 {
     if (n_cells > 1)
-        k_grid_presample<<<blocks_for(n_cells), kThreads, 0, s>>>(cells, n_cells, max_beams, draw_off, rnd, ptr, pdf);
+        k_grid_reduce<<<blocks_for(n_cells), kThreads, 0, s>>>(cells, n_cells, max_beams, reduction, draw_off, rnd,
+                                                               ptr, pdf);
 }
 
 }  // namespace upbp

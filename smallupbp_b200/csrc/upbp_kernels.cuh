@@ -80,6 +80,8 @@ struct GridHeader {
     uint32_t shift[3];           // mIndexShift
     uint32_t n_cells;            // mCells.size(): (res0 + 1)(res1 + 1)(res2 + 1) + 1
     uint32_t max_beams;          // mMaxBeamsInCell (0: no reduction)
+    uint32_t reduction;          // mReductionType: 0 PRESAMPLE, 1 OFFSET, 2 RESAMPLE_FIXED, 3 SAMPLED
+    int32_t seed;                // the evaluator's seed (the per-query draws of reductions 1-3)
 };
 struct BeamGrid {
     const GridHeader* hdr;
@@ -264,7 +266,8 @@ void launch_bb1d_grid(const GatherConsts& K, const LightSoA& L, const BeamGrid& 
 // sorted, unique keys; the PRESAMPLE reduction from the reference's random stream.
 void launch_grid_header(const float* origin, const float* dir, const float* length, const float* rstart,
                         const float* rchange, float radius, int64_t nb, uint32_t grid_res, uint32_t max_beams,
-                        float* partial, int blocks, GridHeader* hdr, cudaStream_t s);
+                        uint32_t reduction, int32_t seed, float* partial, int blocks, GridHeader* hdr,
+                        cudaStream_t s);
 void launch_grid_count(const float* origin, const float* dir, const float* length, const float* rstart,
                        const float* rchange, float radius, int64_t nb, const GridHeader* hdr,
                        unsigned long long* counts, cudaStream_t s);
@@ -272,11 +275,11 @@ void launch_grid_emit(const float* origin, const float* dir, const float* length
                       const float* rchange, float radius, int64_t nb, const GridHeader* hdr,
                       const unsigned long long* offsets, unsigned long long* keys, cudaStream_t s);
 void launch_grid_lists(const unsigned long long* keys, int64_t n, uint32_t* counts, int32_t* ptr, cudaStream_t s);
-void launch_grid_draws(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t* draws,
-                       cudaStream_t s);
+void launch_grid_draws(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t reduction,
+                       uint32_t* draws, cudaStream_t s);
 void launch_mt64_floats(unsigned long long seed, int64_t n, float* out, cudaStream_t s);
-void launch_grid_presample(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, const uint32_t* draw_off,
-                           const float* rnd, int32_t* ptr, float* pdf, cudaStream_t s);
+void launch_grid_reduce(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t reduction,
+                        const uint32_t* draw_off, const float* rnd, int32_t* ptr, float* pdf, cudaStream_t s);
 
 void launch_bb1d_warp(const GatherConsts& K, const LightSoA& L, const BeamBVH& B, const BeamSoA& S,
                       const SegQueriesDev& Q, const upbp_mis* cam, const CamSum* cs, const Outputs& O, int grid,

@@ -3,7 +3,10 @@ evaluator (Beams/PhGrid.hxx, Beams/Grid.hxx, run by the reference harness): the 
 lists and DDA walk reproduce the reference's, so every query's contribution agrees within 1e-4,
 including the pairs that the walk finds in two cells or in none where a closest point falls on a
 cell boundary.  With the PRESAMPLE beam reduction (-gridmax, -gridred 0) the same beams are kept
-in every over-full cell, which only the reference's own random stream and shuffle give.
+in every over-full cell, which only the reference's own random stream and shuffle give.  The
+OFFSET, RESAMPLE_FIXED and SAMPLED reductions draw per query from a stream that does not depend on
+the order of evaluation (the reference's depends on it); they are checked for what the reference's
+estimators guarantee: averaged over seeds, the estimate of the unreduced grid.
 """
 import numpy as np
 import pytest
@@ -95,9 +98,9 @@ def test_grid_reduction_depends_on_the_seed(stage):
 def test_grid_options_rejected(stage):
     path = [p for p in G.GRID_FIXTURES if grid_options(p)[1] > 0][0]
     w, _ = G.load(path)
-    # the order-dependent reductions
+    # reductions beyond SAMPLED, resolutions beyond 1024
     with pytest.raises(engine.UpbpError) as e:
-        stage.set_bb1d_grid(32, 2, 1, 1234)
+        stage.set_bb1d_grid(32, 2, 4, 1234)
     assert e.value.code == -1
     with pytest.raises(engine.UpbpError):
         stage.set_bb1d_grid(4096)
@@ -137,3 +140,52 @@ def test_grid_against_the_reference_at_a_larger_size(stage):
         ref.set_grid_options()
     g = run(stage, w, engine.MODE_PLAIN, grid)
     G.assert_close(g["bb1d"], o["bb1d"], "BB1D, reduced grid, cube128")
+
+
+@pytest.mark.gpu
+def test_grid_graph_replay_matches_direct_evaluation():
+    # upbp_capture_graph records clear + build + evaluate; the grid build then runs without its host
+    # synchronisations, with the sizes of the build before it
+    path = [p for p in G.GRID_FIXTURES if grid_options(p)[1] > 0][0]
+    w, r = G.load(path)
+    s = engine.EstimatorStage(0, engine.MODE_MIXED)
+    try:
+        s.set_bb1d_grid(*grid_options(path))
+        s.run(w)
+        _, direct = s.segment_results()
+        img = s.image()
+        s.capture_graph()
+        for _ in range(2):
+            s.launch_graph()
+            _, replay = s.segment_results()
+            np.testing.assert_array_equal(replay, direct)
+            assert G.image_rel_l2(s.image(), img) < 1e-6
+        G.assert_close(direct, r["bb1d"], "BB1D, reduced grid")
+    finally:
+        s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("reduction", [0, 1, 2, 3], ids=["presample", "offset", "resample_fixed", "sampled"])
+def test_grid_reductions_are_unbiased(stage, reduction):
+    # every reduction divides a cell's contributions by its selection pdf max_beams / beams, so its
+    # mean over seeds is the unreduced grid's estimate; 48 seeds, within 4 standard errors
+    path = [p for p in G.GRID_FIXTURES if grid_options(p)[1] > 0][0]
+    w, _ = G.load(path)
+    res, mx = grid_options(path)[:2]
+    f = run(stage, w, engine.MODE_PLAIN, (res, 0, 0, 1))
+    full = f["bb1d"].astype(np.float64)
+    totals, per_query = [], []
+    for seed in range(48):
+        g = run(stage, w, engine.MODE_PLAIN, (res, mx, reduction, 1000 + seed))
+        assert g["count_bb1d"].sum() < f["count_bb1d"].sum()  # fewer pairs tested and accepted
+        per_query.append(g["bb1d"].astype(np.float64))
+        totals.append(per_query[-1].sum())
+    totals = np.array(totals)
+    ref_total = full.sum()
+    se = totals.std(ddof=1) / np.sqrt(len(totals))
+    assert se > 0, "the seeds changed nothing"
+    assert abs(totals.mean() - ref_total) <= 4 * se + 1e-4 * abs(ref_total), (totals.mean(), ref_total, se)
+    # and query by query the seed average approaches the unreduced estimate
+    mean = np.mean(per_query, axis=0)
+    assert G.image_rel_l2(mean, full) < 0.25
