@@ -398,10 +398,18 @@ __device__ __forceinline__ void finish_warp(const GenOut& O, int64_t q, const Rg
 // ------------------------------------------------------------------ kernels
 constexpr int kGenQueue = 64;
 
+// Blocks per SM the compiler must fit: the adjoint's dual-number gathers take every register a
+// thread can have, which leaves 2 blocks of 128 threads per SM; asking for 3 costs some spills and
+// runs the diff512 adjoint 8 % faster (4 spills more than it gains).  The FP64 gathers keep theirs.
+template <class T>
+struct GenMinBlocks {
+    static constexpr int value = is_dual<T>::value ? 3 : 1;
+};
+
 // PB2D, warp per query with a candidate queue (the scheme of the BB1D kernel below, over the
 // photon LBVH): the lanes test 32 photons at a time and evaluate the accepted ones 32 at a time.
 template <class T>
-__global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ GatherConsts K,
+__global__ void __launch_bounds__(128, GenMinBlocks<T>::value) k_gen_pb2d(const __grid_constant__ GatherConsts K,
                                                   const __grid_constant__ GenConsts G, const LightSoA Lv,
                                                   const PhotonBVH B, const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
@@ -481,7 +489,7 @@ __global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ Gather
 // BB1D, warp per query with the two queues of the FP32 warp kernel: pieces past the predicate's
 // first check, then accepted candidates.
 template <class T>
-__global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ GatherConsts K,
+__global__ void __launch_bounds__(128, GenMinBlocks<T>::value) k_gen_bb1d(const __grid_constant__ GatherConsts K,
                                                   const __grid_constant__ GenConsts G, const BeamBVH B,
                                                   const BeamSoA Bs, const LightSum* __restrict__ lsums,
                                                   const SegQueriesDev Q,
