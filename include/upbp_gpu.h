@@ -485,8 +485,11 @@ int upbp_trace_camera_paths(upbp_ctx* ctx, const upbp_scene* scene, uint32_t ite
  * sq_origin, sq_direction, sq_seg_begin, sq_seg_count, sq_flags, sq_path_length,
  * sq_last_pdf_w_inv, sq_throughput, sq_pixel, sq_cam_mis_begin, seg_dist_min, seg_dist_max,
  * seg_pdf, seg_rev_pdf, seg_attenuation, seg_medium, pq_position, pq_dir_fix, pq_medium_id,
- * pq_path_length, pq_throughput, pq_pixel, pq_cam_mis_begin.  *bytes receives the array's size;
- * dst may be NULL to query it. */
+ * pq_path_length, pq_throughput, pq_pixel, pq_cam_mis_begin; and after a build over the beam grid
+ * (upbp_set_bb1d_grid) its structure as the reference holds it (Grid.hxx:644-646):
+ * bb1d_grid_cells (mCells, uint32), bb1d_grid_beams (mPointers as beam indices, int32) and, with a
+ * reduction, bb1d_grid_pdfs (mPdfs, float).  *bytes receives the array's size; dst may be NULL to
+ * query it. */
 int upbp_read_input(upbp_ctx* ctx, const char* name, void* dst, int64_t capacity_bytes, int64_t* bytes);
 
 /* Releases the per-iteration structures; replaces EmbreeBre::destroy and

@@ -115,6 +115,22 @@ class Session:
         self._l.ref_eval(self._h, max(self.n_segment, self.n_point), 1, C.byref(o))  # no queries: reads the build time
         self.build_ms = o.build_ms
 
+    def grid_structure(self) -> Dict[str, np.ndarray]:
+        """The reference grid's cell lists (a session prepared with BB1D_GRID): ``cells`` (mCells),
+        ``beams`` (mPointers as beam indices) and ``pdfs`` (mPdfs)."""
+        l = self._l
+        l.ref_grid_structure.restype = C.c_int
+        l.ref_grid_structure.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        nc, ne = C.c_int64(), C.c_int64()
+        if l.ref_grid_structure(self._h, None, None, None, C.byref(nc), C.byref(ne)) != 0:
+            raise RuntimeError("ref_grid_structure failed")
+        cells = np.zeros(nc.value, np.uint32)
+        beams = np.zeros(ne.value, np.int32)
+        pdfs = np.zeros(max(nc.value - 1, 0), np.float32)
+        l.ref_grid_structure(self._h, cells.ctypes.data, beams.ctypes.data, pdfs.ctypes.data, C.byref(nc), C.byref(ne))
+        return {"cells": cells, "beams": beams, "pdfs": pdfs}
+
     def eval(self, offset: int, stride: int) -> float:
         """Evaluate queries offset, offset+stride, ...; returns the wall time in ms."""
         o = RefOutputs()

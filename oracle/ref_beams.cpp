@@ -18,8 +18,31 @@
 #if defined(UPBP_REF_USE_BRUTE)
 #define PhotonBeamsEvaluator PhotonBeamsEvaluatorBrute
 #define AccelStruct AccelStructBrute
+#else
+// the grid's cell lists are private members (Grid.hxx:644-646); ref_grid_export reads them
+#define private public
+#define protected public
 #endif
 #include "Beams/PhBeams.cxx"
+
+#if !defined(UPBP_REF_USE_BRUTE)
+/* The grid of a built evaluator: mCells, mPointers as indices from `base` (the beams array) and
+ * mPdfs.  AccelStruct derives privately from Grid<AccelStruct> (PhGrid.hxx:36): a C-style cast
+ * reaches the base. */
+int ref_grid_export(const PhotonBeamsEvaluator& e, const PhotonBeam* base, uint32_t* cells, int32_t* beams, float* pdfs,
+                    int64_t* n_cells, int64_t* n_entries)
+{
+    if (!e.accelStruct) return -2;
+    const Grid<AccelStruct>* g = (const Grid<AccelStruct>*)e.accelStruct;
+    if (n_cells) *n_cells = (int64_t)g->mCells.size();
+    if (n_entries) *n_entries = (int64_t)g->mPointers.size();
+    if (cells) std::copy(g->mCells.begin(), g->mCells.end(), cells);
+    if (beams)
+        for (size_t i = 0; i < g->mPointers.size(); ++i) beams[i] = (int32_t)(g->mPointers[i] - base);
+    if (pdfs) std::copy(g->mPdfs.begin(), g->mPdfs.end(), pdfs);
+    return 0;
+}
+#endif
 
 #if defined(UPBP_REF_USE_BRUTE)
 /* Opaque entry points so the main harness TU (which sees the grid class

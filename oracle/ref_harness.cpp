@@ -385,6 +385,22 @@ extern "C" int ref_radii(void* h, float* ph_r2, float* bm_start, float* bm_end, 
     return 0;
 }
 
+/* The reference grid of a session prepared with REF_BB1D_GRID: mCells, mPointers as beam indices
+ * and mPdfs (ref_beams.cpp:ref_grid_export, where the grid class is visible).  NULL outputs only
+ * report the sizes. */
+int ref_grid_export(const PhotonBeamsEvaluator& e, const PhotonBeam* base, uint32_t* cells, int32_t* beams, float* pdfs,
+                    int64_t* n_cells, int64_t* n_entries);
+
+extern "C" int ref_grid_structure(void* h, uint32_t* cells, int32_t* beams, float* pdfs, int64_t* n_cells,
+                                  int64_t* n_entries)
+{
+    RefSession* S = static_cast<RefSession*>(h);
+    if (!S || S->worlds.empty() || !S->worlds[0]) return -1;
+    UPBP& U = *S->worlds[0]->upbp;
+    if (!U.mBB1DPhotonBeams.accelStruct || U.mPhotonBeamsArray.empty()) return -2;
+    return ref_grid_export(U.mBB1DPhotonBeams, &U.mPhotonBeamsArray[0], cells, beams, pdfs, n_cells, n_entries);
+}
+
 /* Evaluate queries q = offset + k*stride; returns the wall time in ms through out->gather_ms. */
 extern "C" int ref_eval(void* h, int64_t offset, int64_t stride, ref_outputs* out)
 {

@@ -1653,6 +1653,12 @@ int upbp_read_input(upbp_ctx* c, const char* name, void* dst, int64_t capacity, 
             {"pq_medium_id", &c->pq_med, 4 * np}, {"pq_path_length", &c->pq_plen, 4 * np},
             {"pq_throughput", &c->pq_thr, 12 * np}, {"pq_pixel", &c->pq_pixel, 4 * np},
             {"pq_cam_mis_begin", &c->pq_cam_begin, 8 * np},
+            // the beam grid of the last build (upbp_set_bb1d_grid): the reference's mCells,
+            // mPointers as beam ids, mPdfs
+            {"bb1d_grid_cells", &c->gr_cells, c->gr_valid ? 4 * (int64_t)c->gr_host.n_cells : 0},
+            {"bb1d_grid_beams", &c->gr_ptr, c->gr_valid ? 4 * c->gr_pairs : 0},
+            {"bb1d_grid_pdfs", &c->gr_pdf,
+             c->gr_valid && c->bgrid.max_beams_in_cell > 0 ? 4 * ((int64_t)c->gr_host.n_cells - 1) : 0},
         };
         for (const Entry& e : table) {
             if (std::strcmp(e.name, name) != 0) continue;

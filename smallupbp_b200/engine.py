@@ -230,6 +230,20 @@ class EstimatorStage:
         self._ck(self._l.upbp_read_input(self._ctx, name.encode(), None, 0, C.byref(n)))
         return n.value
 
+    def grid_structure(self) -> Dict[str, np.ndarray]:
+        """The beam grid of the last build (upbp_set_bb1d_grid) as the reference holds it: ``cells``
+        (mCells), ``beams`` (mPointers as beam indices) and ``pdfs`` (mPdfs, empty without a
+        reduction)."""
+        out = {}
+        for key, name, dt in (("cells", "bb1d_grid_cells", np.uint32), ("beams", "bb1d_grid_beams", np.int32),
+                              ("pdfs", "bb1d_grid_pdfs", np.float32)):
+            nbytes = self.input_bytes(name)
+            a = np.zeros(nbytes // 4, dt)
+            if nbytes:
+                self._ck(self._l.upbp_read_input(self._ctx, name.encode(), C.c_void_p(a.ctypes.data), nbytes, None))
+            out[key] = a
+        return out
+
     def read_inputs(self, names=None) -> Dict[str, np.ndarray]:
         """Copy stored input arrays back (as the workload dict names and shapes them)."""
         from .workload import MIS_DTYPE

@@ -189,3 +189,35 @@ def test_grid_reductions_are_unbiased(stage, reduction):
     # and query by query the seed average approaches the unreduced estimate
     mean = np.mean(per_query, axis=0)
     assert G.image_rel_l2(mean, full) < 0.25
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", G.GRID_FIXTURES, ids=G.name)
+def test_grid_structure_bit_exact_with_the_reference(path):
+    # the cells' first entries, the beams of every cell in the reference's order (after the build's
+    # shuffles) and the selection pdfs, against the reference grid itself (PhGrid.hxx / Grid.hxx)
+    from oracle import ref
+
+    w, _ = G.load(path)
+    grid = grid_options(path)
+    for reduction in ((0, 1) if grid[1] > 0 else (0,)):
+        opts = (grid[0], grid[1], reduction, grid[3])
+        ref.set_grid_options(*opts)
+        try:
+            sess = ref.Session(w, what=ref.BB1D_GRID, threads=1)
+            want = sess.grid_structure()
+            sess.close()
+        finally:
+            ref.set_grid_options()
+        s = engine.EstimatorStage(0, engine.MODE_PLAIN)
+        try:
+            s.set_bb1d_grid(*opts)
+            s.run(w)
+            got = s.grid_structure()
+        finally:
+            s.close()
+        np.testing.assert_array_equal(got["cells"], want["cells"])
+        np.testing.assert_array_equal(got["beams"], want["beams"])
+        if grid[1] > 0:
+            np.testing.assert_array_equal(got["pdfs"], want["pdfs"])
+        assert want["beams"].size > 0
