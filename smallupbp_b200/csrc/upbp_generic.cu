@@ -398,19 +398,10 @@ __device__ __forceinline__ void finish_warp(const GenOut& O, int64_t q, const Rg
 // ------------------------------------------------------------------ kernels
 constexpr int kGenQueue = 64;
 
-// Blocks per SM the compiler must fit: the adjoint's dual-number gathers take every register a
-// thread can have, which leaves 2 blocks of 128 threads per SM; asking for 3 costs some spills and
-// runs the diff512 adjoint 8 % faster (4 spills more than it gains).  The FP64 gathers keep theirs.
-template <class T>
-struct GenMinBlocks {
-    static constexpr int value = is_dual<T>::value ? 3 : 1;
-};
-
 // PB2D, warp per query with a candidate queue (the scheme of the BB1D kernel below, over the
 // photon LBVH): the lanes test 32 photons at a time and evaluate the accepted ones 32 at a time.
 template <class T>
-__global__ void __launch_bounds__(128, GenMinBlocks<T>::value) k_gen_pb2d(const __grid_constant__ GatherConsts K,
-                                                  const __grid_constant__ GenConsts G, const LightSoA Lv,
+__device__ __forceinline__ void gen_pb2d_body(const GatherConsts& K, const GenConsts& G, const LightSoA Lv,
                                                   const PhotonBVH B, const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
                                                   const GenOut O, unsigned int* __restrict__ work,
@@ -489,8 +480,7 @@ __global__ void __launch_bounds__(128, GenMinBlocks<T>::value) k_gen_pb2d(const 
 // BB1D, warp per query with the two queues of the FP32 warp kernel: pieces past the predicate's
 // first check, then accepted candidates.
 template <class T>
-__global__ void __launch_bounds__(128, GenMinBlocks<T>::value) k_gen_bb1d(const __grid_constant__ GatherConsts K,
-                                                  const __grid_constant__ GenConsts G, const BeamBVH B,
+__device__ __forceinline__ void gen_bb1d_body(const GatherConsts& K, const GenConsts& G, const BeamBVH B,
                                                   const BeamSoA Bs, const LightSum* __restrict__ lsums,
                                                   const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
@@ -806,6 +796,52 @@ __global__ void __launch_bounds__(128) k_gen_bp2d(const __grid_constant__ Gather
     }
 }
 
+// The warp gathers as kernels.  The adjoint's dual-number instantiations would take every register a
+// thread can have, which leaves 2 blocks of 128 threads per SM; asking for 3 blocks costs some
+// spills and runs the diff512 adjoint 8 % faster (4 spills more than it gains).  The FP64 ones keep
+// the compiler's own choice (156 and 126 registers, no spills): a minimum of blocks changes it.
+template <class T>
+__global__ void __launch_bounds__(128) k_gen_pb2d(const __grid_constant__ GatherConsts K,
+                                                  const __grid_constant__ GenConsts G, const LightSoA Lv,
+                                                  const PhotonBVH B, const SegQueriesDev Q,
+                                                  const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
+                                                  const GenOut O, unsigned int* __restrict__ work,
+                                                  int* __restrict__ status, const int32_t* __restrict__ order)
+{
+    gen_pb2d_body<T>(K, G, Lv, B, Q, cam, cs, O, work, status, order);
+}
+__global__ void __launch_bounds__(128, 3) k_gen_pb2d_dual(const __grid_constant__ GatherConsts K,
+                                                          const __grid_constant__ GenConsts G, const LightSoA Lv,
+                                                          const PhotonBVH B, const SegQueriesDev Q,
+                                                          const upbp_mis* __restrict__ cam,
+                                                          const CamSum* __restrict__ cs, const GenOut O,
+                                                          unsigned int* __restrict__ work, int* __restrict__ status,
+                                                          const int32_t* __restrict__ order)
+{
+    gen_pb2d_body<DualF>(K, G, Lv, B, Q, cam, cs, O, work, status, order);
+}
+template <class T>
+__global__ void __launch_bounds__(128) k_gen_bb1d(const __grid_constant__ GatherConsts K,
+                                                  const __grid_constant__ GenConsts G, const BeamBVH B,
+                                                  const BeamSoA Bs, const LightSum* __restrict__ lsums,
+                                                  const SegQueriesDev Q,
+                                                  const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
+                                                  const GenOut O, unsigned int* __restrict__ work,
+                                                  int* __restrict__ status, const int32_t* __restrict__ order)
+{
+    gen_bb1d_body<T>(K, G, B, Bs, lsums, Q, cam, cs, O, work, status, order);
+}
+__global__ void __launch_bounds__(128, 3) k_gen_bb1d_dual(const __grid_constant__ GatherConsts K,
+                                                          const __grid_constant__ GenConsts G, const BeamBVH B,
+                                                          const BeamSoA Bs, const LightSum* __restrict__ lsums,
+                                                          const SegQueriesDev Q, const upbp_mis* __restrict__ cam,
+                                                          const CamSum* __restrict__ cs, const GenOut O,
+                                                          unsigned int* __restrict__ work, int* __restrict__ status,
+                                                          const int32_t* __restrict__ order)
+{
+    gen_bb1d_body<DualF>(K, G, B, Bs, lsums, Q, cam, cs, O, work, status, order);
+}
+
 }  // namespace
 
 template <class T>
@@ -817,11 +853,23 @@ static void launch_all(const GenLaunch& A, cudaStream_t s)
     if (A.pq.n > 0 && A.beams.n > 0 && (A.K.P.techniques & UPBP_BP2D))
         k_gen_bp2d<T><<<A.bp2d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.pq, A.out_bp2d, A.work + 2, A.status);
     if (A.sq.n > 0 && A.photons.n > 0)
-        k_gen_pb2d<T><<<A.pb2d_grid, 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam, A.cs_seg, A.out_pb2d,
-                                                  A.work + 1, A.status, A.order);
+    {
+        if constexpr (is_dual<T>::value)
+            k_gen_pb2d_dual<<<A.pb2d_grid, 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam, A.cs_seg, A.out_pb2d,
+                                                        A.work + 1, A.status, A.order);
+        else
+            k_gen_pb2d<T><<<A.pb2d_grid, 128, 0, s>>>(A.K, A.G, A.L, A.photons, A.sq, A.cam, A.cs_seg, A.out_pb2d,
+                                                      A.work + 1, A.status, A.order);
+    }
     if (A.sq.n > 0 && A.beams.n > 0)
-        k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.L.sums, A.sq, A.cam, A.cs_seg,
-                                                  A.out_bb1d, A.work, A.status, A.order);
+    {
+        if constexpr (is_dual<T>::value)
+            k_gen_bb1d_dual<<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.L.sums, A.sq, A.cam, A.cs_seg,
+                                                        A.out_bb1d, A.work, A.status, A.order);
+        else
+            k_gen_bb1d<T><<<A.bb1d_grid, 128, 0, s>>>(A.K, A.G, A.beams, A.bs, A.L.sums, A.sq, A.cam, A.cs_seg,
+                                                      A.out_bb1d, A.work, A.status, A.order);
+    }
 }
 
 void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream)
@@ -833,7 +881,7 @@ void launch_generic(const GenLaunch& A, bool adjoint, cudaStream_t stream)
 int generic_pb2d_blocks_per_sm(bool adjoint)
 {
     int nb = 0;
-    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<DualF>, 128, 0);
+    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d_dual, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_pb2d<double>, 128, 0);
     return nb > 0 ? nb : 1;
 }
@@ -849,7 +897,7 @@ int generic_bp2d_blocks_per_sm(bool adjoint)
 int generic_bb1d_blocks_per_sm(bool adjoint)
 {
     int nb = 0;
-    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bb1d<DualF>, 128, 0);
+    if (adjoint) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bb1d_dual, 128, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gen_bb1d<double>, 128, 0);
     return nb > 0 ? nb : 1;
 }
