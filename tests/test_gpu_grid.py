@@ -221,3 +221,36 @@ def test_grid_structure_bit_exact_with_the_reference(path):
         if grid[1] > 0:
             np.testing.assert_array_equal(got["pdfs"], want["pdfs"])
         assert want["beams"].size > 0
+
+
+@pytest.mark.gpu
+def test_grid_at_cube512_against_the_reference():
+    # configuration-size check: the cube512 iteration (262,144 light paths, 512 x 512, UPBP MIS)
+    # over the reference grid at -gridres 64, against the reference harness on the same inputs:
+    # the grid structure bit for bit, every query's contribution within 1e-4
+    import os
+    from oracle import ref
+    from smallupbp_b200 import workload as W
+
+    w = W.generate(W.config("cube512"), 0)
+    ref.set_grid_options(64, 0, 0, 1234)
+    try:
+        sess = ref.Session(w, what=ref.BB1D_GRID, threads=os.cpu_count() or 8)
+        try:
+            want = sess.grid_structure()
+            o = sess.eval_outputs(0, 1)
+        finally:
+            sess.close()
+    finally:
+        ref.set_grid_options()
+    s = engine.EstimatorStage(0, engine.MODE_PLAIN)
+    try:
+        s.set_bb1d_grid(64)
+        s.run(w)
+        got = s.grid_structure()
+        _, bb1d = s.segment_results()
+    finally:
+        s.close()
+    np.testing.assert_array_equal(got["cells"], want["cells"])
+    np.testing.assert_array_equal(got["beams"], want["beams"])
+    G.assert_close(bb1d, o["bb1d"], "BB1D over the reference grid, cube512")
