@@ -91,7 +91,7 @@ struct upbp_ctx {
     // BB1D over the reference's uniform grid (upbp_set_bb1d_grid)
     upbp_bb1d_grid bgrid{};
     DBuf gr_hdr, gr_partial, gr_counts, gr_offsets, gr_keys, gr_keys_sorted, gr_keys_unique, gr_num, gr_cellcount,
-        gr_cells, gr_ptr, gr_pdf, gr_draws, gr_draw_off, gr_rnd;
+        gr_cells, gr_ptr, gr_pdf, gr_draws, gr_draw_off, gr_rnd, gr_rec_a, gr_rec_b;
     GridHeader gr_host{};           // the last build's header
     int64_t gr_raw = 0, gr_pairs = 0, gr_draws_total = 0;  // its sizes (a replay reuses them)
     bool gr_valid = false;
@@ -384,6 +384,13 @@ void build_grid(upbp_ctx* c, cudaStream_t s, float radius, const float* rstart, 
                            c->gr_pdf.as<float>(), s);
         c->build_launches += 5;
     }
+    // the entries' beam geometry in the final cell order (after the shuffles)
+    ensure(c, c->gr_rec_a, sizeof(float4) * std::max<int64_t>(np, 1));
+    ensure(c, c->gr_rec_b, sizeof(float4) * std::max<int64_t>(np, 1));
+    launch_grid_records(c->gr_ptr.as<int32_t>(), np, org, dir, len,
+                        (c->P.bb1d_knn > 0) ? c->bm_r2max.as<float>() : nullptr, radius * radius,
+                        c->gr_rec_a.as<float4>(), c->gr_rec_b.as<float4>(), s);
+    c->build_launches += 1;
     c->gr_valid = true;
 }
 
@@ -840,11 +847,9 @@ BeamGrid grid_dev(upbp_ctx* c)
     G.cells = c->gr_cells.as<uint32_t>();
     G.pdf = c->bgrid.max_beams_in_cell > 0 ? c->gr_pdf.as<float>() : nullptr;
     G.ptr = c->gr_ptr.as<int32_t>();
-    G.origin = c->b_origin.as<float>();
-    G.dir = c->b_dir.as<float>();
-    G.length = c->b_len.as<float>();
+    G.rec_a = c->gr_rec_a.as<float4>();
+    G.rec_b = c->gr_rec_b.as<float4>();
     G.medium = c->b_med_in.as<int32_t>();
-    G.r2max = (c->P.bb1d_knn > 0) ? c->bm_r2max.as<float>() : nullptr;
     return G;
 }
 

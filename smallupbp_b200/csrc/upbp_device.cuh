@@ -140,6 +140,22 @@ __device__ __forceinline__ bool beam_beam_near(V3 O1, V3 d1, V3 O2, V3 d2, float
     return !(xmul(ad, ad) >= xmul(maxDistSqr, sinThetaSqr));
 }
 
+// The second part of test_beam_beam: the near-parallel rejection and the query parameter t1 of the
+// lines' closest points, with d1.d2, d1.O2 and e = d2.O1 - d2.O2 (false: near-parallel).
+__device__ __forceinline__ bool beam_beam_t1(V3 O1, V3 d1, V3 O2, V3 d2, float& d1d2, float& d1O1, float& d1O2,
+                                             float& e, float& t1)
+{
+    d1d2 = xdot3(d1, d2);
+    const float d1d2Sqr = xmul(d1d2, d1d2);
+    const float d1d2SqrMinus1 = xsub(d1d2Sqr, 1.0f);
+    if (d1d2SqrMinus1 < 1e-5f && d1d2SqrMinus1 > -1e-5f) return false;
+    d1O1 = xdot3(d1, O1);
+    d1O2 = xdot3(d1, O2);
+    e = xsub(xdot3(d2, O1), xdot3(d2, O2));
+    t1 = xdiv(xsub(xsub(d1O1, d1O2), xmul(d1d2, e)), d1d2SqrMinus1);
+    return true;
+}
+
 // PhotonBeam::testIntersectionBeamBeam (Beams/PhotonBeam.hxx:238-296).  On acceptance it can also
 // return b = d1.d2 and e = d2.O1 - d2.O2, the terms of the line solution that piece_takes_fast uses.
 __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float maxT1, V3 O2, V3 d2, float minT2,
@@ -150,14 +166,8 @@ __device__ __forceinline__ bool test_beam_beam(V3 O1, V3 d1, float minT1, float 
     const float sinThetaSqr = xdot3(c, c);
     const float ad = xdot3(xsub3(O2, O1), c);
     if (xmul(ad, ad) >= xmul(maxDistSqr, sinThetaSqr)) return false;
-    const float d1d2 = xdot3(d1, d2);
-    const float d1d2Sqr = xmul(d1d2, d1d2);
-    const float d1d2SqrMinus1 = xsub(d1d2Sqr, 1.0f);
-    if (d1d2SqrMinus1 < 1e-5f && d1d2SqrMinus1 > -1e-5f) return false;
-    const float d1O1 = xdot3(d1, O1);
-    const float d1O2 = xdot3(d1, O2);
-    const float e = xsub(xdot3(d2, O1), xdot3(d2, O2));
-    const float t1 = xdiv(xsub(xsub(d1O1, d1O2), xmul(d1d2, e)), d1d2SqrMinus1);
+    float d1d2, d1O1, d1O2, e, t1;
+    if (!beam_beam_t1(O1, d1, O2, d2, d1d2, d1O1, d1O2, e, t1)) return false;
     if (t1 <= minT1 || t1 >= maxT1) return false;
     const float t2 = xdiv(xsub(xadd(t1, d1O1), d1O2), d1d2);
     if (t2 <= minT2 || t2 >= maxT2 || isnan(t2)) return false;

@@ -1275,13 +1275,16 @@ __device__ __forceinline__ void grid_walk(const GridHeader& h, V3 o, V3 d, float
     }
 }
 
-// The cells of one warp's walk waiting for their beams to be tested.
-constexpr int kGridQueue = 32;
+// The cells of one warp's walk waiting for their beams to be tested, and the (cell, entry) items
+// past the first check of the predicate waiting for the rest of it.
+constexpr int kGridQueue = 32, kGridNear = 64;
 struct GridQueue {
     float tmin[kGridQueue], tmax[kGridQueue], pdf[kGridQueue];
     uint32_t begin[kGridQueue], beams[kGridQueue];
     unsigned long long key[kGridQueue];  // the cell's draws (reductions 1-3)
     uint32_t first[kGridQueue + 1];      // the first item of every queued cell; first[n] = all items
+    float ntmin[kGridNear], ntmax[kGridNear], npdf[kGridNear];
+    uint32_t nat[kGridNear];             // the item's entry in the cell lists
 };
 
 // The per-query draws of the OFFSET, RESAMPLE_FIXED and SAMPLED reductions (Grid.hxx:466-548).  The
@@ -1302,32 +1305,57 @@ __device__ __forceinline__ float grid_draw(unsigned long long key, uint32_t j)
 
 // BB1D of one query by one warp over the beam grid.  The walk runs on every lane alike and queues
 // the visited cells that hold beams (max_beams_in_cell items of an over-full cell of a reduced
-// grid, Grid.hxx:453-548); once 32 or more (cell, beam) items wait, the lanes test them 32 at a
-// time: PhotonBeam::accumulate / accumulate2 (PhotonBeam.hxx:315-367, 375-480) with the query
-// restricted to the cell's t range, the contribution divided by the cell's selection pdf.
+// grid, Grid.hxx:453-548); once 32 or more (cell, beam) items wait, the lanes take them 32 at a
+// time through the first checks of PhotonBeam::testIntersectionBeamBeam (the distance of the two
+// lines, then the closest point's t1 within the cell's t range), from the entries' packed geometry.
+// The items that pass them go to a second queue, whose 32-wide batches run the rest: the medium,
+// the whole predicate, the radius, and PhotonBeam::accumulate / accumulate2 (PhotonBeam.hxx:315-367,
+// 375-480) divided by the cell's selection pdf.
 template <bool kMixed>
 __device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMedium* media, const LightSoA& Lv,
                                                const BeamGrid& G, const GridHeader& hdr, const BeamSoA& Bs,
                                                const SegQueriesDev& Q, int64_t q, SegCtx& s, GridQueue& gq,
-                                               int lane, unsigned long long& cnt, unsigned long long& h)
+                                               int lane, unsigned long long& cnt, unsigned long long& h,
+                                               unsigned long long& tested)
 {
-    const float r2c = __fmul_rn(Bs.radius_const, Bs.radius_const);  // mMaxRadiusSqr of a constant radius
-    unsigned cnt32 = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned cnt32 = 0, tested32 = 0;
     const Rgb res = segment_loop(K, media, Q, q, s, [&](const DMedium& m) {
         Rgb part = rgb(0.f);
         const int mid = (int)(&m - media);
-        int qc = 0;  // queued cells (warp-uniform)
-        auto flush = [&]() {
-            const uint32_t total = gq.first[qc];
-            for (uint32_t base = 0; base < total; base += 32) {
+        int qc = 0, nq = 0;  // queued cells and items past the first check (warp-uniform)
+        auto finish = [&](int k) {
+            const uint32_t at = gq.nat[k];
+            const int b = __ldg(&G.ptr[at]);
+            if (__ldg(&G.medium[b]) != mid) return;  // mMedium == medium
+            const float4 a = __ldg(&G.rec_a[at]), bd = __ldg(&G.rec_b[at]);
+            const V3 o2 = v3(a.x, a.y, a.z), d2 = v3(bd.x, bd.y, bd.z);
+            float dist, sinT, t1, t2;
+            if (!test_beam_beam(s.o, s.d, gq.ntmin[k], gq.ntmax[k], o2, d2, 0.f, a.w, bd.w, &dist, &sinT, &t1, &t2))
+                return;
+            const float radius = beam_radius_at(Bs, b, beam_start_radius(Bs, &Bs.radius[b]), t2);
+            if (radius < dist) return;  // PhotonBeam.hxx:334-336 / 411-413
+            ++cnt32;
+            h += mix64((unsigned long long)b);
+            Rgb c = bb1d_contrib<kMixed>(K, m, Lv, Bs, s, b, o2, d2, radius, dist, sinT, t1, t2);
+            const float pdf = gq.npdf[k];
+            if (pdf != 1.f) c = c * __fdiv_rn(1.f, pdf);
+            part = part + c;
+        };
+        // the queued cells' items; final: also the last items past the first check
+        auto flush = [&](bool final) {
+            const uint32_t total = qc > 0 ? gq.first[qc] : 0u;
+            for (uint32_t base = 0; base < total || (final && nq > 0); base += 32) {
                 const uint32_t it = base + (uint32_t)lane;
+                bool near = false;
+                int e = 0;
+                uint32_t at = 0;
                 if (it < total) {
-                    int e = 0;
                     while (e + 1 < qc && gq.first[e + 1] <= it) ++e;
                     const uint32_t j = it - gq.first[e], begin = gq.begin[e], beams = gq.beams[e];
-                    // the beam of item j: intersectPresampled / intersectOffsetted / intersectFixedSampled /
+                    // the entry of item j: intersectPresampled / intersectOffsetted / intersectFixedSampled /
                     // intersectSampled (Grid.hxx:453-548); unreduced cells and PRESAMPLE: the j-th of the list
-                    uint32_t at = begin + j;
+                    at = begin + j;
                     bool take = true;
                     if (gq.pdf[e] != 1.f && hdr.reduction != 0) {
                         if (hdr.reduction == 1) {
@@ -1340,25 +1368,34 @@ __device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMed
                             take = grid_draw(gq.key[e], j) < gq.pdf[e];
                         }
                     }
-                    const int b = __ldg(&G.ptr[at]);
-                    if (take && __ldg(&G.medium[b]) == mid) {  // mMedium == medium
-                        const V3 o2 = v3(__ldg(&G.origin[3 * b]), __ldg(&G.origin[3 * b + 1]), __ldg(&G.origin[3 * b + 2]));
-                        const V3 d2 = v3(__ldg(&G.dir[3 * b]), __ldg(&G.dir[3 * b + 1]), __ldg(&G.dir[3 * b + 2]));
-                        const float r2 = G.r2max ? __ldg(&G.r2max[b]) : r2c;
-                        float dist, sinT, t1, t2;
-                        if (test_beam_beam(s.o, s.d, gq.tmin[e], gq.tmax[e], o2, d2, 0.f, __ldg(&G.length[b]), r2, &dist,
-                                           &sinT, &t1, &t2)) {
-                            const float radius = beam_radius_at(Bs, b, beam_start_radius(Bs, &Bs.radius[b]), t2);
-                            if (!(radius < dist)) {  // PhotonBeam.hxx:334-336 / 411-413
-                                ++cnt32;
-                                h += mix64((unsigned long long)b);
-                                Rgb c = bb1d_contrib<kMixed>(K, m, Lv, Bs, s, b, o2, d2, radius, dist, sinT, t1, t2);
-                                const float pdf = gq.pdf[e];
-                                if (pdf != 1.f) c = c * __fdiv_rn(1.f, pdf);
-                                part = part + c;
-                            }
+                    if (take) {
+                        ++tested32;
+                        const float4 a = __ldg(&G.rec_a[at]), bd = __ldg(&G.rec_b[at]);
+                        const V3 o2 = v3(a.x, a.y, a.z), d2 = v3(bd.x, bd.y, bd.z);
+                        if (beam_beam_near(s.o, s.d, o2, d2, bd.w)) {
+                            // a beam near the query's line is listed in every cell it crosses along the
+                            // walk; only the cell holding the lines' closest point accepts it
+                            float b12, b1o1, b1o2, be, t1;
+                            near = beam_beam_t1(s.o, s.d, o2, d2, b12, b1o1, b1o2, be, t1) &&
+                                   !(t1 <= gq.tmin[e] || t1 >= gq.tmax[e]);
                         }
                     }
+                }
+                const unsigned bal = __ballot_sync(kFull, near);
+                if (near) {
+                    const int slot = nq + __popc(bal & lt);
+                    gq.ntmin[slot] = gq.tmin[e];
+                    gq.ntmax[slot] = gq.tmax[e];
+                    gq.npdf[slot] = gq.pdf[e];
+                    gq.nat[slot] = at;
+                }
+                nq += __popc(bal);
+                __syncwarp();
+                if (nq >= 32 || (final && base + 32 >= total && nq > 0)) {
+                    const int n = min(nq, 32);
+                    nq -= n;
+                    if (lane < n) finish(nq + lane);
+                    __syncwarp();
                 }
             }
             qc = 0;
@@ -1387,17 +1424,21 @@ __device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMed
             }
             __syncwarp();
             ++qc;
-            if (qc == kGridQueue || gq.first[qc] >= 32) flush();
+            if (qc == kGridQueue || gq.first[qc] >= 32) flush(false);
         });
-        if (qc > 0) flush();
+        if (qc > 0 || nq > 0) flush(true);
         return part;
     });
     cnt += cnt32;
+    tested += tested32;
     return res;
 }
 
+// Persistent, one warp per query from the atomic work queue.  Compiled for 7 blocks of 4 warps per
+// SM (72 registers): the walk and the first checks stream the cell entries and wait on their loads,
+// so resident warps matter more than the spills of the rare contribution path.
 template <bool kMixed>
-__global__ void __launch_bounds__(128) k_bb1d_grid(const __grid_constant__ GatherConsts K, const LightSoA Lv,
+__global__ void __launch_bounds__(128, 7) k_bb1d_grid(const __grid_constant__ GatherConsts K, const LightSoA Lv,
                                                   const BeamGrid G, const BeamSoA Bs, const SegQueriesDev Q,
                                                   const upbp_mis* __restrict__ cam, const CamSum* __restrict__ cs,
                                                   const Outputs O, unsigned int* __restrict__ work,
@@ -1419,17 +1460,19 @@ __global__ void __launch_bounds__(128) k_bb1d_grid(const __grid_constant__ Gathe
         if (item >= Q.n) break;
         const int64_t q = order ? (int64_t)__ldg(&order[item]) : item;
         Rgb acc = rgb(0.f);
-        unsigned long long cnt = 0, h = 0;
+        unsigned long long cnt = 0, h = 0, tested = 0;
         if ((Q.flags[q] & UPBP_Q_BB1D) && (K.P.techniques & UPBP_BB1D)) {
             SegCtx s;
             init_seg_ctx<kMixed>(s, K, Q, cam, cs, q, &s_e[warp], &s_cs[warp], lane == 0);
             __syncwarp();
-            acc = bb1d_query_grid<kMixed>(K, media, Lv, G, s_hdr, Bs, Q, q, s, s_q[warp], lane, cnt, h);
+            acc = bb1d_query_grid<kMixed>(K, media, Lv, G, s_hdr, Bs, Q, q, s, s_q[warp], lane, cnt, h, tested);
         }
         const float r = warp_sum(acc.r), g = warp_sum(acc.g), b = warp_sum(acc.b);
         cnt = warp_sum_u64(cnt);
         h = warp_sum_u64(h);
+        tested = warp_sum_u64(tested);
         if (lane == 0) {
+            if (O.tested && tested) atomicAdd(O.tested, tested);
             O.rgb[3 * q + 0] = r;
             O.rgb[3 * q + 1] = g;
             O.rgb[3 * q + 2] = b;

@@ -244,6 +244,21 @@ __global__ void k_grid_lists(const unsigned long long* __restrict__ keys, int64_
     }
 }
 
+// The beam geometry of every cell entry, in the cells' (final, shuffled) order: (origin, length) and
+// (direction, maximal radius squared).  The gather reads 32 consecutive entries with two coalesced
+// 16-byte loads per lane instead of scattered loads through the beam id.
+__global__ void k_grid_records(const int32_t* __restrict__ ptr, int64_t n, const float* __restrict__ origin,
+                               const float* __restrict__ dir, const float* __restrict__ length,
+                               const float* __restrict__ r2max, float r2c, float4* __restrict__ rec_a,
+                               float4* __restrict__ rec_b)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int b = ptr[i];
+        rec_a[i] = make_float4(origin[3 * b], origin[3 * b + 1], origin[3 * b + 2], length[b]);
+        rec_b[i] = make_float4(dir[3 * b], dir[3 * b + 1], dir[3 * b + 2], r2max ? r2max[b] : r2c);
+    }
+}
+
 // the build's draws of every cell (Grid.hxx:571-631): PRESAMPLE max_beams and OFFSET beams - 1 for
 // an over-full cell, the resampling reductions none
 __global__ void k_grid_draws(const uint32_t* __restrict__ cells, uint32_t n_cells, uint32_t max_beams,
@@ -375,6 +390,11 @@ void launch_grid_emit(const float* origin, const float* dir, const float* length
 void launch_grid_lists(const unsigned long long* keys, int64_t n, uint32_t* counts, int32_t* ptr, cudaStream_t s)
 {
     if (n > 0) k_grid_lists<<<blocks_for(n), kThreads, 0, s>>>(keys, n, counts, ptr);
+}
+void launch_grid_records(const int32_t* ptr, int64_t n, const float* origin, const float* dir, const float* length,
+                         const float* r2max, float r2c, float4* rec_a, float4* rec_b, cudaStream_t s)
+{
+    if (n > 0) k_grid_records<<<blocks_for(n), kThreads, 0, s>>>(ptr, n, origin, dir, length, r2max, r2c, rec_a, rec_b);
 }
 void launch_grid_draws(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t reduction,
                        uint32_t* draws, cudaStream_t s)

@@ -88,11 +88,9 @@ struct BeamGrid {
     const uint32_t* cells;  // mCells: the first entry of every cell's list (n_cells entries)
     const float* pdf;       // mPdfs, NULL: 1 in every cell (no reduction)
     const int32_t* ptr;     // mPointers: beam ids, each cell's beams in descending id order
-    const float* origin;    // the beams as uploaded: origin xyz, direction xyz, length, medium
-    const float* dir;
-    const float* length;
-    const int32_t* medium;
-    const float* r2max;     // KNN radii: mMaxRadiusSqr per beam; NULL: radius^2
+    const float4* rec_a;    // per entry of ptr: the beam's origin xyz, length
+    const float4* rec_b;    // per entry of ptr: the beam's direction xyz, mMaxRadiusSqr
+    const int32_t* medium;  // per beam, as uploaded
 };
 
 // Beam payload (index = beam id).
@@ -275,6 +273,8 @@ void launch_grid_emit(const float* origin, const float* dir, const float* length
                       const float* rchange, float radius, int64_t nb, const GridHeader* hdr,
                       const unsigned long long* offsets, unsigned long long* keys, cudaStream_t s);
 void launch_grid_lists(const unsigned long long* keys, int64_t n, uint32_t* counts, int32_t* ptr, cudaStream_t s);
+void launch_grid_records(const int32_t* ptr, int64_t n, const float* origin, const float* dir, const float* length,
+                         const float* r2max, float r2c, float4* rec_a, float4* rec_b, cudaStream_t s);
 void launch_grid_draws(const uint32_t* cells, uint32_t n_cells, uint32_t max_beams, uint32_t reduction,
                        uint32_t* draws, cudaStream_t s);
 void launch_mt64_floats(unsigned long long seed, int64_t n, float* out, cudaStream_t s);
