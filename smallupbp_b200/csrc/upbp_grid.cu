@@ -234,13 +234,23 @@ __global__ void k_grid_emit(const float* __restrict__ origin, const float* __res
     }
 }
 
-// counts per cell and the beam of every sorted unique key
+// counts per cell and the beam of every sorted unique key.  The keys are sorted, so the lanes of a
+// warp mostly share a cell: one atomic per cell and warp (the lanes with the same cell counted by
+// __match_any_sync) instead of one per entry on the same address.
 __global__ void k_grid_lists(const unsigned long long* __restrict__ keys, int64_t n, uint32_t* counts, int32_t* ptr)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const unsigned long long k = keys[i];
-        atomicAdd(&counts[(uint32_t)(k >> 32)], 1u);
-        ptr[i] = (int32_t)(~(uint32_t)k);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    // every lane of a warp runs the same number of iterations, so the match is over full warps
+    const int64_t warp0 = first - (threadIdx.x & 31);
+    for (int64_t w = warp0; w < n; w += stride) {
+        const int64_t i = w + (threadIdx.x & 31);
+        const bool in = i < n;
+        const unsigned long long k = in ? keys[i] : ~0ull;
+        const uint32_t cell = (uint32_t)(k >> 32);
+        const unsigned peers = __match_any_sync(0xffffffffu, cell);
+        if (in && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counts[cell], (uint32_t)__popc(peers));
+        if (in) ptr[i] = (int32_t)(~(uint32_t)k);
     }
 }
 
