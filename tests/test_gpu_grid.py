@@ -56,15 +56,23 @@ def test_grid_without_mis_matches_reference(stage, path):
 @pytest.mark.parametrize("path", G.GRID_FIXTURES, ids=G.name)
 def test_grid_mixed_mode_same_candidates(stage, path):
     # mixed mode: the same (cell, beam) pairs as plain FP32; the FP64 closest approach of
-    # near-parallel pairs moves only their contributions
+    # near-parallel pairs moves only their contributions.  Every query is within 1e-4 of the
+    # reference's FP32 grid estimate or, where the grid takes the same pairs as the beam-piece
+    # LBVH (same count and hash), of the LBVH's mixed-mode estimate, which the parity tests pin to
+    # the FP64 oracle where the reference's FP32 geometry cancels.
     w, r = G.load(path)
     grid = grid_options(path)
     p = run(stage, w, engine.MODE_PLAIN, grid)
     m = run(stage, w, engine.MODE_MIXED, grid)
+    lb = run(stage, w, engine.MODE_MIXED, (0, 0, 0, 0))
     np.testing.assert_array_equal(m["count_bb1d"], p["count_bb1d"])
     np.testing.assert_array_equal(m["hash_bb1d"], p["hash_bb1d"])
-    err = G.rel_errors(m["bb1d"].astype(np.float64), r["bb1d"].astype(np.float64))
-    assert (err <= G.RTOL).mean() >= 0.99, float(err.max())
+    got = m["bb1d"].astype(np.float64)
+    err = G.rel_errors(got, r["bb1d"].astype(np.float64))
+    same = (lb["count_bb1d"] == m["count_bb1d"]) & (lb["hash_bb1d"] == m["hash_bb1d"])
+    err = np.where(same, np.minimum(err, G.rel_errors(got, lb["bb1d"].astype(np.float64))), err)
+    worst = int(np.argmax(err))
+    assert (err <= G.RTOL).all(), (int((err > G.RTOL).sum()), len(err), float(err[worst]), bool(same[worst]))
     assert G.image_rel_l2(m["image"], r["image"]) <= 1e-4
 
 
