@@ -1188,7 +1188,10 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->bo_codes_sorted, &c->bo_idx, &c->bo_idx_sorted, &c->bo_bbox, &c->bo_leaf_codes, &c->bo_nodes,
                    &c->bo_parent_int, &c->bo_parent_leaf, &c->bo_leaf_boxes, &c->bo_node_boxes, &c->bo_flags,
                    &c->tr_cnt, &c->tr_off, &c->tr_status, &c->bb_keys, &c->bb_keys_sorted, &c->bb_iota,
-                   &c->bb_order, &c->bb_sum};
+                   &c->bb_order, &c->bb_sum, &c->gr_hdr, &c->gr_partial, &c->gr_counts, &c->gr_offsets,
+                   &c->gr_keys, &c->gr_keys_sorted, &c->gr_keys_unique, &c->gr_num, &c->gr_cellcount,
+                   &c->gr_cells, &c->gr_ptr, &c->gr_pdf, &c->gr_draws, &c->gr_draw_off, &c->gr_rnd,
+                   &c->gr_rec_a, &c->gr_rec_b};
     for (DBuf* b : all) free_buf(*b);
     if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)

@@ -72,3 +72,17 @@ def test_no_cpu_fallback_in_product_package():
             text = open(os.path.join(pkg, f)).read()
             assert not re.search(r"^\s*(from|import)\s+oracle", text, re.M), f
             assert "liboracle" not in text and "libupbp_ref" not in text, f
+
+
+def test_context_destroy_frees_every_device_buffer():
+    # upbp_ctx_destroy frees the buffers it lists; every DBuf member of the context must be listed,
+    # or its device memory outlives the context
+    src = open(os.path.join(ROOT, "smallupbp_b200", "csrc", "upbp_capi.cu")).read()
+    i = src.index("struct upbp_ctx")
+    body = src[i:src.index("\n};\n", i)]
+    members = set()
+    for m in re.finditer(r"\bDBuf\s+([^;]+);", body):
+        members.update(n.strip() for n in m.group(1).split(","))
+    k = src.index("DBuf* all[] = {")
+    freed = set(re.findall(r"&c->(\w+)", src[k:src.index("};", k)]))
+    assert members and members <= freed, sorted(members - freed)
