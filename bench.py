@@ -89,7 +89,14 @@ def parse():
     ap.add_argument("--dropin", action="store_true",
                     help="the plain FP32 drop-in: thread-per-query BB1D gather, plain mode, leaves of 2 and 3 r "
                          "pieces (the best of a leaf / piece sweep for that gather on cube512)")
+    ap.add_argument("--bb1d-grid", type=int, default=0,
+                    help="BB1D over the reference's uniform beam grid of this resolution (-gridres) instead of the "
+                         "LBVH of beam pieces; keeps the library's tuning and skips the e2e, accuracy, device-pass, "
+                         "comparison-arm, parity and secondary measurements, which are defined for the LBVH path")
     a = ap.parse_args()
+    if a.bb1d_grid:
+        a.no_autotune = a.no_e2e = a.no_accuracy = a.no_device_passes = a.no_arms = a.no_parity = True
+        a.no_secondary = True
     if a.dropin:
         a.mode, a.no_autotune = "plain", True
         t = dict(DROPIN_TUNING)
@@ -221,7 +228,7 @@ def kernel_source_hash() -> str:
     return h.hexdigest()[:16]
 
 
-def make_stages(works, dev, mode, stream, tuning=None):
+def make_stages(works, dev, mode, stream, tuning=None, bb1d_grid=0):
     from smallupbp_b200 import abi, engine
     stages, structs = [], []
     for w in works:
@@ -232,6 +239,8 @@ def make_stages(works, dev, mode, stream, tuning=None):
         st.set_queries(w, s)
         if tuning:
             st.set_tuning(**tuning)
+        if bb1d_grid:
+            st.set_bb1d_grid(bb1d_grid)
         stages.append(st)
         structs.append(s)
     return stages, structs
@@ -369,7 +378,8 @@ def run_b200(args, cfg, rank, world, local_rank):
     stream = torch.cuda.Stream(device=dev)
     npix = cfg.width * cfg.height
     img_t = torch.zeros(npix * 3, dtype=torch.float32, device="cuda")
-    stages, all_structs = make_stages(works, dev, mode, stream, json.loads(args.tuning) if args.tuning else None)
+    stages, all_structs = make_stages(works, dev, mode, stream, json.loads(args.tuning) if args.tuning else None,
+                                      args.bb1d_grid)
     tuning = {"best": {k: getattr(stages[0].get_tuning(), k) for k, _ in abi.Tuning._fields_}, "autotuned": False}
     if not args.no_autotune and not args.tuning:
         tuning = tune_stages(stages, all_structs, stream)
@@ -398,7 +408,9 @@ def run_b200(args, cfg, rank, world, local_rank):
     achieved = alg[dom] / (avg[dom + "_ms"] / 1000.0) / 1e9 if avg[dom + "_ms"] > 0 else None
     traffic, traffic_note = None, "no ncu capture committed for this kernel and workload"
     tfile = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (dom, cfg.name))
-    if os.path.exists(tfile):
+    if args.bb1d_grid:
+        traffic_note = "BB1D over the reference grid: no ncu traffic figure committed for this path"
+    elif os.path.exists(tfile):
         try:
             with open(tfile) as fh:
                 tj = json.load(fh)
@@ -526,9 +538,11 @@ def run_b200(args, cfg, rank, world, local_rank):
                        parallelism=("dp%d: each rank builds the iteration's structures and evaluates its 32x32 pixel "
                                     "tiles of the queries; framebuffer all-reduce" % world) if shard == "queries" else
                                    ("dp%d: one iteration per rank, framebuffer all-reduce" % world),
-                       candidate_sets="the reference's brute-force BB1D estimator (PhBrute.hxx) under the reach rule "
-                                      "(FP64 segment distance <= r(u) + 2e-5 + 1e-3 r); the reference's default grid "
-                                      "(USE_GRID) differs where a closest approach falls on a DDA cell boundary",
+                       candidate_sets=("the reference's default grid evaluator (USE_GRID, Grid.hxx) at -gridres %d: "
+                                       "its cells, cell lists and DDA walk" % args.bb1d_grid) if args.bb1d_grid else
+                                      ("the reference's brute-force BB1D estimator (PhBrute.hxx) under the reach rule "
+                                       "(FP64 segment distance <= r(u) + 2e-5 + 1e-3 r); the reference's default grid "
+                                       "(USE_GRID) differs where a closest approach falls on a DDA cell boundary"),
                        tuning=tuning, cuda_graph=not args.no_graph),
         "ms_per_iteration": ms_max / args.steps,
         "kernels_ms": avg,
