@@ -91,7 +91,7 @@ struct upbp_ctx {
     // BB1D over the reference's uniform grid (upbp_set_bb1d_grid)
     upbp_bb1d_grid bgrid{};
     DBuf gr_hdr, gr_partial, gr_counts, gr_offsets, gr_keys, gr_keys_sorted, gr_keys_unique, gr_num, gr_cellcount,
-        gr_cells, gr_ptr, gr_pdf, gr_draws, gr_draw_off, gr_rnd, gr_rec_a, gr_rec_b;
+        gr_cells, gr_ptr, gr_pdf, gr_draws, gr_draw_off, gr_rnd, gr_rec_a, gr_rec_b, gr_pay;
     GridHeader gr_host{};           // the last build's header
     int64_t gr_raw = 0, gr_pairs = 0, gr_draws_total = 0;  // its sizes (a replay reuses them)
     bool gr_valid = false;
@@ -719,6 +719,15 @@ void do_build(upbp_ctx* c)
                                  mis ? c->lv_info4.as<int4>() : nullptr, mis ? c->lv_mis.as<upbp_mis>() : nullptr,
                                  mis ? c->light_sums.as<LightSum>() : nullptr, c->pc_pay.as<PiecePayload>(), s);
             c->build_launches += 1;
+            if (c->bgrid.grid_res > 0) {
+                // the grid gather's payload: one per beam (the piece payload's layout)
+                ensure(c, c->gr_pay, sizeof(PiecePayload) * nb);
+                launch_piece_payload(nullptr, (int)nb, c->bm_thr4.as<float4>(), c->bm_pdf4.as<float4>(),
+                                     c->bm_link.as<int2>(), c->bm_radius.as<float>(),
+                                     mis ? c->lv_info4.as<int4>() : nullptr, mis ? c->lv_mis.as<upbp_mis>() : nullptr,
+                                     mis ? c->light_sums.as<LightSum>() : nullptr, c->gr_pay.as<PiecePayload>(), s);
+                c->build_launches += 1;
+            }
         }
         if (c->bgrid.grid_res > 0) build_grid(c, s, r, rchange ? c->bm_radius.as<float>() : nullptr, rchange);
     }
@@ -850,6 +859,7 @@ BeamGrid grid_dev(upbp_ctx* c)
     G.rec_a = c->gr_rec_a.as<float4>();
     G.rec_b = c->gr_rec_b.as<float4>();
     G.medium = c->b_med_in.as<int32_t>();
+    G.pay = c->mode != UPBP_MODE_PLAIN ? c->gr_pay.as<PiecePayload>() : nullptr;
     return G;
 }
 
@@ -1191,7 +1201,7 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->bb_order, &c->bb_sum, &c->gr_hdr, &c->gr_partial, &c->gr_counts, &c->gr_offsets,
                    &c->gr_keys, &c->gr_keys_sorted, &c->gr_keys_unique, &c->gr_num, &c->gr_cellcount,
                    &c->gr_cells, &c->gr_ptr, &c->gr_pdf, &c->gr_draws, &c->gr_draw_off, &c->gr_rnd,
-                   &c->gr_rec_a, &c->gr_rec_b};
+                   &c->gr_rec_a, &c->gr_rec_b, &c->gr_pay};
     for (DBuf* b : all) free_buf(*b);
     if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)

@@ -1333,11 +1333,21 @@ __device__ __forceinline__ Rgb bb1d_query_grid(const GatherConsts& K, const DMed
             float dist, sinT, t1, t2;
             if (!test_beam_beam(s.o, s.d, gq.ntmin[k], gq.ntmax[k], o2, d2, 0.f, a.w, bd.w, &dist, &sinT, &t1, &t2))
                 return;
-            const float radius = beam_radius_at(Bs, b, beam_start_radius(Bs, &Bs.radius[b]), t2);
+            const float rs = beam_start_radius(Bs, kMixed ? &G.pay[b].lv.z : &Bs.radius[b]);
+            const float radius = beam_radius_at(Bs, b, rs, t2);
             if (radius < dist) return;  // PhotonBeam.hxx:334-336 / 411-413
             ++cnt32;
             h += mix64((unsigned long long)b);
-            Rgb c = bb1d_contrib<kMixed>(K, m, Lv, Bs, s, b, o2, d2, radius, dist, sinT, t1, t2);
+            Rgb c;
+            if (kMixed) {
+                // the beam's packed payload, and the FP64 closest approach of near-parallel lines
+                // (the candidate decision above stays FP32)
+                const float cb = s.d.x * d2.x + s.d.y * d2.y + s.d.z * d2.z;
+                if (1.f - cb * cb < 1e-2f) closest_approach_f64(s.o, s.d, o2, d2, dist, sinT, t1, t2);
+                c = bb1d_contrib_packed(K, m, s, G.pay[b], o2, d2, dist, sinT, t1, t2, beam_radius_at(Bs, b, rs, t2));
+            } else {
+                c = bb1d_contrib<false>(K, m, Lv, Bs, s, b, o2, d2, radius, dist, sinT, t1, t2);
+            }
             const float pdf = gq.npdf[k];
             if (pdf != 1.f) c = c * __fdiv_rn(1.f, pdf);
             part = part + c;
@@ -1636,7 +1646,7 @@ __global__ void k_piece_payload(const float4* __restrict__ pc, int n, const floa
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int beam = __float_as_int(pc[i].z);
+    const int beam = pc ? __float_as_int(pc[i].z) : i;  // pc == NULL: one payload per beam
     const int lv = bm_link[beam].x;
     // without MIS (lv_info == nullptr) the beams need not have light vertices
     upbp_mis m{};

@@ -91,6 +91,7 @@ struct BeamGrid {
     const float4* rec_a;    // per entry of ptr: the beam's origin xyz, length
     const float4* rec_b;    // per entry of ptr: the beam's direction xyz, mMaxRadiusSqr
     const int32_t* medium;  // per beam, as uploaded
+    const PiecePayload* pay;  // mixed mode: the contribution's inputs per beam (PiecePayload layout)
 };
 
 // Beam payload (index = beam id).
