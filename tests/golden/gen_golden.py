@@ -58,6 +58,8 @@ GRID_CASES = [
     ("boxes_nomis_grid_reduced", "boxes", dict(seed=47), (16, 3, 0, 77)),
     ("cube_nomis_grid_short", "cube24x1536", dict(query_beam_type=W.SHORT_BEAM, photon_beam_type=W.SHORT_BEAM,
                                                   radius=0.03, seed=43), (64, 0, 0, 1234)),
+    # KNN radii (the reference's kd-tree search): per-beam radii in the rasterisation and the test
+    ("cube_nomis_grid_knn", "cube24x1536", dict(radius=0.25, pb2d_knn=8, bb1d_knn=6, seed=53), (24, 3, 0, 99)),
 ]
 
 
