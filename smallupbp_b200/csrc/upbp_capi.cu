@@ -100,7 +100,8 @@ struct upbp_ctx {
     DBuf pb_r2, bm_rchange, bm_r2max, knn_status;
     // the reference's kd-tree search for the KNN radii (knn_exact = 0): working array, tree, node
     // boxes, partition scratch
-    DBuf kd_org, kd_tree, kd_boxes, kd_pa, kd_pb;
+    DBuf kd_org, kd_tree, kd_boxes, kd_pa, kd_pb, kd_qpts, kd_qcodes, kd_qcodes_sorted, kd_qidx, kd_qidx_sorted,
+        kd_qd2;
     DBuf bo_pos, bo_pts, bo_codes, bo_codes_sorted, bo_idx, bo_idx_sorted, bo_bbox, bo_leaf_codes, bo_nodes,
         bo_parent_int, bo_parent_leaf, bo_leaf_boxes, bo_node_boxes, bo_flags;
     int bo_n_leaves = 0;
@@ -628,10 +629,26 @@ void do_build(upbp_ctx* c)
             if (!P.knn_exact) {
                 // the reference's search over the beam origins in beam order (PhBeams.cxx:80-91)
                 build_kd_tree(c, c->bo_pos.as<float4>(), nullptr, n, c->bo_bbox.as<float>());
-                launch_kd_beam_radii(c->kd_tree.as<float4>(), n, c->b_origin.as<float>(), c->b_dir.as<float>(),
-                                     c->b_len.as<float>(), n, P.bb1d_knn, r, c->bm_radius.as<float>(),
-                                     c->bm_rchange.as<float>(), c->bm_r2max.as<float>(), s);
-                c->build_launches += 1;
+                // two searches per beam (origin, end point), taken in Morton order of the points
+                const int nq = 2 * n;
+                ensure(c, c->kd_qpts, sizeof(float4) * nq);
+                ensure(c, c->kd_qcodes, sizeof(uint32_t) * nq);
+                ensure(c, c->kd_qcodes_sorted, sizeof(uint32_t) * nq);
+                ensure(c, c->kd_qidx, sizeof(int32_t) * nq);
+                ensure(c, c->kd_qidx_sorted, sizeof(int32_t) * nq);
+                ensure(c, c->kd_qd2, sizeof(float) * nq);
+                launch_kd_beam_points(c->b_origin.as<float>(), c->b_dir.as<float>(), c->b_len.as<float>(), n,
+                                      c->kd_qpts.as<float4>(), s);
+                k_iota<<<(nq + 255) / 256, 256, 0, s>>>(c->kd_qidx.as<int32_t>(), nq);
+                launch_morton_points(c->kd_qpts.as<float4>(), c->kd_qidx.as<int32_t>(), nq, c->bo_bbox.as<float>(),
+                                     c->kd_qcodes.as<uint32_t>(), s);
+                sort_pairs(c, c->kd_qcodes.as<uint32_t>(), c->kd_qcodes_sorted.as<uint32_t>(),
+                           c->kd_qidx.as<int32_t>(), c->kd_qidx_sorted.as<int32_t>(), nq, 30);
+                launch_kd_knn_sorted(c->kd_tree.as<float4>(), n, c->kd_qpts.as<float4>(),
+                                     c->kd_qidx_sorted.as<int32_t>(), nq, P.bb1d_knn, c->kd_qd2.as<float>(), s);
+                launch_kd_beam_finish(c->kd_qd2.as<float>(), c->b_len.as<float>(), n, r, c->bm_radius.as<float>(),
+                                      c->bm_rchange.as<float>(), c->bm_r2max.as<float>(), s);
+                c->build_launches += 5;
             } else {  // the exact search: an LBVH over the beam origins, two queries per beam
                 k_iota<<<(n + 255) / 256, 256, 0, s>>>(c->bo_idx.as<int32_t>(), n);
                 launch_morton_points(c->bo_pos.as<float4>(), c->bo_idx.as<int32_t>(), n, c->bo_bbox.as<float>(),
@@ -1201,7 +1218,8 @@ int upbp_ctx_destroy(upbp_ctx* c)
                    &c->bb_order, &c->bb_sum, &c->gr_hdr, &c->gr_partial, &c->gr_counts, &c->gr_offsets,
                    &c->gr_keys, &c->gr_keys_sorted, &c->gr_keys_unique, &c->gr_num, &c->gr_cellcount,
                    &c->gr_cells, &c->gr_ptr, &c->gr_pdf, &c->gr_draws, &c->gr_draw_off, &c->gr_rnd,
-                   &c->gr_rec_a, &c->gr_rec_b, &c->gr_pay};
+                   &c->gr_rec_a, &c->gr_rec_b, &c->gr_pay, &c->kd_qpts, &c->kd_qcodes, &c->kd_qcodes_sorted,
+                   &c->kd_qidx, &c->kd_qidx_sorted, &c->kd_qd2};
     for (DBuf* b : all) free_buf(*b);
     if (c->status_host) cudaFreeHost(c->status_host);
     for (auto& e : c->ev)

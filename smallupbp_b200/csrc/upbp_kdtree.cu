@@ -34,7 +34,9 @@ namespace upbp {
 namespace {
 
 constexpr int kBigSeg = 4096;
+constexpr int kWarpSeg = 64;
 constexpr int kSplitThreads = 512;
+constexpr unsigned kAllLanes = 0xffffffffu;
 
 __host__ __device__ __forceinline__ int kd_median(int start, int end)
 {
@@ -118,7 +120,7 @@ __global__ void k_kd_level_small(float4* __restrict__ org, float4* __restrict__ 
         tree[idx] = make_float4(p.x, p.y, p.z, __int_as_float(0));
         return;
     }
-    if (end - start + 1 > kBigSeg) return;  // k_kd_level_big
+    if (end - start + 1 > kWarpSeg) return;  // k_kd_level_warp, k_kd_level_big
     float box[6];
     for (int c = 0; c < 6; ++c) box[c] = boxes[6 * idx + c];
     const int axis = kd_axis(box);
@@ -140,6 +142,72 @@ __global__ void k_kd_level_small(float4* __restrict__ org, float4* __restrict__ 
         if (i <= median) left = i + 1;
     }
     kd_emit(tree, boxes, org, idx, n, median, axis, box);
+}
+
+// one level, the segments of kWarpSeg + 1 to kBigSeg points: one warp each, the partition of
+// k_kd_level_big (below) with ballots in place of the block scans.  The sequential loop's pivots
+// make some segments take many partition passes (up to one per element on ordered input); each
+// pass then costs a warp sweep of the segment instead of one thread's.
+__global__ void k_kd_level_warp(float4* __restrict__ org, float4* __restrict__ tree, float* __restrict__ boxes,
+                                int* __restrict__ pa, int* __restrict__ pb, int n, int first, int count)
+{
+    const int w = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= count) return;  // the whole warp: w is the same on its lanes
+    const int idx = first + w;
+    int start, end;
+    if (idx > n || !kd_segment(idx, n, start, end)) return;
+    if (end - start + 1 <= kWarpSeg || end - start + 1 > kBigSeg) return;
+    float box[6];
+    for (int c = 0; c < 6; ++c) box[c] = boxes[6 * idx + c];
+    const int axis = kd_axis(box);
+    const int median = kd_median(start, end);
+    const unsigned lt = (1u << lane) - 1u;
+    int left = start, right = end;
+    while (right > left) {
+        const float v = axis_of(org[right], axis);
+        // A: ascending positions in [left, right] with key >= v; B: ascending positions in
+        // (left, right) with key <= v
+        int na = 0, nb = 0;
+        for (int base = left; base <= right; base += 32) {
+            const int i = base + lane;
+            const float key = i <= right ? axis_of(org[i], axis) : 0.f;
+            const bool fa = i <= right && key >= v;
+            const bool fb = i > left && i < right && key <= v;
+            const unsigned ba = __ballot_sync(kAllLanes, fa), bb = __ballot_sync(kAllLanes, fb);
+            if (fa) pa[start + na + __popc(ba & lt)] = i;
+            if (fb) pb[start + nb + __popc(bb & lt)] = i;
+            na += __popc(ba);
+            nb += __popc(bb);
+        }
+        __syncwarp();
+        // m = the first k with A[k] >= B'[k] (B'[k]: the k-th of B from the right, then `left`);
+        // A ascends and B' descends, so the test turns true once, at the latest at A's last entry
+        int m = na - 1;
+        for (int k0 = 0; k0 < na; k0 += 32) {
+            const int k = k0 + lane;
+            bool hit = false;
+            if (k < na) hit = pa[start + k] >= (k < nb ? pb[start + nb - 1 - k] : left);
+            const unsigned bh = __ballot_sync(kAllLanes, hit);
+            if (bh) {
+                m = k0 + __ffs(bh) - 1;
+                break;
+            }
+        }
+        for (int k = lane; k < m; k += 32) kd_swap(org, pa[start + k], pb[start + nb - 1 - k]);
+        __syncwarp();
+        int i = 0;
+        if (lane == 0) {
+            const int a = pa[start + m];
+            i = m == 0 ? a : min(a, pb[start + nb - m]);
+            kd_swap(org, i, right);
+        }
+        i = __shfl_sync(kAllLanes, i, 0);
+        __syncwarp();
+        if (i >= median) right = i - 1;
+        if (i <= median) left = i + 1;
+    }
+    if (lane == 0) kd_emit(tree, boxes, org, idx, n, median, axis, box);
 }
 
 // one level, the segments of more than kBigSeg points: one block each.  pa, pb: position scratch
@@ -309,23 +377,49 @@ __device__ __forceinline__ float kd_beam_radius(float d2, float r)
     return fmaxf(__fmul_rn(__fmul_rn(2.0f, __fsqrt_rn(d2)), r), 0.001f);  // PhBeams.cxx:100, 105
 }
 
-__global__ void k_kd_beam_radii(const float4* __restrict__ tree, int n, const float* __restrict__ origin,
-                                const float* __restrict__ dir, const float* __restrict__ length, int nb, int k, float r,
-                                float* rstart, float* rchange, float* r2max)
+// The beams' two query points (PhBeams.cxx:94-115): j < nb the origin of beam j, j >= nb the end
+// point of beam j - nb, mRay.target(mLength).
+__global__ void k_kd_beam_points(const float* __restrict__ origin, const float* __restrict__ dir,
+                                 const float* __restrict__ length, int nb, float4* __restrict__ pts)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= 2 * nb) return;
+    const int b = j < nb ? j : j - nb;
+    const V3 o = v3(origin[3 * b], origin[3 * b + 1], origin[3 * b + 2]);
+    if (j < nb) {
+        pts[j] = make_float4(o.x, o.y, o.z, 0.f);
+        return;
+    }
+    const V3 d = v3(dir[3 * b], dir[3 * b + 1], dir[3 * b + 2]);
+    const float len = length[b];
+    pts[j] = make_float4(__fadd_rn(o.x, __fmul_rn(d.x, len)), __fadd_rn(o.y, __fmul_rn(d.y, len)),
+                         __fadd_rn(o.z, __fmul_rn(d.z, len)), 0.f);
+}
+
+// KNNQuery at the query points in the given order (neighbouring threads on neighbouring points, so
+// that a warp's walks through the tree stay alike): d2[j] = dist2[1] of point order[i]
+__global__ void k_kd_knn_sorted(const float4* __restrict__ tree, int n, const float4* __restrict__ pts,
+                                const int32_t* __restrict__ order, int nq, int k, float* __restrict__ d2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const int j = order[i];
+    const float4 p = pts[j];
+    d2[j] = kd_knn_d2(tree, n, v3(p.x, p.y, p.z), k);
+}
+
+// the beam's radii from its two searches (PhBeams.cxx:94-115)
+__global__ void k_kd_beam_finish(const float* __restrict__ d2, const float* __restrict__ length, int nb, float r,
+                                 float* rstart, float* rchange, float* r2max)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
-    const V3 o = v3(origin[3 * b], origin[3 * b + 1], origin[3 * b + 2]);
-    const V3 d = v3(dir[3 * b], dir[3 * b + 1], dir[3 * b + 2]);
-    const float len = length[b];
-    const V3 e = v3(__fadd_rn(o.x, __fmul_rn(d.x, len)), __fadd_rn(o.y, __fmul_rn(d.y, len)),
-                    __fadd_rn(o.z, __fmul_rn(d.z, len)));  // mRay.target(mLength)
-    const float rs = kd_beam_radius(kd_knn_d2(tree, n, o, k), r);
-    const float re = kd_beam_radius(kd_knn_d2(tree, n, e, k), r);
+    const float rs = kd_beam_radius(d2[b], r);
+    const float re = kd_beam_radius(d2[nb + b], r);
     const float mx = fmaxf(rs, re);
     rstart[b] = rs;
     r2max[b] = __fmul_rn(mx, mx);
-    rchange[b] = __fdiv_rn(__fsub_rn(re, rs), len);
+    rchange[b] = __fdiv_rn(__fsub_rn(re, rs), length[b]);
 }
 
 constexpr int kThreads = 128;
@@ -392,6 +486,8 @@ void launch_kd_build(const float4* pos, const int32_t* idx, int n, const float* 
         const int count = min(first, n - first + 1);
         if (sizes[L] > kBigSeg)
             k_kd_level_big<<<count, kSplitThreads, 0, s>>>(org, tree, boxes, pa, pb, n, first);
+        if (sizes[L] > kWarpSeg)
+            k_kd_level_warp<<<blocks_for(32LL * count), kThreads, 0, s>>>(org, tree, boxes, pa, pb, n, first, count);
         k_kd_level_small<<<blocks_for(count), kThreads, 0, s>>>(org, tree, boxes, n, first, count);
     }
 }
@@ -401,7 +497,7 @@ int kd_build_launches(int n)
     if (n < 2) return n;
     int sizes[32], c = 2;
     level_max_sizes(n, sizes, 32);
-    for (int L = 0; L < 32 && (1 << L) <= n; ++L) c += sizes[L] > kBigSeg ? 2 : 1;
+    for (int L = 0; L < 32 && (1 << L) <= n; ++L) c += 1 + (sizes[L] > kBigSeg ? 1 : 0) + (sizes[L] > kWarpSeg ? 1 : 0);
     return c;
 }
 
@@ -411,12 +507,20 @@ void launch_kd_photon_r2(const float4* tree, int n, const float4* queries, int n
     if (nq > 0) k_kd_photon_r2<<<blocks_for(nq), kThreads, 0, s>>>(tree, n, queries, nq, k, r, r2);
 }
 
-void launch_kd_beam_radii(const float4* tree, int n, const float* origin, const float* dir, const float* length,
-                          int nb, int k, float r, float* rstart, float* rchange, float* r2max, cudaStream_t s)
+void launch_kd_beam_points(const float* origin, const float* dir, const float* length, int nb, float4* pts,
+                           cudaStream_t s)
 {
-    if (nb > 0)
-        k_kd_beam_radii<<<blocks_for(nb), kThreads, 0, s>>>(tree, n, origin, dir, length, nb, k, r, rstart, rchange,
-                                                             r2max);
+    if (nb > 0) k_kd_beam_points<<<blocks_for(2LL * nb), kThreads, 0, s>>>(origin, dir, length, nb, pts);
+}
+void launch_kd_knn_sorted(const float4* tree, int n, const float4* pts, const int32_t* order, int nq, int k,
+                          float* d2, cudaStream_t s)
+{
+    if (nq > 0) k_kd_knn_sorted<<<blocks_for(nq), kThreads, 0, s>>>(tree, n, pts, order, nq, k, d2);
+}
+void launch_kd_beam_finish(const float* d2, const float* length, int nb, float r, float* rstart, float* rchange,
+                           float* r2max, cudaStream_t s)
+{
+    if (nb > 0) k_kd_beam_finish<<<blocks_for(nb), kThreads, 0, s>>>(d2, length, nb, r, rstart, rchange, r2max);
 }
 
 }  // namespace upbp

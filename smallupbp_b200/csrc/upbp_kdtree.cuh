@@ -18,8 +18,15 @@ int kd_build_launches(int n);
 // PB2D photon radii^2 from the reference's search: query i at queries[i].xyz
 void launch_kd_photon_r2(const float4* tree, int n, const float4* queries, int nq, int k, float r, float* r2,
                          cudaStream_t stream);
-// BB1D beam start radius, radius change and max radius^2 from the reference's search
-void launch_kd_beam_radii(const float4* tree, int n, const float* origin, const float* dir, const float* length,
-                          int nb, int k, float r, float* rstart, float* rchange, float* r2max, cudaStream_t stream);
+// BB1D beam radii from the reference's search, in three steps: the 2 nb query points (the beams'
+// origins, then their end points), the searches in a given order of the points (a Morton order
+// keeps a warp's walks alike; d2 indexed by point), and the start radius, radius change and max
+// radius^2 of every beam
+void launch_kd_beam_points(const float* origin, const float* dir, const float* length, int nb, float4* pts,
+                           cudaStream_t stream);
+void launch_kd_knn_sorted(const float4* tree, int n, const float4* pts, const int32_t* order, int nq, int k,
+                          float* d2, cudaStream_t stream);
+void launch_kd_beam_finish(const float* d2, const float* length, int nb, float r, float* rstart, float* rchange,
+                           float* r2max, cudaStream_t stream);
 
 }  // namespace upbp

@@ -164,8 +164,9 @@ def test_knn_radii_bit_exact_with_the_oracle(stage, mode, knn_exact):
 @pytest.mark.gpu
 def test_knn_reference_search_at_cube512(stage):
     # The reference's KNN search on 10^5-point sets: the top levels of the kd-tree are partitioned
-    # block-parallel (segments of more than 4096 points), the rest one thread per segment.  A sample of
-    # the queries (every 97th) must see the oracle's candidate sets, which follow the reference's radii.
+    # block-parallel (segments of more than 4096 points), then one warp per segment, the smallest
+    # one thread per segment.  A sample of the queries (every 97th) must see the oracle's candidate
+    # sets, which follow the reference's radii.
     from oracle import port
     from smallupbp_b200 import workload as W
 
