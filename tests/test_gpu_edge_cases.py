@@ -72,17 +72,30 @@ def test_no_beams(stage, mode):
             G.assert_close(e[est], o[est], est + " without beams")
 
 
+def with_knn(w):
+    # KNN radii from the reference's kd-tree search (8 photons, 6 beam origins)
+    out = dict(w)
+    p = np.array(w["params"], copy=True)
+    p["pb2d_knn"], p["bb1d_knn"], p["knn_exact"] = 8, 6, 0
+    out["params"] = p
+    return out
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("subset", ["one", "sparse"])
-def test_few_beams_match_the_oracle(stage, subset):
+@pytest.mark.parametrize("knn", [False, True], ids=["constant_radius", "knn_radii"])
+@pytest.mark.parametrize("subset", ["one", "two", "sparse"])
+def test_few_beams_match_the_oracle(stage, subset, knn):
+    # with KNN radii this covers the kd-tree over one and two beam origins and a small tree
     from oracle import port
 
-    w = workload()
+    w = with_knn(workload()) if knn else workload()
     nb = len(w["beam_length"])
-    if subset == "one":
-        # the beam with the most accepted pairs in the full workload (by the oracle)
+    if subset in ("one", "two"):
+        # the beam with the most accepted pairs in the full workload (by the oracle), and its successor
         counts = [int(port.run(with_beams(w, np.array([k])))["count_bb1d"].sum()) for k in range(0, nb, max(1, nb // 64))]
         idx = np.array([int(np.argmax(counts)) * max(1, nb // 64)])
+        if subset == "two":
+            idx = np.array([idx[0], (idx[0] + 1) % nb])
     else:
         idx = np.arange(0, nb, 97)
     ws = with_beams(w, idx)
