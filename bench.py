@@ -89,6 +89,9 @@ def parse():
     ap.add_argument("--dropin", action="store_true",
                     help="the plain FP32 drop-in: thread-per-query BB1D gather, plain mode, leaves of 2 and 3 r "
                          "pieces (the best of a leaf / piece sweep for that gather on cube512)")
+    ap.add_argument("--knn", default=None, metavar="PB2D,BB1D",
+                    help="KNN radii: photons and beam origins per search (-r_initial_pb2d_knn, "
+                         "-r_initial_bb1d_knn), found by the reference's kd-tree search")
     ap.add_argument("--bb1d-grid", type=int, default=0,
                     help="BB1D over the reference's uniform beam grid of this resolution (-gridres) instead of the "
                          "LBVH of beam pieces; keeps the library's tuning and skips the e2e, accuracy, device-pass, "
@@ -408,8 +411,9 @@ def run_b200(args, cfg, rank, world, local_rank):
     achieved = alg[dom] / (avg[dom + "_ms"] / 1000.0) / 1e9 if avg[dom + "_ms"] > 0 else None
     traffic, traffic_note = None, "no ncu capture committed for this kernel and workload"
     tfile = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (dom, cfg.name))
-    if args.bb1d_grid:
-        traffic_note = "BB1D over the reference grid: no ncu traffic figure committed for this path"
+    if args.bb1d_grid or args.knn:
+        traffic_note = "no ncu traffic figure committed for this path (%s)" % (
+            "BB1D over the reference grid" if args.bb1d_grid else "KNN radii")
     elif os.path.exists(tfile):
         try:
             with open(tfile) as fh:
@@ -665,6 +669,24 @@ def run_secondary(dev, stream):
             st.close()
     cg["image_rel_l2_grid_vs_pieces"] = rel_l2(cg["reference_grid"].pop("image"), cg["lbvh_pieces"].pop("image"))
     out["cube1024_reference_grid"] = cg
+    # KNN radii (-r_initial_pb2d_knn 8, -r_initial_bb1d_knn 6) on the headline workload: the
+    # reference's own kd-tree search (the default) and the exact k-th nearest
+    ck = {"pb2d_knn": 8, "bb1d_knn": 6}
+    for name, exact in (("reference_search", 0), ("exact", 1)):
+        cfg = W.config("cube1024")
+        cfg.pb2d_knn, cfg.bb1d_knn = ck["pb2d_knn"], ck["bb1d_knn"]
+        w = W.make(cfg)
+        w["params"]["knn_exact"] = exact
+        with torch.cuda.stream(stream):
+            st = engine.EstimatorStage(dev, engine.MODE_MIXED)
+            st.set_stream(stream.cuda_stream)
+            st.run(w)
+            ms = timed(st, lambda: (st.build(), st.clear_image(), st.evaluate()))
+            t = st.timings()
+            ck[name] = {"ms_per_iteration": ms, "build_ms": t["build_ms"], "bb1d_ms": t["bb1d_ms"],
+                        "accepted_pairs": int(st.query_stats()["count_bb1d"].astype(np.int64).sum())}
+            st.close()
+    out["cube1024_knn_radii"] = ck
     # configuration 4
     w = W.make(W.config("diff512"))
     media = np.array(w["media"], copy=True)
@@ -1037,6 +1059,8 @@ def main():
         sys.exit(spawn_ranks(args.gpus))
     from smallupbp_b200 import workload as W
     cfg = W.config(args.config)
+    if args.knn:
+        cfg.pb2d_knn, cfg.bb1d_knn = (int(x) for x in args.knn.split(","))
     if args.impl == "reference":
         line = run_reference(args, cfg, rank, world)
     elif args.adjoint:

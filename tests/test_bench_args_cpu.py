@@ -38,3 +38,9 @@ def test_dropin_is_the_plain_thread_per_query_gather():
     assert a.mode == "plain" and a.no_autotune
     t = json.loads(a.tuning)
     assert t["bb1d_kernel"] == 0 and t["pb2d_kernel"] == 0
+
+
+def test_knn_option_names_the_two_neighbour_counts():
+    a = _parse(["--knn", "8,6"])
+    assert a.knn == "8,6"
+    assert tuple(int(x) for x in a.knn.split(",")) == (8, 6)
