@@ -35,7 +35,7 @@ namespace {
 
 constexpr int kBigSeg = 4096;
 constexpr int kWarpSeg = 64;
-constexpr int kSplitThreads = 512;
+constexpr int kSplitThreads = 1024;
 constexpr unsigned kAllLanes = 0xffffffffu;
 
 __host__ __device__ __forceinline__ int kd_median(int start, int end)
